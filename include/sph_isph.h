@@ -1,0 +1,251 @@
+/*
+ * sph_isph.h -- C ABI of the B200-native ISPH time step.
+ *
+ * Drop-in boundary for the step the reference drives from
+ * SOPHIA_single_ISPH (ISPH_Calc.cuh:4-233).  The reference has no library or
+ * ABI: its "operator surface" is a set of __global__ kernels that take raw
+ * device pointers to the AoS particle arrays part1/part2/part3
+ * (class_Cuda_Particle_Array.cuh:11-112) and read every parameter from the
+ * __constant__ tables k_vii[64] / k_vif[32] (SOPHIA_gpu.cu:47-48, names in
+ * function_init.cuh:84-163).  This header keeps both: the particle records
+ * below have the reference's exact layout (Real = float), and sph_params
+ * carries the same two tables plus the constants the reference hard-wires as
+ * #defines or literals (each field names the line it replaces).
+ *
+ * Conventions:
+ *   - every call returns an int status (SPH_OK = 0, > 0 warnings, < 0 errors);
+ *     no exception or exit() crosses the boundary;
+ *   - a context owns all of its device memory, is bound to one device and one
+ *     CUDA stream, and is not thread-safe (one host thread at a time);
+ *   - calls are stream-ordered; only the *_download / *_export calls and
+ *     sph_ppe's statistics synchronise the stream;
+ *   - particle indices in exported arrays are in the reference's sorted
+ *     order (the order KERNEL_reorder produces, functions_NNPS.cuh:840-843).
+ */
+#ifndef SPH_ISPH_H
+#define SPH_ISPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SPH_OK                 0
+#define SPH_NOT_CONVERGED      1   /* PPE stopped at max_iter above tol      */
+#define SPH_ERR_BAD_ARG       -1
+#define SPH_ERR_CUDA          -2
+#define SPH_ERR_BREAKDOWN     -3   /* Krylov breakdown that restart could not cure */
+#define SPH_ERR_STATE         -4   /* call made in the wrong order           */
+#define SPH_ERR_NO_DEVICE     -5
+#define SPH_ERR_OUT_OF_MEMORY -6
+#define SPH_ERR_UNSUPPORTED   -7
+
+/* ---- precision forms --------------------------------------------------- */
+#define SPH_PREC_MIXED 0   /* FP32 state and neighbour sums, FP64 Krylov scalars */
+#define SPH_PREC_FP64  1   /* whole step in FP64 (the plain form)              */
+
+/* ---- pressure solve modes ---------------------------------------------- */
+#define SPH_PPE_REF_SWEEP  0  /* one point-Jacobi sweep, KERNEL_PPE3D semantics
+                                 (functions_PPE.cuh:2-175) without its race   */
+#define SPH_PPE_BICGSTAB   1  /* Jacobi-preconditioned BiCGSTAB in the context's
+                                 precision, FP64 reductions                   */
+#define SPH_PPE_MIXED_IR   2  /* FP32 BiCGSTAB inside FP64 iterative refinement */
+#define SPH_PPE_LEARNED    3  /* MIXED_IR warm-started by the per-particle net   */
+
+/* ---- particle records: class_Cuda_Particle_Array.cuh:11-112, Real=float --- */
+typedef struct sph_part1 {
+    int32_t i_type, buffer_type, MOST_buffer, p_type;
+    float x, y, z;
+    float ux, uy, uz;
+    float m, h, temp, pres, pres0, rho, flt_s, enthalpy, concn, concentration;
+    float k_turb, e_turb;
+    float eli, vol;
+    float m_ref, h_ref;
+    float vis_t;
+    float fbx, fby, fbz;
+    float fmx, fmy, hmz;
+    float float1, float2, float3;
+    int32_t ncell, source;
+} sph_part1;                                      /* 152 bytes */
+
+typedef struct sph_part2 {
+    float rho_ref, SR;
+    float x0, y0, z0;
+    float ux0, uy0, uz0;
+    float rho0, drho0, temp0, concn0, enthalpy0;
+} sph_part2;                                      /* 52 bytes */
+
+typedef struct sph_part3 {
+    float drho, dconcn, denthalpy;
+    float ftotalx, ftotaly, ftotalz, ftotal;
+    float fpx, fpy, fpz, fbody;
+    float dtemp;
+    float dk_turb, de_trub;
+    float cc;
+    float nx, ny, nz;
+    float Cm[3][3];
+    float inv_cm_xx, inv_cm_yy, inv_cm_zz;
+    float inv_cm_xy, inv_cm_yz, inv_cm_zx;
+    float Gxx, Gxy, Gyx, Gyy;
+    float L11, L12, L21, L22;
+} sph_part3;                                      /* 164 bytes */
+
+/* ---- k_vii / k_vif slots (function_init.cuh:84-163) ------------------- */
+enum sph_vii_slot {
+    SPH_VII_SOLVER_TYPE = 0, SPH_VII_DIM = 1, SPH_VII_PROP_TABLE = 2, SPH_VII_KERNEL_TYPE = 3,
+    SPH_VII_TIME_TYPE = 4, SPH_VII_OPEN_BOUNDARY = 5, SPH_VII_FREQ_FILT = 8,
+    SPH_VII_FREQ_OUTPUT = 11, SPH_VII_FP_SOLVE = 12, SPH_VII_FV_SOLVE = 13, SPH_VII_FG_SOLVE = 14,
+    SPH_VII_CON_SOLVE = 15, SPH_VII_BOUSSINESQ = 16, SPH_VII_KGC_SOLVE = 17,
+    SPH_VII_TURBULENCE = 18, SPH_VII_CONCN_SOLVE = 19, SPH_VII_MIN_ITER = 20, SPH_VII_MAX_ITER = 21,
+    SPH_VII_NUM_PART = 23, SPH_VII_NI = 24, SPH_VII_NJ = 25, SPH_VII_NK = 26, SPH_VII_COUNT = 27,
+    SPH_VII_NUM_CELLS = 28, SPH_VII_NGPU = 29, SPH_VII_NUM_PART2 = 32, SPH_VII_NOSLIP_BC = 34,
+    SPH_VII_APR_SOLV = 35, SPH_VII_H_CHANGE = 36, SPH_VII_FREQ_APR = 37
+};
+enum sph_vif_slot {
+    SPH_VIF_KAPPA = 0, SPH_VIF_P_REF = 1, SPH_VIF_DT = 2, SPH_VIF_TIME = 3, SPH_VIF_TIME_END = 4,
+    SPH_VIF_U_LIMIT = 5, SPH_VIF_DP_TH = 7, SPH_VIF_X_MIN = 9, SPH_VIF_X_MAX = 10,
+    SPH_VIF_Y_MIN = 11, SPH_VIF_Y_MAX = 12, SPH_VIF_Z_MIN = 13, SPH_VIF_Z_MAX = 14,
+    SPH_VIF_SEARCH_INCR = 16, SPH_VIF_SEARCH_KAPPA = 17, SPH_VIF_DCELL = 18,
+    SPH_VIF_BUFFERSIZE = 19, SPH_VIF_DT_STRUCTURE = 20
+};
+
+#define SPH_MAX_PROFILE 32
+
+/* ---- parameters --------------------------------------------------------- */
+typedef struct sph_params {
+    int32_t vii[64];      /* k_vii, same slots as the reference            */
+    float   vif[32];      /* k_vif, same slots as the reference            */
+
+    /* constants the reference hard-wires; defaults are the reference values.
+       Stored as double: kernels convert each one to the type the reference
+       evaluates it in at that use site (a double literal or a Real). */
+    double cs_sgs;            /* Cs_sgs 0.15                 Parameters.cuh:135  */
+    double l2, l3;            /* L2, L3 buffer planes         functions_NNPS.cuh:5-6 */
+    double l_left, l_right;   /* periodic-y planes            functions_NNPS.cuh:9-10 */
+    double outlet_probe_dx;   /* xg = L3 - 0.008              functions_BC.cuh:732 */
+    double partner_tol;       /* exact-position match 1e-3    functions_BC.cuh:737,1122 */
+    double ghost_tol;         /* ghost-node match 0.1         functions_BC.cuh:361, functions_MOST.cuh:294 */
+    double ib_box[6];         /* IB face planes x0,x1,y0,y1,z0,z1  functions_PREP.cuh:958-963 */
+    double ib_face_tol;       /* 1e-5                         functions_PREP.cuh:958 */
+    double most_z0, most_z0h; /* MOST_z0 1.0, MOST_z0h 0.1    Parameters.cuh:114-115 */
+    double most_ghost_dz;     /* ghost 5 m above              functions_MOST.cuh:266 */
+    double rho_air;           /* Rho_air 1.225                Parameters.cuh:143 */
+    double ibm_target_coeff;  /* Ubtx = 0.2*profile(z)        functions_IBM.cuh:470 */
+    double visc_fluid, visc_wall, visc_marker; /* viscosity2  functions_PROP.cuh:121-131 */
+    double av_alpha, av_beta, av_c0;  /* artificial viscosity functions_PPE.cuh:268-271 */
+    double pressure_length, ibm_length, neumann_coeff; /* Parameters.cuh:105-106, functions_BC.cuh:308 */
+    double t_ini, t_con, t_start, t_con_t;    /* wall temperature ramp Parameters.cuh:121-124 */
+    double boundary_velocity; /* MOVING wall speed            Parameters.cuh:76 */
+    int32_t n_profile;        /* wall-model target table      functions_IBM.cuh:289-304 */
+    int32_t pad0;
+    double profile_z[SPH_MAX_PROFILE];
+    double profile_u[SPH_MAX_PROFILE];
+
+    /* pressure solve (new work: the reference runs one sweep per step) */
+    int32_t ppe_mode;        /* SPH_PPE_*                                      */
+    int32_t ppe_max_iter;
+    double  ppe_tol;         /* relative residual ||b-Ap||/||b||               */
+    int32_t ppe_pin;         /* 1: pin one fluid row to p=0 (pure-Neumann domains) */
+    int32_t recompute_gc;    /* 1: recompute the correction matrix every step  */
+    int32_t reserved[14];
+} sph_params;
+
+typedef struct sph_ppe_stats {
+    int32_t status;          /* SPH_OK / SPH_NOT_CONVERGED / error             */
+    int32_t iterations;      /* Krylov iterations (all refinement sweeps)      */
+    int32_t refinements;     /* outer FP64 refinement sweeps (MIXED_IR)        */
+    int32_t restarts;        /* breakdown restarts                             */
+    double  rel_residual;    /* final ||b-Ap||_2/||b||_2, FP64                 */
+    double  solve_ms;        /* device time from rhs ready to convergence      */
+} sph_ppe_stats;
+
+typedef struct sph_ctx sph_ctx;
+
+/* Fills the reference defaults (read_solv_input zeroes, then the values a
+ * Case-H solv.txt sets) and the promoted constants. */
+int sph_params_init(sph_params *p);
+
+/* Host-side domain set-up of ISPH.cuh:83-97 and clc_num_cells
+ * (functions_NNPS.cuh:533-546): x/y/z min-max over records 0..n-2 exactly as
+ * find_minmax (function_init.cuh:678-708) does, dcell = 1.1*kappa*h_ref[0]/2,
+ * NI/NJ/NK and num_cells = NI*NJ*NK+1.  Also sets num_part and num_part2. */
+int sph_domain_setup(sph_params *p, const sph_part1 *P1, int num_part);
+
+/* Creates a context for num_part2 records on `device`, in `precision`
+ * (SPH_PREC_*), ordered on `stream` (a cudaStream_t, NULL = default). */
+int sph_create(const sph_params *p, int precision, int device, void *stream, sph_ctx **out);
+void sph_destroy(sph_ctx *ctx);
+
+/* Replaces the parameters (dt, time, flags); grid fields must not change. */
+int sph_set_params(sph_ctx *ctx, const sph_params *p);
+
+/* Uploads host AoS records (the reference's DHP1 after
+ * c_initial_inner_outer_particle_single, ISPH_Calc.cuh:386-387).  P2 may be
+ * NULL (zeroed as at ISPH_Calc.cuh:357).  Resets the step counter to
+ * vii[count]. */
+int sph_upload(sph_ctx *ctx, const sph_part1 *P1, const sph_part2 *P2, int n);
+
+/* Same as sph_upload for state that is already sorted by an earlier
+ * sph_nnps of this context: only the time-varying fields are replaced and the
+ * neighbour structures are kept. */
+int sph_upload_state(sph_ctx *ctx, const sph_part1 *P1, int n);
+
+/* Downloads the state in the reference layout: P1 (= dev_P1 after the step),
+ * P2 (= dev_SP2), P3 (= dev_P3).  Any pointer may be NULL.  Synchronises. */
+int sph_download(sph_ctx *ctx, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3);
+
+/* NNPS, ISPH_Calc.cuh:20-45: set_ncell, cell hash, stable sort, cell
+ * start/end, reorder, plus the compacted neighbour lists every later pass
+ * reads.  Runs automatically at the first step. */
+int sph_nnps(sph_ctx *ctx);
+
+/* Copies the NNPS arrays to host buffers: g_idx/p_idx [num_part2],
+ * g_str/g_end [num_cells+1] in the reference's conventions (g_str = -1 for an
+ * empty cell; g_end of an empty cell is left 0).  Any pointer may be NULL. */
+int sph_nnps_export(sph_ctx *ctx, int32_t *g_idx, int32_t *p_idx, int32_t *g_str, int32_t *g_end);
+
+/* Canonical neighbour list of every particle i (sorted index): all j, in the
+ * reference's visit order (z, y, x cells ascending around the cell
+ * floor((x-xmin)/dcell), j ascending within a cell, functions_PPE.cuh:52-72),
+ * with sqrt(r2) < search_kappa*max(h_i,h_j) in FP32 (functions_PPE.cuh:96-100).
+ * If `list` is NULL only *nnz and `offsets` are written. */
+int sph_neighbors_export(sph_ctx *ctx, int64_t *offsets, int32_t *list, int64_t *nnz);
+
+/* Interaction phase, ISPH_Calc.cuh:65-127: correction matrix, prep/LES,
+ * no-slip walls, MOST, (step 0) Neumann, advection forces, predictor,
+ * periodic and free-slip buffers. */
+int sph_interaction(sph_ctx *ctx);
+
+/* Pressure phase, ISPH_Calc.cuh:137-154: PPE in p->ppe_mode, then Neumann
+ * wall pressure and the outlet copy.  `stats` may be NULL. */
+int sph_ppe(sph_ctx *ctx, sph_ppe_stats *stats);
+
+/* Time-update phase, ISPH_Calc.cuh:160-214: pressure force, IBM force and
+ * spreading, corrector, IBM corrector, boundary passes on the new state;
+ * advances count and time. */
+int sph_time_update(sph_ctx *ctx);
+
+/* nsteps full steps (interaction + ppe + time update).  `stats` receives the
+ * last step's PPE statistics. */
+int sph_step(sph_ctx *ctx, int nsteps, sph_ppe_stats *stats);
+
+/* Diagnostics of ISPH_Calc.cuh:500-514 (kernel_copy_max + CUB Max):
+ * max |u|, max |rho-rho_ref|/rho_ref*100 and max |ftotal|. */
+int sph_diagnostics(sph_ctx *ctx, float *max_umag, float *max_drho_pct, float *max_ftotal);
+
+/* Device-time breakdown of the last step in milliseconds, one entry per
+ * phase: [0] nnps, [1] interaction, [2] ppe, [3] time update. */
+int sph_last_phase_ms(sph_ctx *ctx, float *ms4);
+
+/* Kernel launches issued by this context since creation. */
+int64_t sph_launch_count(sph_ctx *ctx);
+
+const char *sph_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPH_ISPH_H */

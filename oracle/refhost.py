@@ -1,0 +1,97 @@
+"""ctypes driver for oracle/_ref/libsophia_ref.so (test infrastructure only).
+
+The library is the reference's own device code compiled for the host by
+oracle/Makefile (see ref_shim.cpp).  ``RefHost`` keeps the reference's arrays
+(dev_P1, dev_SP1, dev_P2, dev_SP2, dev_P3, g_idx, p_idx, g_str, g_end of
+ISPH_Calc.cuh:327-344) as numpy records and advances them with ref_step,
+the host restatement of SOPHIA_single_ISPH's launch sequence.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libsophia_ref.so")
+
+_lib = None
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} not built (make -C oracle ref)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.ref_set_params.argtypes = [vp, vp]
+        L.ref_get_params.argtypes = [vp, vp]
+        L.ref_domain_setup.argtypes = [vp, ctypes.c_int]
+        L.ref_nnps.argtypes = [vp] * 8
+        L.ref_step.argtypes = [vp] * 9 + [ctypes.c_int, ctypes.c_float, ctypes.c_int]
+        L.ref_set_parallel.argtypes = [ctypes.c_int]
+        L.ref_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RefHost:
+    """Reference step on the host, one instance per deck."""
+
+    def __init__(self, P1, params, parallel=True):
+        from sph_b200.layout import PART2, PART3
+        L = lib()
+        self.params = params.copy()
+        self.n = len(P1)
+        L.ref_set_parallel(1 if parallel else 0)
+        vii = np.ctypeslib.as_array(self.params.vii).copy()
+        vif = np.ctypeslib.as_array(self.params.vif).copy()
+        L.ref_set_params(_p(vii), _p(vif))
+        self.P1 = np.array(P1, copy=True)
+        self.SP1 = np.zeros_like(self.P1)
+        self.P2 = np.zeros(self.n, dtype=PART2)
+        self.SP2 = np.zeros(self.n, dtype=PART2)
+        self.P3 = np.zeros(self.n, dtype=PART3)
+        nc = self.params.geti("num_cells")
+        self.g_idx = np.zeros(self.n, np.int32)
+        self.p_idx = np.zeros(self.n, np.int32)
+        self.g_str = np.full(nc + 1, -1, np.int32)
+        self.g_end = np.zeros(nc + 1, np.int32)
+        self.count = self.params.geti("count")
+        self.time = np.float32(self.params.getf("time"))
+
+    def _load_params(self):
+        vii = np.ctypeslib.as_array(self.params.vii).copy()
+        vif = np.ctypeslib.as_array(self.params.vif).copy()
+        lib().ref_set_params(_p(vii), _p(vif))
+
+    def step(self, nsteps=1, ppe_snapshot=True):
+        L = lib()
+        self._load_params()
+        for _ in range(nsteps):
+            L.ref_step(_p(self.P1), _p(self.SP1), _p(self.P2), _p(self.SP2), _p(self.P3),
+                       _p(self.g_idx), _p(self.p_idx), _p(self.g_str), _p(self.g_end),
+                       int(self.count), float(self.time), 1 if ppe_snapshot else 0)
+            # ISPH_Calc.cuh:496-497
+            self.time = np.float32(self.time + np.float32(self.params.getf("dt")))
+            self.count += 1
+
+    def nnps(self):
+        """Step-0 NNPS only (ISPH_Calc.cuh:20-45) on a copy of P1."""
+        L = lib()
+        self._load_params()
+        P1 = np.array(self.P1, copy=True)
+        P2 = np.array(self.P2, copy=True)
+        SP1 = np.zeros_like(P1)
+        SP2 = np.zeros_like(P2)
+        L.ref_nnps(_p(P1), _p(P2), _p(SP1), _p(SP2), _p(self.g_idx), _p(self.p_idx),
+                   _p(self.g_str), _p(self.g_end))
+        return SP1, self.g_idx.copy(), self.p_idx.copy(), self.g_str.copy(), self.g_end.copy()
