@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ISPH step on the urban-canyon workload.
+
+One JSON line on rank 0:
+  metric  particle-steps/s: particles x steps / device time of the full step
+          (interaction passes, PPE converged to ||b-Ap||/||b|| <= 1e-6 with
+          FP32 BiCGSTAB inside FP64 refinement, time update); NNPS runs at
+          step 0 inside the warm-up (the reference runs it only at step 0,
+          ISPH_Calc.cuh:23-52, because particles never move).
+  e2e     the same step through the C ABI with host buffers: every step
+          uploads the particle records (part1, pinned host memory), runs the
+          step and downloads the records again.
+  roofline of the dominant kernel (the PPE operator), from live CUDA-event
+          timing of its launches inside the timed region.
+  cpu_baseline  the reference's own step compiled for the host cores
+          (oracle/_ref), timed on a bounded sample of the same deck.
+With --impl reference only the reference arm runs (rank 0).
+Multi-GPU: the step is a one-GPU path; N ranks run N independent replicas
+(weak scaling, no collective in the step).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "urban-sph_a100_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "particle-steps/s"
+WORKLOAD = "urban canyon 2.4x1.2x0.6 m, dx=0.01 m: 240x120x60 fluid + floor walls + free-slip ceiling + IBM cube, neutral MOST, SSM Cs=0.12"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(name):
+    """DRAM bytes per launch of the operator from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            d = json.load(f)
+        return d
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(steps):
+    """The reference's own step on the host cores, bounded sample of the deck."""
+    import numpy as np
+    import refhost
+    from sph_b200 import decks
+    if not refhost.available():
+        return None
+    P, p = decks.canyon(scale=0.3)
+    R = refhost.RefHost(P, p, parallel=True)
+    R.step(1)   # step 0: NNPS + first step (untimed)
+    t0 = time.perf_counter()
+    R.step(steps)
+    dt = time.perf_counter() - t0
+    cores = int(refhost.lib().ref_num_threads())
+    return {"value": len(P) * steps / dt, "unit": METRIC, "cores": cores, "kind": "reference",
+            "sample": f"canyon deck at scale 0.3 ({len(P)} particles), {steps} steps of the reference "
+                      f"step (one in-place PPE sweep) after its step-0 NNPS, host build of the "
+                      f"reference kernels with the reference's own hard-wired Case-H constants",
+            "seconds": dt}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import refhost
+    if not refhost.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsophia_ref.so not built"}))
+        return 0
+    from sph_b200 import decks
+    P, p = decks.canyon(scale=0.3)
+    R = refhost.RefHost(P, p, parallel=True)
+    for _ in range(max(args.warmup, 1)):
+        R.step(1)
+    t0 = time.perf_counter()
+    R.step(args.steps)
+    dt = time.perf_counter() - t0
+    value = len(P) * args.steps / dt
+    cores = int(refhost.lib().ref_num_threads())
+    out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "impl": "reference",
+           "config": {"workload": WORKLOAD, "sample_particles": len(P), "scale": 0.3},
+           "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
+                            "sample": f"canyon deck at scale 0.3 ({len(P)} particles) per step"},
+           "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "ref_sweep"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--matrix-free", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from sph_b200 import abi, decks, layout
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    P, p = decks.canyon(scale=args.scale)
+    mode = {"mixed_ir": layout.PPE_MIXED_IR, "bicgstab": layout.PPE_BICGSTAB,
+            "ref_sweep": layout.PPE_REF_SWEEP}[args.mode]
+    p.ppe_mode = mode
+    p.ppe_tol = 1e-6
+    if args.matrix_free:
+        p.reserved[0] = 1
+    n = len(P)
+    sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
+    sim.upload(P)
+    for _ in range(args.warmup):
+        sim.step(1)
+
+    # ---- device-timed region ----
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sim.profile(True)
+    sim.operator_stats(reset=True)
+    l0 = sim.launches()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stats, phases = [], []
+    e0.record()
+    for _ in range(args.steps):
+        s = sim.step(1)
+        stats.append((s.iterations, s.refinements, s.rel_residual, s.solve_ms, s.status))
+        phases.append(sim.phase_ms().copy())
+    e1.record()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = sim.launches() - l0
+    op_n, op_ms, op_bytes = sim.operator_stats(reset=True)
+    sim.profile(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = n * args.steps * world / (ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    host = torch.empty(n * layout.PART1.itemsize, dtype=torch.uint8, pin_memory=True).numpy().view(layout.PART1)
+    sim.download_into(host)
+    ke = max(3, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(ke):
+        sim.upload_state(host)
+        sim.step(1)
+        sim.download_into(host)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = n * ke * world / (e2e_ms / 1e3)
+
+    # ---- plain FP64 form on the same deck (the >=3x comparison) ----
+    fp64 = None
+    if not args.no_fp64 and rank == 0:
+        sim.close()
+        q = p.copy()
+        q.ppe_mode = layout.PPE_BICGSTAB
+        sd = abi.Simulation(q, precision=layout.PREC_FP64, device=local)
+        sd.upload(P)
+        for _ in range(2):
+            sd.step(1)
+        kd = max(3, args.steps // 4)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        dstats = []
+        g0.record()
+        for _ in range(kd):
+            s = sd.step(1)
+            dstats.append((s.iterations, s.rel_residual, s.solve_ms))
+        g1.record()
+        torch.cuda.synchronize()
+        dms = g0.elapsed_time(g1)
+        fp64 = {"value": n * kd / (dms / 1e3), "ms_per_step": dms / kd, "steps": kd,
+                "ppe_ms": statistics.mean(d[2] for d in dstats),
+                "ppe_iterations": statistics.mean(d[0] for d in dstats),
+                "rel_residual_max": max(d[1] for d in dstats), "ppe_tol": 1e-6}
+        sd.close()
+    else:
+        sim.close()
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    hbm, peak_kind = peaks()
+    per_launch_ms = op_ms / max(op_n, 1)
+    achieved = op_bytes / (per_launch_ms / 1e3) / 1e9 if op_n else 0.0
+    nc = ncu_traffic("ppe_operator_canyon.json")
+    traffic = None
+    if nc and abs(nc.get("particles", 0) - n) <= 1 and "dram_bytes_per_launch" in nc:
+        traffic = nc["dram_bytes_per_launch"]
+    ph = np.mean(np.array(phases), axis=0) if phases else np.zeros(4)
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": n, "scale": args.scale, "precision": "mixed FP32/FP64",
+                   "ppe": args.mode, "ppe_tol": 1e-6,
+                   "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
+                   "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": n * layout.PART1.itemsize,
+                "d2h_bytes_per_step": n * layout.PART1.itemsize, "steps": ke},
+        "gpu_launches": int(launches),
+        "ppe": {"iterations_mean": statistics.mean(s[0] for s in stats),
+                "refinements_mean": statistics.mean(s[1] for s in stats),
+                "rel_residual_max": max(s[2] for s in stats),
+                "solve_ms_mean": statistics.mean(s[3] for s in stats),
+                "not_converged_steps": sum(1 for s in stats if s[4] != 0)},
+        "phase_ms": {"interaction": float(ph[1]), "ppe": float(ph[2]), "time_update": float(ph[3])},
+        "roofline": {"bound": "hbm", "kernel": "PPE operator (k_spmv, cached c_ij)" if not args.matrix_free
+                     else "PPE operator (k_spmv_mf)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": op_bytes, "launch_ms": per_launch_ms, "launches": op_n},
+        "plain_fp64": fp64,
+        "clocks": ck,
+    }
+    if fp64:
+        out["mixed_vs_fp64"] = value / fp64["value"] if fp64["value"] else None
+    if world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(steps=4)
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

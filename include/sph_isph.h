@@ -148,9 +148,13 @@ typedef struct sph_params {
     int32_t ppe_mode;        /* SPH_PPE_*                                      */
     int32_t ppe_max_iter;
     double  ppe_tol;         /* relative residual ||b-Ap||/||b||               */
-    int32_t ppe_pin;         /* 1: pin one fluid row to p=0 (pure-Neumann domains) */
+    int32_t ppe_pin;         /* singular (pure-Neumann) pressure problems: 0 none,
+                                1 rank-one mean-pressure term per singular
+                                component (default), 2 one row pinned to p=0 */
     int32_t recompute_gc;    /* 1: recompute the correction matrix every step  */
-    int32_t reserved[14];
+    int32_t reserved[14];    /* reserved[0] = 1: matrix-free PPE operator (c_ij
+                                recomputed per application) instead of cached */
+    double  ppe_inner_tol;   /* inner FP32 tolerance of SPH_PPE_MIXED_IR (0: 1e-3) */
 } sph_params;
 
 typedef struct sph_ppe_stats {
@@ -243,7 +247,19 @@ int sph_last_phase_ms(sph_ctx *ctx, float *ms4);
 /* Kernel launches issued by this context since creation. */
 int64_t sph_launch_count(sph_ctx *ctx);
 
+/* Live timing of the PPE operator kernel (the dominant kernel of a step):
+ * with `enable` set, every operator launch is bracketed by CUDA events on the
+ * context's stream.  sph_operator_stats returns the launches timed since the
+ * last reset, their summed device time, and the algorithmic bytes of one
+ * launch (per row: kind, x_i, y_i, A_i; per stored neighbour: index and
+ * coefficient).  `reset` clears the counters after reading. */
+int sph_profile(sph_ctx *ctx, int enable);
+int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
+
 const char *sph_status_string(int status);
+
+/* Text of the last error raised on the calling host thread. */
+const char *sph_last_error(void);
 
 #ifdef __cplusplus
 }

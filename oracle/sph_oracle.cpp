@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <vector>
 
@@ -227,6 +228,9 @@ struct Oracle {
     int count = 0;
     float time = 0.f;
     int pin_row = -1;
+    std::vector<int> pins;
+    std::vector<int> comp_of;     // rank-one component of each fluid row (-1: none)
+    std::vector<int> comp_size;
     int stop_after = 1000;   // debugging: phases of step() to run
 
     P q() const { return P{prm}; }
@@ -885,21 +889,14 @@ struct Oracle {
     // weights) p = 0; outlet rows: p_o - p_partner = 0; identity rows: p = p_old.
     void assemble(const State<Real> &A, Real tdt, std::vector<int64_t> &ro, std::vector<int> &ci,
                   std::vector<double> &va, std::vector<double> &rhs) {
-        const P Q = q();
         const int N = n();
         ro.assign(N + 1, 0); ci.clear(); va.clear(); rhs.assign(N, 0.0);
         std::vector<std::pair<int, Real>> cs;
-        pin_row = -1;
-        if (prm.ppe_pin) {
-            // the highest sorted index among interior fluid rows (top of the
-            // last occupied cell, i.e. the downstream upper corner)
-            for (int i = N - 1; i >= 0; --i)
-                if (row_class(A, i) == 1 && A.buffer_type[i] == 0) { pin_row = i; break; }
-        }
+        std::vector<int> kind(N);
         for (int i = 0; i < N; ++i) {
             ro[i] = (int64_t)ci.size();
-            int rc = row_class(A, i);
-            if (i == pin_row) { ci.push_back(i); va.push_back(1.0); rhs[i] = 0.0; continue; }
+            const int rc = row_class(A, i);
+            kind[i] = rc;
             if (rc == 0) { ci.push_back(i); va.push_back(1.0); rhs[i] = A.pres[i]; continue; }
             if (rc == 1) {
                 Real bi, Aij;
@@ -915,14 +912,70 @@ struct Oracle {
                 if (partner >= 0) { ci.push_back(partner); va.push_back(-1.0); }
                 continue;
             }
-            // Neumann row
             std::vector<std::pair<int, double>> w;
             neumann_weights(A, i, w);
             ci.push_back(i); va.push_back(1.0);
             for (auto &c : w) { ci.push_back(c.first); va.push_back(-c.second); }
         }
         ro[N] = (int64_t)ci.size();
-        (void)Q;
+        pins.clear();
+        comp_of.assign(N, -1);
+        comp_size.clear();
+        if (prm.ppe_pin) {
+            // Connected components of the operator's graph; a component with no
+            // anchor row (a row that is only its diagonal: identity rows,
+            // Neumann rows without fluid in range, outlet rows without
+            // partner) is singular (its rows sum to zero, M 1 = 0).
+            //  ppe_pin == 1: rank-one regularisation M' = M + u w^T per such
+            //    component, u = its fluid rows, w = u/|u|: the constant mode
+            //    gets a well-conditioned eigenvalue and the compatibility
+            //    defect of b becomes the uniform source lambda = w^T p;
+            //  ppe_pin == 2: one row pinned to p = 0, the highest-index fluid
+            //    row with buffer_type 0 (else the highest-index fluid row).
+            std::vector<int> par(N);
+            std::iota(par.begin(), par.end(), 0);
+            std::function<int(int)> find = [&](int x) { while (par[x] != x) { par[x] = par[par[x]]; x = par[x]; } return x; };
+            for (int i = 0; i < N; ++i)
+                for (int64_t e = ro[i]; e < ro[i + 1]; ++e) {
+                    int a = find(i), b = find(ci[e]);
+                    if (a != b) par[std::max(a, b)] = std::min(a, b);
+                }
+            std::vector<char> anchored(N, 0);
+            std::vector<int> cand(N, -1), cand_any(N, -1), cid(N, -1);
+            for (int i = 0; i < N; ++i) {
+                const int r = find(i);
+                if (ro[i + 1] - ro[i] == 1 && kind[i] != 1) anchored[r] = 1;
+                if (kind[i] == 1) {
+                    cand_any[r] = std::max(cand_any[r], i);
+                    if (A.buffer_type[i] == 0) cand[r] = std::max(cand[r], i);
+                }
+            }
+            for (int r = 0; r < N; ++r) {
+                if (find(r) != r || anchored[r] || cand_any[r] < 0) continue;
+                if (prm.ppe_pin == 2 || (int)comp_size.size() >= 8) {
+                    pins.push_back(cand[r] >= 0 ? cand[r] : cand_any[r]);
+                } else {
+                    cid[r] = (int)comp_size.size();
+                    comp_size.push_back(0);
+                }
+            }
+            for (int i = 0; i < N; ++i)
+                if (kind[i] == 1 && cid[find(i)] >= 0) { comp_of[i] = cid[find(i)]; comp_size[comp_of[i]]++; }
+            std::sort(pins.begin(), pins.end());
+            if (!pins.empty()) {
+                // rebuild with the pinned rows replaced by p = 0
+                std::vector<int64_t> r2(N + 1, 0); std::vector<int> c2; std::vector<double> v2;
+                size_t q = 0;
+                for (int i = 0; i < N; ++i) {
+                    r2[i] = (int64_t)c2.size();
+                    if (q < pins.size() && pins[q] == i) { c2.push_back(i); v2.push_back(1.0); rhs[i] = 0.0; ++q; continue; }
+                    for (int64_t e = ro[i]; e < ro[i + 1]; ++e) { c2.push_back(ci[e]); v2.push_back(va[e]); }
+                }
+                r2[N] = (int64_t)c2.size();
+                ro.swap(r2); ci.swap(c2); va.swap(v2);
+            }
+        }
+        pin_row = pins.empty() ? -1 : pins.back();
     }
 
     int outlet_partner(const State<Real> &A, int i) const {
@@ -993,10 +1046,17 @@ struct Oracle {
         for (int i = 0; i < N; ++i)
             for (int64_t e = ro[i]; e < ro[i + 1]; ++e)
                 if (ci[e] == i && va[e] != 0) dinv[i] = 1.0 / va[e];
+        const int NC = (int)comp_size.size();
         auto spmv = [&](const std::vector<double> &v, std::vector<double> &y) {
+            std::vector<double> mean(NC, 0.0);
+            if (NC) {
+                for (int i = 0; i < N; ++i) if (comp_of[i] >= 0) mean[comp_of[i]] += v[i];
+                for (int k = 0; k < NC; ++k) mean[k] /= comp_size[k];
+            }
             for (int i = 0; i < N; ++i) {
                 double s = 0;
                 for (int64_t e = ro[i]; e < ro[i + 1]; ++e) s += va[e] * v[ci[e]];
+                if (NC && comp_of[i] >= 0) s += mean[comp_of[i]];
                 y[i] = s;
             }
         };
@@ -1044,7 +1104,7 @@ struct Oracle {
         assemble(A, tdt, ro, ci, va, rhs);
         std::vector<double> x(n());
         for (int i = 0; i < n(); ++i) x[i] = (double)A.pres[i];
-        if (pin_row >= 0) x[pin_row] = 0;
+        for (int pr : pins) x[pr] = 0;
         int st = bicgstab(ro, ci, va, rhs, x, tol, maxit, relres, iters);
         for (int i = 0; i < n(); ++i) A.pres[i] = (Real)x[i];
         return st;
@@ -1440,9 +1500,39 @@ int orc_download_work(void *hh, sph_part1 *P1) {
     return SPH_OK;
 }
 
+// assembles the converged-PPE system of the current working state (call
+// after a step stopped at phase 10 with orc_set_stop_after); returns nnz
+int64_t orc_assemble(void *hh, int64_t *ro, int32_t *ci, double *va, double *rhs) {
+    OracleHandle *h = (OracleHandle *)hh;
+    int64_t nnz = 0;
+    auto go = [&](auto *o) {
+        std::vector<int64_t> r; std::vector<int> c; std::vector<double> v, b;
+        o->assemble(o->S, o->q().dt(), r, c, v, b);
+        nnz = (int64_t)c.size();
+        if (ro) std::memcpy(ro, r.data(), 8 * r.size());
+        if (ci) std::memcpy(ci, c.data(), 4 * c.size());
+        if (va) std::memcpy(va, v.data(), 8 * v.size());
+        if (rhs) std::memcpy(rhs, b.data(), 8 * b.size());
+    };
+    if (h->f) go(h->f); else go(h->d);
+    return nnz;
+}
+
 int orc_pin_row(void *hh) {
     OracleHandle *h = (OracleHandle *)hh;
     return h->f ? h->f->pin_row : h->d->pin_row;
+}
+
+int orc_ncomp(void *hh) {
+    OracleHandle *h = (OracleHandle *)hh;
+    return h->f ? (int)h->f->comp_size.size() : (int)h->d->comp_size.size();
+}
+
+int orc_pins(void *hh, int32_t *out) {
+    OracleHandle *h = (OracleHandle *)hh;
+    const std::vector<int> &v = h->f ? h->f->pins : h->d->pins;
+    if (out) std::memcpy(out, v.data(), 4 * v.size());
+    return (int)v.size();
 }
 
 int orc_download(void *hh, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3) {

@@ -1,0 +1,98 @@
+"""Converged pressure solves on the GPU (needs a B200).
+
+The reference runs one pressure sweep per step; the converged modes are new
+work and are judged against the CPU oracle's FP64 BiCGSTAB on the same
+operator (same rows, same pinned rows):
+  * FP64 BiCGSTAB: ||b-Ap||/||b|| <= 1e-8 and pressure within PRES_TOL_FP64 of
+    the oracle's converged pressure (both solves stop at 1e-8 / 1e-10);
+  * mixed form (FP32 BiCGSTAB inside FP64 refinement): ||b-Ap||/||b|| <= 1e-6
+    and pressure / velocity within MIXED_TOL of the plain FP64 form;
+  * the matrix-free operator gives the cached operator's answer.
+"""
+import numpy as np
+import pytest
+
+from sph_b200 import abi, decks, layout
+
+import restated
+
+pytestmark = pytest.mark.gpu
+
+PRES_TOL_FP64 = 1e-6
+MIXED_TOL = 1e-4
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _gpu_step(P, p, precision, mode, tol, nsteps=1, matrix_free=False):
+    q = p.copy()
+    q.ppe_mode = mode
+    q.ppe_tol = tol
+    q.ppe_max_iter = 4000
+    if matrix_free:
+        q.reserved[0] = 1
+    sim = abi.Simulation(q, precision=precision)
+    sim.upload(P)
+    stats = [sim.step(1) for _ in range(nsteps)]
+    A, _, _ = sim.download()
+    sim.close()
+    return A, stats
+
+
+@pytest.fixture(scope="module")
+def deck():
+    return decks.caseh_mini(nx=14, ny=8, nz=5)
+
+
+def test_fp64_bicgstab_matches_oracle(deck):
+    P, p = deck
+    A, stats = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8)
+    assert stats[-1].status == 0 and stats[-1].rel_residual <= 1e-8, (stats[-1].rel_residual, stats[-1].iterations)
+    O = restated.Restated(P, p, 1)
+    st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-10, maxit=5000)
+    assert st == 0
+    B, _, _ = O.download()
+    assert rel_err(A["pres"], B["pres"]) <= PRES_TOL_FP64
+    for f in ("ux", "uy", "uz"):
+        assert rel_err(A[f], B[f]) <= PRES_TOL_FP64, f
+
+
+def test_mixed_ir_reaches_tolerance_and_matches_fp64(deck):
+    P, p = deck
+    A, st32 = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_MIXED_IR, 1e-6, nsteps=2)
+    for s in st32:
+        assert s.status == 0 and s.rel_residual <= 1e-6, (s.rel_residual, s.iterations, s.refinements)
+    B, st64 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8, nsteps=2)
+    for f in ("pres", "ux", "uy", "uz"):
+        assert rel_err(A[f], B[f]) <= MIXED_TOL, f
+
+
+def test_fp32_bicgstab_converges(deck):
+    P, p = deck
+    A, st = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_BICGSTAB, 1e-5)
+    assert st[-1].status == 0 and st[-1].rel_residual <= 1e-5
+
+
+def test_matrix_free_equals_cached(deck):
+    P, p = deck
+    A, s1 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-9)
+    B, s2 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-9, matrix_free=True)
+    assert s1[-1].status == 0 and s2[-1].status == 0
+    assert rel_err(A["pres"], B["pres"]) <= 1e-7
+
+
+def test_not_converged_status_with_tiny_iteration_budget(deck):
+    P, p = deck
+    q = p.copy()
+    q.ppe_mode = layout.PPE_BICGSTAB
+    q.ppe_tol = 1e-12
+    q.ppe_max_iter = 3
+    sim = abi.Simulation(q, precision=layout.PREC_FP64)
+    sim.upload(P)
+    s = sim.step(1)
+    assert s.status == 1 and s.iterations <= 3
+    sim.close()

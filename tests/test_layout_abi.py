@@ -1,0 +1,79 @@
+"""Layout of the drop-in records and the C ABI surface (no GPU needed)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from sph_b200 import abi, layout, params
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "sph_isph.h")
+
+
+def test_record_sizes_match_reference():
+    # part1/part2/part3 of class_Cuda_Particle_Array.cuh with Real = float
+    assert layout.PART1.itemsize == 152
+    assert layout.PART2.itemsize == 52
+    assert layout.PART3.itemsize == 164
+
+
+def test_header_struct_sizes(tmp_path):
+    src = tmp_path / "sz.c"
+    src.write_text('#include "sph_isph.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   'int main(){printf("%zu %zu %zu %zu %zu %zu\\n",sizeof(sph_params),sizeof(sph_part1),'
+                   'sizeof(sph_part2),sizeof(sph_part3),sizeof(sph_ppe_stats),offsetof(sph_params,ppe_tol));}')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I" + os.path.dirname(HEADER), str(src), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)]).decode().split()
+    assert int(out[0]) == ctypes.sizeof(layout.SphParams)
+    assert [int(v) for v in out[1:4]] == [152, 52, 164]
+    assert int(out[4]) == ctypes.sizeof(layout.PpeStats)
+    assert int(out[5]) == layout.SphParams.ppe_tol.offset
+
+
+def test_library_loads_and_exports_every_symbol():
+    L = abi.lib()
+    declared = set()
+    import re
+    for line in open(HEADER):
+        m = re.match(r"^(?:const char \*|int64_t |int |void )(sph_\w+)\(", line.strip())
+        if m:
+            declared.add(m.group(1))
+    assert declared == set(abi.SYMBOLS)
+    for name in declared:
+        assert hasattr(L, name), name
+
+
+def test_c_defaults_equal_python_defaults():
+    c = abi.params_init()
+    p = params.default_params()
+    for f, _ in layout.SphParams._fields_:
+        a, b = getattr(c, f), getattr(p, f)
+        if hasattr(a, "__len__"):
+            assert list(a) == list(b), f
+        else:
+            assert a == b, f
+
+
+def test_domain_setup_c_equals_python():
+    from sph_b200 import decks
+    P, p = decks.caseh_mini()
+    c = abi.params_init()
+    c.setf("kappa", p.getf("kappa"))
+    abi.domain_setup(c, P)
+    for name in ("NI", "NJ", "NK", "num_cells", "num_part2"):
+        assert c.geti(name) == p.geti(name), name
+    for name in ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max", "dcell", "search_kappa"):
+        assert np.float32(c.getf(name)) == np.float32(p.getf(name)), name
+
+
+def test_create_without_gpu_fails_loudly():
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    from sph_b200 import decks
+    P, p = decks.caseh_mini(nx=6, ny=4, nz=3)
+    with pytest.raises(abi.SphError):
+        abi.Simulation(p)

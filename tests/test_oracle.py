@@ -1,0 +1,216 @@
+"""Pins the CPU oracle (oracle/sph_oracle.cpp) to the reference itself.
+
+* against the reference's own kernels compiled for the host (oracle/_ref,
+  built from the reference sources by oracle/Makefile): NNPS arrays and the
+  full step are bit-identical in FP32 for several physics variants;
+* against the committed golden fixture (tests/golden/caseh_mini_ref.npz,
+  made by tests/golden/make_golden.py from the same host build), so the pin
+  holds where the reference tree is absent;
+* the converged pressure solve (new work, no reference counterpart) by its
+  residual and by the pinned row.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from sph_b200 import decks, layout
+
+import refhost
+import restated
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden", "caseh_mini_ref.npz")
+FIELDS = ["ux", "uy", "uz", "pres", "vis_t", "flt_s", "fbx", "fby", "fbz", "fmx", "fmy", "hmz",
+          "float1", "float2", "float3", "temp", "concentration", "k_turb", "e_turb"]
+
+needs_ref = pytest.mark.skipif(not refhost.available(), reason="reference host build absent")
+
+VARIANTS = {
+    "ssm_cleary_w6": dict(),
+    "ddf_monaghan": dict(turbulence="DDF", viscous=layout.MONAGHAN),
+    "wendland2": dict(kernel="Wendland2"),
+    "quartic_laminar": dict(kernel="Quartic", turbulence="Laminar"),
+    "no_slip_off": dict(noslip=0),
+}
+
+
+def _deck(kw, **extra):
+    return decks.caseh_mini(nx=12, ny=6, nz=5, **kw, **extra)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(VARIANTS))
+def test_nnps_bit_exact_vs_reference(name):
+    P, p = _deck(VARIANTS[name])
+    R = refhost.RefHost(P, p, parallel=False)
+    _, g_idx, p_idx, g_str, g_end = R.nnps()
+    O = restated.Restated(P, p, 0)
+    O.nnps()
+    og, op, os_, oe = O.export_nnps()
+    assert np.array_equal(g_idx, og)
+    assert np.array_equal(p_idx, op)
+    assert np.array_equal(g_str, os_)
+    assert np.array_equal(g_end, oe)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(VARIANTS))
+def test_step_bit_exact_vs_reference(name):
+    P, p = _deck(VARIANTS[name])
+    R = refhost.RefHost(P, p, parallel=False)
+    O = restated.Restated(P, p, 0)
+    for _ in range(3):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, B2, B3 = O.download()
+    for f in FIELDS:
+        assert np.array_equal(R.P1[f], B[f]), f
+    for f in ("ftotalx", "ftotaly", "ftotalz", "ftotal", "fpx", "fpy", "fpz", "inv_cm_xx", "inv_cm_yy",
+              "inv_cm_zz", "inv_cm_xy", "inv_cm_yz", "inv_cm_zx", "nx", "ny", "nz"):
+        assert np.array_equal(R.P3[f], B3[f]), f
+    for f in ("SR", "rho_ref", "ux0", "uy0", "uz0"):
+        assert np.array_equal(R.SP2[f], B2[f]), f
+
+
+@needs_ref
+def test_euler_time_stepping_bit_exact_vs_reference():
+    P, p = _deck({})
+    p.seti("time_type", layout.EULER)
+    R = refhost.RefHost(P, p, parallel=False)
+    O = restated.Restated(P, p, 0)
+    for _ in range(2):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, _, _ = O.download()
+    for f in FIELDS:
+        assert np.array_equal(R.P1[f], B[f]), f
+
+
+@needs_ref
+def test_most_newton_branch_vs_reference():
+    # wall-layer air at 1.5 m above a z0 = 1 m surface, +-3 K: Newton for L runs
+    P, p = decks.most_column()
+    R = refhost.RefHost(P, p, parallel=False)
+    O = restated.Restated(P, p, 0)
+    for _ in range(2):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, _, _ = O.download()
+    most = R.P1["MOST_buffer"] == 1
+    L = R.P1["float3"][most]
+    assert np.all(np.isfinite(L)) and np.any(np.abs(L) < 1e5), "Newton branch not exercised"
+    for f in ("fmx", "fmy", "hmz", "float1", "float2", "float3", "ux", "uy", "pres"):
+        assert np.array_equal(R.P1[f], B[f]), f
+
+
+def test_oracle_matches_golden_fixture():
+    g = np.load(GOLDEN)
+    P = g["deck"].view(layout.PART1)
+    p = layout.SphParams.from_buffer_copy(g["params"].tobytes())
+    O = restated.Restated(P, p, 0)
+    O.nnps()
+    og, op, os_, oe = O.export_nnps()
+    assert np.array_equal(og, g["g_idx"]) and np.array_equal(op, g["p_idx"])
+    assert np.array_equal(os_, g["g_str"]) and np.array_equal(oe, g["g_end"])
+    O = restated.Restated(P, p, 0)
+    O.step(2, mode=layout.PPE_REF_SWEEP)
+    B, _, _ = O.download()
+    for k in g.files:
+        if k.startswith("p1_"):
+            assert np.array_equal(B[k[3:]], g[k]), k
+
+
+def test_golden_fixture_matches_reference_when_present():
+    if not refhost.available():
+        pytest.skip("reference host build absent")
+    g = np.load(GOLDEN)
+    P = g["deck"].view(layout.PART1)
+    p = layout.SphParams.from_buffer_copy(g["params"].tobytes())
+    R = refhost.RefHost(P, p, parallel=False)
+    R.step(2)
+    for k in g.files:
+        if k.startswith("p1_"):
+            assert np.array_equal(R.P1[k[3:]], g[k]), k
+
+
+def test_neighbor_lists_follow_reference_visit_order():
+    # the list of i is the sequence of j the reference's cell loop evaluates
+    # (z, y, x cells ascending, j ascending) that pass the FP32 radius test
+    P, p = _deck({})
+    O = restated.Restated(P, p, 0)
+    O.nnps()
+    off, lst = O.neighbors()
+    g_idx, _, g_str, g_end = O.export_nnps()
+    B, _, _ = O.download()
+    NI, NJ, NK = p.geti("NI"), p.geti("NJ"), p.geti("NK")
+    f = np.float32
+    dcell, kap = f(p.getf("dcell")), f(p.getf("search_kappa"))
+    mins = [f(p.getf(k)) for k in ("x_min", "y_min", "z_min")]
+    rng = np.random.default_rng(0)
+    for i in rng.choice(len(B), 60, replace=False):
+        if B["i_type"][i] == 3:
+            continue
+        xi = [B[a][i] for a in ("x", "y", "z")]
+        c = [min(int(np.floor(f(xi[a] - mins[a]) / dcell)), N - 1) for a, N in enumerate((NI, NJ, NK))]
+        c = [max(v, 0) for v in c]
+        exp = []
+        nc = B["ncell"][i]
+        for z in range(-nc, nc + 1):
+            for y in range(-nc, nc + 1):
+                for x in range(-nc, nc + 1):
+                    X, Y, Z = c[0] + x, c[1] + y, c[2] + z
+                    if not (0 <= X < NI and 0 <= Y < NJ and 0 <= Z < NK):
+                        continue
+                    k = X + NI * Y + NI * NJ * Z
+                    if g_str[k] < 0:
+                        continue
+                    for j in range(g_str[k], g_end[k]):
+                        d = [f(xi[a] - B[b][j]) for a, b in enumerate(("x", "y", "z"))]
+                        r = np.sqrt(f(f(f(d[0] * d[0]) + f(d[1] * d[1])) + f(d[2] * d[2])), dtype=f)
+                        if r < f(kap * max(B["h"][i], B["h"][j])):
+                            exp.append(j)
+        assert list(lst[off[i]:off[i + 1]]) == exp
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_oracle_converged_ppe_residual(precision):
+    P, p = _deck({})
+    O = restated.Restated(P, p, precision)
+    tol = 1e-6 if precision == 0 else 1e-10
+    st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=tol, maxit=5000)
+    assert st == 0, (rel, it)
+    assert rel <= tol
+    # the deck has two pure-Neumann fluid components (main channel and the
+    # outlet island): each carries the rank-one mean-pressure term
+    L = restated.lib()
+    L.orc_ncomp.argtypes = [ctypes.c_void_p]
+    assert L.orc_ncomp(O.h) == 2
+
+
+@pytest.mark.parametrize("pin_mode", [1, 2])
+def test_oracle_singular_components_regularised(pin_mode):
+    P, p = _deck({})
+    q = p.copy()
+    q.ppe_pin = pin_mode
+    O = restated.Restated(P, q, 1)
+    st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-9, maxit=5000)
+    assert st == 0 and rel <= 1e-9
+    q.ppe_pin = 0   # no regularisation: the singular system does not converge
+    O2 = restated.Restated(P, q, 1)
+    st2, rel2, _ = O2.step(1, mode=layout.PPE_BICGSTAB, tol=1e-9, maxit=400)
+    assert st2 != 0
+
+
+def test_oracle_fp32_vs_fp64_one_sweep_close():
+    P, p = _deck({})
+    A = restated.Restated(P, p, 0)
+    B = restated.Restated(P, p, 1)
+    A.step(2, mode=layout.PPE_REF_SWEEP)
+    B.step(2, mode=layout.PPE_REF_SWEEP)
+    a, _, _ = A.download()
+    b, _, _ = B.download()
+    for f in ("ux", "uy", "uz", "pres"):
+        err = np.abs(a[f].astype(np.float64) - b[f]).max() / np.abs(b[f]).max()
+        assert err < 1e-3, (f, err)

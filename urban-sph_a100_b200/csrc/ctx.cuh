@@ -1,0 +1,206 @@
+// Device-side context of one ISPH simulation: SoA particle state in HBM,
+// NNPS structures, neighbour lists and PPE workspace.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sph {
+
+// Time-varying per-particle fields of one particle-array copy (the
+// reference's dev_P1 or dev_SP1, class_Cuda_Particle_Array.cuh:11-67).
+template <class Real>
+struct VarSet {
+    typedef typename V4<Real>::type R4;
+    R4 *u = nullptr;        // ux, uy, uz, vis_t
+    Real *p = nullptr;      // pres
+    Real *temp = nullptr;
+    Real *flt = nullptr;    // flt_s
+    Real *kt = nullptr;     // k_turb
+    Real *et = nullptr;     // e_turb
+    R4 *fb = nullptr;       // fbx, fby, fbz, concentration
+    R4 *fm = nullptr;       // fmx, fmy, hmz, -
+    R4 *fl = nullptr;       // float1, float2, float3, -
+    Real *concn = nullptr;
+    Real *enth = nullptr;
+};
+
+// Precomputed, time-invariant lists of the boundary passes.
+struct SideLists {
+    // IBM marker interpolation (markers i, fluid j) and spreading (fluid i,
+    // markers j): CSR over the rows in `rows`.
+    int n_mk = 0, n_sp = 0;
+    int *mk_rows = nullptr, *mk_off = nullptr, *mk_nbr = nullptr;
+    int *sp_rows = nullptr, *sp_off = nullptr, *sp_nbr = nullptr;
+    int *sp_zero = nullptr; int n_sp_zero = 0;   // fluid rows with no marker in range
+    // Neumann rows (p_type != 1): CSR of fluid j (p_type 1, buffer 0) in range
+    int n_nm = 0;
+    int *nm_rows = nullptr, *nm_off = nullptr, *nm_nbr = nullptr;
+    int *nm_ghost = nullptr;     // 1 for mirror (inlet) rows
+    // partners of periodic (buffer 3/4) and outlet (buffer 2) particles
+    int n_per = 0, n_out = 0;
+    int *per_rows = nullptr, *per_partner = nullptr;
+    int *out_rows = nullptr, *out_partner = nullptr;
+    // MOST wall-layer particles and their ghost-node targets
+    int n_most = 0;
+    int *most_rows = nullptr, *most_off = nullptr, *most_tgt = nullptr;
+    // row lists of the passes
+    int n_fluid = 0, n_wall = 0, n_fs = 0, n_pf = 0;
+    int *fluid_rows = nullptr;   // i_type<=2, 0<p_type<1000 (prep/PPE rows)
+    int *wall_rows = nullptr;    // no-slip walls (p_type 0, i_type<=2)
+    int *fs_rows = nullptr;      // free-slip (p_type -1)
+};
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+template <class Real>
+struct Ctx {
+    typedef typename V4<Real>::type R4;
+    typedef typename V2<Real>::type R2;
+
+    sph_params prm;
+    DevParams dp;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0;
+    int num_cells = 0;
+    int count = 0;
+    float time = 0.f;
+    bool uploaded = false;
+    bool built = false;
+    bool gc_valid = false;
+    long long launches = 0;
+    float phase_ms[4] = {0, 0, 0, 0};
+    cudaEvent_t ev[8] = {};
+
+    // device allocations owned by the context (held through a pointer so Ctx
+    // stays trivially copyable and bulk kernels can take it by value)
+    std::vector<void *> *allocs = nullptr;
+
+    // ---- constant per particle (sorted order after NNPS) ----
+    float4 *pf = nullptr;   // FP32 x, y, z, h (NNPS precision)
+    R4 *pr = nullptr;       // Real x, y, z, h
+    R2 *mr = nullptr;       // m, rho
+    int4 *ty = nullptr;     // i_type, buffer_type, MOST_buffer, p_type
+    int *jc = nullptr;      // neighbour-class bits
+    int *ncell = nullptr;
+    Real *vol = nullptr, *m_ref = nullptr, *h_ref = nullptr, *eli = nullptr, *pres0 = nullptr;
+    int *source = nullptr;
+    // ---- time-varying ----
+    VarSet<Real> A, S;
+    Real *rho_ref_A = nullptr, *rho_ref_S = nullptr, *SR = nullptr;
+    R4 *u0 = nullptr;       // SP2: ux0, uy0, uz0, (x0 written flag)
+    R4 *ft = nullptr;       // P3: ftotalx, ftotaly, ftotalz, ftotal
+    R4 *fp = nullptr;       // P3: fpx, fpy, fpz
+    Real *dtemp = nullptr;
+    R4 *nrm = nullptr;      // P3: nx, ny, nz
+    Real *g6 = nullptr;     // inv_cm: 6 arrays of n (xx, yy, zz, xy, yz, zx)
+    // ---- NNPS ----
+    int *key = nullptr, *perm = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
+    int *g_idx = nullptr;   // sorted keys (reference g_idx)
+    int *scan_tmp = nullptr;
+    // ---- SELL-32 canonical neighbour list ----
+    int *ncnt = nullptr;          // list length per particle
+    long long *slice_off = nullptr;
+    int *nbr = nullptr;
+    long long nnz = 0, nnz_padded = 0;
+    long long nbr_cap = 0;
+    SideLists L;
+    // ---- PPE ----
+    Real *diag = nullptr;         // A_i of fluid rows
+    int *row_kind = nullptr;      // 0 identity, 1 fluid, 2 Neumann, 3 outlet copy, 4 pinned
+    int *row_aux = nullptr;       // outlet partner of kind-3 rows, -1 otherwise
+    int n_pins = 0;               // rows pinned to p = 0 (one per unanchored component)
+    int n_comp = 0;               // components carrying the rank-one mean-pressure term
+    int *comp_id = nullptr;       // component of each fluid row (-1: none)
+    double *comp_inv = nullptr;   // 1 / fluid rows of each component
+    double *nm_w = nullptr;       // Neumann row weights (CSR aligned with nm_nbr)
+    double *nm_gw = nullptr;      // mirror-row gradient weights
+    float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
+    double *coef_d = nullptr;     // cached c_ij, FP64 form
+    bool coef_valid = false;
+    // Krylov workspace
+    Real *kv[10] = {};            // r, rh, p, v, s, t, ph, sh, x, b
+    double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
+    float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
+    sph_ppe_stats last_ppe = {};
+    // live operator timing (sph_profile)
+    bool prof = false;
+    cudaEvent_t *prof_ev = nullptr;   // 512 events, created on first use
+    int prof_pending = 0;
+    long long prof_launches = 0;
+    double prof_ms = 0;
+    double *red = nullptr;        // block partial sums
+    double *red_host = nullptr;   // pinned
+    int red_blocks = 0;
+    double *scal = nullptr;       // device scalars
+    float *ml_w = nullptr;        // learned warm-start weights
+    R4 *sc_u = nullptr;           // pass scratch
+    Real *sc_p = nullptr, *sc_t = nullptr;
+
+    // staging for AoS upload/download
+    void *aos = nullptr;
+    size_t aos_bytes = 0;
+
+    template <class T>
+    int alloc(T *&ptr, size_t count) {
+        void *p = nullptr;
+        size_t bytes = sizeof(T) * (count ? count : 1);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+            return e == cudaErrorMemoryAllocation ? SPH_ERR_OUT_OF_MEMORY : SPH_ERR_CUDA;
+        }
+        allocs->push_back(p);
+        ptr = (T *)p;
+        return SPH_OK;
+    }
+    template <class T>
+    void release(T *&ptr) {
+        if (!ptr) return;
+        for (size_t k = 0; k < allocs->size(); ++k)
+            if ((*allocs)[k] == (void *)ptr) {
+                cudaFree(ptr);
+                (*allocs)[k] = allocs->back();
+                allocs->pop_back();
+                break;
+            }
+        ptr = nullptr;
+    }
+    void free_all() {
+        if (!allocs) return;
+        for (void *p : *allocs) cudaFree(p);
+        allocs->clear();
+    }
+};
+
+// ---- phases (nnps.cu, passes.cu, ppe.cu) ------------------------------------
+template <class Real> int ctx_allocate(Ctx<Real> &c);
+template <class Real> int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n);
+template <class Real> int ctx_upload_state(Ctx<Real> &c, const sph_part1 *P1, int n);
+template <class Real> int ctx_download(Ctx<Real> &c, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3);
+template <class Real> int nnps_build(Ctx<Real> &c);
+template <class Real> int nnps_export(Ctx<Real> &c, int32_t *g_idx, int32_t *p_idx, int32_t *g_str, int32_t *g_end);
+template <class Real> int neighbors_export(Ctx<Real> &c, int64_t *off, int32_t *list, int64_t *nnz);
+template <class Real> int phase_interaction(Ctx<Real> &c);
+template <class Real> int phase_ppe(Ctx<Real> &c, sph_ppe_stats *st);
+template <class Real> int phase_time_update(Ctx<Real> &c);
+template <class Real> int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax);
+template <class Real> int gradient_correction(Ctx<Real> &c);
+template <class Real> int neumann_pass(Ctx<Real> &c, VarSet<Real> &V);
+template <class Real> int outlet_pass(Ctx<Real> &c, VarSet<Real> &V);
+template <class Real> int periodic_pass(Ctx<Real> &c, VarSet<Real> &V);
+template <class Real> int freeslip_pass(Ctx<Real> &c, VarSet<Real> &V);
+template <class Real> int build_side_lists(Ctx<Real> &c);
+template <class Real> int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *bytes, int reset);
+
+// launch helper: grid for n threads
+inline dim3 grid_for(long long n, int block) { return dim3((unsigned)((n + block - 1) / block)); }
+
+}  // namespace sph

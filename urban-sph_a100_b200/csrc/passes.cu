@@ -1,0 +1,973 @@
+// Interaction and time-update passes of the ISPH step, one thread per
+// particle over the SELL-32 neighbour lists (or over precomputed side lists
+// for the boundary subsets).  Each kernel cites the reference kernel whose
+// formula it evaluates.  Semantics differ from the reference only where the
+// reference races: every pass reads the state as it was before the pass.
+#include <algorithm>
+#include <cfloat>
+#include <cstdio>
+
+#include "ctx.cuh"
+
+namespace sph {
+
+#define SELL_LOOP_BEGIN(i)                                                \
+    const long long sbase_ = slice_off[(i) >> 5] + ((i)&31);              \
+    const int scnt_ = ncnt[(i)];                                          \
+    for (int k_ = 0; k_ < scnt_; ++k_) {                                  \
+        const int j = __ldg(&nbr[sbase_ + 32LL * k_]);
+#define SELL_LOOP_END }
+
+#define LIST_ARGS const long long *__restrict__ slice_off, const int *__restrict__ ncnt, const int *__restrict__ nbr
+
+template <class Real>
+struct SoA {
+    typedef typename V4<Real>::type R4;
+    typedef typename V2<Real>::type R2;
+    const float4 *__restrict__ pf;
+    const R4 *__restrict__ pr;
+    const R2 *__restrict__ mr;
+    const int4 *__restrict__ ty;
+    const int *__restrict__ jc;
+};
+
+// FP32 radius test of the individual kernels against kappa*h_i, needed only
+// when h_j > h_i (the canonical list already holds r < kappa*max(h_i, h_j)).
+__device__ __forceinline__ bool within_hi(const DevParams &P, float4 a, float4 b) {
+    if (b.w <= a.w) return true;
+    return dist_rn(a.x, a.y, a.z, b.x, b.y, b.z) < __fmul_rn(P.skappa, a.w);
+}
+
+// ---------------------------------------------------------------------------
+// step start: SP1 <- P1, SP2 <- P2, memset(P3) (ISPH_Calc.cuh:42-61)
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_begin_step(Ctx<Real> c) {
+    typedef typename V4<Real>::type R4;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const VarSet<Real> &A = c.A;
+    const VarSet<Real> &S = c.S;
+    S.u[i] = A.u[i]; S.p[i] = A.p[i]; S.temp[i] = A.temp[i]; S.flt[i] = A.flt[i];
+    S.kt[i] = A.kt[i]; S.et[i] = A.et[i]; S.fb[i] = A.fb[i]; S.fm[i] = A.fm[i]; S.fl[i] = A.fl[i];
+    S.concn[i] = A.concn[i]; S.enth[i] = A.enth[i];
+    c.rho_ref_S[i] = c.rho_ref_A[i];
+    c.SR[i] = 0;
+    const R4 z = mk4<Real>(0, 0, 0, 0);
+    c.u0[i] = z; c.ft[i] = z; c.fp[i] = z; c.nrm[i] = z;
+    c.dtemp[i] = 0;
+}
+
+// KERNEL_clc_IB_normal_vector3D, functions_PREP.cuh:923-1015 (step 0 only)
+template <class Real>
+__global__ void k_ib_normals(DevParams P, const typename V4<Real>::type *pr, const int4 *ty,
+                             typename V4<Real>::type *nrm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || ty[i].w < 1000) return;
+    const auto x = pr[i];
+    Real nx = 0, ny = 0, nz = 0;
+    const double t = P.ib_face_tol;
+    if (fabs((double)x.x - P.ib_box[0]) < t) nx = -1;
+    if (fabs((double)x.x - P.ib_box[1]) < t) nx = 1;
+    if (fabs((double)x.y - P.ib_box[2]) < t) ny = -1;
+    if (fabs((double)x.y - P.ib_box[3]) < t) ny = 1;
+    if (fabs((double)x.z - P.ib_box[4]) < t) nz = -1;
+    if (fabs((double)x.z - P.ib_box[5]) < t) nz = 1;
+    const Real mag = sqrt(nx * nx + ny * ny + nz * nz);
+    if (mag > (Real)1e-9) nrm[i] = mk4<Real>(nx / mag, ny / mag, nz / mag, 0);
+    else nrm[i] = mk4<Real>(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_clc_gradient_correction_3D, functions_KNL.cuh:216-324
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void __launch_bounds__(128) k_grad_corr(DevParams P, SoA<Real> s, LIST_ARGS, Real *__restrict__ g6, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = (size_t)n;
+    const float4 fi = s.pf[i];
+    const auto xi = s.pr[i];
+    const int pti = s.ty[i].w;
+    Real txx = 0, tyy = 0, tzz = 0, txy = 0, tyz = 0, tzx = 0;
+    if (s.ty[i].x != 3) {
+        const Real hi = xi.w;
+        const Real tA = calc_tmpA<Real>(P, hi);
+        SELL_LOOP_BEGIN(i)
+            const float4 fj = s.pf[j];
+            if (fj.x == fi.x && fj.y == fi.y && fj.z == fi.z) continue;   // tdist > 0
+            if (!within_hi(P, fi, fj)) continue;
+            if (!(s.jc[j] & JB_PT1)) continue;
+            const auto xj = s.pr[j];
+            const auto mj = s.mr[j];
+            const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const Real tdist = sqrt(dx * dx + dy * dy + dz * dz);
+            const Real tdwij = calc_dwij<Real>(P, tA, hi, tdist);
+            const Real mtd = mj.x * tdwij;
+            const Real rtd = (Real)1 / (mj.y * tdist);
+            txx += -mtd * dx * dx * rtd;
+            txy += -mtd * dy * dx * rtd;
+            tyy += -mtd * dy * dy * rtd;
+            tzx += -mtd * dx * dz * rtd;
+            tyz += -mtd * dy * dz * rtd;
+            tzz += -mtd * dz * dz * rtd;
+        SELL_LOOP_END
+    }
+    Real det = txx * (tyy * tzz - tyz * tyz);
+    det -= txy * (txy * tzz - tyz * tzx);
+    det += tzx * (txy * tyz - tyy * tzx);
+    Real gxx = 1, gyy = 1, gzz = 1, gxy = 0, gyz = 0, gzx = 0;
+    if (fabs((double)det) > DBL_EPSILON && pti == 1) {
+        const Real r = (Real)1 / det;
+        gxx = (tyy * tzz - tyz * tyz) * r;
+        gxy = (tzx * tyz - txy * tzz) * r;
+        gzx = (txy * tyz - tzx * tyy) * r;
+        gyy = (txx * tzz - tzx * tzx) * r;
+        gyz = (tzx * txy - txx * tyz) * r;
+        gzz = (txx * tyy - txy * txy) * r;
+    }
+    g6[i] = gxx; g6[N + i] = gyy; g6[2 * N + i] = gzz; g6[3 * N + i] = gxy; g6[4 * N + i] = gyz; g6[5 * N + i] = gzx;
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_clc_prep3D, functions_PREP.cuh:287-488 (Shepard filter, strain rate,
+// SSM / DDF sub-grid viscosity, reference density)
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ g6,
+                                              const typename V4<Real>::type *__restrict__ u, Real *__restrict__ flt,
+                                              Real *__restrict__ vis_out, Real *__restrict__ kt, Real *__restrict__ et,
+                                              Real *__restrict__ SR, Real *__restrict__ rho_ref, int tcount, Real tdt, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
+    const size_t N = (size_t)n;
+    const float4 fi = s.pf[i];
+    const auto xi = s.pr[i];
+    const auto ui = u[i];
+    const auto mri = s.mr[i];
+    const Real gc11 = g6[i], gc22 = g6[N + i], gc33 = g6[2 * N + i], gc12 = g6[3 * N + i], gc23 = g6[4 * N + i], gc31 = g6[5 * N + i];
+    const Real hi = xi.w;
+    const Real tA = calc_tmpA<Real>(P, hi);
+    const bool filt = (tcount % P.freq_filt) == 0;
+    const bool les = P.fv_solve != 0 && P.turb != 0;
+    Real tmp_flt = 0, tmp_sigma = 0;
+    Real st11 = 0, st12 = 0, st22 = 0, st23 = 0, st31 = 0, st33 = 0;
+    SELL_LOOP_BEGIN(i)
+        const float4 fj = s.pf[j];
+        if (!within_hi(P, fi, fj)) continue;
+        const auto xj = s.pr[j];
+        const auto mj = s.mr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+        const Real w = calc_wij<Real>(P, tA, hi, tdist);
+        const Real vj = mj.x / mj.y;
+        if (filt) tmp_flt += vj * w;
+        if (les) {
+            tmp_sigma += tdist * tdist * w * vj;
+            if (s.jc[j] & JB_PT1) {
+                const Real dw = calc_dwij<Real>(P, tA, hi, tdist);
+                const Real tdwx = dw * dx / tdist, tdwy = dw * dy / tdist, tdwz = dw * dz / tdist;
+                const Real cx = gc11 * tdwx + gc12 * tdwy + gc31 * tdwz;
+                const Real cy = gc12 * tdwx + gc22 * tdwy + gc23 * tdwz;
+                const Real cz = gc31 * tdwx + gc23 * tdwy + gc33 * tdwz;
+                const auto uj = u[j];
+                const Real ux = uj.x - ui.x, uy = uj.y - ui.y, uz = uj.z - ui.z;
+                st11 += vj * ux * cx;
+                st12 += (Real)0.5 * vj * (ux * cy + uy * cx);
+                st22 += vj * uy * cy;
+                st23 += (Real)0.5 * vj * (uy * cz + uz * cy);
+                st31 += (Real)0.5 * vj * (ux * cz + uz * cx);
+                st33 += vj * uz * cz;
+            }
+        }
+    SELL_LOOP_END
+    if (les) {
+        Real tmp_SR = 2 * (st11 * st11 + st22 * st22 + st33 * st33 + 2 * st12 * st12 + 2 * st31 * st31 + 2 * st23 * st23);
+        tmp_SR = sqrt(tmp_SR);
+        SR[i] = tmp_SR;
+        tmp_sigma = sqrt((Real)0.3333 * tmp_sigma);
+        const Real cl = (tmp_sigma > hi) ? tmp_sigma : hi;
+        const int bt = ti.y;
+        if (P.turb == 4) {
+            const Real v = (Real)(P.cs_sgs * P.cs_sgs) * cl * cl * tmp_SR;
+            if (bt != 1) vis_out[i] = v;
+        } else if (P.turb == 5) {
+            Real ki = kt[i] > 0 ? kt[i] : (Real)0;
+            const Real nui = u[i].w;
+            const Real pp = nui * tmp_SR * tmp_SR;
+            const Real eps = (Real)0.93 * ki * sqrt(ki) / cl;     // Ce_sgs, Parameters.cuh:133
+            ki += (pp - eps) * tdt;
+            ki = (ki > (Real)1e-4) ? ki : (Real)1e-4;
+            const Real v = (Real)0.1 * cl * sqrt(ki);              // Ck_sgs, Parameters.cuh:132
+            if (bt != 1) { vis_out[i] = v; kt[i] = ki; et[i] = eps; }
+        }
+    }
+    if (tcount == 0) rho_ref[i] = mri.y;
+    if (filt) flt[i] = tmp_flt;
+}
+
+// vis_t lives in u.w; the LES result is staged and merged so that neighbours
+// read the step-start value (the reference reads nu_j only in the unused Tk term)
+template <class Real>
+__global__ void k_merge_vis(typename V4<Real>::type *u, const Real *vis, const int4 *ty, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 t = ty[i];
+    if (t.x > 2 || t.w >= 1000 || t.w <= 0 || t.y == 1) return;
+    u[i].w = vis[i];
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_boundary3D, functions_BC.cuh:100-190: wall velocity from fluid
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void __launch_bounds__(128) k_boundary(DevParams P, SoA<Real> s, LIST_ARGS,
+                                                  typename V4<Real>::type *__restrict__ u, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.x > 2 || ti.w != 0) return;
+    const float4 fi = s.pf[i];
+    const auto xi = s.pr[i];
+    const Real hi = xi.w;
+    const Real tA = calc_tmpA<Real>(P, hi);
+    Real tx = 0, ty_ = 0, tz = 0, flt = (Real)1.0e-10;
+    SELL_LOOP_BEGIN(i)
+        if (!(s.jc[j] & JB_POSN9)) continue;
+        const float4 fj = s.pf[j];
+        if (!within_hi(P, fi, fj)) continue;
+        const auto xj = s.pr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
+        const Real w = calc_wij<Real>(P, tA, hi, tdist);
+        const auto uj = u[j];
+        tx += uj.x * w; ty_ += uj.y * w; tz += uj.z * w; flt += w;
+    SELL_LOOP_END
+    auto ui = u[i];
+    ui.x = -tx / flt; ui.y = -ty_ / flt; ui.z = -tz / flt;
+    u[i] = ui;
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_MOST_boundary3D, functions_MOST.cuh:151-322 (FP32 as written there)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float most_clamp(float v, float lo, float hi) { return fmaxf(lo, fminf(v, hi)); }
+__device__ __forceinline__ double most_psi_m(float zeta) {
+    if (zeta < 0.0f) {
+        const float x = sqrtf(sqrtf(1.0f - 16.0f * zeta));
+        return 3.14159265358979323846 * 0.5f - 2.0f * atanf(x) + logf((1.0f + x) * (1.0f + x) * (1.0f + x * x) * 0.125f);
+    }
+    return -5.0f * zeta;
+}
+__device__ __forceinline__ double most_psi_h(float zeta) {
+    if (zeta < 0.0f) return 2.0f * logf(0.5f * (1.0f + sqrtf(1.0f - 16.0f * zeta)));
+    return -5.0f * zeta;
+}
+__device__ __forceinline__ double most_Phi_m(float L, float z, float z0) { return logf(z / z0) - most_psi_m(z / L) + most_psi_m(z0 / L); }
+__device__ __forceinline__ double most_Phi_h(float L, float z, float z0h) { return logf(z / z0h) - most_psi_h(z / L) + most_psi_h(z0h / L); }
+
+template <class Real>
+__global__ void k_most(DevParams P, SoA<Real> s, const int *rows, const int *off, const int *tgt, int nrows,
+                       const typename V4<Real>::type *u, const Real *temp, typename V4<Real>::type *fm,
+                       typename V4<Real>::type *fl, Real *dtemp, int tcount, float tdt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    const auto xi = s.pr[i];
+    const auto ui = u[i];
+    const float zi = (float)xi.z, tempi = (float)temp[i], rhoi = (float)s.mr[i].y, mi = (float)s.mr[i].x;
+    const float uxi = (float)ui.x, uyi = (float)ui.y;
+    const Real space = xi.w / (Real)1.5;    // h_coeff, Parameters.cuh:68
+    const float z0 = (float)P.most_z0, z0h = (float)P.most_z0h;
+    float u_star, theta_star, OB;
+    float ts;
+    if (tdt * tcount >= P.t_start && tdt * tcount < P.t_con_t) ts = P.t_ini + tdt * tcount * (P.t_con - P.t_ini) / (P.t_con_t - P.t_start);
+    else if (tdt * tcount < P.t_start) ts = P.t_ini;
+    else ts = P.t_con;
+    float ws = sqrtf(uxi * uxi + uyi * uyi);
+    ws = most_clamp(ws, 0.001f, 100.0f);
+    const float Ri_b = (9.810 / tempi) * (tempi - ts) * zi / (ws * ws + 1e-10);
+    if ((double)fabsf(Ri_b) > 1e-3) {
+        OB = most_clamp(zi / Ri_b, -500.0f, 500.0f);
+        for (int it = 0; it < 200; it++) {   // MAX_ITER, Parameters.cuh:109
+            const float om = OB, ol = 0.999 * om, ou = 1.001 * om;
+            const float fL = Ri_b - (zi / om) * most_Phi_h(om, zi, z0h) / powf((float)most_Phi_m(om, zi, z0), 2);
+            const double pu = most_Phi_m(ou, zi, z0), pl = most_Phi_m(ol, zi, z0);
+            const float dfL = ((-(zi / ou) * most_Phi_h(ou, zi, z0h) / (pu * pu)) - (-(zi / ol) * most_Phi_h(ol, zi, z0h) / (pl * pl))) / (ou - ol);
+            OB -= 1.0f * fL / dfL;
+            if ((double)fabsf(OB) > 1e-6) {   // TOLERANCE, Parameters.cuh:110
+                if ((double)fabsf((OB - om) / OB) < 1e-5) break;
+                else if ((double)fabsf(OB - om) < 1e-5) break;
+            }
+        }
+        u_star = 0.4 * ws / most_Phi_m(OB, zi, z0);
+        theta_star = 0.4 * (tempi - ts) / most_Phi_h(OB, zi, z0h);
+    } else {
+        OB = 1e6f;
+        u_star = 0.4 * ws / logf(zi / z0);
+        theta_star = 0.4 * (tempi - ts) / logf(zi / z0h);
+    }
+    const float mx = -rhoi * u_star * (uxi * u_star / ws);
+    const float my = -rhoi * u_star * (uyi * u_star / ws);
+    const Real shf = (Real)(-rhoi * 1005 * u_star * theta_star * 100.0);   // Air_cp, Parameters.cuh:119
+    const Real q = (Real)0.5 * shf / (space * (Real)rhoi * (Real)1005);
+    for (int e = off[k]; e < off[k + 1]; ++e) {
+        const int j = tgt[e];
+        atomicAdd(&dtemp[j], q);
+        fm[j].z = q;
+    }
+    auto f = fm[i];
+    f.x = (Real)(1.0 * mx * space * space / mi);
+    f.y = (Real)(1.0 * my * space * space / mi);
+    f.z = q;
+    fm[i] = f;
+    atomicAdd(&dtemp[i], q);
+    fl[i] = mk4<Real>(u_star, theta_star, OB, 0);
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_Neumann_boundary3D, functions_BC.cuh:290-446, from the precomputed
+// weights: p_w = sum w p (or the mirror extrapolation), u of p_type -1 from
+// the Shepard weights; rows without fluid in range get p = 0.
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_neumann_gather(const int *rows, const int *off, const int *nb, const int *mirror,
+                                 const double *w, const double *gw, int nrows, const Real *p,
+                                 const typename V4<Real>::type *u, const int4 *ty, Real *out_p,
+                                 typename V4<Real>::type *out_u) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    const int s = off[k], e = off[k + 1];
+    auto ui = u[i];
+    Real pv = 0;
+    if (e > s) {
+        const bool mir = mirror[k] != 0;
+        Real sp = 0, sx = 0, sy = 0, sz = 0;
+        for (int q = s; q < e; ++q) {
+            const int j = nb[q];
+            const Real wj = (Real)w[q];
+            sp += (mir ? (Real)gw[q] : wj) * p[j];
+            if (ty[i].w == -1) { const auto uj = u[j]; sx += wj * uj.x; sy += wj * uj.y; sz += wj * uj.z; }
+        }
+        pv = sp;
+        if (ty[i].w == -1) { ui.x = sx; ui.y = sy; ui.z = sz; }
+    }
+    out_p[k] = pv;
+    out_u[k] = ui;
+}
+
+template <class Real>
+__global__ void k_neumann_scatter(const int *rows, int nrows, const Real *in_p, const typename V4<Real>::type *in_u,
+                                  Real *p, typename V4<Real>::type *u) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    p[i] = in_p[k];
+    u[i] = in_u[k];
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_advection_force3D, functions_PPE.cuh:191-480: viscous (Cleary or
+// Monaghan), Eulerian convective term, artificial viscosity, gravity
+// ---------------------------------------------------------------------------
+template <class Real, int FV>
+__global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIST_ARGS,
+                                                   const typename V4<Real>::type *__restrict__ u,
+                                                   const Real *__restrict__ eli,
+                                                   typename V4<Real>::type *__restrict__ ft, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.x > 2 || ti.w == 1000 || ti.w <= 0) return;
+    const int jci = s.jc[i];
+    const auto xi = s.pr[i];
+    const auto ui = u[i];
+    const auto mri = s.mr[i];
+    const Real hi = xi.w, mi = mri.x, rhoi = mri.y;
+    const Real tA = calc_tmpA<Real>(P, hi);
+    const Real visi = visc2<Real>(P, jci) + ui.w * rhoi;
+    const Real el = eli[i];
+    const Real Alpha = (Real)(float)P.av_alpha, Beta = (Real)(float)P.av_beta, c0 = (Real)(float)P.av_c0;
+    const bool kgc = P.kgc_solve == 1;
+    Real tx = 0, ty_ = 0, tz = 0, ex = 0, ey = 0, ez = 0;
+    SELL_LOOP_BEGIN(i)
+        const int jcj = s.jc[j];
+        if (!(jcj & JB_LT1000)) continue;
+        const auto xj = s.pr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+        Real dw = calc_dwij<Real>(P, tA, hi, tdist);
+        if (kgc) dw = 0;   // Cm is never filled on this path (all zero)
+        const Real tdwx = dw * dx / tdist, tdwy = dw * dy / tdist, tdwz = dw * dz / tdist;
+        const auto uj = u[j];
+        const auto mj = s.mr[j];
+        const Real ux = ui.x - uj.x, uy = ui.y - uj.y, uz = ui.z - uj.z;
+        if (FV == 1) {
+            const Real visj = visc2<Real>(P, jcj) + uj.w * mj.y;
+            Real C = dx * tdwx + dy * tdwy + dz * tdwz;
+            C *= (visi * visj) / (visi + visj);
+            C *= 4 * (mj.x / (rhoi * mj.y));
+            C /= tdist;
+            C /= tdist;
+            tx += C * ux; ty_ += C * uy; tz += C * uz;
+        } else if (FV == 2) {
+            const Real uij_xij = ux * dx + uy * dy + uz * dz;
+            const Real visj = visc2<Real>(P, jcj) + uj.w * mj.y;
+            Real phi = uij_xij / (tdist * tdist + (Real)0.01 * hi * hi);
+            Real Pij = (Real)(-2.0 * (3 + 2.0)) * phi * mj.x / mj.y;
+            const Real Cv = (Real)2 * (visi * visj) / (visi + visj - (Real)1e-20);
+            Pij *= Cv / rhoi;
+            if ((jci & JB_MON0) || (jcj & JB_MON0)) Pij = 0;
+            tx += -Pij * tdwx; ty_ += -Pij * tdwy; tz += -Pij * tdwz;
+        }
+        if (el < (Real)1) {
+            const Real vj = mj.x / mj.y * ((Real)1 - el);
+            ex += (ui.x * (-ux) * tdwx + ui.y * (-ux) * tdwy + ui.z * (-ux) * tdwz) * vj;
+            ey += (ui.x * (-uy) * tdwx + ui.y * (-uy) * tdwy + ui.z * (-uy) * tdwz) * vj;
+            ez += (ui.x * (-uz) * tdwx + ui.y * (-uz) * tdwy + ui.z * (-uz) * tdwz) * vj;
+        }
+        const Real uij_xij = ux * dx + uy * dy + uz * dz;
+        if (uij_xij < 0) {
+            const Real hij = (hi + xj.w) * (Real)0.5;
+            Real phi = hij * uij_xij / (tdist * tdist + (Real)0.01 * hij * hij);
+            Real Pij = mi * phi * (-Alpha * c0 + Beta * phi);
+            Pij /= (rhoi + mj.y);
+            Pij *= (Real)0.5;
+            tx += -Pij * tdwx; ty_ += -Pij * tdwy; tz += -Pij * tdwz;
+        }
+    SELL_LOOP_END
+    if (P.fg_solve) tz += (Real)-9.810;
+    ft[i] = mk4<Real>(tx - ex, ty_ - ey, tz - ez, sqrt(tx * tx + ty_ * ty_ + tz * tz));
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_clc_projection, functions_TIME_ISPH.cuh:2-112 (predictor)
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::type *u,
+                             typename V4<Real>::type *u0, const typename V4<Real>::type *ft,
+                             const typename V4<Real>::type *fm, Real *rho_ref, const typename V2<Real>::type *mr,
+                             Real tdt, float ttime, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 t = ty[i];
+    if (t.x >= 3 || t.w >= 1000) return;
+    auto ui = u[i];
+    if (t.w == 9) {
+        const Real bv = (Real)(float)P.boundary_velocity;
+        ui.x = bv; ui.y = 0; ui.z = 0;
+        u0[i] = mk4<Real>(bv, 0, 0, 1);
+    } else {
+        u0[i] = mk4<Real>(ui.x, ui.y, ui.z, 1);
+        if (t.w > 0) {
+            const Real on = (t.y == 0 || t.z == 1) ? (Real)1 : (Real)0;
+            const auto f = ft[i];
+            const auto m = fm[i];
+            ui.x = ui.x + (f.x * on + m.x) * tdt;
+            ui.y = ui.y + (f.y * on + m.y) * tdt;
+            ui.z = ui.z + (f.z * on) * tdt;
+        }
+    }
+    u[i] = ui;
+    if (ttime == 0) rho_ref[i] = mr[i].y;
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_periodic_boundary3D (functions_BC.cuh:1015-1154) and
+// KERNEL_donothing_buffer3D (functions_BC.cuh:673-761): copy u, p, T from the
+// precomputed partner (zero when the reference finds none).  Gather first,
+// then scatter, so every buffer particle reads the pre-pass state.
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_partner_gather(const int *rows, const int *partner, int nrows,
+                                 const typename V4<Real>::type *u, const Real *p, const Real *temp,
+                                 typename V4<Real>::type *ou, Real *op, Real *ot) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k], j = partner[k];
+    auto ui = u[i];
+    if (j >= 0) {
+        const auto uj = u[j];
+        ui.x = uj.x; ui.y = uj.y; ui.z = uj.z;
+        op[k] = p[j]; ot[k] = temp[j];
+    } else {
+        ui.x = 0; ui.y = 0; ui.z = 0;
+        op[k] = 0; ot[k] = 0;
+    }
+    ou[k] = ui;
+}
+
+template <class Real>
+__global__ void k_partner_scatter(const int *rows, int nrows, const typename V4<Real>::type *ou, const Real *op,
+                                  const Real *ot, typename V4<Real>::type *u, Real *p, Real *temp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    u[i] = ou[k]; p[i] = op[k]; temp[i] = ot[k];
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_freeslip_boundary3D, functions_BC.cuh:1156-1271
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void __launch_bounds__(128) k_freeslip(DevParams P, SoA<Real> s, LIST_ARGS,
+                                                  const typename V4<Real>::type *__restrict__ u,
+                                                  const Real *__restrict__ p, const Real *__restrict__ temp,
+                                                  typename V4<Real>::type *__restrict__ ou,
+                                                  Real *__restrict__ op, Real *__restrict__ ot, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.w != -1 || ti.x >= 3) return;
+    const float4 fi = s.pf[i];
+    const auto xi = s.pr[i];
+    const Real hi = xi.w;
+    const Real tA = calc_tmpA<Real>(P, hi);
+    Real tux = 0, tuy = 0, tuz = 0, tp = 0, tt = 0, tf = 0;
+    SELL_LOOP_BEGIN(i)
+        if (!(s.jc[j] & JB_PT1)) continue;
+        const float4 fj = s.pf[j];
+        if (!within_hi(P, fi, fj)) continue;
+        const auto xj = s.pr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
+        const auto mj = s.mr[j];
+        const Real vw = mj.x / mj.y * calc_wij<Real>(P, tA, hi, tdist);
+        const auto uj = u[j];
+        tux += uj.x * vw; tuy += uj.y * vw; tuz += uj.z * vw; tp += p[j] * vw; tt += temp[j] * vw; tf += vw;
+    SELL_LOOP_END
+    auto uo = u[i];
+    Real po = p[i], to = temp[i];
+    if (tf > (Real)1e-5) { uo.x = tux / tf; uo.y = tuy / tf; uo.z = tuz / tf; po = tp / tf; to = tt / tf; }
+    ou[i] = uo; op[i] = po; ot[i] = to;
+}
+
+template <class Real>
+__global__ void k_copy_rows(const int *rows, int nrows, const typename V4<Real>::type *su, const Real *sp,
+                            const Real *st, typename V4<Real>::type *u, Real *p, Real *temp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    u[i] = su[i]; p[i] = sp[i]; temp[i] = st[i];
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_pressureforce3D, functions_PPE.cuh:482-647 (h_ij = (h_i+h_j)/2)
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void __launch_bounds__(128) k_pressure_force(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ p,
+                                                        const Real *__restrict__ pres0,
+                                                        typename V4<Real>::type *__restrict__ fp, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0 || ti.y != 0) return;
+    const auto xi = s.pr[i];
+    const auto mri = s.mr[i];
+    const Real hi = xi.w, rhoi = mri.y, pi = p[i] - pres0[i];
+    const bool kgc = P.kgc_solve == 1;
+    const bool uniform_hint = true;
+    Real tA_ii = calc_tmpA<Real>(P, hi);
+    Real tx = 0, ty_ = 0, tz = 0;
+    if (P.fp_solve) {
+        SELL_LOOP_BEGIN(i)
+            if (!(s.jc[j] & JB_LT1000)) continue;
+            const auto xj = s.pr[j];
+            const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
+            const Real hij = (Real)0.5 * (hi + xj.w);
+            const Real tA = (uniform_hint && xj.w == hi) ? tA_ii : calc_tmpA<Real>(P, hij);
+            Real dw = calc_dwij<Real>(P, tA, hij, tdist);
+            if (kgc) dw = 0;
+            const auto mj = s.mr[j];
+            const Real pj = p[j] - pres0[j];
+            const Real Cp = (Real)-2 * mj.x / (rhoi * mj.y) * (pi * mj.y + pj * rhoi) / (rhoi + mj.y);
+            const Real f = Cp * dw / tdist;
+            tx += f * dx; ty_ += f * dy; tz += f * dz;
+        SELL_LOOP_END
+    }
+    fp[i] = mk4<Real>(tx, ty_, tz, 0);
+}
+
+// ---------------------------------------------------------------------------
+// IBM_force_interpolation3D (functions_IBM.cuh:342-490) and
+// IBM_spreading_interpolation3D (functions_IBM.cuh:492-613)
+// ---------------------------------------------------------------------------
+__device__ double wall_profile(const DevParams &P, double z) {
+    const int NP = P.n_profile;
+    const double *Z = P.profile_z, *U = P.profile_u;
+    if (z <= Z[0]) return U[0] + (z - Z[0]) * ((U[1] - U[0]) / ((Z[1] - Z[0]) + 1e-300));
+    if (z >= Z[NP - 1]) return U[NP - 2] + (z - Z[NP - 2]) * ((U[NP - 1] - U[NP - 2]) / ((Z[NP - 1] - Z[NP - 2]) + 1e-300));
+    int lo = 0, hi = NP - 1;
+    while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (z < Z[mid]) hi = mid; else lo = mid; }
+    const double t = (z - Z[lo]) / (Z[hi] - Z[lo] + 1e-300);
+    return U[lo] + t * (U[hi] - U[lo]);
+}
+
+template <class Real>
+__global__ void k_ibm_force(DevParams P, SoA<Real> s, const int *rows, const int *off, const int *nb, int nrows,
+                            const typename V4<Real>::type *u, const typename V4<Real>::type *nrm,
+                            typename V4<Real>::type *fb, Real t_dt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    const auto xi = s.pr[i];
+    const Real th = (Real)(P.ibm_length * (double)xi.w);
+    const Real tA = calc_tmpA<Real>(P, th);
+    Real tux = 0, tuy = 0, tuz = 0, filt = 0;
+    for (int e = off[k]; e < off[k + 1]; ++e) {
+        const int j = nb[e];
+        const auto xj = s.pr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+        const auto mj = s.mr[j];
+        const Real vw = mj.x / mj.y * calc_wij<Real>(P, tA, th, tdist);
+        const auto uj = u[j];
+        tux += uj.x * vw; tuy += uj.y * vw; tuz += uj.z * vw; filt += vw;
+    }
+    const Real ufx = tux / (filt + (Real)1e-10), ufy = tuy / (filt + (Real)1e-10), ufz = tuz / (filt + (Real)1e-10);
+    const auto nv = nrm[i];
+    Real nx = nv.x, ny = nv.y, nz = nv.z;
+    const Real nmag = sqrt(nx * nx + ny * ny + nz * nz) + (Real)1e-20;
+    nx /= nmag; ny /= nmag; nz /= nmag;
+    const Real un = ufx * nx + ufy * ny + ufz * nz;
+    const Real utx = ufx - un * nx, uty = ufy - un * ny, utz = ufz - un * nz;
+    const Real Ubtx = (Real)(P.ibm_target_coeff * wall_profile(P, (double)xi.z));
+    const Real cx = -un * nx + (Ubtx - utx), cy = -un * ny + (0 - uty), cz = -un * nz + (0 - utz);
+    fb[i] = mk4<Real>((Real)(P.rho_air * (double)cx / (double)t_dt), (Real)(P.rho_air * (double)cy / (double)t_dt),
+                      (Real)(P.rho_air * (double)cz / (double)t_dt), filt);
+}
+
+template <class Real>
+__global__ void k_ibm_spread(DevParams P, SoA<Real> s, const int *rows, const int *off, const int *nb, int nrows,
+                             const typename V4<Real>::type *fbm, typename V4<Real>::type *fb) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    const auto xi = s.pr[i];
+    const Real th = (Real)(P.ibm_length * (double)xi.w);
+    const Real tA = calc_tmpA<Real>(P, th);
+    Real fx = 0, fy = 0, fz = 0, filt = 0;
+    for (int e = off[k]; e < off[k + 1]; ++e) {
+        const int j = nb[e];
+        const auto xj = s.pr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+        const auto mj = s.mr[j];
+        const Real vw = mj.x / mj.y * calc_wij<Real>(P, tA, th, tdist);
+        const auto f = fbm[j];
+        fx += f.x * vw; fy += f.y * vw; fz += f.z * vw; filt += vw;
+    }
+    if (filt < (Real)1e-12) fb[i] = mk4<Real>(0, 0, 0, 0);
+    else fb[i] = mk4<Real>(fx / (filt + (Real)1e-10), fy / (filt + (Real)1e-10), fz / (filt + (Real)1e-10), filt);
+}
+
+template <class Real>
+__global__ void k_zero_rows4(const int *rows, int nrows, typename V4<Real>::type *a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nrows) a[rows[k]] = mk4<Real>(0, 0, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// KERNEL_time_update_projection (functions_TIME_ISPH.cuh:115-296) and
+// IBM_corrector (functions_IBM.cuh:615-725): SP1 -> P1
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_time_update(Ctx<Real> c, Real tdt, int tcount) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int4 t = c.ty[i];
+    const VarSet<Real> &S = c.S;
+    const VarSet<Real> &A = c.A;
+    const DevParams &P = c.dp;
+    if (t.w >= 1000) {   // IBM_corrector
+        A.fb[i] = S.fb[i];
+        A.p[i] = S.p[i];
+        return;
+    }
+    if (t.x >= 3) return;
+    auto us = S.u[i];
+    auto ua = A.u[i];
+    if (t.w == 9) {
+        ua.x = us.x; ua.y = us.y; ua.z = us.z;
+    } else {
+        Real ux0, uy0, uz0, ax = 0, ay = 0, az = 0;
+        const auto u0 = c.u0[i];
+        if (t.w > 0) {
+            ux0 = us.x; uy0 = us.y; uz0 = us.z;
+            if (t.y == 1 || t.y == -1) { ux0 = u0.x; uy0 = u0.y; uz0 = u0.z; }
+            const Real on = (t.y == 0) ? (Real)1 : (Real)0;
+            const auto fp = c.fp[i];
+            const auto fb = S.fb[i];
+            const auto fm = S.fm[i];
+            const Real rho = c.mr[i].y;
+            ax = fp.x * on + fb.x / rho + fm.x;
+            ay = fp.y * on + fb.y / rho + fm.y;
+            az = fp.z * on + fb.z / rho;
+        } else {
+            ux0 = u0.x; uy0 = u0.y; uz0 = u0.z;
+        }
+        Real uxc = ux0 + ax * tdt, uyc = uy0 + ay * tdt, uzc = uz0 + az * tdt;
+        const Real ul = (Real)P.u_limit;
+        if (uxc * uxc + uyc * uyc + uzc * uzc >= ul * ul) { uxc = ux0; uyc = uy0; uzc = uz0; }
+        ua.x = uxc; ua.y = uyc; ua.z = uzc;
+    }
+    ua.w = us.w;   // vis_t
+    A.u[i] = ua;
+    Real temp = S.temp[i];
+    if (t.w == 0) {
+        const double tt = (double)(tdt * (Real)tcount);
+        if (tt >= P.t_start && tt < P.t_con_t) temp = (Real)(P.t_ini + tt * (P.t_con - P.t_ini) / (P.t_con_t - P.t_start));
+        else if (tt < P.t_start) temp = (Real)P.t_ini;
+        else temp = (Real)P.t_con;
+    }
+    A.temp[i] = temp;
+    A.enth[i] = S.enth[i];
+    Real concn = S.concn[i];
+    if (c.source[i] == 1) concn += (Real)0.5 * tdt;
+    A.concn[i] = concn;
+    A.p[i] = S.p[i]; A.flt[i] = S.flt[i]; A.kt[i] = S.kt[i]; A.et[i] = S.et[i];
+    A.fb[i] = S.fb[i]; A.fm[i] = S.fm[i]; A.fl[i] = S.fl[i];
+    c.rho_ref_A[i] = c.rho_ref_S[i];
+}
+
+// ---------------------------------------------------------------------------
+// diagnostics, kernel_copy_max (functions_OUTPUT.cuh:19-33) + max reduction
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_diag(Ctx<Real> c, unsigned int *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float mu = 0, mr = 0, mf = 0;
+    if (i < c.n) {
+        const int4 t = c.ty[i];
+        if (!(t.w == 0 || t.x >= 2)) {
+            const auto u = c.A.u[i];
+            mu = (float)sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
+            const Real rr = c.rho_ref_S[i];
+            mr = (float)((c.mr[i].y - rr) / rr * (Real)100.0);
+            mf = (float)c.ft[i].w;
+        }
+    }
+    // order-preserving float -> unsigned map for atomicMax
+    auto key = [](float f) -> unsigned int {
+        unsigned int b = __float_as_uint(f);
+        return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    };
+    for (int o = 16; o > 0; o >>= 1) {
+        mu = fmaxf(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+        mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+        mf = fmaxf(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[0], key(mu));
+        atomicMax(&out[1], key(mr));
+        atomicMax(&out[2], key(mf));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+template <class Real>
+static SoA<Real> soa(Ctx<Real> &c) {
+    SoA<Real> s;
+    s.pf = c.pf; s.pr = c.pr; s.mr = c.mr; s.ty = c.ty; s.jc = c.jc;
+    return s;
+}
+
+#define LIST(c) (c).slice_off, (c).ncnt, (c).nbr
+
+template <class Real>
+int gradient_correction(Ctx<Real> &c) {
+    k_grad_corr<Real><<<grid_for(c.n, 128), 128, 0, c.stream>>>(c.dp, soa(c), LIST(c), c.g6, c.n);
+    ++c.launches;
+    SPH_CUDA_TRY(cudaGetLastError());
+    c.gc_valid = true;
+    return SPH_OK;
+}
+
+// scratch for the gather/scatter passes (n-long u, p and temp buffers)
+template <class Real>
+static int scratch_rows(Ctx<Real> &c, typename V4<Real>::type *&ou, Real *&op, Real *&ot) {
+    if (!c.sc_u) {
+        SPH_TRY(c.alloc(c.sc_u, (size_t)c.n));
+        SPH_TRY(c.alloc(c.sc_p, (size_t)c.n));
+        SPH_TRY(c.alloc(c.sc_t, (size_t)c.n));
+    }
+    ou = c.sc_u;
+    op = c.sc_p;
+    ot = c.sc_t;
+    return SPH_OK;
+}
+
+template <class Real>
+int neumann_pass(Ctx<Real> &c, VarSet<Real> &V) {
+    const SideLists &L = c.L;
+    if (L.n_nm == 0) return SPH_OK;
+    typename V4<Real>::type *ou; Real *op, *ot;
+    SPH_TRY(scratch_rows(c, ou, op, ot));
+    k_neumann_gather<Real><<<grid_for(L.n_nm, 128), 128, 0, c.stream>>>(L.nm_rows, L.nm_off, L.nm_nbr, L.nm_ghost,
+                                                                        c.nm_w, c.nm_gw, L.n_nm, V.p, V.u, c.ty, op, ou);
+    k_neumann_scatter<Real><<<grid_for(L.n_nm, 128), 128, 0, c.stream>>>(L.nm_rows, L.n_nm, op, ou, V.p, V.u);
+    c.launches += 2;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+template <class Real>
+static int partner_pass(Ctx<Real> &c, VarSet<Real> &V, const int *rows, const int *partner, int nrows) {
+    if (nrows == 0) return SPH_OK;
+    typename V4<Real>::type *ou; Real *op, *ot;
+    SPH_TRY(scratch_rows(c, ou, op, ot));
+    k_partner_gather<Real><<<grid_for(nrows, 128), 128, 0, c.stream>>>(rows, partner, nrows, V.u, V.p, V.temp, ou, op, ot);
+    k_partner_scatter<Real><<<grid_for(nrows, 128), 128, 0, c.stream>>>(rows, nrows, ou, op, ot, V.u, V.p, V.temp);
+    c.launches += 2;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+template <class Real>
+int outlet_pass(Ctx<Real> &c, VarSet<Real> &V) {
+    return partner_pass(c, V, c.L.out_rows, c.L.out_partner, c.L.n_out);
+}
+
+template <class Real>
+int periodic_pass(Ctx<Real> &c, VarSet<Real> &V) {
+    return partner_pass(c, V, c.L.per_rows, c.L.per_partner, c.L.n_per);
+}
+
+template <class Real>
+int freeslip_pass(Ctx<Real> &c, VarSet<Real> &V) {
+    if (c.L.n_fs == 0) return SPH_OK;
+    typename V4<Real>::type *ou; Real *op, *ot;
+    SPH_TRY(scratch_rows(c, ou, op, ot));
+    k_freeslip<Real><<<grid_for(c.n, 128), 128, 0, c.stream>>>(c.dp, soa(c), LIST(c), V.u, V.p, V.temp, ou, op, ot, c.n);
+    k_copy_rows<Real><<<grid_for(c.L.n_fs, 128), 128, 0, c.stream>>>(c.L.fs_rows, c.L.n_fs, ou, op, ot, V.u, V.p, V.temp);
+    c.launches += 2;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+template <class Real>
+int phase_interaction(Ctx<Real> &c) {
+    cudaStream_t st = c.stream;
+    const int n = c.n;
+    const int tc = c.count;
+    const Real tdt = (Real)c.dp.dt;
+    c.dp.count = tc;
+    c.dp.time = c.time;
+    k_begin_step<Real><<<grid_for(n, 256), 256, 0, st>>>(c);
+    ++c.launches;
+    if (tc == 0) {
+        k_ib_normals<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.pr, c.ty, c.nrm, n);
+        ++c.launches;
+    }
+    if (!c.gc_valid || c.prm.recompute_gc) SPH_TRY(gradient_correction(c));
+    // prep / LES
+    Real *vis_stage = c.diag;   // staging (diag is rebuilt by the PPE)
+    k_prep<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
+                                                   c.S.et, c.SR, c.rho_ref_S, tc, tdt, n);
+    ++c.launches;
+    if (c.dp.fv_solve != 0 && (c.dp.turb == 4 || c.dp.turb == 5)) {
+        k_merge_vis<Real><<<grid_for(n, 256), 256, 0, st>>>(c.S.u, vis_stage, c.ty, n);
+        ++c.launches;
+    }
+    if (c.dp.noslip == 1) {
+        k_boundary<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, n);
+        ++c.launches;
+    }
+    if (c.L.n_most > 0) {
+        k_most<Real><<<grid_for(c.L.n_most, 128), 128, 0, st>>>(c.dp, soa(c), c.L.most_rows, c.L.most_off, c.L.most_tgt,
+                                                               c.L.n_most, c.S.u, c.S.temp, c.S.fm, c.S.fl, c.dtemp, tc, (float)tdt);
+        ++c.launches;
+    }
+    if (tc == 0) SPH_TRY(neumann_pass(c, c.S));
+    if (c.dp.fv_solve == 2)
+        k_advection<Real, 2><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, n);
+    else if (c.dp.fv_solve == 1)
+        k_advection<Real, 1><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, n);
+    else
+        k_advection<Real, 0><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, n);
+    ++c.launches;
+    if (c.dp.time_type == 1) {
+        k_projection<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.ty, c.S.u, c.u0, c.ft, c.S.fm, c.rho_ref_S, c.mr,
+                                                             tdt, c.time, n);
+        ++c.launches;
+    }
+    SPH_TRY(periodic_pass(c, c.S));
+    SPH_TRY(freeslip_pass(c, c.S));
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+template <class Real>
+int phase_time_update(Ctx<Real> &c) {
+    cudaStream_t st = c.stream;
+    const int n = c.n;
+    const Real tdt = (Real)c.dp.dt;
+    k_pressure_force<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.p, c.pres0, c.fp, n);
+    ++c.launches;
+    if (c.L.n_mk > 0) {
+        k_ibm_force<Real><<<grid_for(c.L.n_mk, 128), 128, 0, st>>>(c.dp, soa(c), c.L.mk_rows, c.L.mk_off, c.L.mk_nbr,
+                                                                  c.L.n_mk, c.S.u, c.nrm, c.S.fb, tdt);
+        ++c.launches;
+    }
+    if (c.L.n_sp > 0) {
+        k_ibm_spread<Real><<<grid_for(c.L.n_sp, 128), 128, 0, st>>>(c.dp, soa(c), c.L.sp_rows, c.L.sp_off, c.L.sp_nbr,
+                                                                   c.L.n_sp, c.S.fb, c.S.fb);
+        ++c.launches;
+    }
+    if (c.L.n_sp_zero > 0) {
+        k_zero_rows4<Real><<<grid_for(c.L.n_sp_zero, 256), 256, 0, st>>>(c.L.sp_zero, c.L.n_sp_zero, c.S.fb);
+        ++c.launches;
+    }
+    k_time_update<Real><<<grid_for(n, 256), 256, 0, st>>>(c, tdt, c.count);
+    ++c.launches;
+    SPH_TRY(neumann_pass(c, c.A));
+    SPH_TRY(outlet_pass(c, c.A));
+    SPH_TRY(periodic_pass(c, c.A));
+    SPH_TRY(freeslip_pass(c, c.A));
+    SPH_CUDA_TRY(cudaGetLastError());
+    c.time = c.time + c.dp.dt;
+    c.count += 1;
+    return SPH_OK;
+}
+
+template <class Real>
+int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax) {
+    unsigned int *d = (unsigned int *)c.cell_fill;   // reused scratch
+    SPH_CUDA_TRY(cudaMemsetAsync(d, 0, 3 * sizeof(unsigned int), c.stream));
+    k_diag<Real><<<grid_for(c.n, 256), 256, 0, c.stream>>>(c, d);
+    ++c.launches;
+    unsigned int h[3];
+    SPH_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    auto val = [](unsigned int k) {
+        unsigned int b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+        float f;
+        memcpy(&f, &b, 4);
+        return f;
+    };
+    if (umax) *umax = val(h[0]);
+    if (drho) *drho = val(h[1]);
+    if (fmax) *fmax = val(h[2]);
+    return SPH_OK;
+}
+
+#define INST(R)                                                          \
+    template int gradient_correction<R>(Ctx<R> &);                       \
+    template int neumann_pass<R>(Ctx<R> &, VarSet<R> &);                 \
+    template int outlet_pass<R>(Ctx<R> &, VarSet<R> &);                  \
+    template int periodic_pass<R>(Ctx<R> &, VarSet<R> &);                \
+    template int freeslip_pass<R>(Ctx<R> &, VarSet<R> &);                \
+    template int phase_interaction<R>(Ctx<R> &);                         \
+    template int phase_time_update<R>(Ctx<R> &);                         \
+    template int ctx_diagnostics<R>(Ctx<R> &, float *, float *, float *);
+INST(float)
+INST(double)
+#undef INST
+
+}  // namespace sph

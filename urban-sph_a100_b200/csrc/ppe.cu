@@ -1,0 +1,717 @@
+// Pressure phase of the ISPH step (ISPH_Calc.cuh:137-154).
+//
+// The reference runs one in-place point-Jacobi sweep of KERNEL_PPE3D
+// (functions_PPE.cuh:2-175) per step:
+//     p_i = p0_i + (b_i + sum_j c_ij (p_j - p0_j)) / A_i,   A_i = sum_j c_ij
+//     b_i = sum_j m_j/rho_j (u_j - u_i).G_i gradW_ij 2 rho_i rho_j/(rho_i+rho_j) / dt
+//     c_ij = 2 m_j/rho_j (r_ij . G_i gradW_ij) / |r_ij|^2
+// followed by the Neumann wall pressure and the outlet copy.  SPH_PPE_REF_SWEEP
+// reproduces that sweep with Jacobi (race-free) semantics.  The converged
+// modes solve the linear system whose fixed point that sweep iterates
+// towards: fluid rows A_i p_i - sum c_ij p_j = b_i, Neumann rows
+// p_w - sum w p = 0, outlet rows p_o - p_partner = 0, optionally one pinned
+// fluid row p = 0 for domains without a Dirichlet row.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+
+#include "ctx.cuh"
+
+namespace sph {
+
+// ---- device scalars of the Krylov solver -----------------------------------
+enum {
+    SC_RHO = 0, SC_ALPHA, SC_OMEGA, SC_BETA, SC_RR, SC_BB, SC_RV, SC_TS, SC_TT, SC_FLAG, SC_TOL2,
+    SC_RHO_NEW, SC_COUNT
+};
+enum { FLAG_RUN = 0, FLAG_CONVERGED = 1, FLAG_BREAKDOWN = 2 };
+
+// block-sum of NV doubles; the last block to finish sums the per-block
+// partials in block order (deterministic) and calls finish(sums) on thread 0
+template <int NV, class F>
+__device__ __forceinline__ void reduce_finish(double (&v)[NV], double *partials, unsigned int *counter, F finish) {
+    __shared__ double sh[NV][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0;
+            for (int w = 0; w < nw; ++w) s += sh[q][w];
+            partials[(size_t)q * gridDim.x + blockIdx.x] = s;
+        }
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double tot[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = 0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += ((volatile double *)partials)[(size_t)q * gridDim.x + b];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[q][wid] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0;
+            for (int w = 0; w < nw; ++w) s += sh[q][w];
+            tot[q] = s;
+        }
+        finish(tot);
+        *counter = 0;
+    }
+}
+
+#define LIST_ARGS const long long *__restrict__ slice_off, const int *__restrict__ ncnt, const int *__restrict__ nbr
+
+static inline int red_grid(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
+
+struct PpeRows {
+    const int4 *ty;
+    const int *kind;      // 0 identity, 1 fluid, 2 Neumann, 3 outlet copy, 4 pinned
+    const int *aux;       // outlet partner per row (kind 3)
+};
+
+// ---------------------------------------------------------------------------
+// PPE row assembly: b_i, A_i and (optionally) the cached c_ij
+// ---------------------------------------------------------------------------
+template <class Real, class C>
+__global__ void __launch_bounds__(128) k_ppe_rows(DevParams P, const float4 *__restrict__ pf,
+                                                  const typename V4<Real>::type *__restrict__ pr,
+                                                  const typename V2<Real>::type *__restrict__ mr,
+                                                  const int4 *__restrict__ ty, const int *__restrict__ jc, LIST_ARGS,
+                                                  const Real *__restrict__ g6, const typename V4<Real>::type *__restrict__ u,
+                                                  Real tdt, Real *__restrict__ b, Real *__restrict__ diag,
+                                                  C *__restrict__ coef, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
+    const size_t N = (size_t)n;
+    const auto xi = pr[i];
+    const auto ui = u[i];
+    const Real rhoi = mr[i].y;
+    const Real gc11 = g6[i], gc22 = g6[N + i], gc33 = g6[2 * N + i], gc12 = g6[3 * N + i], gc23 = g6[4 * N + i], gc31 = g6[5 * N + i];
+    const Real hi = (Real)(P.pressure_length * (double)xi.w);
+    const Real tA = calc_tmpA<Real>(P, hi);
+    Real bx = 0, by = 0, bz = 0, Aij = 0;
+    const long long base = slice_off[i >> 5] + (i & 31);
+    const int cnt = ncnt[i];
+    for (int k = 0; k < cnt; ++k) {
+        const long long e = base + 32LL * k;
+        const int j = __ldg(&nbr[e]);
+        const int jcj = jc[j];
+        Real c = 0;
+        if ((jcj & JB_LT1000) && !(jcj & JB_IT4)) {
+            const auto xj = pr[j];
+            const auto mj = mr[j];
+            const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+            const Real dw = calc_dwij_pressure<Real>(P, tA, hi, tdist);
+            const Real tdx = dw * dx / tdist, tdy = dw * dy / tdist, tdz = dw * dz / tdist;
+            const Real cx = gc11 * tdx + gc12 * tdy + gc31 * tdz;
+            const Real cy = gc12 * tdx + gc22 * tdy + gc23 * tdz;
+            const Real cz = gc31 * tdx + gc23 * tdy + gc33 * tdz;
+            const auto uj = u[j];
+            const Real vj = mj.x / mj.y;
+            const Real wr = (Real)2 * rhoi * mj.y / (rhoi + mj.y);
+            bx += vj * (uj.x - ui.x) * cx * wr;
+            by += vj * (uj.y - ui.y) * cy * wr;
+            bz += vj * (uj.z - ui.z) * cz * wr;
+            c = (Real)2 * vj * (dx * cx + dy * cy + dz * cz) / tdist / tdist;
+            Aij += c;
+        }
+        if (coef) coef[e] = (C)c;
+    }
+    b[i] = (bx + by + bz) / tdt;
+    diag[i] = Aij;
+}
+
+// one Jacobi sweep of KERNEL_PPE3D with the cached row: p_new = p0 + (b + sum c (p_j - p0_j)) / A
+template <class Real, class C>
+__global__ void __launch_bounds__(128) k_ppe_sweep(const int4 *__restrict__ ty, LIST_ARGS, const C *__restrict__ coef,
+                                                   const Real *__restrict__ b, const Real *__restrict__ diag,
+                                                   const Real *__restrict__ p, const Real *__restrict__ p0,
+                                                   Real *__restrict__ pout, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) { pout[i] = p[i]; return; }
+    const long long base = slice_off[i >> 5] + (i & 31);
+    const int cnt = ncnt[i];
+    Real s = 0;
+    for (int k = 0; k < cnt; ++k) {
+        const long long e = base + 32LL * k;
+        const int j = __ldg(&nbr[e]);
+        s += (Real)coef[e] * (p[j] - p0[j]);
+    }
+    pout[i] = p0[i] + (b[i] + s) / diag[i];
+}
+
+// ---------------------------------------------------------------------------
+// operator y = M x with the cached coefficients (vectors of type V)
+// ---------------------------------------------------------------------------
+template <class V, class C, class D>
+__global__ void __launch_bounds__(128) k_spmv(const int *__restrict__ kind, const int *__restrict__ aux, LIST_ARGS,
+                                              const C *__restrict__ coef, const D *__restrict__ diag,
+                                              const int *__restrict__ comp_id, const double *__restrict__ cmean,
+                                              const V *__restrict__ x, V *__restrict__ y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int kd = kind[i];
+    const V xi = x[i];
+    V yi = xi;   // identity / pinned; Neumann rows are applied by k_spmv_neumann
+    if (kd == 1) {
+        const long long base = slice_off[i >> 5] + (i & 31);
+        const int cnt = ncnt[i];
+        V s = 0;
+        for (int k = 0; k < cnt; ++k) {
+            const long long e = base + 32LL * k;
+            s += (V)coef[e] * x[__ldg(&nbr[e])];
+        }
+        yi = (V)diag[i] * xi - s;
+        if (comp_id) {
+            const int cc = comp_id[i];
+            if (cc >= 0) yi += (V)cmean[cc];
+        }
+    } else if (kd == 3) {
+        const int j = aux[i];
+        if (j >= 0) yi = xi - x[j];
+    }
+    y[i] = yi;
+}
+
+// per-component mean of x over the fluid rows of the singular components:
+// cmean[c] = (1/|u_c|) sum_{i in u_c} x_i, deterministic (block partials)
+template <class V>
+__global__ void k_comp_mean(const int *comp_id, const V *x, int n, int ncomp, const double *inv, double *partials,
+                            unsigned int *counter, double *cmean) {
+    double v[SPH_MAX_COMP];
+#pragma unroll
+    for (int q = 0; q < SPH_MAX_COMP; ++q) v[q] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int cc = comp_id[i];
+#pragma unroll
+        for (int q = 0; q < SPH_MAX_COMP; ++q)
+            if (cc == q) v[q] += (double)x[i];
+    }
+    reduce_finish<SPH_MAX_COMP>(v, partials, counter, [&](double *t) {
+        for (int q = 0; q < ncomp; ++q) cmean[q] = t[q] * inv[q];
+    });
+}
+
+// matrix-free variant: c_ij recomputed from the positions at every application
+template <class Real, class V>
+__global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restrict__ kind, const int *__restrict__ aux,
+                                                 const typename V4<Real>::type *__restrict__ pr,
+                                                 const typename V2<Real>::type *__restrict__ mr,
+                                                 const int *__restrict__ jc, LIST_ARGS, const Real *__restrict__ g6,
+                                                 const Real *__restrict__ diag, const int *__restrict__ comp_id,
+                                                 const double *__restrict__ cmean, const V *__restrict__ x,
+                                                 V *__restrict__ y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int kd = kind[i];
+    const V xi = x[i];
+    V yi = xi;
+    if (kd == 1) {
+        const size_t N = (size_t)n;
+        const auto xp = pr[i];
+        const Real gc11 = g6[i], gc22 = g6[N + i], gc33 = g6[2 * N + i], gc12 = g6[3 * N + i], gc23 = g6[4 * N + i], gc31 = g6[5 * N + i];
+        const Real hi = (Real)(P.pressure_length * (double)xp.w);
+        const Real tA = calc_tmpA<Real>(P, hi);
+        const long long base = slice_off[i >> 5] + (i & 31);
+        const int cnt = ncnt[i];
+        V s = 0;
+        for (int k = 0; k < cnt; ++k) {
+            const int j = __ldg(&nbr[base + 32LL * k]);
+            const int jcj = jc[j];
+            if (!(jcj & JB_LT1000) || (jcj & JB_IT4)) continue;
+            const auto xj = pr[j];
+            const auto mj = mr[j];
+            const Real dx = xp.x - xj.x, dy = xp.y - xj.y, dz = xp.z - xj.z;
+            const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+            const Real dw = calc_dwij_pressure<Real>(P, tA, hi, tdist);
+            const Real tdx = dw * dx / tdist, tdy = dw * dy / tdist, tdz = dw * dz / tdist;
+            const Real cx = gc11 * tdx + gc12 * tdy + gc31 * tdz;
+            const Real cy = gc12 * tdx + gc22 * tdy + gc23 * tdz;
+            const Real cz = gc31 * tdx + gc23 * tdy + gc33 * tdz;
+            const Real c = (Real)2 * (mj.x / mj.y) * (dx * cx + dy * cy + dz * cz) / tdist / tdist;
+            s += (V)c * x[j];
+        }
+        yi = (V)diag[i] * xi - s;
+        if (comp_id) {
+            const int cc = comp_id[i];
+            if (cc >= 0) yi += (V)cmean[cc];
+        }
+    } else if (kd == 3) {
+        const int j = aux[i];
+        if (j >= 0) yi = xi - x[j];
+    }
+    y[i] = yi;
+}
+
+// Neumann rows: y_w = x_w - sum_k w_k x_k (mirror rows use the extrapolation weights)
+template <class V>
+__global__ void k_spmv_neumann(const int *rows, const int *off, const int *nb, const int *mirror, const double *w,
+                               const double *gw, int nrows, const V *x, V *y) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    V s = 0;
+    const bool mir = mirror[k] != 0;
+    for (int q = off[k]; q < off[k + 1]; ++q) s += (V)(mir ? gw[q] : w[q]) * x[nb[q]];
+    y[i] = x[i] - s;
+}
+
+// ---------------------------------------------------------------------------
+// BiCGSTAB vector kernels (device-resident scalars, enum SC_*)
+// ---------------------------------------------------------------------------
+template <class V>
+__global__ void k_norm2(const V *a, int n, double *partials, unsigned int *counter, double *scal, int slot) {
+    double v[1] = {0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += (double)a[i] * (double)a[i];
+    reduce_finish<1>(v, partials, counter, [&](double *t) { scal[slot] = t[0]; });
+}
+
+// after v = M ph: alpha = rho / (rh, v)
+template <class V>
+__global__ void k_alpha(const V *rh, const V *v, int n, double *partials, unsigned int *counter, double *scal) {
+    if (scal[SC_FLAG] != FLAG_RUN) return;
+    double d[1] = {0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[0] += (double)rh[i] * (double)v[i];
+    reduce_finish<1>(d, partials, counter, [&](double *t) {
+        scal[SC_RV] = t[0];
+        if (t[0] == 0.0 || !isfinite(t[0])) { scal[SC_FLAG] = FLAG_BREAKDOWN; return; }
+        scal[SC_ALPHA] = scal[SC_RHO] / t[0];
+    });
+}
+
+// s = r - alpha v ; sh = dinv s
+template <class V>
+__global__ void k_s_update(const V *r, const V *v, V *s, V *sh, const V *dinv, int n, const double *scal) {
+    if (scal[SC_FLAG] != FLAG_RUN) return;
+    const V alpha = (V)scal[SC_ALPHA];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V si = r[i] - alpha * v[i];
+        s[i] = si;
+        sh[i] = dinv[i] * si;
+    }
+}
+
+// after t = M sh: omega = (t, s) / (t, t)
+template <class V>
+__global__ void k_omega(const V *t, const V *s, int n, double *partials, unsigned int *counter, double *scal) {
+    if (scal[SC_FLAG] != FLAG_RUN) return;
+    double d[2] = {0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d[0] += (double)t[i] * (double)s[i];
+        d[1] += (double)t[i] * (double)t[i];
+    }
+    reduce_finish<2>(d, partials, counter, [&](double *tt) {
+        scal[SC_TS] = tt[0];
+        scal[SC_TT] = tt[1];
+        scal[SC_OMEGA] = tt[1] > 0 ? tt[0] / tt[1] : 0.0;
+    });
+}
+
+// x += alpha ph + omega sh ; r = s - omega t ; rho' = (rh, r), rr = (r, r)
+template <class V>
+__global__ void k_xr_update(V *x, V *r, const V *ph, const V *sh, const V *s, const V *t, const V *rh, int n,
+                            double *partials, unsigned int *counter, double *scal) {
+    if (scal[SC_FLAG] != FLAG_RUN) return;
+    const V alpha = (V)scal[SC_ALPHA], omega = (V)scal[SC_OMEGA];
+    double d[2] = {0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] += alpha * ph[i] + omega * sh[i];
+        const V ri = s[i] - omega * t[i];
+        r[i] = ri;
+        d[0] += (double)rh[i] * (double)ri;
+        d[1] += (double)ri * (double)ri;
+    }
+    reduce_finish<2>(d, partials, counter, [&](double *tt) {
+        const double rho_new = tt[0];
+        scal[SC_RR] = tt[1];
+        if (tt[1] <= scal[SC_TOL2]) scal[SC_FLAG] = FLAG_CONVERGED;
+        else if (rho_new == 0.0 || scal[SC_OMEGA] == 0.0 || !isfinite(tt[1])) scal[SC_FLAG] = FLAG_BREAKDOWN;
+        scal[SC_BETA] = (rho_new / scal[SC_RHO]) * (scal[SC_ALPHA] / scal[SC_OMEGA]);
+        scal[SC_RHO] = rho_new;
+    });
+}
+
+// p = r + beta (p - omega v) ; ph = dinv p
+template <class V>
+__global__ void k_p_update(V *p, V *ph, const V *r, const V *v, const V *dinv, int n, const double *scal) {
+    if (scal[SC_FLAG] != FLAG_RUN) return;
+    const V beta = (V)scal[SC_BETA], omega = (V)scal[SC_OMEGA];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V pi = r[i] + beta * (p[i] - omega * v[i]);
+        p[i] = pi;
+        ph[i] = dinv[i] * pi;
+    }
+}
+
+// r = b - y ; rh = r ; p = v = 0 (start / restart)
+template <class V>
+__global__ void k_residual_init(const V *b, const V *y, V *r, V *rh, V *p, V *v, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V ri = b[i] - y[i];
+        r[i] = ri; rh[i] = ri; p[i] = 0; v[i] = 0;
+    }
+}
+
+// refinement residual: rd = bd - yd (FP64); rf = (float) rd; ef = 0
+__global__ void k_ir_residual(const double *bd, const double *yd, double *rd, float *rf, float *ef, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double r = bd[i] - yd[i];
+        rd[i] = r;
+        rf[i] = (float)r;
+        ef[i] = 0.f;
+    }
+}
+
+template <class V, class D>
+__global__ void k_dinv(const int *kind, const D *diag, V *dinv, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = 1.0;
+    if (kind[i] == 1) {
+        a = (double)diag[i];
+        if (a == 0.0 || !isfinite(a)) a = 1.0;
+    }
+    dinv[i] = (V)(1.0 / a);
+}
+
+// right-hand side and initial guess (previous pressure) of the converged system
+template <class Real>
+__global__ void k_rhs(const int *kind, const Real *b, const Real *p_old, double *rhs, double *x0, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int kd = kind[i];
+    double v = 0, x = (double)p_old[i];
+    if (kd == 1) v = (double)b[i];
+    else if (kd == 0) v = (double)p_old[i];
+    else if (kd == 4) x = 0;
+    rhs[i] = v;
+    x0[i] = x;
+}
+
+template <class A, class B>
+__global__ void k_cast(const A *a, B *b, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (B)a[i];
+}
+template <class A, class B>
+__global__ void k_axpy_cast(const A *e, B *x, int n) {   // x += e
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += (B)e[i];
+}
+__global__ void k_set_scal(double *scal, double rho, double tol2) {
+    scal[SC_RHO] = rho; scal[SC_ALPHA] = 1; scal[SC_OMEGA] = 1; scal[SC_BETA] = 0;
+    scal[SC_FLAG] = FLAG_RUN; scal[SC_TOL2] = tol2;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// y = M x, vectors of type V (V = Real for the Krylov iterations, V = double
+// for the FP64 refinement residual of the mixed form)
+// drains the pending operator timings into the running totals
+template <class Real>
+static void prof_drain(Ctx<Real> &c) {
+    if (c.prof_pending == 0) return;
+    cudaEventSynchronize(c.prof_ev[2 * c.prof_pending - 1]);
+    for (int k = 0; k < c.prof_pending; ++k) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.prof_ev[2 * k], c.prof_ev[2 * k + 1]);
+        c.prof_ms += ms;
+        ++c.prof_launches;
+    }
+    c.prof_pending = 0;
+}
+
+template <class Real, class V>
+static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
+    const int n = c.n;
+    const bool timed = c.prof && sizeof(V) == sizeof(Real);
+    if (timed) {
+        if (c.prof_pending == 256) prof_drain(c);
+        if (!c.prof_ev) {
+            c.prof_ev = new cudaEvent_t[512];
+            for (int k = 0; k < 512; ++k) cudaEventCreate(&c.prof_ev[k]);
+        }
+        cudaEventRecord(c.prof_ev[2 * c.prof_pending], c.stream);
+    }
+    const int *cid = nullptr;
+    double *cmean = c.scal + 40;
+    if (c.n_comp > 0) {
+        cid = c.comp_id;
+        k_comp_mean<V><<<red_grid(n), 256, 0, c.stream>>>(c.comp_id, x, n, c.n_comp, c.comp_inv, c.red,
+                                                          (unsigned int *)(c.scal + 32), cmean);
+        ++c.launches;
+    }
+    if (cached) {
+        if (sizeof(Real) == 4)
+            k_spmv<V, float, Real><<<grid_for(n, 128), 128, 0, c.stream>>>(c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr,
+                                                                          c.coef, c.diag, cid, cmean, x, y, n);
+        else
+            k_spmv<V, double, Real><<<grid_for(n, 128), 128, 0, c.stream>>>(c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr,
+                                                                           c.coef_d, c.diag, cid, cmean, x, y, n);
+    } else {
+        k_spmv_mf<Real, V><<<grid_for(n, 128), 128, 0, c.stream>>>(c.dp, c.row_kind, c.row_aux, c.pr, c.mr, c.jc, c.slice_off,
+                                                                  c.ncnt, c.nbr, c.g6, c.diag, cid, cmean, x, y, n);
+    }
+    ++c.launches;
+    if (timed) {
+        cudaEventRecord(c.prof_ev[2 * c.prof_pending + 1], c.stream);
+        ++c.prof_pending;
+    }
+    if (c.L.n_nm > 0) {
+        k_spmv_neumann<V><<<grid_for(c.L.n_nm, 128), 128, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.L.nm_ghost,
+                                                                       c.nm_w, c.nm_gw, c.L.n_nm, x, y);
+        ++c.launches;
+    }
+}
+
+template <class Real>
+int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *bytes, int reset) {
+    prof_drain(c);
+    if (launches) *launches = c.prof_launches;
+    if (total_ms) *total_ms = c.prof_ms;
+    if (bytes) {
+        // per row: kind (4) + x_i + y_i + A_i (Real); per stored entry: index (4) + coefficient (Real)
+        *bytes = (double)c.n * (4.0 + 3.0 * sizeof(Real)) + (double)c.nnz * (4.0 + sizeof(Real));
+    }
+    if (reset) { c.prof_launches = 0; c.prof_ms = 0; }
+    return SPH_OK;
+}
+
+// Jacobi-preconditioned BiCGSTAB on M x = b in Real vectors with FP64 dots;
+// x holds the initial guess.  Returns SPH_OK, SPH_NOT_CONVERGED or
+// SPH_ERR_BREAKDOWN (more than 20 restarts).
+template <class Real>
+static int bicgstab(Ctx<Real> &c, Real *x, const Real *b, double bnorm2, double tol, int maxit, bool cached,
+                    int *iters, double *relres, int *restarts) {
+    const int n = c.n;
+    cudaStream_t st = c.stream;
+    Real *r = c.kv[0], *rh = c.kv[1], *p = c.kv[2], *v = c.kv[3], *s = c.kv[4];
+    Real *t = c.kv[5], *ph = c.kv[6], *sh = c.kv[7], *dinv = c.kv[8];
+    const int G = red_grid(n);
+    unsigned int *counter = (unsigned int *)(c.scal + 32);
+    const double tol2 = tol * tol * bnorm2;
+    k_dinv<Real, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
+    ++c.launches;
+    int it = 0;
+    *restarts = 0;
+    int status = SPH_NOT_CONVERGED;
+    while (true) {
+        apply_op<Real, Real>(c, x, t, cached);
+        k_residual_init<Real><<<G, 256, 0, st>>>(b, t, r, rh, p, v, n);
+        k_norm2<Real><<<G, 256, 0, st>>>(r, n, c.red, counter, c.scal, SC_RR);
+        c.launches += 2;
+        SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
+        SPH_CUDA_TRY(cudaStreamSynchronize(st));
+        const double rr0 = c.red_host[SC_RR];
+        *relres = std::sqrt(rr0 / bnorm2);
+        if (rr0 <= tol2) { status = SPH_OK; break; }
+        if (it >= maxit) break;
+        if (getenv("SPH_TRACE_PPE")) fprintf(stderr, "  bicgstab start it %d relres %.3e\n", it, *relres);
+        k_set_scal<<<1, 1, 0, st>>>(c.scal, rr0, tol2);   // beta = 0: p = r on the first pass
+        ++c.launches;
+        bool restart = false;
+        const int check = 4;
+        while (it < maxit) {
+            k_p_update<Real><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
+            apply_op<Real, Real>(c, ph, v, cached);
+            k_alpha<Real><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
+            k_s_update<Real><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
+            apply_op<Real, Real>(c, sh, t, cached);
+            k_omega<Real><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
+            k_xr_update<Real><<<G, 256, 0, st>>>(x, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
+            c.launches += 5;
+            ++it;
+            if (it % check == 0 || it >= maxit) {
+                SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
+                SPH_CUDA_TRY(cudaStreamSynchronize(st));
+                const double flag = c.red_host[SC_FLAG];
+                *relres = std::sqrt(c.red_host[SC_RR] / bnorm2);
+                if (getenv("SPH_TRACE_PPE") && it % 20 == 0)
+                    fprintf(stderr, "    it %d rr-rel %.3e alpha %.3e omega %.3e rho %.3e flag %g\n", it, *relres,
+                            c.red_host[SC_ALPHA], c.red_host[SC_OMEGA], c.red_host[SC_RHO], flag);
+                if (flag == FLAG_CONVERGED) { status = SPH_OK; break; }
+                if (flag == FLAG_BREAKDOWN) { restart = true; break; }
+            }
+        }
+        if (status == SPH_OK) break;
+        if (restart) {
+            if (++*restarts > 20) { status = SPH_ERR_BREAKDOWN; break; }
+            continue;
+        }
+        break;   // iteration limit
+    }
+    SPH_CUDA_TRY(cudaGetLastError());
+    *iters = it;
+    return status;
+}
+
+template <class Real>
+static int ensure_ppe_ws(Ctx<Real> &c) {
+    const int n = c.n;
+    if (!c.kv[0]) for (int k = 0; k < 10; ++k) SPH_TRY(c.alloc(c.kv[k], (size_t)n));
+    if (!c.xd) { SPH_TRY(c.alloc(c.xd, n)); SPH_TRY(c.alloc(c.rd, n)); SPH_TRY(c.alloc(c.bd, n)); }
+    if (!c.xf) { SPH_TRY(c.alloc(c.xf, n)); SPH_TRY(c.alloc(c.bf, n)); }
+    if (!c.red) {
+        SPH_TRY(c.alloc(c.red, (size_t)SPH_MAX_COMP * 2048));
+        SPH_TRY(c.alloc(c.scal, 64));
+        SPH_CUDA_TRY(cudaMemsetAsync(c.scal, 0, 64 * sizeof(double), c.stream));
+        SPH_CUDA_TRY(cudaMallocHost(&c.red_host, 64 * sizeof(double)));
+    }
+    if (!c.coef_valid) {
+        const size_t m = (size_t)std::max(c.nnz_padded, 1LL);
+        if (sizeof(Real) == 4) { c.release(c.coef); SPH_TRY(c.alloc(c.coef, m)); }
+        else { c.release(c.coef_d); SPH_TRY(c.alloc(c.coef_d, m)); }
+    }
+    return SPH_OK;
+}
+
+template <class Real>
+int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
+    cudaStream_t st = c.stream;
+    const int n = c.n;
+    const Real tdt = (Real)c.dp.dt;
+    const int mode = c.prm.ppe_mode;
+    const bool cached = c.prm.reserved[0] == 0;   // reserved[0] = 1 selects the matrix-free operator
+    sph_ppe_stats S{};
+    SPH_TRY(ensure_ppe_ws(c));
+    Real *b = c.kv[9];
+    SPH_CUDA_TRY(cudaEventRecord(c.ev[4], st));
+    // b_i, A_i every step; c_ij once per neighbour-list build (time-invariant
+    // while the particles do not move)
+    if (sizeof(Real) == 4)
+        k_ppe_rows<Real, float><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.pr, c.mr, c.ty, c.jc, c.slice_off, c.ncnt,
+                                                                 c.nbr, c.g6, c.S.u, tdt, b, c.diag,
+                                                                 c.coef_valid ? nullptr : c.coef, n);
+    else
+        k_ppe_rows<Real, double><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.pr, c.mr, c.ty, c.jc, c.slice_off, c.ncnt,
+                                                                  c.nbr, c.g6, c.S.u, tdt, b, c.diag,
+                                                                  c.coef_valid ? nullptr : c.coef_d, n);
+    ++c.launches;
+    SPH_CUDA_TRY(cudaGetLastError());
+    c.coef_valid = true;
+
+    if (mode == SPH_PPE_REF_SWEEP) {
+        Real *pout = c.kv[8];
+        if (sizeof(Real) == 4)
+            k_ppe_sweep<Real, float><<<grid_for(n, 128), 128, 0, st>>>(c.ty, c.slice_off, c.ncnt, c.nbr, c.coef, b, c.diag,
+                                                                      c.S.p, c.pres0, pout, n);
+        else
+            k_ppe_sweep<Real, double><<<grid_for(n, 128), 128, 0, st>>>(c.ty, c.slice_off, c.ncnt, c.nbr, c.coef_d, b, c.diag,
+                                                                       c.S.p, c.pres0, pout, n);
+        ++c.launches;
+        SPH_CUDA_TRY(cudaMemcpyAsync(c.S.p, pout, sizeof(Real) * n, cudaMemcpyDeviceToDevice, st));
+        S.status = SPH_OK;
+        S.iterations = 1;
+    } else {
+        double *xd = c.xd, *rd = c.rd, *bd = c.bd;
+        k_rhs<Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, b, c.S.p, bd, xd, n);
+        const int G = red_grid(n);
+        unsigned int *counter = (unsigned int *)(c.scal + 32);
+        k_norm2<double><<<G, 256, 0, st>>>(bd, n, c.red, counter, c.scal, SC_BB);
+        c.launches += 2;
+        SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
+        SPH_CUDA_TRY(cudaStreamSynchronize(st));
+        double bb = c.red_host[SC_BB];
+        if (!(bb > 0)) bb = 1.0;
+        const double tol = c.prm.ppe_tol > 0 ? c.prm.ppe_tol : 1e-6;
+        const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
+        int status = SPH_OK, iters = 0, restarts = 0, refinements = 0;
+        double relres = 0;
+        const bool mixed_ir = (sizeof(Real) == 4) && (mode == SPH_PPE_MIXED_IR || mode == SPH_PPE_LEARNED);
+        if (sizeof(Real) == 8) {
+            // plain form: BiCGSTAB entirely in FP64
+            status = bicgstab<Real>(c, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres, &restarts);
+        } else if (!mixed_ir) {
+            // FP32 BiCGSTAB with FP64 reductions
+            k_cast<double, float><<<grid_for(n, 256), 256, 0, st>>>(xd, c.xf, n);
+            k_cast<double, float><<<grid_for(n, 256), 256, 0, st>>>(bd, c.bf, n);
+            c.launches += 2;
+            status = bicgstab<Real>(c, (Real *)c.xf, (const Real *)c.bf, bb, tol, maxit, cached, &iters, &relres, &restarts);
+            if (getenv("SPH_TRACE_PPE"))
+                fprintf(stderr, "FP32 BiCGSTAB st %d it %d rel %.3e restarts %d\n", status, iters, relres, restarts);
+            k_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(c.xf, xd, n);
+            ++c.launches;
+        } else {
+            // FP32 BiCGSTAB inside FP64 iterative refinement: the outer residual
+            // r = b - M x and the correction x += e are FP64
+            float *ef = c.xf, *rf = c.bf;
+            const double inner_tol = c.prm.ppe_inner_tol > 0 ? c.prm.ppe_inner_tol : 1e-3;
+            status = SPH_NOT_CONVERGED;
+            for (refinements = 0; refinements < 50; ++refinements) {
+                apply_op<Real, double>(c, xd, rd, cached);
+                k_ir_residual<<<G, 256, 0, st>>>(bd, rd, rd, rf, ef, n);
+                k_norm2<double><<<G, 256, 0, st>>>(rd, n, c.red, counter, c.scal, SC_RR);
+                c.launches += 2;
+                SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
+                SPH_CUDA_TRY(cudaStreamSynchronize(st));
+                const double rr = c.red_host[SC_RR];
+                relres = std::sqrt(rr / bb);
+                if (relres <= tol) { status = SPH_OK; break; }
+                if (iters >= maxit) break;
+                int it_in = 0, rs = 0;
+                double rel_in = 0;
+                const int st_in = bicgstab<Real>(c, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters, cached,
+                                                 &it_in, &rel_in, &rs);
+                if (getenv("SPH_TRACE_PPE"))
+                    fprintf(stderr, "IR %d outer relres %.3e inner st %d it %d rel %.3e restarts %d\n", refinements, relres,
+                            st_in, it_in, rel_in, rs);
+                iters += it_in;
+                restarts += rs;
+                if (st_in == SPH_ERR_BREAKDOWN && it_in == 0) { status = SPH_ERR_BREAKDOWN; break; }
+                k_axpy_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(ef, xd, n);
+                ++c.launches;
+            }
+        }
+        k_cast<double, Real><<<grid_for(n, 256), 256, 0, st>>>(xd, c.S.p, n);
+        ++c.launches;
+        S.status = status;
+        S.iterations = iters;
+        S.refinements = refinements;
+        S.restarts = restarts;
+        S.rel_residual = relres;
+    }
+    SPH_CUDA_TRY(cudaEventRecord(c.ev[5], st));
+    SPH_TRY(neumann_pass(c, c.S));
+    SPH_TRY(outlet_pass(c, c.S));
+    SPH_CUDA_TRY(cudaGetLastError());
+    SPH_CUDA_TRY(cudaEventSynchronize(c.ev[5]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c.ev[4], c.ev[5]);
+    S.solve_ms = ms;
+    c.last_ppe = S;
+    if (stats) *stats = S;
+    return S.status < 0 ? S.status : SPH_OK;
+}
+
+#define INST(R) template int phase_ppe<R>(Ctx<R> &, sph_ppe_stats *); \
+    template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int);
+INST(float)
+INST(double)
+#undef INST
+
+}  // namespace sph

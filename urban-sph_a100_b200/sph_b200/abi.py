@@ -1,0 +1,206 @@
+"""ctypes binding of lib/libsph_b200.so (include/sph_isph.h).
+
+``Simulation`` is the host-side mirror of the reference's step driver
+(SOPHIA_single_ISPH, ISPH_Calc.cuh:4-233): it owns one device context and
+exposes the reference phases (NNPS, interaction, PPE, time update) over the
+reference's part1/part2/part3 records.  There is no CPU fallback: loading the
+library or creating a context on a machine without the CUDA build or a GPU
+raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .layout import PART1, PART2, PART3, PpeStats, SphParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libsph_b200.so")
+
+# every entry point declared in include/sph_isph.h
+SYMBOLS = (
+    "sph_params_init", "sph_domain_setup", "sph_create", "sph_destroy", "sph_set_params",
+    "sph_upload", "sph_upload_state", "sph_download", "sph_nnps", "sph_nnps_export",
+    "sph_neighbors_export", "sph_interaction", "sph_ppe", "sph_time_update", "sph_step",
+    "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_status_string",
+    "sph_last_error", "sph_profile", "sph_operator_stats",
+)
+
+_lib = None
+
+
+class SphError(RuntimeError):
+    def __init__(self, where, status):
+        L = lib()
+        msg = L.sph_status_string(status).decode()
+        detail = L.sph_last_error().decode()
+        super().__init__(f"{where}: {msg} ({status}) {detail}")
+        self.status = status
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} missing: build it with urban-sph_a100_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+        L.sph_params_init.argtypes = [vp]
+        L.sph_domain_setup.argtypes = [vp, vp, i32]
+        L.sph_create.argtypes = [vp, i32, i32, vp, ctypes.POINTER(vp)]
+        L.sph_destroy.argtypes = [vp]
+        L.sph_destroy.restype = None
+        L.sph_set_params.argtypes = [vp, vp]
+        L.sph_upload.argtypes = [vp, vp, vp, i32]
+        L.sph_upload_state.argtypes = [vp, vp, i32]
+        L.sph_download.argtypes = [vp, vp, vp, vp]
+        L.sph_nnps.argtypes = [vp]
+        L.sph_nnps_export.argtypes = [vp, vp, vp, vp, vp]
+        L.sph_neighbors_export.argtypes = [vp, vp, vp, ctypes.POINTER(i64)]
+        L.sph_interaction.argtypes = [vp]
+        L.sph_ppe.argtypes = [vp, vp]
+        L.sph_time_update.argtypes = [vp]
+        L.sph_step.argtypes = [vp, i32, vp]
+        L.sph_diagnostics.argtypes = [vp, vp, vp, vp]
+        L.sph_last_phase_ms.argtypes = [vp, vp]
+        L.sph_launch_count.argtypes = [vp]
+        L.sph_launch_count.restype = i64
+        L.sph_status_string.argtypes = [i32]
+        L.sph_status_string.restype = ctypes.c_char_p
+        L.sph_last_error.restype = ctypes.c_char_p
+        L.sph_profile.argtypes = [vp, i32]
+        L.sph_operator_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double), i32]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(where, st, ok=(0,)):
+    if st not in ok and st < 0:
+        raise SphError(where, st)
+    return st
+
+
+def params_init():
+    p = SphParams()
+    _check("sph_params_init", lib().sph_params_init(ctypes.byref(p)))
+    return p
+
+
+def domain_setup(p, P1):
+    P1 = np.ascontiguousarray(P1, dtype=PART1)
+    _check("sph_domain_setup", lib().sph_domain_setup(ctypes.byref(p), _p(P1), len(P1)))
+    return p
+
+
+class Simulation:
+    """One device context: the reference's dev_P1/SP1/P2/SP2/P3 and NNPS arrays."""
+
+    def __init__(self, params, precision=0, device=0, stream=None):
+        self.params = params.copy()
+        self.n = self.params.geti("num_part2")
+        self.num_cells = self.params.geti("num_cells")
+        h = ctypes.c_void_p()
+        _check("sph_create", lib().sph_create(ctypes.byref(self.params), int(precision), int(device),
+                                              stream, ctypes.byref(h)))
+        self.h = h
+        self.precision = precision
+        self.last_stats = PpeStats()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        self.params = params.copy()
+        _check("sph_set_params", lib().sph_set_params(self.h, ctypes.byref(self.params)))
+
+    def upload(self, P1, P2=None):
+        P1 = np.ascontiguousarray(P1, dtype=PART1)
+        P2 = None if P2 is None else np.ascontiguousarray(P2, dtype=PART2)
+        _check("sph_upload", lib().sph_upload(self.h, _p(P1), _p(P2), len(P1)))
+
+    def upload_state(self, P1):
+        P1 = np.ascontiguousarray(P1, dtype=PART1)
+        _check("sph_upload_state", lib().sph_upload_state(self.h, _p(P1), len(P1)))
+
+    def download(self, want=(1, 2, 3)):
+        P1 = np.zeros(self.n, PART1) if 1 in want else None
+        P2 = np.zeros(self.n, PART2) if 2 in want else None
+        P3 = np.zeros(self.n, PART3) if 3 in want else None
+        _check("sph_download", lib().sph_download(self.h, _p(P1), _p(P2), _p(P3)))
+        return P1, P2, P3
+
+    def download_into(self, P1):
+        _check("sph_download", lib().sph_download(self.h, _p(P1), None, None))
+
+    def nnps(self):
+        _check("sph_nnps", lib().sph_nnps(self.h))
+
+    def export_nnps(self):
+        g_idx = np.zeros(self.n, np.int32); p_idx = np.zeros(self.n, np.int32)
+        g_str = np.zeros(self.num_cells + 1, np.int32); g_end = np.zeros(self.num_cells + 1, np.int32)
+        _check("sph_nnps_export", lib().sph_nnps_export(self.h, _p(g_idx), _p(p_idx), _p(g_str), _p(g_end)))
+        return g_idx, p_idx, g_str, g_end
+
+    def neighbors(self):
+        nnz = ctypes.c_int64(0)
+        off = np.zeros(self.n + 1, np.int64)
+        _check("sph_neighbors_export", lib().sph_neighbors_export(self.h, _p(off), None, ctypes.byref(nnz)))
+        lst = np.zeros(max(nnz.value, 1), np.int32)
+        _check("sph_neighbors_export", lib().sph_neighbors_export(self.h, _p(off), _p(lst), ctypes.byref(nnz)))
+        return off, lst[:nnz.value]
+
+    def interaction(self):
+        _check("sph_interaction", lib().sph_interaction(self.h))
+
+    def ppe(self):
+        st = PpeStats()
+        _check("sph_ppe", lib().sph_ppe(self.h, ctypes.byref(st)))
+        self.last_stats = st
+        return st
+
+    def time_update(self):
+        _check("sph_time_update", lib().sph_time_update(self.h))
+
+    def step(self, nsteps=1):
+        st = PpeStats()
+        _check("sph_step", lib().sph_step(self.h, int(nsteps), ctypes.byref(st)))
+        self.last_stats = st
+        return st
+
+    def diagnostics(self):
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        _check("sph_diagnostics", lib().sph_diagnostics(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def phase_ms(self):
+        ms = np.zeros(4, np.float32)
+        _check("sph_last_phase_ms", lib().sph_last_phase_ms(self.h, _p(ms)))
+        return ms
+
+    def launches(self):
+        return int(lib().sph_launch_count(self.h))
+
+    def profile(self, enable=True):
+        _check("sph_profile", lib().sph_profile(self.h, 1 if enable else 0))
+
+    def operator_stats(self, reset=True):
+        n = ctypes.c_int64(0)
+        ms = ctypes.c_double(0)
+        by = ctypes.c_double(0)
+        _check("sph_operator_stats", lib().sph_operator_stats(self.h, ctypes.byref(n), ctypes.byref(ms),
+                                                              ctypes.byref(by), 1 if reset else 0))
+        return n.value, ms.value, by.value

@@ -200,6 +200,34 @@ def canyon(scale=1.0, dx=0.01, seed=SEED, ustar=0.3, z0=0.01, cs=0.12, dt=2e-4, 
     return P, p
 
 
+def most_column(dx=1.0, n=6, nz=5, seed=SEED, **pkw):
+    """Wall-layer deck at atmospheric heights (z = 1.5 .. 5.5 m above walls)
+    where the reference's MOST Newton branch (functions_MOST.cuh:217-247,
+    hard-wired z0 = 1 m) converges: stable and unstable wall-layer air."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    xs = (np.arange(n) + 0.5) * dx
+    fx, fy, fz = _grid(xs, xs, (np.arange(nz) + 1.5) * dx)
+    Pf = _records(fx, fy, fz); Pf["p_type"] = 1
+    wx, wy, wz = _grid(xs, xs, (0.5 - np.arange(3)) * dx)
+    Pw = _records(wx, wy, wz); Pw["p_type"] = 0
+    P = np.concatenate([Pf, Pw])
+    _common_fields(P, dx)
+    fl = P["p_type"] == 1
+    zz = P["z"].astype(np.float64)
+    u = np.where(fl, 0.3 / 0.4 * np.log(np.maximum(zz, 1.0) / 0.5), 0.0)
+    P["ux"] = (u * (1 + 0.05 * rng.uniform(-1, 1, len(P)))).astype(f)
+    P["uy"] = (0.1 * u * rng.uniform(-1, 1, len(P))).astype(f)
+    most = fl & (P["z"] < 2.0 * dx)
+    P["MOST_buffer"][most] = 1
+    P["temp"][most] = (300.0 + rng.uniform(-3.0, 3.0, most.sum())).astype(f)
+    P = P[rng.permutation(len(P))]
+    p = default_params(**pkw)
+    p.setf("dt", 1e-3)
+    domain_setup(p, P)
+    return P, p
+
+
 def describe(P):
     counts = {}
     for name, mask in (("fluid", P["p_type"] == 1), ("wall", P["p_type"] == 0),

@@ -112,6 +112,7 @@ class SphParams(ctypes.Structure):
         ("ppe_pin", ctypes.c_int32),
         ("recompute_gc", ctypes.c_int32),
         ("reserved", ctypes.c_int32 * 14),
+        ("ppe_inner_tol", ctypes.c_double),
     ]
 
     def seti(self, name, value):
@@ -141,4 +142,4 @@ class PpeStats(ctypes.Structure):
     ]
 
 
-assert ctypes.sizeof(SphParams) == 1256, ctypes.sizeof(SphParams)
+assert ctypes.sizeof(SphParams) == 1264, ctypes.sizeof(SphParams)

@@ -70,6 +70,7 @@ def default_params(dt=1e-4, kernel="Wendland6", turbulence="SSM", viscous=CLEARY
     p.ppe_tol = 1e-6
     p.ppe_pin = 1
     p.recompute_gc = 0
+    p.ppe_inner_tol = 1e-3
     return p
 
 
