@@ -158,7 +158,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "ref_sweep"])
+    ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "gmres", "ref_sweep"])
+    ap.add_argument("--fp64-mode", default="bicgstab", choices=["gmres", "bicgstab"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--matrix-free", action="store_true")
@@ -182,7 +183,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     P, p = decks.canyon(scale=args.scale)
-    mode = {"mixed_ir": layout.PPE_MIXED_IR, "bicgstab": layout.PPE_BICGSTAB,
+    mode = {"mixed_ir": layout.PPE_MIXED_IR, "bicgstab": layout.PPE_BICGSTAB, "gmres": layout.PPE_GMRES,
             "ref_sweep": layout.PPE_REF_SWEEP}[args.mode]
     p.ppe_mode = mode
     p.ppe_tol = 1e-6
@@ -252,7 +253,7 @@ def main():
     if not args.no_fp64 and rank == 0:
         sim.close()
         q = p.copy()
-        q.ppe_mode = layout.PPE_BICGSTAB
+        q.ppe_mode = layout.PPE_GMRES if args.fp64_mode == "gmres" else layout.PPE_BICGSTAB
         sd = abi.Simulation(q, precision=layout.PREC_FP64, device=local)
         sd.upload(P)
         for _ in range(2):
@@ -269,7 +270,7 @@ def main():
         g1.record()
         torch.cuda.synchronize()
         dms = g0.elapsed_time(g1)
-        fp64 = {"value": n * kd / (dms / 1e3), "ms_per_step": dms / kd, "steps": kd,
+        fp64 = {"value": n * kd / (dms / 1e3), "ms_per_step": dms / kd, "steps": kd, "solver": args.fp64_mode,
                 "ppe_ms": statistics.mean(d[2] for d in dstats),
                 "ppe_iterations": statistics.mean(d[0] for d in dstats),
                 "rel_residual_max": max(d[1] for d in dstats), "ppe_tol": 1e-6}

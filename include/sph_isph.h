@@ -52,8 +52,11 @@ extern "C" {
                                  (functions_PPE.cuh:2-175) without its race   */
 #define SPH_PPE_BICGSTAB   1  /* Jacobi-preconditioned BiCGSTAB in the context's
                                  precision, FP64 reductions                   */
-#define SPH_PPE_MIXED_IR   2  /* FP32 BiCGSTAB inside FP64 iterative refinement */
+#define SPH_PPE_MIXED_IR   2  /* FP32 BiCGSTAB corrections inside FP64 iterative
+                                 refinement; FP64 BiCGSTAB in an FP64 context */
 #define SPH_PPE_LEARNED    3  /* MIXED_IR warm-started by the per-particle net   */
+#define SPH_PPE_GMRES      4  /* restarted GMRES(m) in the context's precision,
+                                 FP64 reductions                              */
 
 /* ---- particle records: class_Cuda_Particle_Array.cuh:11-112, Real=float --- */
 typedef struct sph_part1 {
@@ -153,7 +156,9 @@ typedef struct sph_params {
                                 component (default), 2 one row pinned to p=0 */
     int32_t recompute_gc;    /* 1: recompute the correction matrix every step  */
     int32_t reserved[14];    /* reserved[0] = 1: matrix-free PPE operator (c_ij
-                                recomputed per application) instead of cached */
+                                recomputed per application) instead of cached;
+                                reserved[1]: GMRES restart length (0: 40, max 64);
+                                reserved[2] = 1: GMRES inner solver in MIXED_IR */
     double  ppe_inner_tol;   /* inner FP32 tolerance of SPH_PPE_MIXED_IR (0: 1e-3) */
 } sph_params;
 

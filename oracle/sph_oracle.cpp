@@ -912,8 +912,10 @@ struct Oracle {
                 if (partner >= 0) { ci.push_back(partner); va.push_back(-1.0); }
                 continue;
             }
+            // Neumann row with its Shepard weights; the inlet mirror
+            // extrapolation is applied after the solve by the Neumann pass
             std::vector<std::pair<int, double>> w;
-            neumann_weights(A, i, w);
+            neumann_weights(A, i, w, /*operator_row=*/true);
             ci.push_back(i); va.push_back(1.0);
             for (auto &c : w) { ci.push_back(c.first); va.push_back(-c.second); }
         }
@@ -926,10 +928,12 @@ struct Oracle {
             // anchor row (a row that is only its diagonal: identity rows,
             // Neumann rows without fluid in range, outlet rows without
             // partner) is singular (its rows sum to zero, M 1 = 0).
-            //  ppe_pin == 1: rank-one regularisation M' = M + u w^T per such
-            //    component, u = its fluid rows, w = u/|u|: the constant mode
-            //    gets a well-conditioned eigenvalue and the compatibility
-            //    defect of b becomes the uniform source lambda = w^T p;
+            //  ppe_pin == 1: rank-one regularisation M' = M + D u w^T per such
+            //    component, u = its fluid rows, w = u/|u|, D = the rows'
+            //    diagonals (A_i < 0): the constant mode gets the eigenvalue 1
+            //    of the Jacobi-scaled operator, beside the rest of its
+            //    spectrum, and the compatibility defect of b becomes the
+            //    source A_i lambda with lambda = w^T p;
             //  ppe_pin == 2: one row pinned to p = 0, the highest-index fluid
             //    row with buffer_type 0 (else the highest-index fluid row).
             std::vector<int> par(N);
@@ -990,7 +994,14 @@ struct Oracle {
     }
 
     // linear weights of a Neumann row: p_w = sum_k w_k p_k
-    void neumann_weights(const State<Real> &A, int i, std::vector<std::pair<int, double>> &w) const {
+    // linear weights of a Neumann row: p_w = sum_k w_k p_k.  operator_row
+    // selects the weights the converged operator uses: the Shepard weights
+    // also for inlet mirror rows, and for a row whose Shepard set (fluid with
+    // buffer_type 0, functions_BC.cuh:414) is empty -- p = 0 in the reference
+    // -- the Shepard average over all fluid in range, buffers included, so
+    // that such corner rows do not act as point Dirichlet anchors.
+    void neumann_weights(const State<Real> &A, int i, std::vector<std::pair<int, double>> &w,
+                         bool operator_row = false) const {
         const P Q = q();
         w.clear();
         float search_coeff = (float)prm.neumann_coeff;
@@ -1008,32 +1019,41 @@ struct Oracle {
             Real dist = std::sqrt((xg - A.x[j]) * (xg - A.x[j]) + (yg - A.y[j]) * (yg - A.y[j]) + (zg - A.z[j]) * (zg - A.z[j])) - 1e-20;
             if (dist < prm.ghost_tol) g = j;
         });
-        std::vector<std::pair<int, double>> ws, gs;
-        double tflt = 0, gsum = 0;
-        cell_loop(ic, jc, kc, A.ncell[i], [&](int j) {
-            if (A.p_type[j] >= 1000) return;
-            float tdf = std::sqrt(d2f(xgf, yf[i], zf[i], xf[j], yf[j], zf[j]));
-            if (!(tdf < srange)) return;
-            if (!(A.p_type[j] == 1 && A.buffer_type[j] == 0)) return;
-            Real xj = A.x[j], yj = A.y[j], zj = A.z[j];
-            Real tdist = std::sqrt((xg - xj) * (xg - xj) + (yg - yj) * (yg - yj) + (zg - zj) * (zg - zj)) - 1e-20;
-            double vw = (double)(A.m[j] / A.rho[j]);
-            double twij = calc_wij(Q, tmp_A, hi, tdist);
-            double tdwij = calc_dwij(Q, tmp_A, hi, tdist);
-            if (Q.kgc_solve() == 1) tdwij = 0;
-            double proj = ((xi - xg) * (xg - xj) + (yi - yg) * (yg - yj) + (zi - zg) * (zg - zj)) / (double)tdist * tdwij;
-            ws.push_back({j, vw * twij});
-            gs.push_back({j, vw * proj});
-            tflt += vw * twij;
-            gsum += vw * proj;
-        });
-        if (tflt < 1e-6) return;   // p_w = 0
-        if (!mirror) {
-            for (auto &c : ws) w.push_back({c.first, c.second / tflt});
-        } else {
-            // p_w = p_g + sum_j g_j (p_j - p_g)
-            for (auto &c : gs) w.push_back({c.first, c.second});
-            if (g >= 0) w.push_back({g, 1.0 - gsum});
+        for (int pass = 0; pass < 2; ++pass) {
+            // pass 0: the reference's set; pass 1 (operator rows only, when
+            // pass 0 is empty): all fluid in range
+            const bool all_fluid = pass == 1;
+            std::vector<std::pair<int, double>> ws, gs;
+            double tflt = 0, gsum = 0;
+            cell_loop(ic, jc, kc, A.ncell[i], [&](int j) {
+                if (A.p_type[j] >= 1000) return;
+                float tdf = std::sqrt(d2f(xgf, yf[i], zf[i], xf[j], yf[j], zf[j]));
+                if (!(tdf < srange)) return;
+                if (!(A.p_type[j] == 1 && (all_fluid || A.buffer_type[j] == 0))) return;
+                Real xj = A.x[j], yj = A.y[j], zj = A.z[j];
+                Real tdist = std::sqrt((xg - xj) * (xg - xj) + (yg - yj) * (yg - yj) + (zg - zj) * (zg - zj)) - 1e-20;
+                double vw = (double)(A.m[j] / A.rho[j]);
+                double twij = calc_wij(Q, tmp_A, hi, tdist);
+                double tdwij = calc_dwij(Q, tmp_A, hi, tdist);
+                if (Q.kgc_solve() == 1) tdwij = 0;
+                double proj = ((xi - xg) * (xg - xj) + (yi - yg) * (yg - yj) + (zi - zg) * (zg - zj)) / (double)tdist * tdwij;
+                ws.push_back({j, vw * twij});
+                gs.push_back({j, vw * proj});
+                tflt += vw * twij;
+                gsum += vw * proj;
+            });
+            if (tflt < 1e-6) {
+                if (operator_row && pass == 0) continue;
+                return;   // p_w = 0
+            }
+            if (!mirror || operator_row) {
+                for (auto &c : ws) w.push_back({c.first, c.second / tflt});
+            } else {
+                // p_w = p_g + sum_j g_j (p_j - p_g)
+                for (auto &c : gs) w.push_back({c.first, c.second});
+                if (g >= 0) w.push_back({g, 1.0 - gsum});
+            }
+            return;
         }
     }
 
@@ -1054,9 +1074,14 @@ struct Oracle {
                 for (int k = 0; k < NC; ++k) mean[k] /= comp_size[k];
             }
             for (int i = 0; i < N; ++i) {
-                double s = 0;
-                for (int64_t e = ro[i]; e < ro[i + 1]; ++e) s += va[e] * v[ci[e]];
-                if (NC && comp_of[i] >= 0) s += mean[comp_of[i]];
+                double s = 0, diag_i = 0;
+                for (int64_t e = ro[i]; e < ro[i + 1]; ++e) {
+                    s += va[e] * v[ci[e]];
+                    if (ci[e] == i) diag_i = va[e];
+                }
+                // rank-one term scaled by the row's own diagonal (A_i < 0), so
+                // the constant mode lands beside the rest of the spectrum
+                if (NC && comp_of[i] >= 0) s += diag_i * mean[comp_of[i]];
                 y[i] = s;
             }
         };

@@ -5,7 +5,7 @@ work and are judged against the CPU oracle's FP64 BiCGSTAB on the same
 operator (same rows, same pinned rows):
   * FP64 BiCGSTAB: ||b-Ap||/||b|| <= 1e-8 and pressure within PRES_TOL_FP64 of
     the oracle's converged pressure (both solves stop at 1e-8 / 1e-10);
-  * mixed form (FP32 BiCGSTAB inside FP64 refinement): ||b-Ap||/||b|| <= 1e-6
+  * mixed form (FP32 GMRES inside FP64 refinement): ||b-Ap||/||b|| <= 1e-6
     and pressure / velocity within MIXED_TOL of the plain FP64 form;
   * the matrix-free operator gives the cached operator's answer.
 """
@@ -66,15 +66,27 @@ def test_mixed_ir_reaches_tolerance_and_matches_fp64(deck):
     A, st32 = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_MIXED_IR, 1e-6, nsteps=2)
     for s in st32:
         assert s.status == 0 and s.rel_residual <= 1e-6, (s.rel_residual, s.iterations, s.refinements)
-    B, st64 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8, nsteps=2)
+    B, st64 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_GMRES, 1e-9, nsteps=2)
     for f in ("pres", "ux", "uy", "uz"):
         assert rel_err(A[f], B[f]) <= MIXED_TOL, f
 
 
-def test_fp32_bicgstab_converges(deck):
+def test_fp32_gmres_converges(deck):
     P, p = deck
-    A, st = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_BICGSTAB, 1e-5)
-    assert st[-1].status == 0 and st[-1].rel_residual <= 1e-5
+    A, st = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_GMRES, 1e-5, nsteps=2)
+    for s in st:
+        assert s.status == 0 and s.rel_residual <= 1e-5
+
+
+def test_fp64_gmres_matches_oracle(deck):
+    P, p = deck
+    A, stats = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_GMRES, 1e-9)
+    assert stats[-1].status == 0 and stats[-1].rel_residual <= 1e-9
+    O = restated.Restated(P, p, 1)
+    st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-10, maxit=5000)
+    assert st == 0
+    B, _, _ = O.download()
+    assert rel_err(A["pres"], B["pres"]) <= PRES_TOL_FP64
 
 
 def test_matrix_free_equals_cached(deck):

@@ -237,6 +237,7 @@ void sph_destroy(sph_ctx *ctx) {
             delete[] c->prof_ev;
         }
         if (c->red_host) cudaFreeHost(c->red_host);
+        release_solver_ws(*c);
         c->free_all();
         delete c->allocs;
         delete c;

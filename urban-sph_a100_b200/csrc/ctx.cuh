@@ -40,7 +40,8 @@ struct SideLists {
     // Neumann rows (p_type != 1): CSR of fluid j (p_type 1, buffer 0) in range
     int n_nm = 0;
     int *nm_rows = nullptr, *nm_off = nullptr, *nm_nbr = nullptr;
-    int *nm_ghost = nullptr;     // 1 for mirror (inlet) rows
+    int *nm_ghost = nullptr;     // flags: 1 mirror (inlet) row, 2 the pass writes p = 0,
+                                 // 4 no fluid in range at all (operator anchor)
     // partners of periodic (buffer 3/4) and outlet (buffer 2) particles
     int n_per = 0, n_out = 0;
     int *per_rows = nullptr, *per_partner = nullptr;
@@ -122,11 +123,16 @@ struct Ctx {
     double *comp_inv = nullptr;   // 1 / fluid rows of each component
     double *nm_w = nullptr;       // Neumann row weights (CSR aligned with nm_nbr)
     double *nm_gw = nullptr;      // mirror-row gradient weights
+    double *nm_ow = nullptr;      // weights of the Neumann rows in the converged operator
     float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
     double *coef_d = nullptr;     // cached c_ij, FP64 form
     bool coef_valid = false;
     // Krylov workspace
-    Real *kv[10] = {};            // r, rh, p, v, s, t, ph, sh, x, b
+    Real *kv[10] = {};            // r, rh, p, v, s, t, ph, sh, dinv, b
+    double *kd[10] = {};          // FP64 Krylov vectors of the mixed form's fallback
+    double *gm_h = nullptr;       // GMRES Hessenberg column / coefficients (device)
+    void *gm_ws_r = nullptr;      // GMRES workspace in the context precision
+    void *gm_ws_d = nullptr;      // GMRES workspace with FP64 vectors (FP32 context)
     double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
     float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
     sph_ppe_stats last_ppe = {};
@@ -198,6 +204,7 @@ template <class Real> int outlet_pass(Ctx<Real> &c, VarSet<Real> &V);
 template <class Real> int periodic_pass(Ctx<Real> &c, VarSet<Real> &V);
 template <class Real> int freeslip_pass(Ctx<Real> &c, VarSet<Real> &V);
 template <class Real> int build_side_lists(Ctx<Real> &c);
+template <class Real> void release_solver_ws(Ctx<Real> &c);
 template <class Real> int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *bytes, int reset);
 
 // launch helper: grid for n threads

@@ -552,7 +552,7 @@ __global__ void k_cc_jump(int *label, int n) {
 // assemble).
 template <class Real>
 static int null_components(Ctx<Real> &c, std::vector<int> &kind, const std::vector<int> &nm_rows,
-                           const std::vector<int> &nm_off, const std::vector<int> &aux, const std::vector<int4> &ty) {
+                           const std::vector<int> &nm_flags, const std::vector<int> &aux, const std::vector<int4> &ty) {
     const int n = c.n;
     cudaStream_t st = c.stream;
     int *label = nullptr, *flag = nullptr;
@@ -590,7 +590,7 @@ static int null_components(Ctx<Real> &c, std::vector<int> &kind, const std::vect
         }
     }
     for (size_t k = 0; k < nm_rows.size(); ++k)
-        if (nm_off[k + 1] == nm_off[k]) anchored[lab[nm_rows[k]]] = 1;
+        if (nm_flags[k] & 4) anchored[lab[nm_rows[k]]] = 1;
     c.n_pins = 0;
     c.n_comp = 0;
     for (int r = 0; r < n; ++r) {
@@ -733,6 +733,7 @@ int build_side_lists(Ctx<Real> &c) {
         }
         return 0;
     };
+    std::vector<double> ow;
     for (int i = 0; i < n; ++i) {
         if (G.ty[i].w == 1 || G.ty[i].x >= 3) continue;
         rows.push_back(i);
@@ -750,40 +751,48 @@ int build_side_lists(Ctx<Real> &c) {
             const double d = std::sqrt((xg - pr[j].x) * (xg - pr[j].x) + (yid - pr[j].y) * (yid - pr[j].y) + (zid - pr[j].z) * (zid - pr[j].z));
             if (d - 1e-20 < P.ghost_tol) g = j;
         });
-        ghost.push_back(g);
         const double hi = (double)sc * (double)(Real)xi.w;
         const double tA = calc_tmpA_h(hi);
-        std::vector<int> js;
-        std::vector<double> ww, gg;
-        double tflt = 0, gsum = 0;
-        G.cell_loop(ic, jc, kc, G.ncell[i], [&](int j) {
-            if (G.ty[j].w >= 1000) return;
-            if (!(G.ty[j].w == 1 && G.ty[j].y == 0)) return;
-            const float4 xj = G.pf[j];
-            if (!(hdist(xgf, xi.y, xi.z, xj.x, xj.y, xj.z) < srange)) return;
-            const double dx = xg - pr[j].x, dy = yid - pr[j].y, dz = zid - pr[j].z;
-            const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
-            const double vw = (double)mr[j].x / (double)mr[j].y;
-            const double wv = w_h(tA, hi, r);
-            double dwv = (r > 0) ? dw_h(tA, hi, r) : 0.0;
-            if (P.kgc_solve == 1) dwv = 0;
-            const double proj = (r > 0) ? ((xid - xg) * dx + (0.0) * dy + (0.0) * dz) / r * dwv : 0.0;
-            js.push_back(j); ww.push_back(vw * wv); gg.push_back(vw * proj);
-            tflt += vw * wv; gsum += vw * proj;
-        });
-        // w: Shepard weights (pressure of ordinary rows, velocity of p_type -1);
-        // gw: weights of the mirror extrapolation p_g + sum g_j (p_j - p_g).
-        // A row without entries has tflt < 1e-6: p = 0, velocity unchanged.
-        if (tflt >= 1e-6) {
+        // pass 0: the reference's Shepard set (fluid with buffer_type 0);
+        // pass 1, only when pass 0 is empty: all fluid in range, for the
+        // converged operator (the pass itself then writes p = 0)
+        int flags = mirror ? 1 : 0;
+        for (int pass = 0; pass < 2; ++pass) {
+            std::vector<int> js;
+            std::vector<double> ww, gg;
+            double tflt = 0, gsum = 0;
+            G.cell_loop(ic, jc, kc, G.ncell[i], [&](int j) {
+                if (G.ty[j].w >= 1000) return;
+                if (!(G.ty[j].w == 1 && (pass == 1 || G.ty[j].y == 0))) return;
+                const float4 xj = G.pf[j];
+                if (!(hdist(xgf, xi.y, xi.z, xj.x, xj.y, xj.z) < srange)) return;
+                const double dx = xg - pr[j].x, dy = yid - pr[j].y, dz = zid - pr[j].z;
+                const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+                const double vw = (double)mr[j].x / (double)mr[j].y;
+                const double wv = w_h(tA, hi, r);
+                double dwv = (r > 0) ? dw_h(tA, hi, r) : 0.0;
+                if (P.kgc_solve == 1) dwv = 0;
+                const double proj = (r > 0) ? ((xid - xg) * dx) / r * dwv : 0.0;
+                js.push_back(j); ww.push_back(vw * wv); gg.push_back(vw * proj);
+                tflt += vw * wv; gsum += vw * proj;
+            });
+            if (tflt < 1e-6) {
+                if (pass == 0) { flags |= 2; continue; }   // the pass writes p = 0
+                flags |= 4;                                // no fluid at all: anchor (p = 0)
+                break;
+            }
             for (size_t k = 0; k < js.size(); ++k) {
                 nb.push_back(js[k]);
-                w.push_back(ww[k] / tflt);
-                gw.push_back(mirror ? gg[k] : 0.0);
+                const double sh = ww[k] / tflt;
+                ow.push_back(sh);
+                w.push_back(pass == 0 ? sh : 0.0);
+                gw.push_back(pass == 0 && mirror ? gg[k] : 0.0);
             }
-            if (mirror && g >= 0) { nb.push_back(g); w.push_back(0.0); gw.push_back(1.0 - gsum); }
+            if (pass == 0 && mirror && g >= 0) { nb.push_back(g); w.push_back(0.0); gw.push_back(1.0 - gsum); ow.push_back(0.0); }
+            break;
         }
         off.push_back((int)nb.size());
-        mir.push_back(mirror ? 1 : 0);
+        mir.push_back(flags);
     }
     L.n_nm = (int)rows.size();
     const std::vector<int> nmr = rows, nmo = off;
@@ -791,6 +800,8 @@ int build_side_lists(Ctx<Real> &c) {
     SPH_TRY(upload_vec(c, L.nm_ghost, mir));
     SPH_TRY(upload_vec(c, c.nm_w, w));
     SPH_TRY(upload_vec(c, c.nm_gw, gw));
+    SPH_TRY(upload_vec(c, c.nm_ow, ow));
+    const std::vector<int> nmflags = mir;
 
     // periodic partners, functions_BC.cuh:1041-1133
     rows.clear(); nb.clear();
@@ -882,7 +893,7 @@ int build_side_lists(Ctx<Real> &c) {
     c.n_pins = 0;
     c.n_comp = 0;
     if (c.prm.ppe_pin) {
-        SPH_TRY(null_components(c, kind, nmr, nmo, aux, G.ty));
+        SPH_TRY(null_components(c, kind, nmr, nmflags, aux, G.ty));
     } else {
         SPH_CUDA_TRY(cudaMemcpyAsync(c.row_kind, kind.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
         SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));

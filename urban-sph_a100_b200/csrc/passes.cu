@@ -343,8 +343,8 @@ __global__ void k_neumann_gather(const int *rows, const int *off, const int *nb,
     const int s = off[k], e = off[k + 1];
     auto ui = u[i];
     Real pv = 0;
-    if (e > s) {
-        const bool mir = mirror[k] != 0;
+    if (e > s && !(mirror[k] & 2)) {
+        const bool mir = (mirror[k] & 1) != 0;
         Real sp = 0, sx = 0, sy = 0, sz = 0;
         for (int q = s; q < e; ++q) {
             const int j = nb[q];

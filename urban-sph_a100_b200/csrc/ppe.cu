@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 
 #include "ctx.cuh"
 
@@ -177,17 +178,21 @@ __global__ void __launch_bounds__(128) k_spmv(const int *__restrict__ kind, cons
     const V xi = x[i];
     V yi = xi;   // identity / pinned; Neumann rows are applied by k_spmv_neumann
     if (kd == 1) {
+        // A_i x_i - sum_j c_ij x_j with A_i = sum_j c_ij (k_ppe_rows), evaluated
+        // as sum_j c_ij (x_i - x_j): the differences of nearby values are exact,
+        // so a smooth x does not lose (L/h)^2 digits to cancellation, which
+        // in FP32 would stall the Krylov iteration on the smooth modes
         const long long base = slice_off[i >> 5] + (i & 31);
         const int cnt = ncnt[i];
         V s = 0;
         for (int k = 0; k < cnt; ++k) {
             const long long e = base + 32LL * k;
-            s += (V)coef[e] * x[__ldg(&nbr[e])];
+            s += (V)coef[e] * (xi - x[__ldg(&nbr[e])]);
         }
-        yi = (V)diag[i] * xi - s;
+        yi = s;
         if (comp_id) {
             const int cc = comp_id[i];
-            if (cc >= 0) yi += (V)cmean[cc];
+            if (cc >= 0) yi += (V)diag[i] * (V)cmean[cc];   // A_i * mean: beside the spectrum
         }
     } else if (kd == 3) {
         const int j = aux[i];
@@ -252,12 +257,12 @@ __global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restr
             const Real cy = gc12 * tdx + gc22 * tdy + gc23 * tdz;
             const Real cz = gc31 * tdx + gc23 * tdy + gc33 * tdz;
             const Real c = (Real)2 * (mj.x / mj.y) * (dx * cx + dy * cy + dz * cz) / tdist / tdist;
-            s += (V)c * x[j];
+            s += (V)c * (xi - x[j]);   // difference form, as k_spmv
         }
-        yi = (V)diag[i] * xi - s;
+        yi = s;
         if (comp_id) {
             const int cc = comp_id[i];
-            if (cc >= 0) yi += (V)cmean[cc];
+            if (cc >= 0) yi += (V)diag[i] * (V)cmean[cc];   // A_i * mean: beside the spectrum
         }
     } else if (kd == 3) {
         const int j = aux[i];
@@ -266,17 +271,24 @@ __global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restr
     y[i] = yi;
 }
 
-// Neumann rows: y_w = x_w - sum_k w_k x_k (mirror rows use the extrapolation weights)
+// Neumann rows of the operator: y_w = x_w - sum_k w_k x_k with the Shepard
+// weights.  Inlet mirror rows also enter with their Shepard weights: the
+// extrapolation weights (functions_BC.cuh:444) do not form a stochastic row
+// and make the implicit system indefinite; the extrapolated pressure is set
+// after the solve by the Neumann pass, as the reference sets it after its
+// sweep.  Rows whose reference Shepard set is empty (p = 0 in the reference)
+// enter with the Shepard average over all fluid in range, so that corner
+// rows do not act as point Dirichlet anchors; the pass still writes p = 0.
 template <class V>
-__global__ void k_spmv_neumann(const int *rows, const int *off, const int *nb, const int *mirror, const double *w,
-                               const double *gw, int nrows, const V *x, V *y) {
+__global__ void k_spmv_neumann(const int *rows, const int *off, const int *nb, const double *w, int nrows, const V *x,
+                               V *y) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nrows) return;
     const int i = rows[k];
-    V s = 0;
-    const bool mir = mirror[k] != 0;
-    for (int q = off[k]; q < off[k + 1]; ++q) s += (V)(mir ? gw[q] : w[q]) * x[nb[q]];
-    y[i] = x[i] - s;
+    const V xi = x[i];
+    V s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
+    for (int q = off[k]; q < off[k + 1]; ++q) s += (V)w[q] * (xi - x[nb[q]]);
+    y[i] = (off[k + 1] > off[k]) ? s : xi;
 }
 
 // ---------------------------------------------------------------------------
@@ -483,8 +495,8 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
         ++c.prof_pending;
     }
     if (c.L.n_nm > 0) {
-        k_spmv_neumann<V><<<grid_for(c.L.n_nm, 128), 128, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.L.nm_ghost,
-                                                                       c.nm_w, c.nm_gw, c.L.n_nm, x, y);
+        k_spmv_neumann<V><<<grid_for(c.L.n_nm, 128), 128, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow,
+                                                                       c.L.n_nm, x, y);
         ++c.launches;
     }
 }
@@ -502,28 +514,28 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
     return SPH_OK;
 }
 
-// Jacobi-preconditioned BiCGSTAB on M x = b in Real vectors with FP64 dots;
-// x holds the initial guess.  Returns SPH_OK, SPH_NOT_CONVERGED or
-// SPH_ERR_BREAKDOWN (more than 20 restarts).
-template <class Real>
-static int bicgstab(Ctx<Real> &c, Real *x, const Real *b, double bnorm2, double tol, int maxit, bool cached,
-                    int *iters, double *relres, int *restarts) {
+// Jacobi-preconditioned BiCGSTAB on M x = b with vectors of type V (the
+// workspace ws holds 9 of them) and FP64 dots; x holds the initial guess.
+// Returns SPH_OK, SPH_NOT_CONVERGED or SPH_ERR_BREAKDOWN (> 20 restarts).
+template <class Real, class V>
+static int bicgstab_v(Ctx<Real> &c, V *const *ws, V *x, const V *b, double bnorm2, double tol, int maxit, bool cached,
+                      int *iters, double *relres, int *restarts) {
     const int n = c.n;
     cudaStream_t st = c.stream;
-    Real *r = c.kv[0], *rh = c.kv[1], *p = c.kv[2], *v = c.kv[3], *s = c.kv[4];
-    Real *t = c.kv[5], *ph = c.kv[6], *sh = c.kv[7], *dinv = c.kv[8];
+    V *r = ws[0], *rh = ws[1], *p = ws[2], *v = ws[3], *s = ws[4];
+    V *t = ws[5], *ph = ws[6], *sh = ws[7], *dinv = ws[8];
     const int G = red_grid(n);
     unsigned int *counter = (unsigned int *)(c.scal + 32);
     const double tol2 = tol * tol * bnorm2;
-    k_dinv<Real, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
+    k_dinv<V, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
     ++c.launches;
     int it = 0;
     *restarts = 0;
     int status = SPH_NOT_CONVERGED;
     while (true) {
-        apply_op<Real, Real>(c, x, t, cached);
-        k_residual_init<Real><<<G, 256, 0, st>>>(b, t, r, rh, p, v, n);
-        k_norm2<Real><<<G, 256, 0, st>>>(r, n, c.red, counter, c.scal, SC_RR);
+        apply_op<Real, V>(c, x, t, cached);
+        k_residual_init<V><<<G, 256, 0, st>>>(b, t, r, rh, p, v, n);
+        k_norm2<V><<<G, 256, 0, st>>>(r, n, c.red, counter, c.scal, SC_RR);
         c.launches += 2;
         SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
@@ -537,13 +549,13 @@ static int bicgstab(Ctx<Real> &c, Real *x, const Real *b, double bnorm2, double 
         bool restart = false;
         const int check = 4;
         while (it < maxit) {
-            k_p_update<Real><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
-            apply_op<Real, Real>(c, ph, v, cached);
-            k_alpha<Real><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
-            k_s_update<Real><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
-            apply_op<Real, Real>(c, sh, t, cached);
-            k_omega<Real><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
-            k_xr_update<Real><<<G, 256, 0, st>>>(x, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
+            k_p_update<V><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
+            apply_op<Real, V>(c, ph, v, cached);
+            k_alpha<V><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
+            k_s_update<V><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
+            apply_op<Real, V>(c, sh, t, cached);
+            k_omega<V><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
+            k_xr_update<V><<<G, 256, 0, st>>>(x, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
             c.launches += 5;
             ++it;
             if (it % check == 0 || it >= maxit) {
@@ -571,13 +583,247 @@ static int bicgstab(Ctx<Real> &c, Real *x, const Real *b, double bnorm2, double 
 }
 
 template <class Real>
+static int bicgstab(Ctx<Real> &c, Real *x, const Real *b, double bnorm2, double tol, int maxit, bool cached, int *iters,
+                    double *relres, int *restarts) {
+    return bicgstab_v<Real, Real>(c, c.kv, x, b, bnorm2, tol, maxit, cached, iters, relres, restarts);
+}
+
+// FP64 vectors on the context's operator (the mixed form's fallback)
+template <class Real>
+static int bicgstab_fp64(Ctx<Real> &c, double *x, const double *b, double bnorm2, double tol, int maxit, bool cached,
+                         int *iters, double *relres, int *restarts) {
+    return bicgstab_v<Real, double>(c, c.kd, x, b, bnorm2, tol, maxit, cached, iters, relres, restarts);
+}
+
+// ---------------------------------------------------------------------------
+// restarted GMRES(m), right Jacobi preconditioning, classical Gram-Schmidt
+// with a conditional second pass, FP64 dot products; the Hessenberg matrix,
+// its Givens rotations and the small triangular solve live on the host
+// ---------------------------------------------------------------------------
+#define GM_MAXV 64
+
+// h[k] = sum_i V_k[i] w[i], k < nv (runtime count up to GM_MAXV), last block
+// writes the sums to out[0..nv)
+template <class V>
+__global__ void __launch_bounds__(256) k_multidot(V *const *basis, const V *w, int nv, int n, double *partials,
+                                                  unsigned int *counter, double *out) {
+    __shared__ double sh[GM_MAXV][8];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k < nv; ++k) {
+        const V *vk = basis[k];
+        double s = 0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += (double)vk[i] * (double)w[i];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[k][wid] = s;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+        double s = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[k][q];
+        partials[(size_t)k * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int k = wid; k < nv; k += (blockDim.x >> 5)) {
+        double s = 0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) s += ((volatile double *)partials)[(size_t)k * gridDim.x + b];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[k] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
+// w -= sum_k h[k] V_k ; returns ||w||^2 (last block) into out[0]
+template <class V>
+__global__ void __launch_bounds__(256) k_orth_update(V *const *basis, V *w, const double *h, int nv, int n,
+                                                     double *partials, unsigned int *counter, double *out) {
+    double d[1] = {0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double wi = (double)w[i];
+        for (int k = 0; k < nv; ++k) wi -= h[k] * (double)basis[k][i];
+        const V wv = (V)wi;
+        w[i] = wv;
+        d[0] += (double)wv * (double)wv;
+    }
+    reduce_finish<1>(d, partials, counter, [&](double *t) { out[0] = t[0]; });
+}
+
+// v = w / nrm ; z = dinv * v (the next Arnoldi input)
+template <class V>
+__global__ void k_normalize(const V *w, V *v, V *z, const V *dinv, double nrm, int n) {
+    const V s = (V)(1.0 / nrm);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V vi = w[i] * s;
+        v[i] = vi;
+        z[i] = dinv[i] * vi;
+    }
+}
+
+// x += dinv * sum_k y_k V_k
+template <class V>
+__global__ void k_gmres_update(V *const *basis, const double *y, int nv, const V *dinv, V *x, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = 0; k < nv; ++k) s += y[k] * (double)basis[k][i];
+        x[i] += dinv[i] * (V)s;
+    }
+}
+
+template <class V>
+__global__ void k_sub_norm(const V *b, V *w, int n, double *partials, unsigned int *counter, double *out) {
+    double d[1] = {0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V r = b[i] - w[i];
+        w[i] = r;
+        d[0] += (double)r * (double)r;
+    }
+    reduce_finish<1>(d, partials, counter, [&](double *t) { out[0] = t[0]; });
+}
+
+template <class Real, class V>
+struct GmresWs {
+    V **basis_dev = nullptr;   // device array of m+1 basis pointers
+    V *basis[GM_MAXV + 1] = {};
+    V *w = nullptr, *z = nullptr, *dinv = nullptr;
+    int m = 0;
+};
+
+template <class Real, class V>
+static int gmres_ws(Ctx<Real> &c, GmresWs<Real, V> &ws, int m) {
+    ws.m = m;
+    for (int k = 0; k <= m; ++k) SPH_TRY(c.alloc(ws.basis[k], (size_t)c.n));
+    SPH_TRY(c.alloc(ws.w, (size_t)c.n));
+    SPH_TRY(c.alloc(ws.z, (size_t)c.n));
+    SPH_TRY(c.alloc(ws.dinv, (size_t)c.n));
+    SPH_TRY(c.alloc(ws.basis_dev, (size_t)m + 1));
+    SPH_CUDA_TRY(cudaMemcpyAsync(ws.basis_dev, ws.basis, sizeof(V *) * (m + 1), cudaMemcpyHostToDevice, c.stream));
+    return SPH_OK;
+}
+
+// GMRES(m) on M x = b; x holds the initial guess.  bnorm2 = ||b||^2 of the
+// target relative residual.  Returns SPH_OK or SPH_NOT_CONVERGED.
+template <class Real, class V>
+static int gmres(Ctx<Real> &c, GmresWs<Real, V> &ws, V *x, const V *b, double bnorm2, double tol, int maxit,
+                 bool cached, int *iters, double *relres) {
+    const int n = c.n, m = ws.m;
+    cudaStream_t st = c.stream;
+    const int G = red_grid(n);
+    unsigned int *counter = (unsigned int *)(c.scal + 32);
+    double *dres = c.scal + 48;              // 16 doubles: scalar results
+    double *hdev = c.gm_h;                   // GM_MAXV + 1 doubles
+    double *hh = c.red_host;                 // pinned, 64 doubles
+    k_dinv<V, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, ws.dinv, n);
+    ++c.launches;
+    const double bn = std::sqrt(bnorm2);
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    int it = 0;
+    int status = SPH_NOT_CONVERGED;
+    const bool trace = getenv("SPH_TRACE_PPE") != nullptr;
+    while (true) {
+        // r = b - M x ; beta = ||r||
+        apply_op<Real, V>(c, x, ws.w, cached);
+        k_sub_norm<V><<<G, 256, 0, st>>>(b, ws.w, n, c.red, counter, dres);
+        c.launches += 1;
+        SPH_CUDA_TRY(cudaMemcpyAsync(hh, dres, sizeof(double), cudaMemcpyDeviceToHost, st));
+        SPH_CUDA_TRY(cudaStreamSynchronize(st));
+        const double beta = std::sqrt(hh[0]);
+        *relres = beta / bn;
+        if (trace) fprintf(stderr, "  gmres restart it %d relres %.3e\n", it, *relres);
+        if (*relres <= tol) { status = SPH_OK; break; }
+        if (it >= maxit || !(beta > 0) || !std::isfinite(beta)) break;
+        k_normalize<V><<<G, 256, 0, st>>>(ws.w, ws.basis[0], ws.z, ws.dinv, beta, n);
+        ++c.launches;
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        bool done = false;
+        for (; j < m && it < maxit; ++j, ++it) {
+            apply_op<Real, V>(c, ws.z, ws.w, cached);
+            // classical Gram-Schmidt, second pass when the first lost > 30 %
+            k_multidot<V><<<G, 256, 0, st>>>(ws.basis_dev, ws.w, j + 1, n, c.red, counter, hdev);
+            k_orth_update<V><<<G, 256, 0, st>>>(ws.basis_dev, ws.w, hdev, j + 1, n, c.red, counter, dres);
+            c.launches += 2;
+            SPH_CUDA_TRY(cudaMemcpyAsync(hh, hdev, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, st));
+            SPH_CUDA_TRY(cudaMemcpyAsync(hh + GM_MAXV, dres, sizeof(double), cudaMemcpyDeviceToHost, st));
+            SPH_CUDA_TRY(cudaStreamSynchronize(st));
+            double hnorm2 = 0;
+            for (int k = 0; k <= j; ++k) { H[(size_t)k * m + j] = hh[k]; hnorm2 += hh[k] * hh[k]; }
+            double wn2 = hh[GM_MAXV];
+            if (wn2 < 0.49 * (wn2 + hnorm2)) {
+                k_multidot<V><<<G, 256, 0, st>>>(ws.basis_dev, ws.w, j + 1, n, c.red, counter, hdev);
+                k_orth_update<V><<<G, 256, 0, st>>>(ws.basis_dev, ws.w, hdev, j + 1, n, c.red, counter, dres);
+                c.launches += 2;
+                SPH_CUDA_TRY(cudaMemcpyAsync(hh, hdev, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, st));
+                SPH_CUDA_TRY(cudaMemcpyAsync(hh + GM_MAXV, dres, sizeof(double), cudaMemcpyDeviceToHost, st));
+                SPH_CUDA_TRY(cudaStreamSynchronize(st));
+                for (int k = 0; k <= j; ++k) H[(size_t)k * m + j] += hh[k];
+                wn2 = hh[GM_MAXV];
+            }
+            const double hn = std::sqrt(std::max(wn2, 0.0));
+            // apply the previous rotations to column j, then a new one
+            for (int k = 0; k < j; ++k) {
+                const double a = H[(size_t)k * m + j], bb = H[(size_t)(k + 1) * m + j];
+                H[(size_t)k * m + j] = cs[k] * a + sn[k] * bb;
+                H[(size_t)(k + 1) * m + j] = -sn[k] * a + cs[k] * bb;
+            }
+            const double a = H[(size_t)j * m + j];
+            const double rr = std::hypot(a, hn);
+            cs[j] = rr > 0 ? a / rr : 1.0;
+            sn[j] = rr > 0 ? hn / rr : 0.0;
+            H[(size_t)j * m + j] = rr;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            *relres = std::fabs(g[j + 1]) / bn;
+            if (!(hn > 0) || *relres <= tol) { ++j; ++it; done = true; break; }
+            k_normalize<V><<<G, 256, 0, st>>>(ws.w, ws.basis[j + 1], ws.z, ws.dinv, hn, n);
+            ++c.launches;
+        }
+        // y = H^-1 g (upper triangular j x j), x += dinv V y
+        const int nv = j;
+        for (int k = nv - 1; k >= 0; --k) {
+            double s = g[k];
+            for (int q = k + 1; q < nv; ++q) s -= H[(size_t)k * m + q] * y[q];
+            y[k] = H[(size_t)k * m + k] != 0 ? s / H[(size_t)k * m + k] : 0.0;
+        }
+        if (nv > 0) {
+            SPH_CUDA_TRY(cudaMemcpyAsync(hdev, y.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+            k_gmres_update<V><<<G, 256, 0, st>>>(ws.basis_dev, hdev, nv, ws.dinv, x, n);
+            ++c.launches;
+        }
+        if (done && *relres <= tol) {
+            // confirm with the true residual on the next pass of the loop
+            continue;
+        }
+        if (it >= maxit) {
+            apply_op<Real, V>(c, x, ws.w, cached);
+            k_sub_norm<V><<<G, 256, 0, st>>>(b, ws.w, n, c.red, counter, dres);
+            ++c.launches;
+            SPH_CUDA_TRY(cudaMemcpyAsync(hh, dres, sizeof(double), cudaMemcpyDeviceToHost, st));
+            SPH_CUDA_TRY(cudaStreamSynchronize(st));
+            *relres = std::sqrt(hh[0]) / bn;
+            status = *relres <= tol ? SPH_OK : SPH_NOT_CONVERGED;
+            break;
+        }
+    }
+    SPH_CUDA_TRY(cudaGetLastError());
+    *iters = it;
+    return status;
+}
+
+template <class Real>
 static int ensure_ppe_ws(Ctx<Real> &c) {
     const int n = c.n;
     if (!c.kv[0]) for (int k = 0; k < 10; ++k) SPH_TRY(c.alloc(c.kv[k], (size_t)n));
     if (!c.xd) { SPH_TRY(c.alloc(c.xd, n)); SPH_TRY(c.alloc(c.rd, n)); SPH_TRY(c.alloc(c.bd, n)); }
     if (!c.xf) { SPH_TRY(c.alloc(c.xf, n)); SPH_TRY(c.alloc(c.bf, n)); }
     if (!c.red) {
-        SPH_TRY(c.alloc(c.red, (size_t)SPH_MAX_COMP * 2048));
+        SPH_TRY(c.alloc(c.red, (size_t)(GM_MAXV + 1) * 2048));
+        SPH_TRY(c.alloc(c.gm_h, GM_MAXV + 8));
         SPH_TRY(c.alloc(c.scal, 64));
         SPH_CUDA_TRY(cudaMemsetAsync(c.scal, 0, 64 * sizeof(double), c.stream));
         SPH_CUDA_TRY(cudaMallocHost(&c.red_host, 64 * sizeof(double)));
@@ -642,25 +888,56 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
         int status = SPH_OK, iters = 0, restarts = 0, refinements = 0;
         double relres = 0;
-        const bool mixed_ir = (sizeof(Real) == 4) && (mode == SPH_PPE_MIXED_IR || mode == SPH_PPE_LEARNED);
+        const int m = std::max(4, std::min(GM_MAXV, c.prm.reserved[1] > 0 ? c.prm.reserved[1] : 40));
+        auto ws_r = [&]() -> GmresWs<Real, Real> * {
+            if (!c.gm_ws_r) {
+                auto *w = new GmresWs<Real, Real>();
+                if (gmres_ws(c, *w, m) < 0) { delete w; return nullptr; }
+                c.gm_ws_r = w;
+            }
+            return (GmresWs<Real, Real> *)c.gm_ws_r;
+        };
+        auto ws_d = [&]() -> GmresWs<Real, double> * {
+            if (!c.gm_ws_d) {
+                auto *w = new GmresWs<Real, double>();
+                if (gmres_ws(c, *w, m) < 0) { delete w; return nullptr; }
+                c.gm_ws_d = w;
+            }
+            return (GmresWs<Real, double> *)c.gm_ws_d;
+        };
+        const bool trace = getenv("SPH_TRACE_PPE") != nullptr;
         if (sizeof(Real) == 8) {
-            // plain form: BiCGSTAB entirely in FP64
-            status = bicgstab<Real>(c, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres, &restarts);
-        } else if (!mixed_ir) {
-            // FP32 BiCGSTAB with FP64 reductions
+            // plain form: the whole solve in FP64
+            if (mode != SPH_PPE_GMRES)
+                status = bicgstab<Real>(c, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres, &restarts);
+            else {
+                GmresWs<Real, Real> *w = ws_r();
+                if (!w) return SPH_ERR_OUT_OF_MEMORY;
+                status = gmres<Real, Real>(c, *w, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres);
+            }
+        } else if (mode == SPH_PPE_BICGSTAB || mode == SPH_PPE_GMRES) {
+            // FP32 vectors throughout, FP64 reductions
             k_cast<double, float><<<grid_for(n, 256), 256, 0, st>>>(xd, c.xf, n);
             k_cast<double, float><<<grid_for(n, 256), 256, 0, st>>>(bd, c.bf, n);
             c.launches += 2;
-            status = bicgstab<Real>(c, (Real *)c.xf, (const Real *)c.bf, bb, tol, maxit, cached, &iters, &relres, &restarts);
-            if (getenv("SPH_TRACE_PPE"))
-                fprintf(stderr, "FP32 BiCGSTAB st %d it %d rel %.3e restarts %d\n", status, iters, relres, restarts);
+            if (mode == SPH_PPE_BICGSTAB) {
+                status = bicgstab<Real>(c, (Real *)c.xf, (const Real *)c.bf, bb, tol, maxit, cached, &iters, &relres, &restarts);
+            } else {
+                GmresWs<Real, Real> *w = ws_r();
+                if (!w) return SPH_ERR_OUT_OF_MEMORY;
+                status = gmres<Real, Real>(c, *w, (Real *)c.xf, (const Real *)c.bf, bb, tol, maxit, cached, &iters, &relres);
+            }
+            if (trace) fprintf(stderr, "FP32 solve st %d it %d rel %.3e\n", status, iters, relres);
             k_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(c.xf, xd, n);
             ++c.launches;
         } else {
-            // FP32 BiCGSTAB inside FP64 iterative refinement: the outer residual
-            // r = b - M x and the correction x += e are FP64
+            // FP32 Krylov corrections (BiCGSTAB, or GMRES with reserved[2] = 1)
+            // inside FP64 iterative refinement; the outer residual r = b - M x
+            // and the update x += e are FP64
             float *ef = c.xf, *rf = c.bf;
             const double inner_tol = c.prm.ppe_inner_tol > 0 ? c.prm.ppe_inner_tol : 1e-3;
+            GmresWs<Real, Real> *w = c.prm.reserved[2] == 1 ? ws_r() : nullptr;
+            if (c.prm.reserved[2] == 1 && !w) return SPH_ERR_OUT_OF_MEMORY;
             status = SPH_NOT_CONVERGED;
             for (refinements = 0; refinements < 50; ++refinements) {
                 apply_op<Real, double>(c, xd, rd, cached);
@@ -673,16 +950,29 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
                 relres = std::sqrt(rr / bb);
                 if (relres <= tol) { status = SPH_OK; break; }
                 if (iters >= maxit) break;
-                int it_in = 0, rs = 0;
+                int it_in = 0, rs_in = 0;
                 double rel_in = 0;
-                const int st_in = bicgstab<Real>(c, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters, cached,
-                                                 &it_in, &rel_in, &rs);
-                if (getenv("SPH_TRACE_PPE"))
-                    fprintf(stderr, "IR %d outer relres %.3e inner st %d it %d rel %.3e restarts %d\n", refinements, relres,
-                            st_in, it_in, rel_in, rs);
+                const int st_in = c.prm.reserved[2] == 1
+                                      ? gmres<Real, Real>(c, *w, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters,
+                                                          cached, &it_in, &rel_in)
+                                      : bicgstab<Real>(c, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters, cached,
+                                                       &it_in, &rel_in, &rs_in);
+                restarts += rs_in;
+                if (trace)
+                    fprintf(stderr, "IR %d outer relres %.3e inner st %d it %d rel %.3e\n", refinements, relres, st_in, it_in,
+                            rel_in);
                 iters += it_in;
-                restarts += rs;
-                if (st_in == SPH_ERR_BREAKDOWN && it_in == 0) { status = SPH_ERR_BREAKDOWN; break; }
+                if (st_in != SPH_OK && !(rel_in < 1.0)) {
+                    // the FP32 correction made no progress: finish in FP64
+                    if (trace) fprintf(stderr, "IR fallback to FP64 BiCGSTAB at outer %.3e\n", relres);
+                    if (!c.kd[0]) for (int k = 0; k < 10; ++k) SPH_TRY(c.alloc(c.kd[k], (size_t)n));
+                    int it64 = 0, rs64 = 0;
+                    status = bicgstab_fp64(c, xd, bd, bb, tol, std::max(maxit - iters, 1), cached, &it64, &relres, &rs64);
+                    iters += it64;
+                    restarts += rs64;
+                    restarts += 1000;   // marks the FP64 fallback in the statistics
+                    break;
+                }
                 k_axpy_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(ef, xd, n);
                 ++c.launches;
             }
@@ -708,7 +998,16 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     return S.status < 0 ? S.status : SPH_OK;
 }
 
+template <class Real>
+void release_solver_ws(Ctx<Real> &c) {
+    delete (GmresWs<Real, Real> *)c.gm_ws_r;
+    delete (GmresWs<Real, double> *)c.gm_ws_d;
+    c.gm_ws_r = nullptr;
+    c.gm_ws_d = nullptr;
+}
+
 #define INST(R) template int phase_ppe<R>(Ctx<R> &, sph_ppe_stats *); \
+    template void release_solver_ws<R>(Ctx<R> &); \
     template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int);
 INST(float)
 INST(double)
