@@ -163,6 +163,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--matrix-free", action="store_true")
+    ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres"],
+                    help="mixed_ir form: FP64 reliable updates, or refinement restarting the FP32 solver")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -189,6 +191,7 @@ def main():
     p.ppe_tol = 1e-6
     if args.matrix_free:
         p.reserved[0] = 1
+    p.reserved[2] = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2}[args.refinement]
     n = len(P)
     sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
     sim.upload(P)
@@ -298,6 +301,7 @@ def main():
         "config": {"workload": WORKLOAD, "particles": n, "scale": args.scale, "precision": "mixed FP32/FP64",
                    "ppe": args.mode, "ppe_tol": 1e-6,
                    "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
+                   "ppe_refinement": args.refinement,
                    "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": n * layout.PART1.itemsize,

@@ -52,8 +52,10 @@ extern "C" {
                                  (functions_PPE.cuh:2-175) without its race   */
 #define SPH_PPE_BICGSTAB   1  /* Jacobi-preconditioned BiCGSTAB in the context's
                                  precision, FP64 reductions                   */
-#define SPH_PPE_MIXED_IR   2  /* FP32 BiCGSTAB corrections inside FP64 iterative
-                                 refinement; FP64 BiCGSTAB in an FP64 context */
+#define SPH_PPE_MIXED_IR   2  /* FP32 BiCGSTAB with FP64 reliable updates (FP64
+                                 solution, FP64 true residual replacing the
+                                 recurrence residual at every 10x drop);
+                                 FP64 BiCGSTAB in an FP64 context             */
 #define SPH_PPE_LEARNED    3  /* MIXED_IR warm-started by the per-particle net   */
 #define SPH_PPE_GMRES      4  /* restarted GMRES(m) in the context's precision,
                                  FP64 reductions                              */
@@ -158,14 +160,18 @@ typedef struct sph_params {
     int32_t reserved[14];    /* reserved[0] = 1: matrix-free PPE operator (c_ij
                                 recomputed per application) instead of cached;
                                 reserved[1]: GMRES restart length (0: 40, max 64);
-                                reserved[2] = 1: GMRES inner solver in MIXED_IR */
-    double  ppe_inner_tol;   /* inner FP32 tolerance of SPH_PPE_MIXED_IR (0: 1e-3) */
+                                reserved[2] = 1 / 2: MIXED_IR as iterative
+                                refinement restarting FP32 GMRES / BiCGSTAB at
+                                every correction instead of reliable updates */
+    double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
+                                refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
 } sph_params;
 
 typedef struct sph_ppe_stats {
     int32_t status;          /* SPH_OK / SPH_NOT_CONVERGED / error             */
     int32_t iterations;      /* Krylov iterations (all refinement sweeps)      */
-    int32_t refinements;     /* outer FP64 refinement sweeps (MIXED_IR)        */
+    int32_t refinements;     /* FP64 residual replacements / refinement sweeps
+                                (MIXED_IR)                                     */
     int32_t restarts;        /* breakdown restarts                             */
     double  rel_residual;    /* final ||b-Ap||_2/||b||_2, FP64                 */
     double  solve_ms;        /* device time from rhs ready to convergence      */

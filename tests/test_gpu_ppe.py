@@ -5,8 +5,11 @@ work and are judged against the CPU oracle's FP64 BiCGSTAB on the same
 operator (same rows, same pinned rows):
   * FP64 BiCGSTAB: ||b-Ap||/||b|| <= 1e-8 and pressure within PRES_TOL_FP64 of
     the oracle's converged pressure (both solves stop at 1e-8 / 1e-10);
-  * mixed form (FP32 GMRES inside FP64 refinement): ||b-Ap||/||b|| <= 1e-6
-    and pressure / velocity within MIXED_TOL of the plain FP64 form;
+  * mixed form (FP32 BiCGSTAB with FP64 reliable updates): ||b-Ap||/||b||
+    <= 1e-6 and velocity within MIXED_TOL of the plain FP64 form solved to
+    1e-9; pressure within MIXED_PRES_TOL, because a 1e-6 residual bounds the
+    pressure error only through the conditioning of the Poisson operator
+    (smooth error modes), which the velocity update sees through a gradient;
   * the matrix-free operator gives the cached operator's answer.
 """
 import numpy as np
@@ -20,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 PRES_TOL_FP64 = 1e-6
 MIXED_TOL = 1e-4
+MIXED_PRES_TOL = 1e-3
 
 
 def rel_err(a, b):
@@ -67,7 +71,8 @@ def test_mixed_ir_reaches_tolerance_and_matches_fp64(deck):
     for s in st32:
         assert s.status == 0 and s.rel_residual <= 1e-6, (s.rel_residual, s.iterations, s.refinements)
     B, st64 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_GMRES, 1e-9, nsteps=2)
-    for f in ("pres", "ux", "uy", "uz"):
+    assert rel_err(A["pres"], B["pres"]) <= MIXED_PRES_TOL
+    for f in ("ux", "uy", "uz"):
         assert rel_err(A[f], B[f]) <= MIXED_TOL, f
 
 

@@ -279,16 +279,22 @@ __global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restr
 // sweep.  Rows whose reference Shepard set is empty (p = 0 in the reference)
 // enter with the Shepard average over all fluid in range, so that corner
 // rows do not act as point Dirichlet anchors; the pass still writes p = 0.
+// One warp per row: the lanes read the row's CSR entries coalesced.
 template <class V>
-__global__ void k_spmv_neumann(const int *rows, const int *off, const int *nb, const double *w, int nrows, const V *x,
-                               V *y) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nrows) return;
+__global__ void __launch_bounds__(256) k_spmv_neumann(const int *__restrict__ rows, const int *__restrict__ off,
+                                                      const int *__restrict__ nb, const double *__restrict__ w,
+                                                      int nrows, const V *__restrict__ x, V *__restrict__ y) {
+    const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= nrows) return;   // uniform over the warp
     const int i = rows[k];
     const V xi = x[i];
-    V s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
-    for (int q = off[k]; q < off[k + 1]; ++q) s += (V)w[q] * (xi - x[nb[q]]);
-    y[i] = (off[k + 1] > off[k]) ? s : xi;
+    const int q0 = off[k], q1 = off[k + 1];
+    double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
+    for (int q = q0 + lane; q < q1; q += 32) s += __ldcs(&w[q]) * (double)(xi - x[__ldcs(&nb[q])]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[i] = (q1 > q0) ? (V)s : xi;
 }
 
 // ---------------------------------------------------------------------------
@@ -495,8 +501,8 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
         ++c.prof_pending;
     }
     if (c.L.n_nm > 0) {
-        k_spmv_neumann<V><<<grid_for(c.L.n_nm, 128), 128, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow,
-                                                                       c.L.n_nm, x, y);
+        k_spmv_neumann<V><<<div_up((long long)c.L.n_nm * 32, 256), 256, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr,
+                                                                                     c.nm_ow, c.L.n_nm, x, y);
         ++c.launches;
     }
 }
@@ -593,6 +599,147 @@ template <class Real>
 static int bicgstab_fp64(Ctx<Real> &c, double *x, const double *b, double bnorm2, double tol, int maxit, bool cached,
                          int *iters, double *relres, int *restarts) {
     return bicgstab_v<Real, double>(c, c.kd, x, b, bnorm2, tol, maxit, cached, iters, relres, restarts);
+}
+
+// ---------------------------------------------------------------------------
+// mixed-precision BiCGSTAB with reliable updates (Sleijpen & van der Vorst,
+// "Reliable updated residuals in hybrid Bi-CG methods", Computing 56, 1996;
+// the FP32/FP64 use follows Clark et al., "Solving lattice QCD systems of
+// equations using mixed precision solvers on GPUs", CPC 181, 2010).  The
+// Krylov vectors, both operator applications of an iteration and the partial
+// solution x_lo are FP32; the dot products are FP64.  When the recurrence
+// residual has fallen by RELIABLE_DELTA since the last update, x_lo is added
+// into the FP64 solution, the FP64 true residual b - M x replaces the
+// recurrence residual and the search direction carries on: one FP64 operator
+// application per update and no loss of the Krylov space, unlike a
+// refinement loop that restarts the inner solver at every correction.
+// ---------------------------------------------------------------------------
+#define RELIABLE_DELTA 0.1
+
+// r = (float)(b - y); x_lo = 0; rho = (rh, r), rr = ||b - y||^2 (FP64);
+// beta is rescaled to the replaced rho so the next direction stays conjugate
+template <class V>
+__global__ void k_reliable_replace(const double *bd, const double *yd, V *r, V *xlo, const V *rh, int n,
+                                   double *partials, unsigned int *counter, double *scal) {
+    double d[2] = {0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double ri = bd[i] - yd[i];
+        const V rf = (V)ri;
+        r[i] = rf;
+        xlo[i] = 0;
+        d[0] += (double)rh[i] * (double)rf;
+        d[1] += ri * ri;
+    }
+    reduce_finish<2>(d, partials, counter, [&](double *t) {
+        const double rho_rec = scal[SC_RHO];
+        if (rho_rec != 0.0 && isfinite(rho_rec)) scal[SC_BETA] *= t[0] / rho_rec;
+        scal[SC_RHO] = t[0];
+        scal[SC_RR] = t[1];
+        scal[SC_FLAG] = (t[1] <= scal[SC_TOL2]) ? FLAG_CONVERGED : (t[0] == 0.0 ? FLAG_BREAKDOWN : FLAG_RUN);
+    });
+}
+
+// restart: rh = r, p = v = 0
+template <class V>
+__global__ void k_restart_dirs(const V *r, V *rh, V *p, V *v, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        rh[i] = r[i]; p[i] = 0; v[i] = 0;
+    }
+}
+
+// Solves M x = b for the FP64 x (initial guess in x) with FP32 Krylov
+// vectors; yd is FP64 scratch.  *updates counts the reliable updates.
+template <class Real>
+static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *yd, double bnorm2, double tol,
+                             int maxit, bool cached, int *iters, double *relres, int *updates, int *restarts) {
+    const int n = c.n;
+    cudaStream_t st = c.stream;
+    float *const *ws = (float *const *)c.kv;
+    float *r = ws[0], *rh = ws[1], *p = ws[2], *v = ws[3], *s = ws[4];
+    float *t = ws[5], *ph = ws[6], *sh = ws[7], *dinv = ws[8];
+    float *xlo = c.xf;
+    const int G = red_grid(n);
+    unsigned int *counter = (unsigned int *)(c.scal + 32);
+    const double tol2 = tol * tol * bnorm2;
+    const bool trace = getenv("SPH_TRACE_PPE") != nullptr;
+    k_dinv<float, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
+    SPH_CUDA_TRY(cudaMemsetAsync(xlo, 0, sizeof(float) * n, st));
+    ++c.launches;
+    *restarts = 0;
+    *updates = 0;
+    int it = 0;
+    auto read_scal = [&]() -> int {
+        SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
+        SPH_CUDA_TRY(cudaStreamSynchronize(st));
+        return SPH_OK;
+    };
+    // x += x_lo; r = b - M x (FP64), replacing the recurrence residual
+    auto replace = [&]() {
+        k_axpy_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(xlo, x, n);
+        apply_op<Real, double>(c, x, yd, cached);
+        k_reliable_replace<float><<<G, 256, 0, st>>>(b, yd, r, xlo, rh, n, c.red, counter, c.scal);
+        c.launches += 2;
+    };
+    // fresh start from the true residual
+    auto restart = [&]() -> int {
+        replace();
+        k_restart_dirs<float><<<G, 256, 0, st>>>(r, rh, p, v, n);
+        k_norm2<float><<<G, 256, 0, st>>>(r, n, c.red, counter, c.scal, SC_RHO_NEW);
+        c.launches += 2;
+        SPH_TRY(read_scal());
+        k_set_scal<<<1, 1, 0, st>>>(c.scal, c.red_host[SC_RHO_NEW], tol2);
+        ++c.launches;
+        return SPH_OK;
+    };
+    int status = SPH_NOT_CONVERGED;
+    SPH_TRY(restart());
+    double rr = c.red_host[SC_RR];
+    double maxrr = rr;
+    *relres = std::sqrt(rr / bnorm2);
+    if (rr <= tol2) status = SPH_OK;
+    const int check = 4;
+    while (status != SPH_OK && it < maxit) {
+        k_p_update<float><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
+        apply_op<Real, float>(c, ph, v, cached);
+        k_alpha<float><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
+        k_s_update<float><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
+        apply_op<Real, float>(c, sh, t, cached);
+        k_omega<float><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
+        k_xr_update<float><<<G, 256, 0, st>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
+        c.launches += 5;
+        ++it;
+        if (it % check != 0 && it < maxit) continue;
+        SPH_TRY(read_scal());
+        const double flag = c.red_host[SC_FLAG];
+        rr = c.red_host[SC_RR];
+        if (flag == FLAG_BREAKDOWN || !std::isfinite(rr)) {
+            if (++*restarts > 20) { status = SPH_ERR_BREAKDOWN; break; }
+            SPH_TRY(restart());
+            ++*updates;
+        } else if (flag == FLAG_CONVERGED || rr < RELIABLE_DELTA * RELIABLE_DELTA * maxrr || it >= maxit) {
+            replace();
+            SPH_TRY(read_scal());
+            ++*updates;
+            if (trace)
+                fprintf(stderr, "  reliable update %d at it %d: recurrence %.3e true %.3e\n", *updates, it,
+                        std::sqrt(rr / bnorm2), std::sqrt(c.red_host[SC_RR] / bnorm2));
+            if (c.red_host[SC_FLAG] == FLAG_BREAKDOWN) {
+                if (++*restarts > 20) { status = SPH_ERR_BREAKDOWN; break; }
+                SPH_TRY(restart());
+            }
+        } else {
+            maxrr = std::max(maxrr, rr);
+            continue;
+        }
+        rr = c.red_host[SC_RR];
+        maxrr = rr;
+        *relres = std::sqrt(rr / bnorm2);
+        if (rr <= tol2) status = SPH_OK;
+    }
+    if (status != SPH_OK && it > 0 && *updates == 0) *relres = std::sqrt(rr / bnorm2);
+    SPH_CUDA_TRY(cudaGetLastError());
+    *iters = it;
+    return status;
 }
 
 // ---------------------------------------------------------------------------
@@ -930,10 +1077,23 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             if (trace) fprintf(stderr, "FP32 solve st %d it %d rel %.3e\n", status, iters, relres);
             k_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(c.xf, xd, n);
             ++c.launches;
+        } else if (c.prm.reserved[2] == 0) {
+            // FP32 BiCGSTAB with FP64 reliable updates; FP64 BiCGSTAB from
+            // its last iterate if the FP32 recurrence breaks down
+            status = bicgstab_reliable(c, xd, bd, rd, bb, tol, maxit, cached, &iters, &relres, &refinements, &restarts);
+            if (trace) fprintf(stderr, "RU st %d it %d updates %d rel %.3e\n", status, iters, refinements, relres);
+            if (status < 0 || (status != SPH_OK && iters < maxit)) {
+                if (!c.kd[0]) for (int k = 0; k < 10; ++k) SPH_TRY(c.alloc(c.kd[k], (size_t)n));
+                int it64 = 0, rs64 = 0;
+                status = bicgstab_fp64(c, xd, bd, bb, tol, std::max(maxit - iters, 1), cached, &it64, &relres, &rs64);
+                iters += it64;
+                restarts += rs64 + 1000;   // marks the FP64 fallback in the statistics
+            }
         } else {
-            // FP32 Krylov corrections (BiCGSTAB, or GMRES with reserved[2] = 1)
-            // inside FP64 iterative refinement; the outer residual r = b - M x
-            // and the update x += e are FP64
+            // FP32 Krylov corrections restarted at every refinement (BiCGSTAB
+            // with reserved[2] = 2, GMRES with reserved[2] = 1) inside FP64
+            // iterative refinement; the outer residual r = b - M x and the
+            // update x += e are FP64
             float *ef = c.xf, *rf = c.bf;
             const double inner_tol = c.prm.ppe_inner_tol > 0 ? c.prm.ppe_inner_tol : 1e-3;
             GmresWs<Real, Real> *w = c.prm.reserved[2] == 1 ? ws_r() : nullptr;
