@@ -267,6 +267,33 @@ int64_t sph_launch_count(sph_ctx *ctx);
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
 
+/* ---- cell sort without device allocation --------------------------------
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc, such as a host code that gives all of its device memory to its
+ * own pool or arena, or one whose time loop must not allocate once it runs.
+ * It does what sph_nnps + sph_nnps_export do for the cell hash and sort
+ * (KERNEL_index_particle_to_cell and the stable sort by cell), for n
+ * particles given as device arrays in their original order, and writes
+ * g_idx, p_idx (n each) and g_str, g_end (num_cells + 1 each) to device
+ * arrays the caller owns.  `params` needs the cell grid of
+ * sph_domain_setup; i_type 3 marks dummies (key num_cells).  `stream` is a
+ * cudaStream_t (NULL: the legacy default stream).
+ *
+ * The working memory is one static device array per GPU, about 9.5 MB,
+ * which every GPU that loads this library holds until the process exits.
+ * Limits: n <= SPH_NOALLOC_MAX_PARTICLES and num_cells + 2 <=
+ * SPH_NOALLOC_MAX_CELLS; larger inputs return SPH_ERR_BAD_ARG.  The first
+ * call on a device looks up that array's device address, so make it before
+ * any stream capture.  All calls on a device share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race.  The call
+ * waits for its stream before it returns, to report a cell of more than
+ * 4096 particles (SPH_ERR_UNSUPPORTED).  It calls no cudaMalloc or cudaFree. */
+#define SPH_NOALLOC_MAX_PARTICLES 262144
+#define SPH_NOALLOC_MAX_CELLS     524288
+int sph_nnps_sort_noalloc(const sph_params *params, const float *d_x, const float *d_y, const float *d_z,
+                          const int32_t *d_i_type, int32_t n, int32_t *d_g_idx, int32_t *d_p_idx,
+                          int32_t *d_g_str, int32_t *d_g_end, void *stream);
+
 const char *sph_status_string(int status);
 
 /* Text of the last error raised on the calling host thread. */

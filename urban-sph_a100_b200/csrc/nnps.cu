@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "ctx.cuh"
 
@@ -1051,3 +1052,140 @@ INST(double)
 #undef INST
 
 }  // namespace sph
+
+// ---------------------------------------------------------------------------
+// Cell sort without device allocation (sph_nnps_sort_noalloc)
+//
+// For callers that cannot call cudaMalloc: a host code that hands all of its
+// device memory to its own pool or arena, or a solver that must not allocate
+// once its time loop has started.  The hash, counting sort and cell ranges
+// of nnps_build run here on a scratch area that is a file-scope device
+// array, sized for at most SPH_NOALLOC_MAX_PARTICLES particles and
+// SPH_NOALLOC_MAX_CELLS cells (about 9.5 MB, held by every GPU that loads
+// this library until the process exits).
+// ---------------------------------------------------------------------------
+namespace sph {
+namespace noalloc {
+
+constexpr long long kMaxN = SPH_NOALLOC_MAX_PARTICLES;
+constexpr long long kMaxC = SPH_NOALLOC_MAX_CELLS;    // num_cells + 2 entries of the cell arrays
+constexpr long long kScanTmp = 1024;                  // >= scan_tmp_size(max(kMaxN, kMaxC))
+// int slots: key, dummy flag, dummy rank (n each); cell counts, cell starts,
+// long-cell list (kMaxC each); long-cell count, overflow flag; scan scratch
+constexpr long long kKey = 0, kDflag = kMaxN, kDrank = 2 * kMaxN, kCnt = 3 * kMaxN, kStart = kCnt + kMaxC,
+                    kBig = kStart + kMaxC, kNbig = kBig + kMaxC, kErr = kNbig + 2, kTmp = kErr + 2,
+                    kTotal = kTmp + kScanTmp;
+
+static __device__ __align__(256) int g_scratch[kTotal];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_mtx;
+static int *g_ptr[kMaxDevices] = {};
+
+// device address of g_scratch on the current device, looked up once per device
+static int scratch_address(int **out) {
+    int dev = 0;
+    SPH_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) { set_error("sph_nnps_sort_noalloc: device ordinal out of range"); return SPH_ERR_BAD_ARG; }
+    std::lock_guard<std::mutex> lock(g_mtx);
+    if (!g_ptr[dev]) {
+        int *p = nullptr;
+        SPH_CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_scratch));
+        g_ptr[dev] = p;
+    }
+    *out = g_ptr[dev];
+    return SPH_OK;
+}
+
+// KERNEL_index_particle_to_cell (functions_NNPS.cuh:879-907) on separate
+// coordinate arrays, with the cell histogram of the counting sort
+__global__ void k_hash_xyz(DevParams P, const float *x, const float *y, const float *z, const int *i_type, int *key,
+                           int *cell_cnt, int *dflag, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (i_type[i] == 3) {
+        key[i] = P.num_cells;
+        dflag[i] = 1;
+        return;
+    }
+    dflag[i] = 0;
+    const int ic = bin_axis(x[i], P.xmin, P.xmax, P.NI);
+    const int jc = bin_axis(y[i], P.ymin, P.ymax, P.NJ);
+    const int kc = bin_axis(z[i], P.zmin, P.zmax, P.NK);
+    const int k = ic + P.NI * jc + P.NI * P.NJ * kc;
+    key[i] = k;
+    atomicAdd(&cell_cnt[k], 1);
+}
+
+__global__ void k_set_tail(int *cell_start, int num_cells, int n) { cell_start[num_cells + 1] = n; }
+
+// g_str / g_end of KERNEL_reorder (functions_NNPS.cuh:813-844): -1 / 0 for empty cells
+__global__ void k_cell_ranges(const int *cs, int *g_str, int *g_end, int ncells1) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ncells1) return;
+    const int s = cs[k], e = cs[k + 1];
+    const bool occ = e > s;
+    g_str[k] = occ ? s : -1;
+    g_end[k] = occ ? e : 0;
+}
+
+}  // namespace noalloc
+}  // namespace sph
+
+extern "C" int sph_nnps_sort_noalloc(const sph_params *params, const float *d_x, const float *d_y, const float *d_z,
+                                     const int32_t *d_i_type, int32_t n, int32_t *d_g_idx, int32_t *d_p_idx,
+                                     int32_t *d_g_str, int32_t *d_g_end, void *stream) {
+    using namespace sph;
+    using namespace sph::noalloc;
+    if (!params || n < 0) { set_error("sph_nnps_sort_noalloc: null params or negative n"); return SPH_ERR_BAD_ARG; }
+    const int NC = params->vii[SPH_VII_NUM_CELLS];
+    if (NC < 1) { set_error("sph_nnps_sort_noalloc: params hold no cell grid (run sph_domain_setup)"); return SPH_ERR_BAD_ARG; }
+    if ((long long)n > kMaxN) {
+        set_error("sph_nnps_sort_noalloc: more particles than SPH_NOALLOC_MAX_PARTICLES");
+        return SPH_ERR_BAD_ARG;
+    }
+    if ((long long)NC + 2 > kMaxC) {
+        set_error("sph_nnps_sort_noalloc: num_cells + 2 exceeds SPH_NOALLOC_MAX_CELLS");
+        return SPH_ERR_BAD_ARG;
+    }
+    if (!d_g_str || !d_g_end || (n > 0 && (!d_x || !d_y || !d_z || !d_i_type || !d_g_idx || !d_p_idx))) {
+        set_error("sph_nnps_sort_noalloc: null array");
+        return SPH_ERR_BAD_ARG;
+    }
+    int *S = nullptr;
+    SPH_TRY(scratch_address(&S));
+    cudaStream_t st = (cudaStream_t)stream;
+    const DevParams P = make_dev_params(*params);
+    int *key = S + kKey, *dflag = S + kDflag, *drank = S + kDrank, *cnt = S + kCnt, *cs = S + kStart;
+    int *big = S + kBig, *nbig = S + kNbig, *err = S + kErr, *tmp = S + kTmp;
+    long long launches = 0;
+    // the scratch keeps the previous call's contents: clear the counters
+    SPH_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)NC + 2), st));
+    SPH_CUDA_TRY(cudaMemsetAsync(nbig, 0, sizeof(int) * 4, st));   // nbig, its pad, err, its pad
+    if (n > 0) {
+        k_hash_xyz<<<grid_for(n, 256), 256, 0, st>>>(P, d_x, d_y, d_z, d_i_type, key, cnt, dflag, n);
+        SPH_CUDA_TRY(cudaGetLastError());
+    }
+    SPH_TRY(exclusive_scan<int>(cnt, cs, (long long)NC + 1, tmp, st, launches));
+    k_set_tail<<<1, 1, 0, st>>>(cs, NC, n);
+    SPH_CUDA_TRY(cudaGetLastError());
+    if (n > 0) {
+        SPH_TRY(exclusive_scan<int>(dflag, drank, n, tmp, st, launches));
+        SPH_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)NC + 2), st));
+        k_scatter<<<grid_for(n, 256), 256, 0, st>>>(key, cs, cnt, drank, d_p_idx, NC, n);
+        k_sort_small<<<grid_for(NC, 256), 256, 0, st>>>(cs, d_p_idx, big, nbig, NC);
+        k_sort_big<<<std::min(NC, 65535), 256, 0, st>>>(cs, d_p_idx, big, nbig, err);
+        k_sorted_keys<<<grid_for(n, 256), 256, 0, st>>>(key, d_p_idx, d_g_idx, n);
+        SPH_CUDA_TRY(cudaGetLastError());
+    }
+    k_cell_ranges<<<grid_for(NC + 1, 256), 256, 0, st>>>(cs, d_g_str, d_g_end, NC + 1);
+    SPH_CUDA_TRY(cudaGetLastError());
+    int flags[3] = {0, 0, 0};   // nbig, pad, err
+    SPH_CUDA_TRY(cudaMemcpyAsync(flags, nbig, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaStreamSynchronize(st));
+    if (flags[2] || flags[0] > 65535) {
+        set_error("sph_nnps_sort_noalloc: a cell holds more than 4096 particles");
+        return SPH_ERR_UNSUPPORTED;
+    }
+    return SPH_OK;
+}

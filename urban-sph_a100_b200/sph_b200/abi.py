@@ -23,7 +23,7 @@ SYMBOLS = (
     "sph_upload", "sph_upload_state", "sph_download", "sph_nnps", "sph_nnps_export",
     "sph_neighbors_export", "sph_interaction", "sph_ppe", "sph_time_update", "sph_step",
     "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_status_string",
-    "sph_last_error", "sph_profile", "sph_operator_stats",
+    "sph_last_error", "sph_profile", "sph_operator_stats", "sph_nnps_sort_noalloc",
 )
 
 _lib = None
@@ -72,6 +72,7 @@ def lib():
         L.sph_profile.argtypes = [vp, i32]
         L.sph_operator_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double), i32]
+        L.sph_nnps_sort_noalloc.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
