@@ -157,12 +157,16 @@ typedef struct sph_params {
                                 1 rank-one mean-pressure term per singular
                                 component (default), 2 one row pinned to p=0 */
     int32_t recompute_gc;    /* 1: recompute the correction matrix every step  */
-    int32_t reserved[14];    /* reserved[0] = 1: matrix-free PPE operator (c_ij
-                                recomputed per application) instead of cached;
-                                reserved[1]: GMRES restart length (0: 40, max 64);
-                                reserved[2] = 1 / 2: MIXED_IR as iterative
-                                refinement restarting FP32 GMRES / BiCGSTAB at
-                                every correction instead of reliable updates */
+    int32_t ppe_matrix_free; /* 1: PPE operator recomputes c_ij at every
+                                application instead of reading the cache      */
+    int32_t ppe_gmres_restart;   /* GMRES restart length (0: 40, max 64)       */
+    int32_t ppe_refinement;  /* MIXED_IR: 0 reliable updates (default); 1 / 2
+                                iterative refinement restarting FP32 GMRES /
+                                BiCGSTAB at every correction                   */
+    int32_t ppe_coarse_block;    /* BiCGSTAB preconditioner: 0 Jacobi; B > 0
+                                adds a coarse correction on aggregates of
+                                B x B x B NNPS cells (additive two-level)      */
+    int32_t reserved[10];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
 } sph_params;
@@ -262,8 +266,10 @@ int64_t sph_launch_count(sph_ctx *ctx);
  * with `enable` set, every operator launch is bracketed by CUDA events on the
  * context's stream.  sph_operator_stats returns the launches timed since the
  * last reset, their summed device time, and the algorithmic bytes of one
- * launch (per row: kind, x_i, y_i, A_i; per stored neighbour: index and
- * coefficient).  `reset` clears the counters after reading. */
+ * launch (per row: kind, list length, x_i, y_i, and component id and A_i
+ * when the rank-one term is on; per 32 rows the slice offset; per stored
+ * neighbour: index and coefficient; the gathered x_j are not counted).
+ * `reset` clears the counters after reading. */
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
 

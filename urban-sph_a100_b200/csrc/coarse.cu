@@ -1,0 +1,396 @@
+// Two-level preconditioner of the converged pressure solve: Jacobi plus an
+// additive coarse correction on aggregates of B x B x B NNPS cells,
+//     M^-1 r = D^-1 r + Z E^-1 Z^T r,   E = Z^T M Z,
+// with Z the indicator vectors of the aggregates (every row of the operator
+// except identity / pinned rows belongs to exactly one) and M the converged
+// operator of ppe.cu (difference-form fluid rows, Neumann rows with their
+// operator weights, outlet copies, rank-one mean-pressure term).
+//
+// The particles never move, so the aggregates, E and its inverse are built
+// once per neighbour-list build.  Jacobi alone needs O(L/h) BiCGSTAB
+// iterations (the smooth modes); the coarse space removes the modes longer
+// than the aggregate size, which also keeps FP32 Krylov vectors accurate
+// enough for the mixed form.
+//
+// Determinism: E is accumulated in 64-bit fixed point (integer atomics are
+// order-independent), every reduction has a fixed order, and the inverse is
+// Gauss-Jordan with partial pivoting in a fixed sequence of launches.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ctx.cuh"
+
+namespace sph {
+
+constexpr int kCoarseMaxAgg = 4096;
+
+// deterministic block sum (fixed shuffle pattern, warps summed in order)
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < NT / 32; ++w) t += sh[w];
+    __syncthreads();
+    return t;   // valid on thread 0
+}
+
+// ---- set-up -------------------------------------------------------------------
+
+// largest |c_ij| over the stored entries of the fluid rows (non-negative
+// doubles order like their bit patterns, so an integer max is exact)
+template <class C>
+__global__ void k_coef_absmax(const int *kind, const long long *slice_off, const int *ncnt, const C *coef, int n,
+                              unsigned long long *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0;
+    if (i < n && kind[i] == 1) {
+        const long long base = slice_off[i >> 5] + (i & 31);
+        for (int k = 0; k < ncnt[i]; ++k) m = fmax(m, fabs((double)coef[base + 32LL * k]));
+    }
+    if (m > 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// one block per aggregate I: row I of E = Z^T M Z in fixed point, and the
+// sums of A_i of I's fluid rows per rank-one component
+template <class C, class Real>
+__global__ void __launch_bounds__(256) k_coarse_assemble(
+    int m, const int *agg, const int *off, const int *rows, const int *kind, const int *aux,
+    const long long *slice_off, const int *ncnt, const int *nbr, const C *coef, const int *nm_idx, const int *nm_off,
+    const int *nm_nbr, const double *nm_ow, const int *comp_id, const Real *diag, int ncomp, double scale, double *E,
+    double *a_comp) {
+    extern __shared__ unsigned long long acc[];
+    __shared__ double sh[8];
+    const int I = blockIdx.x;
+    for (int J = threadIdx.x; J < m; J += blockDim.x) acc[J] = 0ull;
+    __syncthreads();
+    double asum[SPH_MAX_COMP];
+#pragma unroll
+    for (int q = 0; q < SPH_MAX_COMP; ++q) asum[q] = 0;
+    auto add = [&](int J, double v) {
+        atomicAdd(&acc[J], (unsigned long long)llrint(v * scale));
+    };
+    // (M z_J)_i for i in I: sum over the row's entries of w (z_i - z_j)
+    auto couple = [&](int j, double w) {
+        const int J = (j >= 0) ? agg[j] : -1;
+        if (J == I) return;
+        add(I, w);
+        if (J >= 0) add(J, -w);
+    };
+    for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) {
+        const int i = rows[q];
+        const int kd = kind[i];
+        if (kd == 1) {
+            const long long base = slice_off[i >> 5] + (i & 31);
+            const int cnt = ncnt[i];
+            for (int k = 0; k < cnt; ++k) {
+                const long long e = base + 32LL * k;
+                couple(nbr[e], (double)coef[e]);
+            }
+            const int cc = comp_id ? comp_id[i] : -1;
+#pragma unroll
+            for (int t = 0; t < SPH_MAX_COMP; ++t)
+                if (cc == t) asum[t] += (double)diag[i];
+        } else if (kd == 2) {
+            const int r = nm_idx[i];   // a row without a Neumann entry stays the identity
+            const int q0 = r >= 0 ? nm_off[r] : 0, q1 = r >= 0 ? nm_off[r + 1] : 0;
+            if (q1 == q0) add(I, 1.0);
+            for (int qq = q0; qq < q1; ++qq) couple(nm_nbr[qq], nm_ow[qq]);
+        } else if (kd == 3) {
+            const int pj = aux[i];
+            if (pj < 0) add(I, 1.0);
+            else couple(pj, 1.0);
+        }
+    }
+    __syncthreads();
+    for (int J = threadIdx.x; J < m; J += blockDim.x) E[(size_t)I * m + J] = (double)(long long)acc[J] / scale;
+    for (int t = 0; t < ncomp; ++t) {
+        const double s = block_sum<256>(asum[t], sh);
+        if (threadIdx.x == 0) a_comp[(size_t)I * ncomp + t] = s;
+    }
+}
+
+// rank-one part: E_IJ += sum_c a_comp[I][c] * |J in c| / |c|
+__global__ void k_coarse_rank_one(double *E, const double *a_comp, const int *cnt_comp, const double *comp_inv, int m,
+                                  int ncomp) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)m * m) return;
+    const int I = (int)(t / m), J = (int)(t % m);
+    double v = 0;
+    for (int c = 0; c < ncomp; ++c) v += a_comp[(size_t)I * ncomp + c] * (double)cnt_comp[(size_t)J * ncomp + c] * comp_inv[c];
+    E[t] += v;
+}
+
+// Gauss-Jordan with partial pivoting on W (m x m), Inv starts as identity
+__global__ void k_gj_pivot(const double *W, int m, int k, int *piv, double *pval, int *err) {
+    __shared__ double bv[32];
+    __shared__ int bi[32];
+    double best = -1;
+    int idx = -1;
+    for (int r = k + threadIdx.x; r < m; r += blockDim.x) {
+        const double v = fabs(W[(size_t)r * m + k]);
+        if (v > best) { best = v; idx = r; }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (ov > best || (ov == best && oi >= 0 && (idx < 0 || oi < idx))) { best = ov; idx = oi; }
+    }
+    if (lane == 0) { bv[wid] = best; bi[wid] = idx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = -1;
+        int p = -1;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            if (bv[w] > b || (bv[w] == b && bi[w] >= 0 && (p < 0 || bi[w] < p))) { b = bv[w]; p = bi[w]; }
+        if (!(b > 0) || p < 0) { *err = 1; p = k; }
+        *piv = p;
+        *pval = W[(size_t)p * m + k];
+    }
+}
+
+// swap rows k and piv, scale row k by 1/pivot (one thread per column of [W | Inv])
+__global__ void k_gj_swap_scale(double *W, double *Inv, int m, int k, const int *piv, const double *pval,
+                                const int *err) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= 2 * m || *err) return;
+    const int p = *piv;
+    const double inv = 1.0 / *pval;
+    double *A = col < m ? W : Inv;
+    const int cc = col < m ? col : col - m;
+    const double b = A[(size_t)p * m + cc];
+    if (p != k) A[(size_t)p * m + cc] = A[(size_t)k * m + cc];
+    A[(size_t)k * m + cc] = b * inv;
+}
+
+__global__ void k_gj_col(const double *W, double *colk, int m, int k) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < m) colk[r] = W[(size_t)r * m + k];
+}
+
+// eliminate column k from every row r != k (columns of W left of k are done)
+__global__ void k_gj_elim(double *W, double *Inv, const double *colk, int m, int k, const int *err) {
+    const int r = blockIdx.y;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r == k || *err) return;
+    const double f = colk[r];
+    if (f == 0.0) return;
+    if (col < m) {
+        if (col >= k) W[(size_t)r * m + col] -= f * W[(size_t)k * m + col];
+    } else if (col < 2 * m) {
+        const int cc = col - m;
+        Inv[(size_t)r * m + cc] -= f * Inv[(size_t)k * m + cc];
+    }
+}
+
+__global__ void k_eye(double *A, int m) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < (long long)m * m) A[t] = (t / m == t % m) ? 1.0 : 0.0;
+}
+
+// ---- application ----------------------------------------------------------
+
+template <class V>
+__global__ void __launch_bounds__(256) k_coarse_restrict(const int *off, const int *rows, const V *r, double *s) {
+    __shared__ double sh[8];
+    const int I = blockIdx.x;
+    double v = 0;
+    for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) v += (double)r[rows[q]];
+    v = block_sum<256>(v, sh);
+    if (threadIdx.x == 0) s[I] = v;
+}
+
+// y = E^-1 s, one warp per row
+__global__ void __launch_bounds__(256) k_coarse_solve(const double *__restrict__ Inv, const double *__restrict__ s,
+                                                      double *__restrict__ y, int m) {
+    const int I = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (I >= m) return;
+    const double *row = Inv + (size_t)I * m;
+    double v = 0;
+    for (int J = lane; J < m; J += 32) v += row[J] * s[J];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) y[I] = v;
+}
+
+template <class V>
+__global__ void k_coarse_add(const int *agg, const double *y, V *z, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int a = agg[i];
+    if (a >= 0) z[i] += (V)y[a];
+}
+
+template <class Real, class V>
+void coarse_apply(Ctx<Real> &c, const V *r, V *z) {
+    if (c.cg_m <= 0) return;
+    const int m = c.cg_m;
+    k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, c.cg_s);
+    k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_inv, c.cg_s, c.cg_y, m);
+    k_coarse_add<V><<<grid_for(c.n, 256), 256, 0, c.stream>>>(c.cg_agg, c.cg_y, z, c.n);
+    c.launches += 3;
+}
+
+template <class Real>
+int coarse_build(Ctx<Real> &c) {
+    const int B = c.prm.ppe_coarse_block;
+    c.cg_valid = true;
+    c.cg_block = B;
+    c.cg_m = 0;
+    if (B <= 0) return SPH_OK;
+    const int n = c.n;
+    cudaStream_t st = c.stream;
+    // host copies of what the aggregation needs
+    std::vector<int> kind(n), ncnt(n), comp(n, -1);
+    std::vector<float4> pos(n);
+    SPH_CUDA_TRY(cudaMemcpyAsync(kind.data(), c.row_kind, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaMemcpyAsync(ncnt.data(), c.ncnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaMemcpyAsync(pos.data(), c.pf, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+    if (c.n_comp > 0) SPH_CUDA_TRY(cudaMemcpyAsync(comp.data(), c.comp_id, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    const int nnm = c.L.n_nm;
+    std::vector<int> nm_rows(nnm);
+    if (nnm > 0) SPH_CUDA_TRY(cudaMemcpyAsync(nm_rows.data(), c.L.nm_rows, sizeof(int) * nnm, cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaStreamSynchronize(st));
+
+    // aggregates: blocks of B^3 cells of the binning grid, numbered in order
+    // of their first row (rows ascending), identity and pinned rows excluded
+    const DevParams &P = c.dp;
+    const int NBx = (P.NI + B - 1) / B, NBy = (P.NJ + B - 1) / B, NBz = (P.NK + B - 1) / B;
+    std::vector<int> block_agg((size_t)NBx * NBy * NBz, -1), agg(n, -1), size;
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+        const int kd = kind[i];
+        if (kd != 1 && kd != 2 && kd != 3) continue;
+        const int bx = bin_axis(pos[i].x, P.xmin, P.xmax, P.NI) / B;
+        const int by = bin_axis(pos[i].y, P.ymin, P.ymax, P.NJ) / B;
+        const int bz = bin_axis(pos[i].z, P.zmin, P.zmax, P.NK) / B;
+        int &a = block_agg[((size_t)bz * NBy + by) * NBx + bx];
+        if (a < 0) { a = m++; size.push_back(0); }
+        agg[i] = a;
+        ++size[a];
+    }
+    if (m > kCoarseMaxAgg) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "ppe_coarse_block %d gives %d aggregates (max %d): use a larger block", B, m, kCoarseMaxAgg);
+        set_error(msg);
+        return SPH_ERR_UNSUPPORTED;
+    }
+    if (m == 0) return SPH_OK;
+    std::vector<int> off(m + 1, 0);
+    for (int a = 0; a < m; ++a) off[a + 1] = off[a] + size[a];
+    std::vector<int> rows(std::max(off[m], 1), 0), fill(off.begin(), off.end() - 1);
+    for (int i = 0; i < n; ++i)
+        if (agg[i] >= 0) rows[fill[agg[i]]++] = i;
+    std::vector<int> nm_idx(n, -1);
+    for (int k = 0; k < nnm; ++k) nm_idx[nm_rows[k]] = k;
+    const int ncomp = c.n_comp;
+    std::vector<int> cnt_comp((size_t)m * std::max(ncomp, 1), 0);
+    for (int i = 0; i < n; ++i)
+        if (agg[i] >= 0 && kind[i] == 1 && comp[i] >= 0 && comp[i] < ncomp) ++cnt_comp[(size_t)agg[i] * ncomp + comp[i]];
+    int max_rows = 0, max_cnt = 0;
+    for (int a = 0; a < m; ++a) max_rows = std::max(max_rows, size[a]);
+    for (int i = 0; i < n; ++i) max_cnt = std::max(max_cnt, ncnt[i]);
+
+    // device buffers (released with the context)
+    auto up = [&](int *&dst, const std::vector<int> &v) -> int {
+        c.release(dst);
+        SPH_TRY(c.alloc(dst, v.size()));
+        SPH_CUDA_TRY(cudaMemcpyAsync(dst, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, st));
+        return SPH_OK;
+    };
+    SPH_TRY(up(c.cg_agg, agg));
+    SPH_TRY(up(c.cg_off, off));
+    SPH_TRY(up(c.cg_rows, rows));
+    int *d_nm_idx = nullptr, *d_cnt_comp = nullptr, *d_piv = nullptr, *d_err = nullptr;
+    SPH_TRY(up(d_nm_idx, nm_idx));
+    SPH_TRY(up(d_cnt_comp, cnt_comp));
+    double *E = nullptr, *a_comp = nullptr, *colk = nullptr, *pval = nullptr;
+    unsigned long long *amax = nullptr;
+    c.release(c.cg_inv); c.release(c.cg_s); c.release(c.cg_y);
+    SPH_TRY(c.alloc(c.cg_inv, (size_t)m * m));
+    SPH_TRY(c.alloc(c.cg_s, m));
+    SPH_TRY(c.alloc(c.cg_y, m));
+    SPH_TRY(c.alloc(E, (size_t)m * m));
+    SPH_TRY(c.alloc(a_comp, (size_t)m * std::max(ncomp, 1)));
+    SPH_TRY(c.alloc(colk, m));
+    SPH_TRY(c.alloc(pval, 1));
+    SPH_TRY(c.alloc(amax, 1));
+    SPH_TRY(c.alloc(d_piv, 1));
+    SPH_TRY(c.alloc(d_err, 1));
+
+    // fixed-point scale: every term below 2^61 / (terms per entry)
+    SPH_CUDA_TRY(cudaMemsetAsync(amax, 0, sizeof(unsigned long long), st));
+    if (sizeof(Real) == 4)
+        k_coef_absmax<float><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.slice_off, c.ncnt, c.coef, n, amax);
+    else
+        k_coef_absmax<double><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.slice_off, c.ncnt, c.coef_d, n, amax);
+    unsigned long long hbits = 0;
+    SPH_CUDA_TRY(cudaMemcpyAsync(&hbits, amax, sizeof hbits, cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaStreamSynchronize(st));
+    double cmax = 0;
+    memcpy(&cmax, &hbits, sizeof cmax);
+    cmax = std::max(cmax, 1.0);   // Neumann weights and copy rows contribute <= 1
+    const double terms = (double)max_rows * (double)std::max(max_cnt, 64) + 1.0;
+    const double scale = std::ldexp(1.0, (int)std::floor(61.0 - std::log2(cmax) - std::log2(terms)));
+
+    const size_t shmem = sizeof(unsigned long long) * (size_t)m;
+    if (sizeof(Real) == 4) {
+        SPH_CUDA_TRY(cudaFuncSetAttribute(k_coarse_assemble<float, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)shmem));
+        k_coarse_assemble<float, Real><<<m, 256, shmem, st>>>(
+            m, c.cg_agg, c.cg_off, c.cg_rows, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, d_nm_idx,
+            c.L.nm_off, c.L.nm_nbr, c.nm_ow, ncomp > 0 ? c.comp_id : nullptr, c.diag, ncomp, scale, E, a_comp);
+    } else {
+        SPH_CUDA_TRY(cudaFuncSetAttribute(k_coarse_assemble<double, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)shmem));
+        k_coarse_assemble<double, Real><<<m, 256, shmem, st>>>(
+            m, c.cg_agg, c.cg_off, c.cg_rows, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef_d, d_nm_idx,
+            c.L.nm_off, c.L.nm_nbr, c.nm_ow, ncomp > 0 ? c.comp_id : nullptr, c.diag, ncomp, scale, E, a_comp);
+    }
+    SPH_CUDA_TRY(cudaGetLastError());
+    const long long mm = (long long)m * m;
+    if (ncomp > 0) {
+        k_coarse_rank_one<<<div_up(mm, 256), 256, 0, st>>>(E, a_comp, d_cnt_comp, c.comp_inv, m, ncomp);
+        SPH_CUDA_TRY(cudaGetLastError());
+    }
+    // E^-1
+    k_eye<<<div_up(mm, 256), 256, 0, st>>>(c.cg_inv, m);
+    SPH_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    for (int k = 0; k < m; ++k) {
+        k_gj_pivot<<<1, 1024, 0, st>>>(E, m, k, d_piv, pval, d_err);
+        k_gj_swap_scale<<<div_up(2LL * m, 256), 256, 0, st>>>(E, c.cg_inv, m, k, d_piv, pval, d_err);
+        k_gj_col<<<div_up(m, 256), 256, 0, st>>>(E, colk, m, k);
+        k_gj_elim<<<dim3(div_up(2LL * m, 256), m), 256, 0, st>>>(E, c.cg_inv, colk, m, k, d_err);
+    }
+    c.launches += 4LL * m + 6;
+    SPH_CUDA_TRY(cudaGetLastError());
+    int herr = 0;
+    SPH_CUDA_TRY(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaStreamSynchronize(st));
+    c.release(E); c.release(a_comp); c.release(colk); c.release(pval); c.release(amax);
+    c.release(d_piv); c.release(d_err); c.release(d_nm_idx); c.release(d_cnt_comp);
+    if (herr) {
+        set_error("coarse operator is singular");
+        return SPH_ERR_BREAKDOWN;
+    }
+    c.cg_m = m;
+    return SPH_OK;
+}
+
+template int coarse_build<float>(Ctx<float> &);
+template int coarse_build<double>(Ctx<double> &);
+template void coarse_apply<float, float>(Ctx<float> &, const float *, float *);
+template void coarse_apply<float, double>(Ctx<float> &, const double *, double *);
+template void coarse_apply<double, double>(Ctx<double> &, const double *, double *);
+
+}  // namespace sph

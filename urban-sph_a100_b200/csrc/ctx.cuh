@@ -124,6 +124,7 @@ struct Ctx {
     double *nm_w = nullptr;       // Neumann row weights (CSR aligned with nm_nbr)
     double *nm_gw = nullptr;      // mirror-row gradient weights
     double *nm_ow = nullptr;      // weights of the Neumann rows in the converged operator
+    float *nm_owf = nullptr;      // the same in FP32 (mixed form)
     float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
     double *coef_d = nullptr;     // cached c_ij, FP64 form
     bool coef_valid = false;
@@ -136,6 +137,13 @@ struct Ctx {
     double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
     float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
     sph_ppe_stats last_ppe = {};
+    // two-level preconditioner (coarse.cu), rebuilt with the lists
+    bool cg_valid = false;
+    int cg_block = 0, cg_m = 0;   // aggregate edge in cells, aggregates in use
+    int *cg_agg = nullptr;        // aggregate of each row, -1 for identity / pinned rows
+    int *cg_off = nullptr, *cg_rows = nullptr;   // rows of each aggregate, ascending
+    double *cg_inv = nullptr;     // E^-1, m x m
+    double *cg_s = nullptr, *cg_y = nullptr;     // restricted residual, coarse correction
     // live operator timing (sph_profile)
     bool prof = false;
     cudaEvent_t *prof_ev = nullptr;   // 512 events, created on first use
@@ -196,6 +204,8 @@ template <class Real> int nnps_export(Ctx<Real> &c, int32_t *g_idx, int32_t *p_i
 template <class Real> int neighbors_export(Ctx<Real> &c, int64_t *off, int32_t *list, int64_t *nnz);
 template <class Real> int phase_interaction(Ctx<Real> &c);
 template <class Real> int phase_ppe(Ctx<Real> &c, sph_ppe_stats *st);
+template <class Real> int coarse_build(Ctx<Real> &c);
+template <class Real, class V> void coarse_apply(Ctx<Real> &c, const V *r, V *z);
 template <class Real> int phase_time_update(Ctx<Real> &c);
 template <class Real> int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax);
 template <class Real> int gradient_correction(Ctx<Real> &c);

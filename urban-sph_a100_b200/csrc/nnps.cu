@@ -489,6 +489,7 @@ static inline float hdist(float xi, float yi, float zi, float xj, float yj, floa
 
 template <class Real, class T>
 static int upload_vec(Ctx<Real> &c, T *&dst, const std::vector<T> &v) {
+    c.release(dst);   // a rebuild replaces the previous list
     SPH_TRY(c.alloc(dst, v.size()));
     if (!v.empty()) SPH_CUDA_TRY(cudaMemcpyAsync(dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c.stream));
     return SPH_OK;
@@ -802,6 +803,10 @@ int build_side_lists(Ctx<Real> &c) {
     SPH_TRY(upload_vec(c, c.nm_w, w));
     SPH_TRY(upload_vec(c, c.nm_gw, gw));
     SPH_TRY(upload_vec(c, c.nm_ow, ow));
+    if (sizeof(Real) == 4) {
+        const std::vector<float> owf(ow.begin(), ow.end());
+        SPH_TRY(upload_vec(c, c.nm_owf, owf));
+    }
     const std::vector<int> nmflags = mir;
 
     // periodic partners, functions_BC.cuh:1041-1133
@@ -899,6 +904,7 @@ int build_side_lists(Ctx<Real> &c) {
         SPH_CUDA_TRY(cudaMemcpyAsync(c.row_kind, kind.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
         SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
     }
+    c.cg_valid = false;   // the coarse preconditioner follows the row kinds
     return SPH_OK;
 }
 

@@ -203,19 +203,20 @@ __global__ void __launch_bounds__(128) k_spmv(const int *__restrict__ kind, cons
 
 // per-component mean of x over the fluid rows of the singular components:
 // cmean[c] = (1/|u_c|) sum_{i in u_c} x_i, deterministic (block partials)
-template <class V>
+// (NC = 1 for the common single-component case, SPH_MAX_COMP otherwise)
+template <class V, int NC>
 __global__ void k_comp_mean(const int *comp_id, const V *x, int n, int ncomp, const double *inv, double *partials,
                             unsigned int *counter, double *cmean) {
-    double v[SPH_MAX_COMP];
+    double v[NC];
 #pragma unroll
-    for (int q = 0; q < SPH_MAX_COMP; ++q) v[q] = 0;
+    for (int q = 0; q < NC; ++q) v[q] = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int cc = comp_id[i];
 #pragma unroll
-        for (int q = 0; q < SPH_MAX_COMP; ++q)
+        for (int q = 0; q < NC; ++q)
             if (cc == q) v[q] += (double)x[i];
     }
-    reduce_finish<SPH_MAX_COMP>(v, partials, counter, [&](double *t) {
+    reduce_finish<NC>(v, partials, counter, [&](double *t) {
         for (int q = 0; q < ncomp; ++q) cmean[q] = t[q] * inv[q];
     });
 }
@@ -280,9 +281,9 @@ __global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restr
 // enter with the Shepard average over all fluid in range, so that corner
 // rows do not act as point Dirichlet anchors; the pass still writes p = 0.
 // One warp per row: the lanes read the row's CSR entries coalesced.
-template <class V>
+template <class V, class W>
 __global__ void __launch_bounds__(256) k_spmv_neumann(const int *__restrict__ rows, const int *__restrict__ off,
-                                                      const int *__restrict__ nb, const double *__restrict__ w,
+                                                      const int *__restrict__ nb, const W *__restrict__ w,
                                                       int nrows, const V *__restrict__ x, V *__restrict__ y) {
     const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(256) k_spmv_neumann(const int *__restrict__ ro
     const V xi = x[i];
     const int q0 = off[k], q1 = off[k + 1];
     double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
-    for (int q = q0 + lane; q < q1; q += 32) s += __ldcs(&w[q]) * (double)(xi - x[__ldcs(&nb[q])]);
+    for (int q = q0 + lane; q < q1; q += 32) s += (double)__ldcs(&w[q]) * (double)(xi - x[__ldcs(&nb[q])]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) y[i] = (q1 > q0) ? (V)s : xi;
@@ -480,8 +481,12 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
     double *cmean = c.scal + 40;
     if (c.n_comp > 0) {
         cid = c.comp_id;
-        k_comp_mean<V><<<red_grid(n), 256, 0, c.stream>>>(c.comp_id, x, n, c.n_comp, c.comp_inv, c.red,
-                                                          (unsigned int *)(c.scal + 32), cmean);
+        if (c.n_comp == 1)
+            k_comp_mean<V, 1><<<red_grid(n), 256, 0, c.stream>>>(c.comp_id, x, n, 1, c.comp_inv, c.red,
+                                                                 (unsigned int *)(c.scal + 32), cmean);
+        else
+            k_comp_mean<V, SPH_MAX_COMP><<<red_grid(n), 256, 0, c.stream>>>(c.comp_id, x, n, c.n_comp, c.comp_inv, c.red,
+                                                                            (unsigned int *)(c.scal + 32), cmean);
         ++c.launches;
     }
     if (cached) {
@@ -501,8 +506,15 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
         ++c.prof_pending;
     }
     if (c.L.n_nm > 0) {
-        k_spmv_neumann<V><<<div_up((long long)c.L.n_nm * 32, 256), 256, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr,
-                                                                                     c.nm_ow, c.L.n_nm, x, y);
+        const int gnm = div_up((long long)c.L.n_nm * 32, 256);
+        // FP32 weights in the FP32 applications of the mixed form; the FP64
+        // applications (true residuals) keep the FP64 weights
+        if (sizeof(Real) == 4 && sizeof(V) == 4)
+            k_spmv_neumann<V, float><<<gnm, 256, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.L.n_nm,
+                                                                x, y);
+        else
+            k_spmv_neumann<V, double><<<gnm, 256, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow, c.L.n_nm,
+                                                                 x, y);
         ++c.launches;
     }
 }
@@ -513,8 +525,15 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
     if (launches) *launches = c.prof_launches;
     if (total_ms) *total_ms = c.prof_ms;
     if (bytes) {
-        // per row: kind (4) + x_i + y_i + A_i (Real); per stored entry: index (4) + coefficient (Real)
-        *bytes = (double)c.n * (4.0 + 3.0 * sizeof(Real)) + (double)c.nnz * (4.0 + sizeof(Real));
+        // per row: kind and list length (4 + 4) + x_i + y_i (Real), with the
+        // rank-one term also component id (4) + A_i (Real); per slice of 32
+        // rows its offset (8); per stored entry: index (4) + coefficient
+        // (float in the mixed form, double in the FP64 form).  The gathers
+        // x_j are not counted: an ideal kernel serves them from L2.
+        const double R = (double)sizeof(Real);
+        double row = 8.0 + 2.0 * R;
+        if (c.n_comp > 0) row += 4.0 + R;
+        *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + (double)c.nnz * (4.0 + R);
     }
     if (reset) { c.prof_launches = 0; c.prof_ms = 0; }
     return SPH_OK;
@@ -556,9 +575,11 @@ static int bicgstab_v(Ctx<Real> &c, V *const *ws, V *x, const V *b, double bnorm
         const int check = 4;
         while (it < maxit) {
             k_p_update<V><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
+            coarse_apply<Real, V>(c, p, ph);
             apply_op<Real, V>(c, ph, v, cached);
             k_alpha<V><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
             k_s_update<V><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
+            coarse_apply<Real, V>(c, s, sh);
             apply_op<Real, V>(c, sh, t, cached);
             k_omega<V><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
             k_xr_update<V><<<G, 256, 0, st>>>(x, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
@@ -700,9 +721,11 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     const int check = 4;
     while (status != SPH_OK && it < maxit) {
         k_p_update<float><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
+        coarse_apply<Real, float>(c, p, ph);
         apply_op<Real, float>(c, ph, v, cached);
         k_alpha<float><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
         k_s_update<float><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
+        coarse_apply<Real, float>(c, s, sh);
         apply_op<Real, float>(c, sh, t, cached);
         k_omega<float><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
         k_xr_update<float><<<G, 256, 0, st>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
@@ -989,7 +1012,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     const int n = c.n;
     const Real tdt = (Real)c.dp.dt;
     const int mode = c.prm.ppe_mode;
-    const bool cached = c.prm.reserved[0] == 0;   // reserved[0] = 1 selects the matrix-free operator
+    const bool cached = c.prm.ppe_matrix_free == 0;
     sph_ppe_stats S{};
     SPH_TRY(ensure_ppe_ws(c));
     Real *b = c.kv[9];
@@ -1007,6 +1030,8 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     c.coef_valid = true;
+    if (mode != SPH_PPE_REF_SWEEP && mode != SPH_PPE_GMRES && (!c.cg_valid || c.cg_block != c.prm.ppe_coarse_block))
+        SPH_TRY(coarse_build(c));
 
     if (mode == SPH_PPE_REF_SWEEP) {
         Real *pout = c.kv[8];
@@ -1035,7 +1060,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
         int status = SPH_OK, iters = 0, restarts = 0, refinements = 0;
         double relres = 0;
-        const int m = std::max(4, std::min(GM_MAXV, c.prm.reserved[1] > 0 ? c.prm.reserved[1] : 40));
+        const int m = std::max(4, std::min(GM_MAXV, c.prm.ppe_gmres_restart > 0 ? c.prm.ppe_gmres_restart : 40));
         auto ws_r = [&]() -> GmresWs<Real, Real> * {
             if (!c.gm_ws_r) {
                 auto *w = new GmresWs<Real, Real>();
@@ -1077,7 +1102,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             if (trace) fprintf(stderr, "FP32 solve st %d it %d rel %.3e\n", status, iters, relres);
             k_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(c.xf, xd, n);
             ++c.launches;
-        } else if (c.prm.reserved[2] == 0) {
+        } else if (c.prm.ppe_refinement == 0) {
             // FP32 BiCGSTAB with FP64 reliable updates; FP64 BiCGSTAB from
             // its last iterate if the FP32 recurrence breaks down
             status = bicgstab_reliable(c, xd, bd, rd, bb, tol, maxit, cached, &iters, &relres, &refinements, &restarts);
@@ -1091,13 +1116,13 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             }
         } else {
             // FP32 Krylov corrections restarted at every refinement (BiCGSTAB
-            // with reserved[2] = 2, GMRES with reserved[2] = 1) inside FP64
+            // with ppe_refinement = 2, GMRES with ppe_refinement = 1) inside FP64
             // iterative refinement; the outer residual r = b - M x and the
             // update x += e are FP64
             float *ef = c.xf, *rf = c.bf;
             const double inner_tol = c.prm.ppe_inner_tol > 0 ? c.prm.ppe_inner_tol : 1e-3;
-            GmresWs<Real, Real> *w = c.prm.reserved[2] == 1 ? ws_r() : nullptr;
-            if (c.prm.reserved[2] == 1 && !w) return SPH_ERR_OUT_OF_MEMORY;
+            GmresWs<Real, Real> *w = c.prm.ppe_refinement == 1 ? ws_r() : nullptr;
+            if (c.prm.ppe_refinement == 1 && !w) return SPH_ERR_OUT_OF_MEMORY;
             status = SPH_NOT_CONVERGED;
             for (refinements = 0; refinements < 50; ++refinements) {
                 apply_op<Real, double>(c, xd, rd, cached);
@@ -1112,7 +1137,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
                 if (iters >= maxit) break;
                 int it_in = 0, rs_in = 0;
                 double rel_in = 0;
-                const int st_in = c.prm.reserved[2] == 1
+                const int st_in = c.prm.ppe_refinement == 1
                                       ? gmres<Real, Real>(c, *w, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters,
                                                           cached, &it_in, &rel_in)
                                       : bicgstab<Real>(c, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters, cached,

@@ -111,7 +111,11 @@ class SphParams(ctypes.Structure):
         ("ppe_tol", ctypes.c_double),
         ("ppe_pin", ctypes.c_int32),
         ("recompute_gc", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 14),
+        ("ppe_matrix_free", ctypes.c_int32),
+        ("ppe_gmres_restart", ctypes.c_int32),
+        ("ppe_refinement", ctypes.c_int32),
+        ("ppe_coarse_block", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 10),
         ("ppe_inner_tol", ctypes.c_double),
     ]
 
