@@ -122,6 +122,14 @@ def cpu_baseline(steps):
             "seconds": dt}
 
 
+def lib_sample_count(sim):
+    import ctypes
+    from sph_b200 import abi
+    cnt = ctypes.c_int64(0)
+    abi.lib().sph_ml_samples(sim.h, 0, 0, None, None, ctypes.byref(cnt))
+    return cnt.value
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -165,6 +173,9 @@ def main():
     ap.add_argument("--matrix-free", action="store_true")
     ap.add_argument("--coarse", type=int, default=5,
                     help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi)")
+    ap.add_argument("--warm", default="prev", choices=["prev", "extrap", "learned"],
+                    help="PPE start vector: previous pressure, linear extrapolation in time, or the learned "
+                         "per-particle network (trained on this run's warm-up solves)")
     ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres"],
                     help="mixed_ir form: FP64 reliable updates, or refinement restarting the FP32 solver")
     args = ap.parse_args()
@@ -195,11 +206,34 @@ def main():
         p.ppe_matrix_free = 1
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2}[args.refinement]
     p.ppe_coarse_block = args.coarse
+    p.ppe_warm_start = 1 if args.warm == "extrap" else 0
     n = len(P)
     sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
     sim.upload(P)
-    for _ in range(args.warmup):
-        sim.step(1)
+    learned = None
+    if args.warm == "learned":
+        # samples from the warm-up solves, then Adam on the GPU (not timed)
+        every = max(1, n // 250000)
+        sim.ml_collect(every)
+        wsteps = max(args.warmup, 8)
+        for _ in range(wsteps):
+            sim.step(1)
+        sim.ml_collect(0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = sim.ml_train(epochs=6, batch=4096, lr=1e-3, seed=20261203)
+        train_s = time.perf_counter() - t0
+        nsamp = int(lib_sample_count(sim))
+        q = p.copy()
+        q.ppe_mode = layout.PPE_LEARNED
+        sim.set_params(q)
+        learned = {"samples": nsamp, "warmup_steps_collected": wsteps, "every_kth_fluid_row": every,
+                   "train_s": train_s, "train_loss": loss, "epochs": 6, "batch": 4096}
+        for _ in range(2):
+            sim.step(1)
+    else:
+        for _ in range(args.warmup):
+            sim.step(1)
 
     # ---- device-timed region ----
     clocks = Clocks(local)
@@ -216,7 +250,7 @@ def main():
     e0.record()
     for _ in range(args.steps):
         s = sim.step(1)
-        stats.append((s.iterations, s.refinements, s.rel_residual, s.solve_ms, s.status))
+        stats.append((s.iterations, s.refinements, s.rel_residual, s.solve_ms, s.status, s.initial_residual))
         phases.append(sim.phase_ms().copy())
     e1.record()
     torch.cuda.synchronize()
@@ -320,6 +354,8 @@ def main():
                    "ppe": args.mode, "ppe_tol": 1e-6,
                    "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
                    "ppe_refinement": args.refinement,
+                   "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",
+                                        "learned": "learned per-particle MLP on the previous pressure"}[args.warm],
                    "ppe_preconditioner": f"jacobi + coarse aggregates of {args.coarse}^3 cells" if args.coarse > 0
                    else "jacobi",
                    "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
@@ -331,6 +367,7 @@ def main():
                 "refinements_mean": statistics.mean(s[1] for s in stats),
                 "rel_residual_max": max(s[2] for s in stats),
                 "solve_ms_mean": statistics.mean(s[3] for s in stats),
+                "initial_residual_mean": statistics.mean(s[5] for s in stats),
                 "not_converged_steps": sum(1 for s in stats if s[4] != 0)},
         "phase_ms": {"interaction": float(ph[1]), "ppe": float(ph[2]), "time_update": float(ph[3])},
         "roofline": {"bound": "hbm", "kernel": "PPE operator (k_spmv, cached c_ij)" if not args.matrix_free
@@ -340,6 +377,7 @@ def main():
                      "algorithmic_bytes_per_launch": op_bytes, "launch_ms": per_launch_ms, "launches": op_n},
         "plain_fp64": fp64,
         "fp64_same_preconditioner": fp64_same,
+        "learned_warm_start": learned,
         "reference_step_semantics": sweep,
         "clocks": ck,
     }

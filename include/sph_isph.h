@@ -166,7 +166,10 @@ typedef struct sph_params {
     int32_t ppe_coarse_block;    /* BiCGSTAB preconditioner: 0 Jacobi; B > 0
                                 adds a coarse correction on aggregates of
                                 B x B x B NNPS cells (additive two-level)      */
-    int32_t reserved[10];
+    int32_t ppe_warm_start;  /* start vector of the converged solves: 0 previous
+                                pressure; 1 linear extrapolation in time,
+                                2 p_n - p_(n-1), once two solutions exist     */
+    int32_t reserved[9];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
 } sph_params;
@@ -179,6 +182,7 @@ typedef struct sph_ppe_stats {
     int32_t restarts;        /* breakdown restarts                             */
     double  rel_residual;    /* final ||b-Ap||_2/||b||_2, FP64                 */
     double  solve_ms;        /* device time from rhs ready to convergence      */
+    double  initial_residual;    /* ||b-Ap0||_2/||b||_2 of the start vector p0 */
 } sph_ppe_stats;
 
 typedef struct sph_ctx sph_ctx;
@@ -272,6 +276,40 @@ int64_t sph_launch_count(sph_ctx *ctx);
  * `reset` clears the counters after reading. */
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
+
+/* ---- learned warm start of the pressure solve -----------------------------
+ * No counterpart in the reference (it runs one pressure sweep per step).  A
+ * per-particle MLP, 20 features -> 64 -> 64 -> 1 with ReLU, predicts the
+ * pressure change of the step; in SPH_PPE_LEARNED the Krylov solve starts
+ * from p_old + prediction and still runs to ppe_tol.  Features per fluid
+ * row (BF16, stored 32 per row, columns 20..31 zero): with r = b - M p_old
+ * on the fluid rows and d = r / A_i, the scaled d_i, r_i, b_i, p_i - mean p,
+ * then for each of those four: the c_ij/A_i-weighted neighbour mean, the
+ * weighted mean absolute deviation, the neighbour max and min.  Scales are
+ * the RMS values over the fluid rows; the target is (p_new - p_old) / RMS(d).
+ * Parameters (SPH_ML_NPARAM floats): W1[20][64], b1[64], W2[64][64], b2[64],
+ * w3[64], b3.  Inference: tensor cores (BF16 operands, FP32 accumulation);
+ * training: FP32 forward/backward and Adam on the GPU. */
+#define SPH_ML_NFEAT   20
+#define SPH_ML_NPARAM  5569
+/* Collect training samples from every later converged solve: every `every`-th
+ * fluid row (offset rotating per step), features and target; 0 stops.  At
+ * most 2^21 samples are kept. */
+int sph_ml_collect(sph_ctx *ctx, int every);
+/* Copies samples [first, first+rows) to host (X: rows x 32 BF16 bit
+ * patterns, target: rows floats; either may be NULL) and the count. */
+int sph_ml_samples(sph_ctx *ctx, int64_t first, int64_t rows, uint16_t *X, float *target, int64_t *count);
+/* Adam on the collected samples (mini-batches of `batch`, `epochs` passes,
+ * learning rate `lr`, shuffling and initial weights from `seed` unless
+ * weights were set); *final_loss = mean squared error on up to 65536 samples. */
+int sph_ml_train(sph_ctx *ctx, int epochs, int batch, float lr, uint64_t seed, float *final_loss);
+int sph_ml_set_weights(sph_ctx *ctx, const float *w);
+int sph_ml_get_weights(sph_ctx *ctx, float *w);
+/* Mean squared error and its gradient (FP32, SPH_ML_NPARAM floats) over
+ * samples [first, first+rows), with the current weights. */
+int sph_ml_grad(sph_ctx *ctx, int64_t first, int32_t rows, float *loss, float *grad);
+/* Tensor-core predictions for samples [first, first+rows). */
+int sph_ml_predict_samples(sph_ctx *ctx, int64_t first, int32_t rows, float *y);
 
 /* ---- cell sort without device allocation --------------------------------
  * No counterpart in the reference: an addition for callers that cannot call

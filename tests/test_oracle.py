@@ -214,3 +214,27 @@ def test_oracle_fp32_vs_fp64_one_sweep_close():
     for f in ("ux", "uy", "uz", "pres"):
         err = np.abs(a[f].astype(np.float64) - b[f]).max() / np.abs(b[f]).max()
         assert err < 1e-3, (f, err)
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    # the CPU restatement of the warm-start network that checks the GPU
+    # training kernels is itself checked against central differences
+    import mlp
+    rng = np.random.default_rng(3)
+    w = rng.normal(size=mlp.NPARAM) * 0.1
+    X = rng.normal(size=(40, 32))
+    t = rng.normal(size=40)
+    _, g = mlp.loss_and_grad(w, X, t)
+    eps = 1e-6
+    for i in rng.choice(mlp.NPARAM, 25, replace=False):
+        wp, wm = w.copy(), w.copy()
+        wp[i] += eps
+        wm[i] -= eps
+        fd = (mlp.loss_and_grad(wp, X, t)[0] - mlp.loss_and_grad(wm, X, t)[0]) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
+
+
+def test_bf16_rounding_of_the_oracle():
+    import mlp
+    x = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 0.0], np.float32)
+    assert np.array_equal(mlp.round_bf16(x), np.array([1.0, 1.0, 1.0078125, -3.140625, 0.0], np.float32))

@@ -401,3 +401,45 @@ int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double
     return DISPATCH(ctx, operator_stats(*ctx->f, launches, total_ms, bytes_per_launch, reset),
                     operator_stats(*ctx->d, launches, total_ms, bytes_per_launch, reset));
 }
+
+// ---- learned warm start (learned.cu) ------------------------------------------
+int sph_ml_collect(sph_ctx *ctx, int every) {
+    if (!ctx || every < 0) return SPH_ERR_BAD_ARG;
+    auto go = [&](auto *c) { c->ml_every = every; return SPH_OK; };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
+}
+
+int sph_ml_samples(sph_ctx *ctx, int64_t first, int64_t rows, uint16_t *X, float *target, int64_t *count) {
+    if (!ctx) return SPH_ERR_BAD_ARG;
+    long long cnt = 0;
+    const int st = DISPATCH(ctx, ml_samples(*ctx->f, first, rows, X, target, &cnt),
+                            ml_samples(*ctx->d, first, rows, X, target, &cnt));
+    if (count) *count = cnt;
+    return st;
+}
+
+int sph_ml_train(sph_ctx *ctx, int epochs, int batch, float lr, uint64_t seed, float *final_loss) {
+    if (!ctx || !(lr > 0)) return SPH_ERR_BAD_ARG;
+    return DISPATCH(ctx, ml_train(*ctx->f, epochs, batch, lr, (unsigned long long)seed, final_loss),
+                    ml_train(*ctx->d, epochs, batch, lr, (unsigned long long)seed, final_loss));
+}
+
+int sph_ml_set_weights(sph_ctx *ctx, const float *w) {
+    if (!ctx || !w) return SPH_ERR_BAD_ARG;
+    return DISPATCH(ctx, ml_set_weights(*ctx->f, w), ml_set_weights(*ctx->d, w));
+}
+
+int sph_ml_get_weights(sph_ctx *ctx, float *w) {
+    if (!ctx || !w) return SPH_ERR_BAD_ARG;
+    return DISPATCH(ctx, ml_get_weights(*ctx->f, w), ml_get_weights(*ctx->d, w));
+}
+
+int sph_ml_grad(sph_ctx *ctx, int64_t first, int32_t rows, float *loss, float *grad) {
+    if (!ctx) return SPH_ERR_BAD_ARG;
+    return DISPATCH(ctx, ml_grad(*ctx->f, first, rows, loss, grad), ml_grad(*ctx->d, first, rows, loss, grad));
+}
+
+int sph_ml_predict_samples(sph_ctx *ctx, int64_t first, int32_t rows, float *y) {
+    if (!ctx || !y) return SPH_ERR_BAD_ARG;
+    return DISPATCH(ctx, ml_predict_samples(*ctx->f, first, rows, y), ml_predict_samples(*ctx->d, first, rows, y));
+}

@@ -2,6 +2,7 @@
 // NNPS structures, neighbour lists and PPE workspace.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -137,6 +138,7 @@ struct Ctx {
     double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
     float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
     sph_ppe_stats last_ppe = {};
+    double init_relres = -1;      // residual of the start vector of the current solve
     // two-level preconditioner (coarse.cu), rebuilt with the lists
     bool cg_valid = false;
     int cg_block = 0, cg_m = 0;   // aggregate edge in cells, aggregates in use
@@ -154,7 +156,25 @@ struct Ctx {
     double *red_host = nullptr;   // pinned
     int red_blocks = 0;
     double *scal = nullptr;       // device scalars
-    float *ml_w = nullptr;        // learned warm-start weights
+    // learned warm start (learned.cu)
+    int ml_every = 0;             // sample every k-th fluid row of each converged solve (0: off)
+    bool ml_ready = false, ml_init = false;
+    float *ml_w = nullptr, *ml_m = nullptr, *ml_v = nullptr, *ml_grad = nullptr;   // FP32 parameters, Adam moments
+    __nv_bfloat16 *ml_w1b = nullptr, *ml_w2b = nullptr;   // BF16 B operands of the tensor-core inference
+    double *ml_sc = nullptr, *ml_red = nullptr;           // feature scales, reduction partials
+    unsigned int *ml_cnt = nullptr;
+    __nv_bfloat16 *ml_X = nullptr;                        // features of the step (n x 32)
+    float *ml_y = nullptr, *ml_pold = nullptr, *ml_rr = nullptr, *ml_dd = nullptr;
+    float *ml_pprev = nullptr;                            // p_old of the previous step
+    bool ml_have_prev = false;
+    double *ml_zd = nullptr, *ml_wd = nullptr;            // predicted change and its image
+    __nv_bfloat16 *ml_SX = nullptr;                       // collected samples
+    float *ml_St = nullptr;
+    long long ml_cap = 0, ml_count = 0;
+    int *ml_fluid = nullptr;
+    int ml_nfluid = 0, ml_phase = 0;
+    float *ml_part = nullptr, *ml_lpart = nullptr;        // per-block gradient / loss partials
+    int ml_part_cap = 0;
     R4 *sc_u = nullptr;           // pass scratch
     Real *sc_p = nullptr, *sc_t = nullptr;
 
@@ -205,6 +225,18 @@ template <class Real> int neighbors_export(Ctx<Real> &c, int64_t *off, int32_t *
 template <class Real> int phase_interaction(Ctx<Real> &c);
 template <class Real> int phase_ppe(Ctx<Real> &c, sph_ppe_stats *st);
 template <class Real> int coarse_build(Ctx<Real> &c);
+template <class Real> int ml_prepare(Ctx<Real> &c, const Real *b, bool features);
+template <class Real> int ml_extrapolate(Ctx<Real> &c, double *x);
+template <class Real> int ml_warm_start(Ctx<Real> &c, const double *b, double *x, double *tmp);
+template <class Real> int ml_finish_step(Ctx<Real> &c);
+template <class Real> void ppe_apply_fp64(Ctx<Real> &c, const double *x, double *y);
+template <class Real> int ml_collect(Ctx<Real> &c, const double *xnew);
+template <class Real> int ml_grad(Ctx<Real> &c, long long first, int rows, float *loss, float *grad);
+template <class Real> int ml_train(Ctx<Real> &c, int epochs, int batch, float lr, unsigned long long seed, float *loss);
+template <class Real> int ml_set_weights(Ctx<Real> &c, const float *w);
+template <class Real> int ml_get_weights(Ctx<Real> &c, float *w);
+template <class Real> int ml_samples(Ctx<Real> &c, long long first, long long rows, uint16_t *X, float *t, long long *count);
+template <class Real> int ml_predict_samples(Ctx<Real> &c, long long first, int rows, float *y);
 template <class Real, class V> void coarse_apply(Ctx<Real> &c, const V *r, V *z);
 template <class Real> int phase_time_update(Ctx<Real> &c);
 template <class Real> int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax);

@@ -25,7 +25,7 @@ namespace sph {
 // ---- device scalars of the Krylov solver -----------------------------------
 enum {
     SC_RHO = 0, SC_ALPHA, SC_OMEGA, SC_BETA, SC_RR, SC_BB, SC_RV, SC_TS, SC_TT, SC_FLAG, SC_TOL2,
-    SC_RHO_NEW, SC_COUNT
+    SC_RHO_NEW, SC_ITN, SC_COUNT
 };
 enum { FLAG_RUN = 0, FLAG_CONVERGED = 1, FLAG_BREAKDOWN = 2 };
 
@@ -366,6 +366,7 @@ __global__ void k_xr_update(V *x, V *r, const V *ph, const V *sh, const V *s, co
     reduce_finish<2>(d, partials, counter, [&](double *tt) {
         const double rho_new = tt[0];
         scal[SC_RR] = tt[1];
+        scal[SC_ITN] += 1.0;   // iterations that ran (the kernels idle once the flag is set)
         if (tt[1] <= scal[SC_TOL2]) scal[SC_FLAG] = FLAG_CONVERGED;
         else if (rho_new == 0.0 || scal[SC_OMEGA] == 0.0 || !isfinite(tt[1])) scal[SC_FLAG] = FLAG_BREAKDOWN;
         scal[SC_BETA] = (rho_new / scal[SC_RHO]) * (scal[SC_ALPHA] / scal[SC_OMEGA]);
@@ -519,6 +520,12 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
     }
 }
 
+// y = M x with FP64 vectors and the context's cached or matrix-free operator
+template <class Real>
+void ppe_apply_fp64(Ctx<Real> &c, const double *x, double *y) {
+    apply_op<Real, double>(c, x, y, c.prm.ppe_matrix_free == 0);
+}
+
 template <class Real>
 int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *bytes, int reset) {
     prof_drain(c);
@@ -553,6 +560,7 @@ static int bicgstab_v(Ctx<Real> &c, V *const *ws, V *x, const V *b, double bnorm
     unsigned int *counter = (unsigned int *)(c.scal + 32);
     const double tol2 = tol * tol * bnorm2;
     k_dinv<V, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
+    SPH_CUDA_TRY(cudaMemsetAsync(c.scal + SC_ITN, 0, sizeof(double), st));
     ++c.launches;
     int it = 0;
     *restarts = 0;
@@ -566,6 +574,7 @@ static int bicgstab_v(Ctx<Real> &c, V *const *ws, V *x, const V *b, double bnorm
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
         const double rr0 = c.red_host[SC_RR];
         *relres = std::sqrt(rr0 / bnorm2);
+        if (c.init_relres < 0) c.init_relres = *relres;
         if (rr0 <= tol2) { status = SPH_OK; break; }
         if (it >= maxit) break;
         if (getenv("SPH_TRACE_PPE")) fprintf(stderr, "  bicgstab start it %d relres %.3e\n", it, *relres);
@@ -605,7 +614,7 @@ static int bicgstab_v(Ctx<Real> &c, V *const *ws, V *x, const V *b, double bnorm
         break;   // iteration limit
     }
     SPH_CUDA_TRY(cudaGetLastError());
-    *iters = it;
+    *iters = it > 0 ? (int)c.red_host[SC_ITN] : 0;   // exact, not rounded up to the check interval
     return status;
 }
 
@@ -685,6 +694,7 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     const bool trace = getenv("SPH_TRACE_PPE") != nullptr;
     k_dinv<float, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
     SPH_CUDA_TRY(cudaMemsetAsync(xlo, 0, sizeof(float) * n, st));
+    SPH_CUDA_TRY(cudaMemsetAsync(c.scal + SC_ITN, 0, sizeof(double), st));
     ++c.launches;
     *restarts = 0;
     *updates = 0;
@@ -717,6 +727,8 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     double rr = c.red_host[SC_RR];
     double maxrr = rr;
     *relres = std::sqrt(rr / bnorm2);
+    if (c.init_relres < 0) c.init_relres = *relres;
+    if (trace) fprintf(stderr, "RU start relres %.3e\n", *relres);
     if (rr <= tol2) status = SPH_OK;
     const int check = 4;
     while (status != SPH_OK && it < maxit) {
@@ -761,7 +773,7 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     }
     if (status != SPH_OK && it > 0 && *updates == 0) *relres = std::sqrt(rr / bnorm2);
     SPH_CUDA_TRY(cudaGetLastError());
-    *iters = it;
+    *iters = it > 0 ? (int)c.red_host[SC_ITN] : 0;   // exact, not rounded up to the check interval
     return status;
 }
 
@@ -903,6 +915,7 @@ static int gmres(Ctx<Real> &c, GmresWs<Real, V> &ws, V *x, const V *b, double bn
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
         const double beta = std::sqrt(hh[0]);
         *relres = beta / bn;
+        if (c.init_relres < 0) c.init_relres = *relres;
         if (trace) fprintf(stderr, "  gmres restart it %d relres %.3e\n", it, *relres);
         if (*relres <= tol) { status = SPH_OK; break; }
         if (it >= maxit || !(beta > 0) || !std::isfinite(beta)) break;
@@ -1056,6 +1069,15 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
         double bb = c.red_host[SC_BB];
         if (!(bb > 0)) bb = 1.0;
+        // learned warm start: x0 = p_old + s_d * net(features); the features
+        // are also what the sample collection stores
+        c.init_relres = -1;
+        const bool learned = mode == SPH_PPE_LEARNED && c.ml_ready;
+        const bool extrap = c.prm.ppe_warm_start == 1;
+        const bool history = learned || c.ml_every > 0 || extrap;
+        if (history) SPH_TRY(ml_prepare(c, (const Real *)b, learned || c.ml_every > 0));
+        if (extrap) SPH_TRY(ml_extrapolate(c, xd));
+        if (learned) SPH_TRY(ml_warm_start(c, bd, xd, rd));
         const double tol = c.prm.ppe_tol > 0 ? c.prm.ppe_tol : 1e-6;
         const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
         int status = SPH_OK, iters = 0, restarts = 0, refinements = 0;
@@ -1162,6 +1184,8 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
                 ++c.launches;
             }
         }
+        if (c.ml_every > 0 && status == SPH_OK) SPH_TRY(ml_collect(c, xd));
+        if (history) SPH_TRY(ml_finish_step(c));
         k_cast<double, Real><<<grid_for(n, 256), 256, 0, st>>>(xd, c.S.p, n);
         ++c.launches;
         S.status = status;
@@ -1169,6 +1193,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         S.refinements = refinements;
         S.restarts = restarts;
         S.rel_residual = relres;
+        S.initial_residual = c.init_relres;
     }
     SPH_CUDA_TRY(cudaEventRecord(c.ev[5], st));
     SPH_TRY(neumann_pass(c, c.S));
@@ -1193,7 +1218,8 @@ void release_solver_ws(Ctx<Real> &c) {
 
 #define INST(R) template int phase_ppe<R>(Ctx<R> &, sph_ppe_stats *); \
     template void release_solver_ws<R>(Ctx<R> &); \
-    template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int);
+    template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int); \
+    template void ppe_apply_fp64<R>(Ctx<R> &, const double *, double *);
 INST(float)
 INST(double)
 #undef INST

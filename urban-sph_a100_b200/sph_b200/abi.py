@@ -14,6 +14,8 @@ import numpy as np
 
 from .layout import PART1, PART2, PART3, PpeStats, SphParams
 
+ML_NPARAM = 5569   # SPH_ML_NPARAM
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libsph_b200.so")
 
@@ -24,6 +26,8 @@ SYMBOLS = (
     "sph_neighbors_export", "sph_interaction", "sph_ppe", "sph_time_update", "sph_step",
     "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_status_string",
     "sph_last_error", "sph_profile", "sph_operator_stats", "sph_nnps_sort_noalloc",
+    "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
+    "sph_ml_grad", "sph_ml_predict_samples",
 )
 
 _lib = None
@@ -73,6 +77,14 @@ def lib():
         L.sph_operator_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double), i32]
         L.sph_nnps_sort_noalloc.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        f32p = ctypes.POINTER(ctypes.c_float)
+        L.sph_ml_collect.argtypes = [vp, i32]
+        L.sph_ml_samples.argtypes = [vp, i64, i64, vp, vp, ctypes.POINTER(i64)]
+        L.sph_ml_train.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_uint64, f32p]
+        L.sph_ml_set_weights.argtypes = [vp, vp]
+        L.sph_ml_get_weights.argtypes = [vp, vp]
+        L.sph_ml_grad.argtypes = [vp, i64, i32, f32p, vp]
+        L.sph_ml_predict_samples.argtypes = [vp, i64, i32, vp]
         _lib = L
     return _lib
 
@@ -197,6 +209,47 @@ class Simulation:
 
     def profile(self, enable=True):
         _check("sph_profile", lib().sph_profile(self.h, 1 if enable else 0))
+
+    # ---- learned warm start ----
+    def ml_collect(self, every):
+        _check("sph_ml_collect", lib().sph_ml_collect(self.h, int(every)))
+
+    def ml_samples(self, first=0, rows=None):
+        cnt = ctypes.c_int64(0)
+        _check("sph_ml_samples", lib().sph_ml_samples(self.h, 0, 0, None, None, ctypes.byref(cnt)))
+        rows = cnt.value - first if rows is None else rows
+        X = np.zeros((rows, 32), np.uint16)
+        t = np.zeros(rows, np.float32)
+        if rows > 0:
+            _check("sph_ml_samples", lib().sph_ml_samples(self.h, first, rows, _p(X), _p(t), ctypes.byref(cnt)))
+        return X, t
+
+    def ml_train(self, epochs, batch, lr, seed=0):
+        loss = ctypes.c_float(0)
+        _check("sph_ml_train", lib().sph_ml_train(self.h, int(epochs), int(batch), float(lr), int(seed),
+                                                  ctypes.byref(loss)))
+        return loss.value
+
+    def ml_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == ML_NPARAM
+        _check("sph_ml_set_weights", lib().sph_ml_set_weights(self.h, _p(w)))
+
+    def ml_get_weights(self):
+        w = np.zeros(ML_NPARAM, np.float32)
+        _check("sph_ml_get_weights", lib().sph_ml_get_weights(self.h, _p(w)))
+        return w
+
+    def ml_grad(self, first, rows):
+        loss = ctypes.c_float(0)
+        g = np.zeros(ML_NPARAM, np.float32)
+        _check("sph_ml_grad", lib().sph_ml_grad(self.h, int(first), int(rows), ctypes.byref(loss), _p(g)))
+        return loss.value, g
+
+    def ml_predict_samples(self, first, rows):
+        y = np.zeros(rows, np.float32)
+        _check("sph_ml_predict_samples", lib().sph_ml_predict_samples(self.h, int(first), int(rows), _p(y)))
+        return y
 
     def operator_stats(self, reset=True):
         n = ctypes.c_int64(0)

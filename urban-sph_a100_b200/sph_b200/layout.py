@@ -115,7 +115,8 @@ class SphParams(ctypes.Structure):
         ("ppe_gmres_restart", ctypes.c_int32),
         ("ppe_refinement", ctypes.c_int32),
         ("ppe_coarse_block", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 10),
+        ("ppe_warm_start", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 9),
         ("ppe_inner_tol", ctypes.c_double),
     ]
 
@@ -143,6 +144,7 @@ class PpeStats(ctypes.Structure):
         ("status", ctypes.c_int32), ("iterations", ctypes.c_int32),
         ("refinements", ctypes.c_int32), ("restarts", ctypes.c_int32),
         ("rel_residual", ctypes.c_double), ("solve_ms", ctypes.c_double),
+        ("initial_residual", ctypes.c_double),
     ]
 
 
