@@ -169,9 +169,13 @@ typedef struct sph_params {
     int32_t ppe_warm_start;  /* start vector of the converged solves: 0 previous
                                 pressure; 1 linear extrapolation in time,
                                 2 p_n - p_(n-1), once two solutions exist     */
-    int32_t reserved[9];
+    int32_t apr_max_level;   /* APR (vii[35] = 1, every vii[37] steps): target
+                                level log8(m_ref/m) of fluid near IBM markers */
+    int32_t reserved[8];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
+    double  apr_zone;        /* APR: distance from an IBM marker's cell within
+                                which fluid targets apr_max_level [m]          */
 } sph_params;
 
 typedef struct sph_ppe_stats {
@@ -277,6 +281,17 @@ int64_t sph_launch_count(sph_ctx *ctx);
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
 
+/* ---- adaptive particle refinement ----------------------------------------
+ * One 3-D splitting pass (functions_APR.cuh:270-652, cell-based APR, which the
+ * shipped reference does not compile): every cell splits the first fluid
+ * particle whose target level exceeds its level log8(m_ref/m) by >= 0.75
+ * into eight children (m/8, vol/8, h/2 with vii[36]) written into free
+ * dummy records (i_type 3) the deck reserves; the parent becomes a dummy.
+ * Runs by itself every vii[37] steps when vii[35] = 1.  *n_split: cells
+ * split; *n_wanted: cells that asked (more than the free records allow when
+ * larger).  The next step rebuilds NNPS and the operators. */
+int sph_apr(sph_ctx *ctx, int32_t *n_split, int32_t *n_wanted);
+
 /* ---- learned warm start of the pressure solve -----------------------------
  * No counterpart in the reference (it runs one pressure sweep per step).  A
  * per-particle MLP, 20 features -> 64 -> 64 -> 1 with ReLU, predicts the
@@ -310,6 +325,30 @@ int sph_ml_get_weights(sph_ctx *ctx, float *w);
 int sph_ml_grad(sph_ctx *ctx, int64_t first, int32_t rows, float *loss, float *grad);
 /* Tensor-core predictions for samples [first, first+rows). */
 int sph_ml_predict_samples(sph_ctx *ctx, int64_t first, int32_t rows, float *y);
+
+/* ---- ensembles of independent cases ---------------------------------------
+ * No counterpart in the reference (one case per run there).  A batch holds
+ * one context per case, each on its own non-blocking stream of `device`;
+ * sph_batch_step advances every case by nsteps with a pool of host workers
+ * that take cases largest first, so the kernels of many small cases run on
+ * the GPU side by side.  Results are those of stepping each case alone. */
+typedef struct sph_batch sph_batch;
+/* P1[k] holds n[k] records of case k, params[k] its parameters (after
+ * sph_domain_setup). */
+int sph_batch_create(int ncase, const sph_params *params, const sph_part1 *const *P1, const int32_t *n, int precision,
+                     int device, sph_batch **out);
+void sph_batch_destroy(sph_batch *b);
+/* nsteps steps of every case; stats[k] (may be NULL) gets case k's last PPE
+ * statistics.  Returns the most severe status over the cases. */
+int sph_batch_step(sph_batch *b, int nsteps, sph_ppe_stats *stats);
+/* Cases in flight at once (0: all).  sph_batch_autotune times probe_steps
+ * steps of every case at 1, 2, 4, ... and all workers, keeps the fastest and
+ * reports it (the probe steps advance the cases). */
+int sph_batch_set_workers(sph_batch *b, int workers);
+int sph_batch_autotune(sph_batch *b, int probe_steps, int *workers, double *ms_per_step);
+/* The context of case k (owned by the batch), e.g. for sph_download. */
+int sph_batch_case(sph_batch *b, int k, sph_ctx **ctx);
+int64_t sph_batch_particles(sph_batch *b);
 
 /* ---- cell sort without device allocation --------------------------------
  * No counterpart in the reference: an addition for callers that cannot call

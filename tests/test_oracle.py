@@ -108,7 +108,7 @@ def test_most_newton_branch_vs_reference():
 def test_oracle_matches_golden_fixture():
     g = np.load(GOLDEN)
     P = g["deck"].view(layout.PART1)
-    p = layout.SphParams.from_buffer_copy(g["params"].tobytes())
+    p = layout.params_from_bytes(g["params"].tobytes())
     O = restated.Restated(P, p, 0)
     O.nnps()
     og, op, os_, oe = O.export_nnps()
@@ -127,7 +127,7 @@ def test_golden_fixture_matches_reference_when_present():
         pytest.skip("reference host build absent")
     g = np.load(GOLDEN)
     P = g["deck"].view(layout.PART1)
-    p = layout.SphParams.from_buffer_copy(g["params"].tobytes())
+    p = layout.params_from_bytes(g["params"].tobytes())
     R = refhost.RefHost(P, p, parallel=False)
     R.step(2)
     for k in g.files:

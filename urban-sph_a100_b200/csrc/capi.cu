@@ -443,3 +443,16 @@ int sph_ml_predict_samples(sph_ctx *ctx, int64_t first, int32_t rows, float *y) 
     if (!ctx || !y) return SPH_ERR_BAD_ARG;
     return DISPATCH(ctx, ml_predict_samples(*ctx->f, first, rows, y), ml_predict_samples(*ctx->d, first, rows, y));
 }
+
+int sph_apr(sph_ctx *ctx, int32_t *n_split, int32_t *n_wanted) {
+    if (!ctx) return SPH_ERR_BAD_ARG;
+    int a = 0, b = 0;
+    auto go = [&](auto *c) -> int {
+        SPH_TRY(ensure_built(*c));
+        return apr_split(*c, &a, &b);
+    };
+    const int st = DISPATCH(ctx, go(ctx->f), go(ctx->d));
+    if (n_split) *n_split = a;
+    if (n_wanted) *n_wanted = b;
+    return st;
+}

@@ -225,6 +225,7 @@ template <class Real> int neighbors_export(Ctx<Real> &c, int64_t *off, int32_t *
 template <class Real> int phase_interaction(Ctx<Real> &c);
 template <class Real> int phase_ppe(Ctx<Real> &c, sph_ppe_stats *st);
 template <class Real> int coarse_build(Ctx<Real> &c);
+template <class Real> int apr_split(Ctx<Real> &c, int *n_split, int *n_wanted);
 template <class Real> int ml_prepare(Ctx<Real> &c, const Real *b, bool features);
 template <class Real> int ml_extrapolate(Ctx<Real> &c, double *x);
 template <class Real> int ml_warm_start(Ctx<Real> &c, const double *b, double *x, double *tmp);

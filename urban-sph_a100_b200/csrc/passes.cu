@@ -933,6 +933,10 @@ int phase_time_update(Ctx<Real> &c) {
     SPH_CUDA_TRY(cudaGetLastError());
     c.time = c.time + c.dp.dt;
     c.count += 1;
+    // APR every freq_apr steps (vii[35] = 1: cell-based)
+    const int freq_apr = c.prm.vii[SPH_VII_FREQ_APR];
+    if (c.prm.vii[SPH_VII_APR_SOLV] == 1 && freq_apr > 0 && c.count % freq_apr == 0)
+        SPH_TRY(apr_split(c, nullptr, nullptr));
     return SPH_OK;
 }
 

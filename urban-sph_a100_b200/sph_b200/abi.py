@@ -28,6 +28,8 @@ SYMBOLS = (
     "sph_last_error", "sph_profile", "sph_operator_stats", "sph_nnps_sort_noalloc",
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
+    "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
+    "sph_batch_case", "sph_batch_particles", "sph_apr",
 )
 
 _lib = None
@@ -85,6 +87,16 @@ def lib():
         L.sph_ml_get_weights.argtypes = [vp, vp]
         L.sph_ml_grad.argtypes = [vp, i64, i32, f32p, vp]
         L.sph_ml_predict_samples.argtypes = [vp, i64, i32, vp]
+        L.sph_batch_create.argtypes = [i32, vp, vp, vp, i32, i32, ctypes.POINTER(vp)]
+        L.sph_batch_destroy.argtypes = [vp]
+        L.sph_batch_destroy.restype = None
+        L.sph_batch_step.argtypes = [vp, i32, vp]
+        L.sph_batch_set_workers.argtypes = [vp, i32]
+        L.sph_batch_autotune.argtypes = [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]
+        L.sph_batch_case.argtypes = [vp, i32, ctypes.POINTER(vp)]
+        L.sph_batch_particles.argtypes = [vp]
+        L.sph_batch_particles.restype = i64
+        L.sph_apr.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
         _lib = L
     return _lib
 
@@ -210,6 +222,11 @@ class Simulation:
     def profile(self, enable=True):
         _check("sph_profile", lib().sph_profile(self.h, 1 if enable else 0))
 
+    def apr(self):
+        a, b = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check("sph_apr", lib().sph_apr(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     # ---- learned warm start ----
     def ml_collect(self, every):
         _check("sph_ml_collect", lib().sph_ml_collect(self.h, int(every)))
@@ -258,3 +275,52 @@ class Simulation:
         _check("sph_operator_stats", lib().sph_operator_stats(self.h, ctypes.byref(n), ctypes.byref(ms),
                                                               ctypes.byref(by), 1 if reset else 0))
         return n.value, ms.value, by.value
+
+
+class Batch:
+    """Ensemble of independent cases on one GPU (sph_batch_*)."""
+
+    def __init__(self, cases, precision=0, device=0):
+        self._P = [np.ascontiguousarray(P, dtype=PART1) for P, _ in cases]
+        self._params = (SphParams * len(cases))(*[p for _, p in cases])
+        ptrs = (ctypes.c_void_p * len(cases))(*[P.ctypes.data for P in self._P])
+        ns = np.array([len(P) for P in self._P], np.int32)
+        h = ctypes.c_void_p()
+        _check("sph_batch_create", lib().sph_batch_create(len(cases), self._params, ptrs, _p(ns), int(precision),
+                                                          int(device), ctypes.byref(h)))
+        self.h = h
+        self.n = ns
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sph_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, nsteps=1):
+        st = (PpeStats * len(self.n))()
+        _check("sph_batch_step", lib().sph_batch_step(self.h, int(nsteps), st))
+        return list(st)
+
+    def set_workers(self, w):
+        _check("sph_batch_set_workers", lib().sph_batch_set_workers(self.h, int(w)))
+
+    def autotune(self, probe_steps=1):
+        w, ms = ctypes.c_int32(0), ctypes.c_double(0)
+        _check("sph_batch_autotune", lib().sph_batch_autotune(self.h, int(probe_steps), ctypes.byref(w), ctypes.byref(ms)))
+        return w.value, ms.value
+
+    def download(self, k):
+        c = ctypes.c_void_p()
+        _check("sph_batch_case", lib().sph_batch_case(self.h, int(k), ctypes.byref(c)))
+        P1 = np.zeros(int(self.n[k]), PART1)
+        _check("sph_download", lib().sph_download(c, _p(P1), None, None))
+        return P1
+
+    def particles(self):
+        return int(lib().sph_batch_particles(self.h))

@@ -19,6 +19,9 @@ before upload, plus the solver parameters.
   IBM cube at x = 0.6 m, neutral MOST log-law inflow with u* = 0.3 m/s and
   z0 = 0.01 m, a seeded 5 % uniform velocity perturbation and Cs = 0.12.
   ``scale`` shrinks every extent for small cases.
+* ``cavity``, ``tgv_box``, ``ensemble`` -- the batched-ensemble workload:
+  lid-driven cavities and Taylor-Green boxes of 20k-200k particles with Re in
+  [100, 2000], seeded.
 """
 import numpy as np
 
@@ -137,6 +140,22 @@ def caseh_mini(dx=0.0412, nx=24, ny=12, nz=7, seed=SEED, shuffle=True, **pkw):
     return P, p
 
 
+def with_headroom(P, p, frac):
+    """Appends int(frac * len(P)) free dummy records (i_type 3), the room the
+    reference reserves for buffer and APR particles (ISPH.cuh:116)."""
+    nd = int(frac * len(P))
+    D = np.zeros(nd, dtype=PART1)
+    D["i_type"] = 3
+    D["x"], D["y"], D["z"] = P["x"][0], P["y"][0], P["z"][0]
+    D["h"] = D["h_ref"] = P["h"][0]
+    D["m"] = D["m_ref"] = P["m"][0]
+    D["rho"] = P["rho"][0]
+    D["vol"] = P["vol"][0]
+    Q = np.concatenate([P, D])
+    domain_setup(p, Q)
+    return Q, p
+
+
 def canyon(scale=1.0, dx=0.01, seed=SEED, ustar=0.3, z0=0.01, cs=0.12, dt=2e-4, **pkw):
     """Urban-canyon deck: 2.4 x 1.2 x 0.6 m at dx (scaled by ``scale``)."""
     rng = np.random.default_rng(seed)
@@ -226,6 +245,69 @@ def most_column(dx=1.0, n=6, nz=5, seed=SEED, **pkw):
     p.setf("dt", 1e-3)
     domain_setup(p, P)
     return P, p
+
+
+def _box_case(n, dx, re, lid, seed, ppe_kw):
+    """Cube of n^3 fluid particles inside 3 wall layers; lid-driven (top
+    layers moving at U = 1 m/s in x) or a Taylor-Green initial field in a
+    walled box.  Dynamic viscosity from Re = rho U L / mu."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    L = n * dx
+    c = (np.arange(n) + 0.5) * dx
+    fx, fy, fz = _grid(c, c, c)
+    Pf = _records(fx, fy, fz); Pf["p_type"] = 1
+    w = (np.arange(-3, n + 3) + 0.5) * dx
+    wx, wy, wz = _grid(w, w, w)
+    inside = (wx > 0) & (wx < L) & (wy > 0) & (wy < L) & (wz > 0) & (wz < L)
+    Pw = _records(wx[~inside], wy[~inside], wz[~inside]); Pw["p_type"] = 0
+    if lid:
+        Pw["p_type"][Pw["z"] > L] = 9
+    P = np.concatenate([Pf, Pw])
+    _common_fields(P, dx)
+    fl = P["p_type"] == 1
+    if not lid:
+        k = 2 * np.pi / L
+        x, y, z = (P[a].astype(np.float64) for a in ("x", "y", "z"))
+        P["ux"] = np.where(fl, np.sin(k * x) * np.cos(k * y) * np.cos(k * z), 0.0).astype(f)
+        P["uy"] = np.where(fl, -np.cos(k * x) * np.sin(k * y) * np.cos(k * z), 0.0).astype(f)
+    P = P[rng.permutation(len(P))]
+    p = default_params(dt=0.1 * dx, turbulence="Laminar", open_boundary=0, **ppe_kw)
+    p.visc_fluid = 1.225 * 1.0 * L / re
+    p.boundary_velocity = 1.0
+    p.l2, p.l3, p.l_left, p.l_right = -1e9, 1e9, -1e9, 1e9
+    p.setf("u_limit", 20.0)
+    p.setf("time_end", 1e9)
+    domain_setup(p, P)
+    return P, p
+
+
+def cavity(n=30, dx=0.01, re=1000.0, seed=SEED, **kw):
+    """Lid-driven cavity: n^3 fluid particles, lid speed 1 m/s."""
+    return _box_case(n, dx, re, True, seed, kw)
+
+
+def tgv_box(n=30, dx=0.01, re=1000.0, seed=SEED, **kw):
+    """Taylor-Green initial field in a walled box (the reference's NNPS has
+    no triply periodic mode)."""
+    return _box_case(n, dx, re, False, seed, kw)
+
+
+def ensemble(ncase=64, nmin=20000, nmax=200000, dx=0.01, seed=SEED, **kw):
+    """Seeded ensemble: case k has N_k ~ U[nmin, nmax] fluid particles (cube
+    edge round(N_k^(1/3)) at dx), Re ~ U[100, 2000]; even k lid-driven
+    cavity, odd k Taylor-Green box.  Returns [(P, params, meta)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(ncase):
+        nk = int(rng.integers(nmin, nmax + 1))
+        edge = int(round(nk ** (1.0 / 3.0)))
+        re = float(rng.uniform(100.0, 2000.0))
+        lid = k % 2 == 0
+        P, p = (cavity if lid else tgv_box)(n=edge, dx=dx, re=re, seed=seed + k, **kw)
+        out.append((P, p, {"kind": "cavity" if lid else "taylor-green", "edge": edge, "re": re,
+                           "target_fluid": nk, "particles": len(P)}))
+    return out
 
 
 def describe(P):

@@ -116,8 +116,10 @@ class SphParams(ctypes.Structure):
         ("ppe_refinement", ctypes.c_int32),
         ("ppe_coarse_block", ctypes.c_int32),
         ("ppe_warm_start", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 9),
+        ("apr_max_level", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 8),
         ("ppe_inner_tol", ctypes.c_double),
+        ("apr_zone", ctypes.c_double),
     ]
 
     def seti(self, name, value):
@@ -148,4 +150,13 @@ class PpeStats(ctypes.Structure):
     ]
 
 
-assert ctypes.sizeof(SphParams) == 1264, ctypes.sizeof(SphParams)
+assert ctypes.sizeof(SphParams) == 1272, ctypes.sizeof(SphParams)
+
+
+def params_from_bytes(b):
+    """SphParams from stored bytes; fields appended since they were written
+    (apr_zone) read as 0."""
+    buf = bytearray(ctypes.sizeof(SphParams))
+    b = bytes(b)
+    buf[:len(b)] = b[:len(buf)]
+    return SphParams.from_buffer_copy(buf)
