@@ -192,6 +192,11 @@ __global__ void k_gj_elim(double *W, double *Inv, const double *colk, int m, int
     }
 }
 
+__global__ void k_to_float(const double *a, float *b, long long n) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = (float)a[t];
+}
+
 __global__ void k_eye(double *A, int m) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < (long long)m * m) A[t] = (t / m == t % m) ? 1.0 : 0.0;
@@ -209,15 +214,16 @@ __global__ void __launch_bounds__(256) k_coarse_restrict(const int *off, const i
     if (threadIdx.x == 0) s[I] = v;
 }
 
-// y = E^-1 s, one warp per row
-__global__ void __launch_bounds__(256) k_coarse_solve(const double *__restrict__ Inv, const double *__restrict__ s,
+// y = E^-1 s, one warp per row; E^-1 is stored in FP32 (a preconditioner
+// needs no more, and the m^2 matrix is the largest read of an application)
+__global__ void __launch_bounds__(256) k_coarse_solve(const float *__restrict__ Inv, const double *__restrict__ s,
                                                       double *__restrict__ y, int m) {
     const int I = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (I >= m) return;
-    const double *row = Inv + (size_t)I * m;
+    const float *row = Inv + (size_t)I * m;
     double v = 0;
-    for (int J = lane; J < m; J += 32) v += row[J] * s[J];
+    for (int J = lane; J < m; J += 32) v += (double)row[J] * s[J];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) y[I] = v;
@@ -236,7 +242,7 @@ void coarse_apply(Ctx<Real> &c, const V *r, V *z) {
     if (c.cg_m <= 0) return;
     const int m = c.cg_m;
     k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, c.cg_s);
-    k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_inv, c.cg_s, c.cg_y, m);
+    k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_invf, c.cg_s, c.cg_y, m);
     k_coarse_add<V><<<grid_for(c.n, 256), 256, 0, c.stream>>>(c.cg_agg, c.cg_y, z, c.n);
     c.launches += 3;
 }
@@ -377,6 +383,12 @@ int coarse_build(Ctx<Real> &c) {
     int herr = 0;
     SPH_CUDA_TRY(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
+    c.release(c.cg_invf);
+    SPH_TRY(c.alloc(c.cg_invf, (size_t)m * m));
+    k_to_float<<<div_up(mm, 256), 256, 0, st>>>(c.cg_inv, c.cg_invf, mm);
+    SPH_CUDA_TRY(cudaGetLastError());
+    SPH_CUDA_TRY(cudaStreamSynchronize(st));
+    c.release(c.cg_inv);
     c.release(E); c.release(a_comp); c.release(colk); c.release(pval); c.release(amax);
     c.release(d_piv); c.release(d_err); c.release(d_nm_idx); c.release(d_cnt_comp);
     if (herr) {

@@ -141,9 +141,12 @@ __device__ __forceinline__ Real pw(Real a, int k) {
     return r;
 }
 
+// tR = rr / (kappa tH) as a product with the reciprocal, which the pair loops
+// hoist out (tH is the row's smoothing length); within FP rounding of the
+// reference's rr / tH / kappa
 template <class Real>
 __device__ __forceinline__ Real calc_wij(const DevParams &P, Real tA, Real tH, Real rr) {
-    const Real tR = rr / tH / (Real)P.kappa;
+    const Real tR = rr * ((Real)1 / (tH * (Real)P.kappa));
     const Real o = (Real)1 - tR;
     switch (P.kernel_type) {
         case 0: return tA * (Real)exp(-(double)(2 * tR) * (double)(2 * tR));
@@ -167,7 +170,7 @@ __device__ __forceinline__ Real calc_wij(const DevParams &P, Real tA, Real tH, R
 template <class Real>
 __device__ __forceinline__ Real calc_dwij(const DevParams &P, Real tA, Real tH, Real rr) {
     const Real kap = (Real)P.kappa;
-    const Real tR = rr / tH / kap;
+    const Real tR = rr * ((Real)1 / (tH * kap));
     const Real o = (Real)1 - tR;
     switch (P.kernel_type) {
         case 0: return (1 / tH) * tA * (-4 * tR) * (Real)exp(-(double)(2 * tR) * (double)(2 * tR));
@@ -192,7 +195,7 @@ __device__ __forceinline__ Real calc_dwij(const DevParams &P, Real tA, Real tH, 
 template <class Real>
 __device__ __forceinline__ Real calc_dwij_pressure(const DevParams &P, Real tA, Real tH, Real rr) {
     const Real kap = (Real)P.kappa;
-    const Real tR = rr / tH / kap;
+    const Real tR = rr * ((Real)1 / (tH * kap));
     const Real o = (Real)1 - tR, o2 = o * o, o4 = o2 * o2;
     return (tR < 1) ? (1 / (kap * tH)) * tA * (-22 * tR * o4 * o2 * o * (16 * tR * tR + 7 * tR + 1)) : (Real)0;
 }

@@ -129,6 +129,8 @@ struct Ctx {
     float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
     double *coef_d = nullptr;     // cached c_ij, FP64 form
     bool coef_valid = false;
+    Real *ppe_gb = nullptr;       // cached rhs pair vectors g_ij (3 x SELL arrays)
+    Real *vis_stage = nullptr;    // staging of the LES viscosity in the prep pass
     // Krylov workspace
     Real *kv[10] = {};            // r, rh, p, v, s, t, ph, sh, dinv, b
     double *kd[10] = {};          // FP64 Krylov vectors of the mixed form's fallback
@@ -144,7 +146,8 @@ struct Ctx {
     int cg_block = 0, cg_m = 0;   // aggregate edge in cells, aggregates in use
     int *cg_agg = nullptr;        // aggregate of each row, -1 for identity / pinned rows
     int *cg_off = nullptr, *cg_rows = nullptr;   // rows of each aggregate, ascending
-    double *cg_inv = nullptr;     // E^-1, m x m
+    double *cg_inv = nullptr;     // E^-1 while it is built (FP64 Gauss-Jordan)
+    float *cg_invf = nullptr;     // E^-1, m x m, FP32 copy the solve reads
     double *cg_s = nullptr, *cg_y = nullptr;     // restricted residual, coarse correction
     // live operator timing (sph_profile)
     bool prof = false;

@@ -167,8 +167,8 @@ __global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARG
         if (les) {
             tmp_sigma += tdist * tdist * w * vj;
             if (s.jc[j] & JB_PT1) {
-                const Real dw = calc_dwij<Real>(P, tA, hi, tdist);
-                const Real tdwx = dw * dx / tdist, tdwy = dw * dy / tdist, tdwz = dw * dz / tdist;
+                const Real dwi = calc_dwij<Real>(P, tA, hi, tdist) / tdist;
+                const Real tdwx = dwi * dx, tdwy = dwi * dy, tdwz = dwi * dz;
                 const Real cx = gc11 * tdwx + gc12 * tdwy + gc31 * tdwz;
                 const Real cy = gc12 * tdwx + gc22 * tdwy + gc23 * tdwz;
                 const Real cz = gc31 * tdwx + gc23 * tdwy + gc33 * tdwz;
@@ -399,9 +399,11 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
         const auto xj = s.pr[j];
         const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+        const Real it = (Real)1 / tdist;
         Real dw = calc_dwij<Real>(P, tA, hi, tdist);
         if (kgc) dw = 0;   // Cm is never filled on this path (all zero)
-        const Real tdwx = dw * dx / tdist, tdwy = dw * dy / tdist, tdwz = dw * dz / tdist;
+        const Real dwi = dw * it;
+        const Real tdwx = dwi * dx, tdwy = dwi * dy, tdwz = dwi * dz;
         const auto uj = u[j];
         const auto mj = s.mr[j];
         const Real ux = ui.x - uj.x, uy = ui.y - uj.y, uz = ui.z - uj.z;
@@ -409,9 +411,9 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
             const Real visj = visc2<Real>(P, jcj) + uj.w * mj.y;
             Real C = dx * tdwx + dy * tdwy + dz * tdwz;
             C *= (visi * visj) / (visi + visj);
-            C *= 4 * (mj.x / (rhoi * mj.y));
-            C /= tdist;
-            C /= tdist;
+            C *= 4 * mj.x / (rhoi * mj.y);
+            C *= it;   // twice, not it * it: the self pair has it = 1e20, whose square overflows FP32
+            C *= it;
             tx += C * ux; ty_ += C * uy; tz += C * uz;
         } else if (FV == 2) {
             const Real uij_xij = ux * dx + uy * dy + uz * dz;
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(128) k_pressure_force(DevParams P, SoA<Real> s
             if (kgc) dw = 0;
             const auto mj = s.mr[j];
             const Real pj = p[j] - pres0[j];
-            const Real Cp = (Real)-2 * mj.x / (rhoi * mj.y) * (pi * mj.y + pj * rhoi) / (rhoi + mj.y);
+            const Real Cp = (Real)-2 * mj.x * (pi * mj.y + pj * rhoi) / ((rhoi * mj.y) * (rhoi + mj.y));
             const Real f = Cp * dw / tdist;
             tx += f * dx; ty_ += f * dy; tz += f * dz;
         SELL_LOOP_END
@@ -867,7 +869,8 @@ int phase_interaction(Ctx<Real> &c) {
     }
     if (!c.gc_valid || c.prm.recompute_gc) SPH_TRY(gradient_correction(c));
     // prep / LES
-    Real *vis_stage = c.diag;   // staging (diag is rebuilt by the PPE)
+    if (!c.vis_stage) SPH_TRY(c.alloc(c.vis_stage, n));
+    Real *vis_stage = c.vis_stage;   // LES viscosity staged until every row has read the old one
     k_prep<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
                                                    c.S.et, c.SR, c.rho_ref_S, tc, tdt, n);
     ++c.launches;

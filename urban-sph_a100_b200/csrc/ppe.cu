@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(128) k_ppe_rows(DevParams P, const float4 *__r
                                                   const int4 *__restrict__ ty, const int *__restrict__ jc, LIST_ARGS,
                                                   const Real *__restrict__ g6, const typename V4<Real>::type *__restrict__ u,
                                                   Real tdt, Real *__restrict__ b, Real *__restrict__ diag,
-                                                  C *__restrict__ coef, int n) {
+                                                  C *__restrict__ coef, Real *__restrict__ gb, long long nnzp, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 ti = ty[i];
@@ -136,11 +136,40 @@ __global__ void __launch_bounds__(128) k_ppe_rows(DevParams P, const float4 *__r
             bz += vj * (uj.z - ui.z) * cz * wr;
             c = (Real)2 * vj * (dx * cx + dy * cy + dz * cz) / tdist / tdist;
             Aij += c;
+            if (gb) { gb[e] = vj * cx * wr; gb[nnzp + e] = vj * cy * wr; gb[2 * nnzp + e] = vj * cz * wr; }
+        } else if (gb) {
+            gb[e] = 0; gb[nnzp + e] = 0; gb[2 * nnzp + e] = 0;
         }
         if (coef) coef[e] = (C)c;
     }
     b[i] = (bx + by + bz) / tdt;
     diag[i] = Aij;
+}
+
+// the right-hand side of later steps from the cached pair vectors
+// g_ij = m_j/rho_j * 2 rho_i rho_j / (rho_i + rho_j) * G_i grad W_ij (the
+// particles, masses and densities do not change between steps)
+template <class Real>
+__global__ void __launch_bounds__(128) k_ppe_rhs(const int4 *__restrict__ ty, LIST_ARGS,
+                                                 const typename V4<Real>::type *__restrict__ u,
+                                                 const Real *__restrict__ gb, long long nnzp, Real tdt,
+                                                 Real *__restrict__ b, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
+    const auto ui = u[i];
+    Real bx = 0, by = 0, bz = 0;
+    const long long base = slice_off[i >> 5] + (i & 31);
+    const int cnt = ncnt[i];
+    for (int k = 0; k < cnt; ++k) {
+        const long long e = base + 32LL * k;
+        const auto uj = u[__ldg(&nbr[e])];
+        bx += (uj.x - ui.x) * __ldcs(&gb[e]);
+        by += (uj.y - ui.y) * __ldcs(&gb[nnzp + e]);
+        bz += (uj.z - ui.z) * __ldcs(&gb[2 * nnzp + e]);
+    }
+    b[i] = (bx + by + bz) / tdt;
 }
 
 // one Jacobi sweep of KERNEL_PPE3D with the cached row: p_new = p0 + (b + sum c (p_j - p0_j)) / A
@@ -1015,6 +1044,8 @@ static int ensure_ppe_ws(Ctx<Real> &c) {
         const size_t m = (size_t)std::max(c.nnz_padded, 1LL);
         if (sizeof(Real) == 4) { c.release(c.coef); SPH_TRY(c.alloc(c.coef, m)); }
         else { c.release(c.coef_d); SPH_TRY(c.alloc(c.coef_d, m)); }
+        c.release(c.ppe_gb);
+        SPH_TRY(c.alloc(c.ppe_gb, 3 * m));   // rhs pair vectors, three SELL arrays
     }
     return SPH_OK;
 }
@@ -1032,14 +1063,19 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     SPH_CUDA_TRY(cudaEventRecord(c.ev[4], st));
     // b_i, A_i every step; c_ij once per neighbour-list build (time-invariant
     // while the particles do not move)
-    if (sizeof(Real) == 4)
+    const long long nnzp = std::max(c.nnz_padded, 1LL);
+    if (c.coef_valid && c.ppe_gb) {
+        k_ppe_rhs<Real><<<grid_for(n, 128), 128, 0, st>>>(c.ty, c.slice_off, c.ncnt, c.nbr, c.S.u, c.ppe_gb, nnzp, tdt,
+                                                         b, n);
+    } else if (sizeof(Real) == 4) {
         k_ppe_rows<Real, float><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.pr, c.mr, c.ty, c.jc, c.slice_off, c.ncnt,
                                                                  c.nbr, c.g6, c.S.u, tdt, b, c.diag,
-                                                                 c.coef_valid ? nullptr : c.coef, n);
-    else
+                                                                 c.coef_valid ? nullptr : c.coef, c.ppe_gb, nnzp, n);
+    } else {
         k_ppe_rows<Real, double><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.pr, c.mr, c.ty, c.jc, c.slice_off, c.ncnt,
                                                                   c.nbr, c.g6, c.S.u, tdt, b, c.diag,
-                                                                  c.coef_valid ? nullptr : c.coef_d, n);
+                                                                  c.coef_valid ? nullptr : c.coef_d, c.ppe_gb, nnzp, n);
+    }
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     c.coef_valid = true;
