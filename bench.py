@@ -32,6 +32,8 @@ sys.path[:0] = [os.path.join(ROOT, "urban-sph_a100_b200"), os.path.join(ROOT, "o
 
 METRIC = "particle-steps/s"
 WORKLOAD = "urban canyon 2.4x1.2x0.6 m, dx=0.01 m: 240x120x60 fluid + floor walls + free-slip ceiling + IBM cube, neutral MOST, SSM Cs=0.12"
+WORKLOAD_ARRAY = ("staggered 4x4 array of 0.1 m IBM cubes at 0.3 m pitch in a 4.8x2.4x0.8 m channel, dx=0.01 m, "
+                  "uniform resolution (--apr: two-level APR within 0.1 m of the faces), neutral MOST, SSM Cs=0.12")
 
 
 def peaks():
@@ -126,7 +128,7 @@ def run_ensemble(args, rank, world, local):
     """Batched ensemble: every rank steps its own seeded set of cases."""
     import numpy as np
     import torch
-    from sph_b200 import abi, decks, layout
+    from sph_b200 import abi, decks, layout, replicas
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -155,12 +157,9 @@ def run_ensemble(args, rank, world, local):
     torch.cuda.synchronize()
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     n = b.particles()
-    value = n * args.steps * world / (ms / 1e3)
+    # every rank steps its own seeded cases: all ranks' work over the slowest rank's time
+    value, ms = replicas.throughput(n, args.steps, ms, device="cuda")
     out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
@@ -224,17 +223,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--config", default="canyon", choices=["canyon", "ensemble"],
-                    help="canyon: the urban-canyon step (default); ensemble: 64 seeded cavity / Taylor-Green "
-                         "cases of 20k-200k particles stepped together (sph_batch_*)")
+    ap.add_argument("--config", default="canyon", choices=["canyon", "array", "ensemble"],
+                    help="canyon: the urban-canyon step (default); array: 4x4 cube array with two-level APR; "
+                         "ensemble: 64 seeded cavity / Taylor-Green cases of 20k-200k particles stepped together")
     ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--apr", action="store_true",
+                    help="array config: two-level APR near the faces before timing (default: uniform resolution)")
     ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "gmres", "ref_sweep"])
     ap.add_argument("--fp64-mode", default="bicgstab", choices=["gmres", "bicgstab"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--matrix-free", action="store_true")
-    ap.add_argument("--coarse", type=int, default=5,
-                    help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi)")
+    ap.add_argument("--coarse", type=int, default=None,
+                    help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; "
+                         "default 5 for the canyon, 9 for the cube array)")
     ap.add_argument("--warm", default="prev", choices=["prev", "extrap", "learned"],
                     help="PPE start vector: previous pressure, linear extrapolation in time, or the learned "
                          "per-particle network (trained on this run's warm-up solves)")
@@ -254,14 +256,20 @@ def main():
     import numpy as np
     import torch
     import torch.distributed as dist
-    from sph_b200 import abi, decks, layout
+    from sph_b200 import abi, decks, layout, replicas
 
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    P, p = decks.canyon(scale=args.scale)
+    boxes = None
+    if args.config == "array":
+        P, p, boxes = decks.cube_array(scale=args.scale, apr=args.apr)
+    else:
+        P, p = decks.canyon(scale=args.scale)
+    if args.coarse is None:
+        args.coarse = 9 if args.config == "array" else 5
     mode = {"mixed_ir": layout.PPE_MIXED_IR, "bicgstab": layout.PPE_BICGSTAB, "gmres": layout.PPE_GMRES,
             "ref_sweep": layout.PPE_REF_SWEEP}[args.mode]
     p.ppe_mode = mode
@@ -273,7 +281,23 @@ def main():
     p.ppe_warm_start = 1 if args.warm == "extrap" else 0
     n = len(P)
     sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
+    if boxes is not None:
+        sim.set_ib_boxes(boxes)
     sim.upload(P)
+    apr = None
+    if args.config == "array" and args.apr:
+        # two-level APR near the faces before timing: splitting passes until no
+        # cell asks (one particle per cell and pass); every form starts from
+        # the refined state
+        passes, split = 0, 0
+        for passes in range(1, 16):
+            ns, _ = sim.apr()
+            split += ns
+            if ns == 0:
+                break
+        P, _, _ = sim.download()
+        n = int((P["i_type"] < 3).sum())   # particle-steps count active particles, not free records
+        apr = {"passes": passes, "cells_split": split, "active_particles": n, "records": len(P)}
     learned = None
     if args.warm == "learned":
         # samples from the warm-up solves, then Adam on the GPU (not timed)
@@ -323,15 +347,10 @@ def main():
     launches = sim.launches() - l0
     op_n, op_ms, op_bytes = sim.operator_stats(reset=True)
     sim.profile(False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    value = n * args.steps * world / (ms / 1e3)
+    value, ms = replicas.throughput(n, args.steps, ms, device="cuda")
 
     # ---- end to end through the C ABI with host buffers ----
-    host = torch.empty(n * layout.PART1.itemsize, dtype=torch.uint8, pin_memory=True).numpy().view(layout.PART1)
+    host = torch.empty(len(P) * layout.PART1.itemsize, dtype=torch.uint8, pin_memory=True).numpy().view(layout.PART1)
     sim.download_into(host)
     ke = max(3, args.steps // 2)
     torch.cuda.synchronize()
@@ -346,11 +365,7 @@ def main():
     f1.record()
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = n * ke * world / (e2e_ms / 1e3)
+    e2e, e2e_ms = replicas.throughput(n, ke, e2e_ms, device="cuda")
 
     # ---- other forms on the same deck, rank 0 only ----
     sim.close()
@@ -360,6 +375,8 @@ def main():
         q.ppe_mode = mode
         q.ppe_coarse_block = coarse
         sd = abi.Simulation(q, precision=precision, device=local)
+        if boxes is not None:
+            sd.set_ib_boxes(boxes)
         sd.upload(P)
         for _ in range(2):
             sd.step(1)
@@ -414,7 +431,8 @@ def main():
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": n, "scale": args.scale, "precision": "mixed FP32/FP64",
+        "config": {"workload": WORKLOAD if args.config == "canyon" else WORKLOAD_ARRAY,
+                   "particles": n, "apr": apr, "scale": args.scale, "precision": "mixed FP32/FP64",
                    "ppe": args.mode, "ppe_tol": 1e-6,
                    "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
                    "ppe_refinement": args.refinement,
@@ -424,8 +442,8 @@ def main():
                    else "jacobi",
                    "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": n * layout.PART1.itemsize,
-                "d2h_bytes_per_step": n * layout.PART1.itemsize, "steps": ke},
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": len(P) * layout.PART1.itemsize,
+                "d2h_bytes_per_step": len(P) * layout.PART1.itemsize, "steps": ke},
         "gpu_launches": int(launches),
         "ppe": {"iterations_mean": statistics.mean(s[0] for s in stats),
                 "refinements_mean": statistics.mean(s[1] for s in stats),

@@ -281,6 +281,14 @@ int64_t sph_launch_count(sph_ctx *ctx);
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
 
+/* ---- several IBM obstacles ------------------------------------------------
+ * The reference hard-wires one IB box (functions_PREP.cuh:958-963, here
+ * params.ib_box).  For decks with several obstacles, nbox boxes
+ * (x0, x1, y0, y1, z0, z1 each) replace it in the marker normals, which are
+ * computed at step 0 (set the boxes before the first step); nbox = 0 goes
+ * back to params.ib_box. */
+int sph_set_ib_boxes(sph_ctx *ctx, const double *boxes, int nbox);
+
 /* ---- adaptive particle refinement ----------------------------------------
  * One 3-D splitting pass (functions_APR.cuh:270-652, cell-based APR, which the
  * shipped reference does not compile): every cell splits the first fluid

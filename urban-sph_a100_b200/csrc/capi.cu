@@ -456,3 +456,17 @@ int sph_apr(sph_ctx *ctx, int32_t *n_split, int32_t *n_wanted) {
     if (n_wanted) *n_wanted = b;
     return st;
 }
+
+int sph_set_ib_boxes(sph_ctx *ctx, const double *boxes, int nbox) {
+    if (!ctx || nbox < 0 || (nbox > 0 && !boxes)) return SPH_ERR_BAD_ARG;
+    auto go = [&](auto *c) -> int {
+        c->release(c->ib_boxes);
+        c->n_ib_boxes = nbox;
+        if (nbox == 0) return SPH_OK;
+        SPH_TRY(c->alloc(c->ib_boxes, 6 * (size_t)nbox));
+        SPH_CUDA_TRY(cudaMemcpyAsync(c->ib_boxes, boxes, sizeof(double) * 6 * nbox, cudaMemcpyHostToDevice, c->stream));
+        SPH_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return SPH_OK;
+    };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
+}

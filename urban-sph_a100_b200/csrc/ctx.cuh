@@ -131,6 +131,8 @@ struct Ctx {
     bool coef_valid = false;
     Real *ppe_gb = nullptr;       // cached rhs pair vectors g_ij (3 x SELL arrays)
     Real *vis_stage = nullptr;    // staging of the LES viscosity in the prep pass
+    double *ib_boxes = nullptr;   // obstacle boxes for the IB normals (NULL: params.ib_box)
+    int n_ib_boxes = 0;
     // Krylov workspace
     Real *kv[10] = {};            // r, rh, p, v, s, t, ph, sh, dinv, b
     double *kd[10] = {};          // FP64 Krylov vectors of the mixed form's fallback

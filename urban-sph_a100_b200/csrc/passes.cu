@@ -59,20 +59,29 @@ __global__ void k_begin_step(Ctx<Real> c) {
 }
 
 // KERNEL_clc_IB_normal_vector3D, functions_PREP.cuh:923-1015 (step 0 only)
+// With several obstacles (sph_set_ib_boxes) a marker takes the normal of the
+// first box on whose surface it lies; the reference has one hard-wired box.
 template <class Real>
 __global__ void k_ib_normals(DevParams P, const typename V4<Real>::type *pr, const int4 *ty,
-                             typename V4<Real>::type *nrm, int n) {
+                             typename V4<Real>::type *nrm, const double *boxes, int nbox, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || ty[i].w < 1000) return;
     const auto x = pr[i];
     Real nx = 0, ny = 0, nz = 0;
     const double t = P.ib_face_tol;
-    if (fabs((double)x.x - P.ib_box[0]) < t) nx = -1;
-    if (fabs((double)x.x - P.ib_box[1]) < t) nx = 1;
-    if (fabs((double)x.y - P.ib_box[2]) < t) ny = -1;
-    if (fabs((double)x.y - P.ib_box[3]) < t) ny = 1;
-    if (fabs((double)x.z - P.ib_box[4]) < t) nz = -1;
-    if (fabs((double)x.z - P.ib_box[5]) < t) nz = 1;
+    for (int q = 0; q < (boxes ? nbox : 1); ++q) {
+        const double *bb = boxes ? boxes + 6 * q : P.ib_box;
+        const bool on = (double)x.x > bb[0] - t && (double)x.x < bb[1] + t && (double)x.y > bb[2] - t &&
+                        (double)x.y < bb[3] + t && (double)x.z > bb[4] - t && (double)x.z < bb[5] + t;
+        if (boxes && !on) continue;
+        if (fabs((double)x.x - bb[0]) < t) nx = -1;
+        if (fabs((double)x.x - bb[1]) < t) nx = 1;
+        if (fabs((double)x.y - bb[2]) < t) ny = -1;
+        if (fabs((double)x.y - bb[3]) < t) ny = 1;
+        if (fabs((double)x.z - bb[4]) < t) nz = -1;
+        if (fabs((double)x.z - bb[5]) < t) nz = 1;
+        break;
+    }
     const Real mag = sqrt(nx * nx + ny * ny + nz * nz);
     if (mag > (Real)1e-9) nrm[i] = mk4<Real>(nx / mag, ny / mag, nz / mag, 0);
     else nrm[i] = mk4<Real>(0, 0, 0, 0);
@@ -864,7 +873,7 @@ int phase_interaction(Ctx<Real> &c) {
     k_begin_step<Real><<<grid_for(n, 256), 256, 0, st>>>(c);
     ++c.launches;
     if (tc == 0) {
-        k_ib_normals<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.pr, c.ty, c.nrm, n);
+        k_ib_normals<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.pr, c.ty, c.nrm, c.ib_boxes, c.n_ib_boxes, n);
         ++c.launches;
     }
     if (!c.gc_valid || c.prm.recompute_gc) SPH_TRY(gradient_correction(c));

@@ -29,7 +29,7 @@ SYMBOLS = (
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
-    "sph_batch_case", "sph_batch_particles", "sph_apr",
+    "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_set_ib_boxes",
 )
 
 _lib = None
@@ -97,6 +97,7 @@ def lib():
         L.sph_batch_particles.argtypes = [vp]
         L.sph_batch_particles.restype = i64
         L.sph_apr.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        L.sph_set_ib_boxes.argtypes = [vp, vp, i32]
         _lib = L
     return _lib
 
@@ -221,6 +222,10 @@ class Simulation:
 
     def profile(self, enable=True):
         _check("sph_profile", lib().sph_profile(self.h, 1 if enable else 0))
+
+    def set_ib_boxes(self, boxes):
+        b = np.ascontiguousarray(boxes, np.float64).reshape(-1, 6)
+        _check("sph_set_ib_boxes", lib().sph_set_ib_boxes(self.h, _p(b), len(b)))
 
     def apr(self):
         a, b = ctypes.c_int32(0), ctypes.c_int32(0)

@@ -19,6 +19,8 @@ before upload, plus the solver parameters.
   IBM cube at x = 0.6 m, neutral MOST log-law inflow with u* = 0.3 m/s and
   z0 = 0.01 m, a seeded 5 % uniform velocity perturbation and Cs = 0.12.
   ``scale`` shrinks every extent for small cases.
+* ``cube_array`` -- staggered 4 x 4 array of 0.1 m cubes (IBM) in a
+  4.8 x 2.4 x 0.8 m channel with two-level APR near the faces.
 * ``cavity``, ``tgv_box``, ``ensemble`` -- the batched-ensemble workload:
   lid-driven cavities and Taylor-Green boxes of 20k-200k particles with Re in
   [100, 2000], seeded.
@@ -217,6 +219,114 @@ def canyon(scale=1.0, dx=0.01, seed=SEED, ustar=0.3, z0=0.01, cs=0.12, dt=2e-4, 
     p.setf("time_end", 1e9)
     domain_setup(p, P)
     return P, p
+
+
+def _cube_markers(bx0, bx1, by0, by1, bz0, bz1, dx):
+    nm = int(round((bx1 - bx0) / dx)) + 1
+    gx, gy, gz = np.linspace(bx0, bx1, nm), np.linspace(by0, by1, nm), np.linspace(bz0, bz1, nm)
+    mk = []
+    for xv in (bx0, bx1):
+        mk.append(_grid([xv], gy, gz))
+    for yv in (by0, by1):
+        mk.append(_grid(gx, [yv], gz))
+    for zv in (bz0, bz1):
+        mk.append(_grid(gx, gy, [zv]))
+    return [np.concatenate([m[k] for m in mk]) for k in range(3)]
+
+
+def cube_array(scale=1.0, dx=0.01, seed=SEED, ustar=0.3, z0=0.01, cs=0.12, dt=2e-4, edge=0.1, pitch=0.3,
+               apr=False, apr_zone=0.1, headroom=None, stable_dT=0.0, fill_obstacles=True, **pkw):
+    """Staggered array of 0.1 m cubes at 0.3 m pitch in a 4.8 x 2.4 x 0.8 m
+    channel at dx (extents scaled by ``scale``; 4 x 4 cubes at full size),
+    IBM markers on every face, floor walls, free-slip ceiling, periodic-y
+    and inlet/outlet buffers, log-law inflow.  With ``apr`` the deck carries
+    free dummy records and the parameters for two-level APR (children at
+    dx / 2) of fluid within ``apr_zone`` of a marker.  ``stable_dT`` warms
+    the wall-layer air above the surface; the default 0 keeps MOST neutral
+    (with a temperature difference its Obukhov-length iteration at these
+    wall-layer heights gives NaN, as the reference's does).  Returns
+    (P, params, boxes) with boxes an (ncube, 6) array for sph_set_ib_boxes."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    nx, ny, nz = (int(round(480 * scale)), int(round(240 * scale)), int(round(80 * scale)))
+    nx, ny, nz = max(nx, 40), max(ny, 24), max(nz, 16)
+    xs = (np.arange(nx) + 0.5) * dx
+    ys = (np.arange(ny) + 0.5) * dx - 0.5 * ny * dx
+    zs = (np.arange(nz) + 0.5) * dx
+    Lx, Ly = nx * dx, ny * dx
+    # cube array: columns from x = 0.25 Lx, staggered rows, inside the core in y
+    ncx = max(1, min(4, int((0.6 * Lx) // pitch)))
+    ncy = max(1, min(4, int((0.7 * Ly) // pitch)))
+    boxes = []
+    for a in range(ncx):
+        for b in range(ncy):
+            cx = 0.25 * Lx + a * pitch
+            cy = (b - 0.5 * (ncy - 1)) * pitch + (0.5 * pitch if a % 2 else 0.0)
+            if abs(cy) + 0.5 * edge > 0.5 * Ly - 4 * dx:
+                cy -= pitch
+            boxes.append((cx - edge / 2, cx + edge / 2, cy - edge / 2, cy + edge / 2, 0.0, edge))
+    boxes = np.array(boxes)
+    parts = []
+    fx, fy, fz = _grid(xs, ys, zs)
+    # as in the canyon deck, fluid particles fill the obstacles: the IBM forcing
+    # holds them at rest (removing them leaves voids without a boundary row)
+    inside = np.zeros(len(fx), bool)
+    if not fill_obstacles:
+        for bx0, bx1, by0, by1, bz0, bz1 in boxes:
+            inside |= (fx > bx0) & (fx < bx1) & (fy > by0) & (fy < by1) & (fz < bz1)
+    Pf = _records(fx[~inside], fy[~inside], fz[~inside]); Pf["p_type"] = 1; parts.append(Pf)
+    wx, wy, wz = _grid(xs, ys, -(np.arange(3) + 0.5) * dx)
+    Pw = _records(wx, wy, wz); Pw["p_type"] = 0; parts.append(Pw)
+    cx_, cy_, cz_ = _grid(xs, ys, (nz + np.arange(3) + 0.5) * dx)
+    Pc = _records(cx_, cy_, cz_); Pc["p_type"] = -1; parts.append(Pc)
+    for bx in boxes:
+        Pm = _records(*_cube_markers(*bx, dx)); Pm["p_type"] = 1000; parts.append(Pm)
+    P = np.concatenate(parts)
+    _common_fields(P, dx)
+    l2 = 3 * dx
+    l3 = (nx - 3) * dx
+    l_left = ys[3] - 0.5 * dx
+    l_right = l_left + (ny - 6) * dx
+    _assign_buffers(P, l2, l3, l_left, l_right)
+    fluidlike = (P["p_type"] == 1) | (P["p_type"] == -1)
+    zz = P["z"].astype(np.float64)
+    ulog = np.where(zz > z0, ustar / 0.4 * np.log(np.maximum(zz, z0) / z0), 0.0)
+    P["ux"] = np.where(fluidlike, ulog * (1.0 + 0.05 * rng.uniform(-1, 1, len(P))), 0.0).astype(f)
+    P["uy"] = np.where(fluidlike, 0.05 * ulog * rng.uniform(-1, 1, len(P)), 0.0).astype(f)
+    P["uz"] = np.where(fluidlike, 0.05 * ulog * rng.uniform(-1, 1, len(P)), 0.0).astype(f)
+    most = (P["p_type"] == 1) & (P["buffer_type"] == 0) & (P["z"] < dx)
+    P["MOST_buffer"][most] = 1
+    P["temp"][most] = f(300.0 + stable_dT)
+    # the wall-layer particles sit at z = dx / 2: the MOST roughness length must
+    # lie below them for the Obukhov-length Newton iteration to exist
+    p = default_params(dt=dt, **pkw)
+    p.cs_sgs = cs
+    p.l2, p.l3, p.l_left, p.l_right = l2, l3, l_left, l_right
+    p.outlet_probe_dx = 0.5 * dx
+    for k, v in enumerate(boxes[0]):
+        p.ib_box[k] = v
+    p.most_z0, p.most_z0h = min(z0, 0.1 * dx), 0.01 * dx
+    zt = np.linspace(0.5 * dx, nz * dx, 24)
+    set_profile(p, zt, ustar / 0.4 * np.log(np.maximum(zt, z0) / z0))
+    p.setf("u_limit", 20.0)
+    p.setf("time_end", 1e9)
+    if not apr:
+        domain_setup(p, P)
+        return P, p, boxes
+    p.apr_max_level = 1
+    p.apr_zone = apr_zone
+    p.seti("h_change", 1)
+    near = np.zeros(len(P), bool)
+    fl = P["p_type"] == 1
+    for bx0, bx1, by0, by1, bz0, bz1 in boxes:
+        d = np.sqrt(np.maximum(np.maximum(bx0 - P["x"], P["x"] - bx1), 0) ** 2 +
+                    np.maximum(np.maximum(by0 - P["y"], P["y"] - by1), 0) ** 2 +
+                    np.maximum(P["z"] - bz1, 0) ** 2)
+        # the pass marks whole NNPS cells within ceil(zone / dcell) cells of a marker cell
+        near |= fl & (d <= apr_zone + 2.5 * 1.65 * dx)
+    frac = headroom if headroom is not None else 7.2 * near.sum() / len(P)
+    P, p = with_headroom(P, p, frac)
+    return P, p, boxes
 
 
 def most_column(dx=1.0, n=6, nz=5, seed=SEED, **pkw):
