@@ -237,6 +237,8 @@ def main():
     ap.add_argument("--coarse", type=int, default=None,
                     help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; "
                          "default 5 for the canyon, 9 for the cube array)")
+    ap.add_argument("--gmres-restart", type=int, default=0, help="GMRES(m) restart length (0: 40)")
+    ap.add_argument("--inner-tol", type=float, default=0.0, help="restarted refinement: inner tolerance (0: 1e-3)")
     ap.add_argument("--warm", default="prev", choices=["prev", "extrap", "learned"],
                     help="PPE start vector: previous pressure, linear extrapolation in time, or the learned "
                          "per-particle network (trained on this run's warm-up solves)")
@@ -278,6 +280,9 @@ def main():
         p.ppe_matrix_free = 1
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2}[args.refinement]
     p.ppe_coarse_block = args.coarse
+    p.ppe_gmres_restart = args.gmres_restart
+    if args.inner_tol > 0:
+        p.ppe_inner_tol = args.inner_tol
     p.ppe_warm_start = 1 if args.warm == "extrap" else 0
     n = len(P)
     sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)

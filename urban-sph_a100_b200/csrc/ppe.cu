@@ -885,6 +885,21 @@ __global__ void k_gmres_update(V *const *basis, const double *y, int nv, const V
     }
 }
 
+// u = sum_k y_k V_k
+template <class V>
+__global__ void k_gmres_combine(V *const *basis, const double *y, int nv, V *u, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = 0; k < nv; ++k) s += y[k] * (double)basis[k][i];
+        u[i] = (V)s;
+    }
+}
+// x += d * u
+template <class V>
+__global__ void k_mul_add(const V *d, const V *u, V *x, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] += d[i] * u[i];
+}
+
 template <class V>
 __global__ void k_sub_norm(const V *b, V *w, int n, double *partials, unsigned int *counter, double *out) {
     double d[1] = {0};
@@ -949,6 +964,7 @@ static int gmres(Ctx<Real> &c, GmresWs<Real, V> &ws, V *x, const V *b, double bn
         if (*relres <= tol) { status = SPH_OK; break; }
         if (it >= maxit || !(beta > 0) || !std::isfinite(beta)) break;
         k_normalize<V><<<G, 256, 0, st>>>(ws.w, ws.basis[0], ws.z, ws.dinv, beta, n);
+        coarse_apply<Real, V>(c, ws.basis[0], ws.z);   // z = M^-1 v with the coarse correction
         ++c.launches;
         std::fill(g.begin(), g.end(), 0.0);
         g[0] = beta;
@@ -993,6 +1009,7 @@ static int gmres(Ctx<Real> &c, GmresWs<Real, V> &ws, V *x, const V *b, double bn
             *relres = std::fabs(g[j + 1]) / bn;
             if (!(hn > 0) || *relres <= tol) { ++j; ++it; done = true; break; }
             k_normalize<V><<<G, 256, 0, st>>>(ws.w, ws.basis[j + 1], ws.z, ws.dinv, hn, n);
+            coarse_apply<Real, V>(c, ws.basis[j + 1], ws.z);
             ++c.launches;
         }
         // y = H^-1 g (upper triangular j x j), x += dinv V y
@@ -1004,7 +1021,15 @@ static int gmres(Ctx<Real> &c, GmresWs<Real, V> &ws, V *x, const V *b, double bn
         }
         if (nv > 0) {
             SPH_CUDA_TRY(cudaMemcpyAsync(hdev, y.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
-            k_gmres_update<V><<<G, 256, 0, st>>>(ws.basis_dev, hdev, nv, ws.dinv, x, n);
+            if (c.cg_m > 0) {
+                // x += M^-1 (V y) = dinv (V y) + Z E^-1 Z^T (V y)
+                k_gmres_combine<V><<<G, 256, 0, st>>>(ws.basis_dev, hdev, nv, ws.w, n);
+                k_mul_add<V><<<G, 256, 0, st>>>(ws.dinv, ws.w, x, n);
+                coarse_apply<Real, V>(c, ws.w, x);
+                c.launches += 1;
+            } else {
+                k_gmres_update<V><<<G, 256, 0, st>>>(ws.basis_dev, hdev, nv, ws.dinv, x, n);
+            }
             ++c.launches;
         }
         if (done && *relres <= tol) {
@@ -1079,7 +1104,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     c.coef_valid = true;
-    if (mode != SPH_PPE_REF_SWEEP && mode != SPH_PPE_GMRES && (!c.cg_valid || c.cg_block != c.prm.ppe_coarse_block))
+    if (mode != SPH_PPE_REF_SWEEP && (!c.cg_valid || c.cg_block != c.prm.ppe_coarse_block))
         SPH_TRY(coarse_build(c));
 
     if (mode == SPH_PPE_REF_SWEEP) {
