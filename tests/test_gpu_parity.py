@@ -52,9 +52,10 @@ def _decks():
 
 
 DECKS = _decks()
+NNPS_DECKS = DECKS + [("nnps_stress", decks.nnps_stress())]
 
 
-@pytest.mark.parametrize("name,deck", DECKS, ids=[d[0] for d in DECKS])
+@pytest.mark.parametrize("name,deck", NNPS_DECKS, ids=[d[0] for d in NNPS_DECKS])
 def test_nnps_bit_exact(name, deck):
     P, p = deck
     sim = abi.Simulation(p, precision=layout.PREC_MIXED)

@@ -56,6 +56,23 @@ def test_nnps_bit_exact_vs_reference(name):
 
 
 @needs_ref
+def test_nnps_bit_exact_vs_reference_on_stress_deck():
+    # dummies, a 150-particle cell, duplicates, records on the domain maximum
+    P, p = decks.nnps_stress()
+    R = refhost.RefHost(P, p, parallel=False)
+    _, g_idx, p_idx, g_str, g_end = R.nnps()
+    O = restated.Restated(P, p, 0)
+    O.nnps()
+    og, op, os_, oe = O.export_nnps()
+    assert np.array_equal(g_idx, og)
+    assert np.array_equal(p_idx, op)
+    assert np.array_equal(g_str, os_)
+    assert np.array_equal(g_end, oe)
+    counts = np.where(g_str >= 0, g_end - g_str, 0)
+    assert counts[:-1].max() > 64 and (P["i_type"] == 3).sum() > 0   # the long-cell sort path runs
+
+
+@needs_ref
 @pytest.mark.parametrize("name", list(VARIANTS))
 def test_step_bit_exact_vs_reference(name):
     P, p = _deck(VARIANTS[name])

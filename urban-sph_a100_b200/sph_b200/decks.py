@@ -420,6 +420,36 @@ def ensemble(ncase=64, nmin=20000, nmax=200000, dx=0.01, seed=SEED, **kw):
     return out
 
 
+def nnps_stress(seed=SEED):
+    """Small Case-H deck made hard for the cell sort and the lists: scattered
+    dummy records (i_type 3), one cell crowded with 150 particles (longer
+    than the 64-entry insertion sort), duplicated positions (zero-distance
+    pairs) and records on the domain maximum (clamped cell index)."""
+    rng = np.random.default_rng(seed)
+    P, p = caseh_mini(nx=12, ny=6, nz=5, seed=seed)
+    P = P.copy()
+    fl = np.where((P["p_type"] == 1) & (P["i_type"] == 1))[0]
+    pick = rng.permutation(fl)
+    crowd, dup, edge = pick[:150], pick[150:170], pick[170:180]
+    # crowd: inside a box a fifth of a cell wide around one fluid particle
+    c = pick[200]
+    dcell = p.getf("dcell")
+    for a in ("x", "y", "z"):
+        P[a][crowd] = (P[a][c] + rng.uniform(0.0, 0.2 * dcell, len(crowd))).astype(np.float32)
+    # duplicates of other fluid particles
+    src = pick[300:320]
+    for a in ("x", "y", "z"):
+        P[a][dup] = P[a][src]
+    # on the domain maximum of each axis (not the last record, which find_minmax skips)
+    for a in ("x", "y", "z"):
+        P[a][edge[:3]] = P[a][:-1].max()
+    # scattered dummies
+    dum = rng.choice(len(P) - 1, len(P) // 20, replace=False)
+    P["i_type"][dum] = 3
+    domain_setup(p, P)
+    return P, p
+
+
 def describe(P):
     counts = {}
     for name, mask in (("fluid", P["p_type"] == 1), ("wall", P["p_type"] == 0),
