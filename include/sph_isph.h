@@ -281,6 +281,18 @@ int64_t sph_launch_count(sph_ctx *ctx);
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
 
+/* ---- files in the reference's formats (host code) -------------------------
+ * sph_read_deck reads a particle deck in the format of read_input
+ * (function_init.cuh:550-676): a line of tab-separated variable codes, then
+ * one value per code and record; records get i_type 1.  With out = NULL and
+ * capacity 0 it only counts.  sph_write_vtk writes the legacy binary VTK of
+ * save_vtk_bin_single_flag (functions_OUTPUT.cuh:121-616) for the records
+ * with i_type 1 or 2, one FIELD array per label (the reference's labels and
+ * prefix matching); P2 / P3 may be NULL unless a label needs them. */
+int sph_read_deck(const char *path, sph_part1 *out, int capacity, int *n);
+int sph_write_vtk(const char *path, const sph_part1 *P1, const sph_part2 *P2, const sph_part3 *P3, int n,
+                  const char *const *labels, int nlabels);
+
 /* ---- several IBM obstacles ------------------------------------------------
  * The reference hard-wires one IB box (functions_PREP.cuh:958-963, here
  * params.ib_box).  For decks with several obstacles, nbox boxes

@@ -36,6 +36,7 @@
 #include <vector>
 #include <numeric>
 #include <string>
+#include <time.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -96,6 +97,7 @@ thread_local int sharedHash[129];
 #include "functions_BC.cuh"
 #include "functions_MOST.cuh"
 #include "functions_TIME_ISPH.cuh"
+#include "functions_OUTPUT.cuh"
 
 // ---- launcher ---------------------------------------------------------------
 // Runs `body` for every thread of a <<<ceil(n/128),128>>> launch.  Blocks run in
@@ -298,6 +300,34 @@ void ref_step(part1 *P1, part1 *SP1, part2 *P2, part2 *SP2, part3 *P3, int *g_id
     PHASE(21);
     launch(n, par, [&] { KERNEL_freeslip_boundary3D(g_str, g_end, P1, SP2, P3); });
 #undef PHASE
+}
+
+// read_input (function_init.cuh:550-676) into P1 (capacity records, i_type
+// cleared first); returns the number of records read
+int ref_read_input(part1 *P1, int capacity, const char *path) {
+    for (int i = 0; i < capacity; ++i) P1[i].i_type = 0;
+    read_input(P1, (char *)path);
+    int n = 0;
+    while (n < capacity && P1[n].i_type == 1) ++n;
+    return n;
+}
+
+// save_vtk_bin_single_flag (functions_OUTPUT.cuh:121-616) for n records and
+// the space-separated labels; writes ./<its hard-wired directory>/fluid_<step>stp.vtk
+// relative to the current directory
+void ref_save_vtk(part1 *P1, part2 *P2, part3 *P3, int n, int step, const char *labels) {
+    num_part2 = n;
+    count = step;
+    num_plot_data = 0;
+    char tmp[512];
+    strncpy(tmp, labels, sizeof tmp - 1);
+    tmp[sizeof tmp - 1] = 0;
+    for (char *t = strtok(tmp, " "); t && num_plot_data < 20; t = strtok(nullptr, " ")) {
+        strncpy(plot_data[num_plot_data], t, 19);
+        plot_data[num_plot_data][19] = 0;
+        ++num_plot_data;
+    }
+    save_vtk_bin_single_flag(P1, P2, P3);
 }
 
 }  // extern "C"

@@ -29,7 +29,7 @@ SYMBOLS = (
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
-    "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_set_ib_boxes",
+    "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
 )
 
 _lib = None
@@ -98,6 +98,8 @@ def lib():
         L.sph_batch_particles.restype = i64
         L.sph_apr.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
         L.sph_set_ib_boxes.argtypes = [vp, vp, i32]
+        L.sph_read_deck.argtypes = [ctypes.c_char_p, vp, i32, ctypes.POINTER(i32)]
+        L.sph_write_vtk.argtypes = [ctypes.c_char_p, vp, vp, vp, i32, ctypes.POINTER(ctypes.c_char_p), i32]
         _lib = L
     return _lib
 
@@ -329,3 +331,20 @@ class Batch:
 
     def particles(self):
         return int(lib().sph_batch_particles(self.h))
+
+
+def read_deck(path):
+    """Records of a particle deck in the reference's input format."""
+    n = ctypes.c_int32(0)
+    p = str(path).encode()
+    _check("sph_read_deck", lib().sph_read_deck(p, None, 0, ctypes.byref(n)))
+    P = np.zeros(n.value, PART1)
+    _check("sph_read_deck", lib().sph_read_deck(p, _p(P), len(P), ctypes.byref(n)))
+    return P
+
+
+def write_vtk(path, P1, labels, P2=None, P3=None):
+    """The reference's binary VTK of the records (labels as in its solv.txt)."""
+    arr = (ctypes.c_char_p * len(labels))(*[l.encode() for l in labels])
+    P1 = np.ascontiguousarray(P1, dtype=PART1)
+    _check("sph_write_vtk", lib().sph_write_vtk(str(path).encode(), _p(P1), _p(P2), _p(P3), len(P1), arr, len(labels)))
