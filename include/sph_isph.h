@@ -290,6 +290,26 @@ int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double
  * with i_type 1 or 2, one FIELD array per label (the reference's labels and
  * prefix matching); P2 / P3 may be NULL unless a label needs them. */
 int sph_read_deck(const char *path, sph_part1 *out, int capacity, int *n);
+/* The solver input of read_solv_input (function_init.cuh:166-463) into
+ * p->vii / p->vif: the slots it sets and the switches it clears, the other
+ * slots as the caller left them.  atmospheric-stability, terrain-type and
+ * BAPR_frequency are read but, as in the reference (whose parser writes them
+ * to the host shadow of the constant table, overwritten at
+ * ISPH_Calc.cuh:366), change nothing.  plot-variables labels go to
+ * plot_labels (20 x 20 chars, may be NULL), their count to *n_labels. */
+int sph_read_solv(const char *path, sph_params *p, char *plot_labels, int *n_labels);
+/* The host pass the reference runs on deck records before upload
+ * (c_initial_inner_outer_particle_single, functions_NNPS.cuh:196-373), in
+ * place: i_type 1, buffer_type 0, m_ref = m, uy = uz = 0, temp 300,
+ * ux = p->profile_z/u table at z, k_turb = the k table at z (k_table = n_k
+ * heights then n_k values; NULL = the reference's Case-H table,
+ * functions_NNPS.cuh:156-171), p_type 3 -> 1, rho 1.225 for p_type 0 and
+ * 1000, and with vii[open_boundary] > 0 the buffer classes of p_type +-1
+ * against p->l2, p->l3, l4, p->l_left, p->l_right and l_ceiling
+ * (functions_NNPS.cuh:5-11: 2210 and 1.910).  In 3-D ux is zeroed below
+ * z = 0 and for p_type other than +-1. */
+int sph_initial_records(const sph_params *p, sph_part1 *P1, int n, const double *k_table, int n_k,
+                        double l4, double l_ceiling);
 int sph_write_vtk(const char *path, const sph_part1 *P1, const sph_part2 *P2, const sph_part3 *P3, int n,
                   const char *const *labels, int nlabels);
 

@@ -302,6 +302,34 @@ void ref_step(part1 *P1, part1 *SP1, part2 *P2, part2 *SP2, part3 *P3, int *g_id
 #undef PHASE
 }
 
+// read_solv_input (function_init.cuh:166-463) on the given tables (in/out);
+// copies the plot labels out and returns their count
+int ref_read_solv(const char *path, int *vii_io, float *vif_io, char *labels_out) {
+    std::memcpy(vii, vii_io, sizeof(int_t) * vii_size);
+    std::memcpy(vif, vif_io, sizeof(Real) * vif_size);
+    num_plot_data = 0;
+    read_solv_input(vii, vif, path);
+    std::memcpy(vii_io, vii, sizeof(int_t) * vii_size);
+    std::memcpy(vif_io, vif, sizeof(Real) * vif_size);
+    for (int k = 0; k < num_plot_data && k < 20; ++k) std::memcpy(labels_out + 20 * k, plot_data[k], 20);
+    return num_plot_data;
+}
+
+// c_initial_inner_outer_particle_single (functions_NNPS.cuh:196-373) over n
+// records in place, with the open-boundary switch and dimension given; the
+// terrain switch of the host shadow table is set to the one case that
+// prints nothing per record
+int ref_initial_records(part1 *P, int n, int open, int dimension) {
+    vii[5] = open;
+    vii[1] = dimension;
+    vii[23] = n;
+    k_vii[46] = 3;
+    std::vector<part1> D(n > 0 ? n : 1);
+    c_initial_inner_outer_particle_single(P, D.data(), 0);
+    std::memcpy(P, D.data(), sizeof(part1) * n);
+    return 0;
+}
+
 // read_input (function_init.cuh:550-676) into P1 (capacity records, i_type
 // cleared first); returns the number of records read
 int ref_read_input(part1 *P1, int capacity, const char *path) {

@@ -1,0 +1,89 @@
+"""The case runner: solver input + particle deck in the reference's formats
+through set-up, stepping and VTK output (set-up on the CPU, the run on the
+GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from sph_b200 import abi, decks, driver, layout
+
+SOLV = """\
+solver_type : ISPH
+dimension(1/2/3): 3
+kernel type : Wendland6
+time integration : Predictor_Corrector
+open boundary type: OPEN
+pressure-force : YES
+viscous-force : Cleary
+turbulence-model : SSM
+gravitational-force : NO
+kernel-gradient-correction : NO
+noslip_boundary : YES
+APR_solve : {apr}
+Buffersize: 0.25
+kappa: 2.0
+time-step : 1e-4
+start-time : {t0}
+end-time : 1.0
+filtering : 1
+plot-output : 2
+plot-variables: 3 velocity pressure p_type
+velocity-limit : 50.0
+"""
+
+CODES = (1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 26, 27)
+FIELDS = {1: "x", 2: "y", 3: "z", 4: "ux", 5: "uy", 6: "uz", 7: "m", 8: "p_type", 9: "h", 10: "temp",
+          11: "pres", 12: "rho", 26: "h_ref", 27: "m_ref"}
+
+
+def write_case(tmp_path, apr="NO", t0="0.0"):
+    P, _ = decks.caseh_mini()
+    lines = ["\t".join(str(c) for c in CODES)]
+    for r in P:
+        lines.append("\t".join(str(int(r["p_type"])) if c == 8 else "%.9g" % float(r[FIELDS[c]])
+                               for c in CODES))
+    deck = tmp_path / "deck.txt"
+    deck.write_text("\n".join(lines) + "\n")
+    solv = tmp_path / "solv.txt"
+    solv.write_text(SOLV.format(apr=apr, t0=t0))
+    return solv, deck, P
+
+
+def test_setup_reads_solver_input_and_deck(tmp_path):
+    solv, deck, P = write_case(tmp_path)
+    p, labels, Q = driver.setup(solv, deck)
+    assert labels == ["velocity", "pressure", "p_type"]
+    assert p.geti("solver_type") == 1 and p.geti("time_type") == 1 and p.geti("open_boundary") == 1
+    assert p.geti("freq_output") == 2 and p.getf("dt") == np.float32(1e-4)
+    assert len(Q) == len(P) and p.geti("num_part2") == len(P) and p.geti("count") == 0
+    # the host pass ran: buffer classes assigned, m_ref = m, temp 300
+    assert (Q["i_type"] == 2).sum() > 0
+    assert np.array_equal(Q["m_ref"], Q["m"]) and np.all(Q["temp"] == np.float32(300.0))
+    assert p.geti("NI") > 0 and p.geti("num_cells") == p.geti("NI") * p.geti("NJ") * p.geti("NK") + 1
+
+
+def test_setup_reserves_apr_headroom_and_restart_count(tmp_path):
+    solv, deck, P = write_case(tmp_path, apr="Cell", t0="0.0025")
+    p, _, Q = driver.setup(solv, deck)
+    extra = int(np.float32(0.25) * len(P))
+    assert len(Q) == len(P) + extra and p.geti("num_part") == len(P)
+    assert np.all(Q["i_type"][len(P):] == 3)
+    assert p.geti("count") == 25          # floor(time / dt + 0.5)
+
+
+@pytest.mark.gpu
+def test_run_writes_reference_vtk_series(tmp_path):
+    solv, deck, _ = write_case(tmp_path)
+    out = tmp_path / "out"
+    log = []
+    steps, P = driver.run(solv, deck, out, max_steps=3, log=log.append)
+    assert steps == 3
+    names = sorted(os.listdir(out))
+    assert names == ["fluid_0stp.vtk", "fluid_2stp.vtk"]
+    alive = np.isin(P["i_type"], (1, 2))
+    assert np.all(np.isfinite(P["ux"][alive])) and np.all(np.isfinite(P["pres"][alive]))
+    assert np.abs(P["ux"][alive]).max() < 50.0
+    data = (out / "fluid_2stp.vtk").read_bytes()
+    assert b"POINTS\t%d\tfloat" % alive.sum() in data
+    assert any("tu_max" in line for line in log)

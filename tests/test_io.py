@@ -9,6 +9,7 @@ parsed back independently of the reference.
 import os
 
 import numpy as np
+import pytest
 
 from sph_b200 import abi, layout
 
@@ -82,3 +83,55 @@ def test_label_that_needs_part2_is_rejected_without_it(tmp_path):
     import pytest
     with pytest.raises(abi.SphError):
         abi.write_vtk(tmp_path / "x.vtk", Q, ["rho_ref"])
+
+
+S = np.load(os.path.join(HERE, "golden", "solv_ref.npz"))
+
+
+def test_read_solv_matches_reference_parser(tmp_path):
+    """Every k_vii / k_vif slot and plot label equals what the reference's
+    read_solv_input made of the same file from the same starting tables."""
+    for name in S["names"]:
+        name = str(name)
+        path = tmp_path / (name + ".txt")
+        path.write_bytes(S["text_" + name].tobytes())
+        p = abi.params_init()
+        for k in range(64):
+            p.vii[k] = int(S["vii0"][k])
+        for k in range(32):
+            p.vif[k] = float(S["vif0"][k])
+        q, labels = abi.read_solv(path, p)
+        vii = np.array(q.vii[:64], np.int32)
+        vif = np.array(q.vif[:32], np.float32)
+        assert np.array_equal(vii, S["vii_" + name]), (name, np.nonzero(vii != S["vii_" + name]))
+        assert vif.tobytes() == S["vif_" + name].tobytes(), name
+        n = int(S["nlab_" + name])
+        raw = S["labels_" + name].tobytes()
+        assert labels == [raw[20 * k:20 * k + 20].split(b"\0")[0].decode() for k in range(n)], name
+
+
+def test_read_solv_missing_file_is_an_error(tmp_path):
+    with pytest.raises(abi.SphError):
+        abi.read_solv(tmp_path / "absent.txt")
+
+
+def test_initial_records_match_reference_host_pass():
+    """Records after the host pass equal, byte for byte, what the reference's
+    c_initial_inner_outer_particle_single made of the same deck records."""
+    from sph_b200 import params as sp
+    P = S["init_in"].view(layout.PART1)
+    for tag, open_b, dim in (("open3", 1, 3), ("closed3", 0, 3), ("open2", 1, 2)):
+        p = sp.default_params(open_boundary=open_b)
+        p.seti("dim", dim)
+        Q = abi.initial_records(p, P)
+        R = S["init_" + tag].view(layout.PART1)
+        for f in layout.PART1.names:
+            assert Q[f].tobytes() == R[f].tobytes(), (tag, f)
+
+
+def test_initial_records_rejects_short_tables():
+    from sph_b200 import params as sp
+    p = sp.default_params()
+    P = S["init_in"].view(layout.PART1)[:4]
+    with pytest.raises(abi.SphError):
+        abi.initial_records(p, P, k_table=([0.0], [1.0]))

@@ -168,3 +168,246 @@ extern "C" int sph_write_vtk(const char *path, const sph_part1 *P1, const sph_pa
     if (need) { set_error("sph_write_vtk: a label needs the part2 / part3 records"); return SPH_ERR_BAD_ARG; }
     return SPH_OK;
 }
+
+// ---- solver input file -----------------------------------------------------------
+// read_solv_input (function_init.cuh:166-463).  The file is a stream of
+// whitespace-separated tokens.  For every token read, the keywords are tried
+// in a fixed order against the CURRENT token; a keyword that matches reads
+// its fixed number of tokens (the last one the value) and the later keywords
+// are then tried against that value, exactly as the reference's chain of
+// plain `if`s does.  A read past the end of the file leaves the token as it
+// was, and the pass for the failed read still runs once before the loop
+// ends, as the reference's does.
+//
+// Three keywords never reach the tables the step reads: function_init.cuh
+// redefines atmos_stab, terrain_type (lines 133-134) and freq_bapr (line 128)
+// to k_vii slots before the parser, so the parser clears and sets the host
+// shadow of the __constant__ table, which the upload at ISPH_Calc.cuh:366
+// then overwrites with vii.  Their tokens are read here as there (slot -1)
+// and vii[40], vii[45] and vii[46] keep the caller's values.
+namespace {
+
+enum SolvKind { SOLV_INT, SOLV_FLOAT, SOLV_ENUM, SOLV_BLOCK, SOLV_LABELS };
+
+struct SolvRule {
+    const char *key;
+    int tokens;          // tokens read after the keyword (the last one is the value)
+    SolvKind kind;
+    int slot;            // k_vii slot (INT, ENUM, BLOCK) or k_vif slot (FLOAT); -1 reads only
+    const char *names;   // ENUM: "name=value" pairs, space separated
+};
+
+// Keyword order, token counts and slots of function_init.cuh:194-459.
+const SolvRule kSolvRules[] = {
+    {"solver_type", 2, SOLV_ENUM, 0, "WCSPH=0 ISPH=1"},
+    {"dimension(1/2/3):", 1, SOLV_INT, 1, nullptr},
+    {"property_table(YES/NO):", 1, SOLV_ENUM, 2, "YES=1 NO=0"},
+    {"atmospheric-stability", 2, SOLV_ENUM, -1, "Unstable=0 Neutral=1 Stable=2"},
+    {"terrain-type", 2, SOLV_ENUM, -1, "Flat=0 Grass=1 Forest=2 City=3 Ocean=4"},
+    {"kernel", 3, SOLV_ENUM, 3, "Quartic=2 Gaussian=0 Quintic=1 Wendland2=3 Wendland4=4 Wendland6=5"},
+    {"time", 3, SOLV_ENUM, 4, "Euler=0 Predictor_Corrector=1"},
+    {"structure", 2, SOLV_ENUM, 44, "YES=1 NO=0"},
+    {"open", 3, SOLV_ENUM, 5, "OPEN=1 PERIODIC=2 NO=0"},
+    {"pressure-force", 2, SOLV_ENUM, 12, "YES=1 NO=0"},
+    {"viscous-force", 2, SOLV_ENUM, 13, "NO=0 Cleary=1 Monaghan=2 Violeau=3"},
+    {"turbulence-model", 2, SOLV_ENUM, 18, "Laminar=0 k-lm=1 k-e=2 HB=3 SSM=4 DDF=5"},
+    {"gravitational-force", 2, SOLV_ENUM, 14, "YES=1 NO=0"},
+    {"Conduction(YES/NO):", 1, SOLV_ENUM, 15, "YES=1 NO=0"},
+    {"Boussinesq-natural-convection", 2, SOLV_ENUM, 16, "YES=1 NO=0"},
+    {"Concentration-diffusion(YES/NO):", 1, SOLV_ENUM, 19, "YES=1 NO=0"},
+    {"kernel-gradient-correction", 2, SOLV_ENUM, 17, "NO=0 KGC=1 FPM=2 DFPM=3 KGF=4"},
+    {"switch_ptype", 2, SOLV_ENUM, 33, "YES=1 NO=0"},
+    {"noslip_boundary", 2, SOLV_ENUM, 34, "YES=1 NO=0"},
+    {"APR_solve", 2, SOLV_ENUM, 35, "Cell=1 Switch=2 Block=3 NO=0"},
+    {"Block_configuration", 2, SOLV_BLOCK, 41, nullptr},
+    {"Variable", 2, SOLV_ENUM, 36, "Abrupt=1 Smooth=2 NO=0"},
+    {"Buffersize:", 1, SOLV_FLOAT, 19, nullptr},
+    {"reference-pressure", 2, SOLV_FLOAT, 1, nullptr},
+    {"kappa:", 1, SOLV_FLOAT, 0, nullptr},
+    {"minimum-iteration:", 1, SOLV_INT, 20, nullptr},
+    {"maximum-iteration:", 1, SOLV_INT, 21, nullptr},
+    {"pressure-convergence", 2, SOLV_FLOAT, 7, nullptr},
+    {"density-convergence", 2, SOLV_FLOAT, 6, nullptr},
+    {"pressure-relaxation", 2, SOLV_FLOAT, 8, nullptr},
+    {"time-step", 2, SOLV_FLOAT, 2, nullptr},
+    {"start-time", 2, SOLV_FLOAT, 3, nullptr},
+    {"end-time", 2, SOLV_FLOAT, 4, nullptr},
+    {"neighbor", 4, SOLV_ENUM, 7, "3X3=0 5X5=1"},
+    {"timestep", 3, SOLV_ENUM, 6, "YES=1 NO=0"},
+    {"structure-timestep", 2, SOLV_FLOAT, 20, nullptr},
+    {"filtering", 2, SOLV_INT, 8, nullptr},
+    {"temperature-filtering", 2, SOLV_INT, 10, nullptr},
+    {"plot-output", 2, SOLV_INT, 11, nullptr},
+    {"APR_frequency:", 1, SOLV_INT, 37, nullptr},
+    {"h-reset", 2, SOLV_INT, 38, nullptr},
+    {"BAPR_frequency:", 1, SOLV_INT, -1, nullptr},
+    {"plot-variables:", 1, SOLV_LABELS, 0, nullptr},
+    {"velocity-limit", 2, SOLV_FLOAT, 5, nullptr},
+};
+
+// The value of `tok` in a "name=value" list, or false when it is not there.
+bool solv_enum(const char *names, const char *tok, int *value) {
+    const size_t n = strlen(tok);
+    for (const char *q = names; *q;) {
+        const char *eqs = strchr(q, '=');
+        if ((size_t)(eqs - q) == n && strncmp(q, tok, n) == 0) {
+            *value = atoi(eqs + 1);
+            return true;
+        }
+        q = strchr(eqs, ' ');
+        if (!q) break;
+        ++q;
+    }
+    return false;
+}
+
+}  // namespace
+
+extern "C" int sph_read_solv(const char *path, sph_params *p, char *plot_labels, int *n_labels) {
+    using namespace sph;
+    if (!path || !p) return SPH_ERR_BAD_ARG;
+    FILE *f = fopen(path, "r");
+    if (!f) { set_error("sph_read_solv: cannot open the solver input"); return SPH_ERR_BAD_ARG; }
+    int *vii = p->vii;
+    float *vif = p->vif;
+    // the switches function_init.cuh:168-179 clears before reading
+    vii[0] = 0;
+    for (int s : {12, 13, 14, 15, 16, 17, 18, 19, 35, 44}) vii[s] = 0;
+    char tok[1000];
+    tok[0] = 0;
+    auto next = [&]() { return fscanf(f, "%999s", tok) == 1; };
+    int nlab = 0;
+    for (;;) {
+        const bool got = next();
+        for (const SolvRule &r : kSolvRules) {
+            if (strcmp(tok, r.key) != 0) continue;
+            switch (r.kind) {
+            case SOLV_INT:
+                for (int q = 0; q < r.tokens; ++q) next();
+                if (r.slot >= 0) vii[r.slot] = atoi(tok);
+                break;
+            case SOLV_FLOAT:
+                for (int q = 0; q < r.tokens; ++q) next();
+                vif[r.slot] = (float)atof(tok);
+                break;
+            case SOLV_ENUM: {
+                for (int q = 0; q < r.tokens; ++q) next();
+                int v;
+                if (solv_enum(r.names, tok, &v) && r.slot >= 0) vii[r.slot] = v;
+                break;
+            }
+            case SOLV_BLOCK:   // NBI, NBJ, NBK, each after one skipped token
+                for (int d = 0; d < 3; ++d) {
+                    next();
+                    next();
+                    vii[r.slot + d] = atoi(tok);
+                }
+                break;
+            case SOLV_LABELS: {
+                next();
+                const int k = atoi(tok);
+                nlab = k;
+                for (int q = 0; q < k; ++q) {
+                    char lab[1000];
+                    if (fscanf(f, "%999s", lab) != 1) continue;
+                    if (plot_labels && q < 20) {
+                        strncpy(plot_labels + 20 * q, lab, 19);
+                        plot_labels[20 * q + 19] = 0;
+                    }
+                }
+                break;
+            }
+            }
+        }
+        if (!got) break;
+    }
+    fclose(f);
+    if (n_labels) *n_labels = nlab;
+    return SPH_OK;
+}
+
+// ---- record initialisation -------------------------------------------------------
+// c_initial_inner_outer_particle_single (functions_NNPS.cuh:196-373): the
+// host pass that turns deck records into the records the step starts from.
+namespace {
+
+// Case-H turbulent kinetic energy profile of Interpolate_k_caseH
+// (functions_NNPS.cuh:156-171), z then k.
+const double kCaseHK[2][22] = {
+    {0.00393, 0.01178, 0.02356, 0.04123, 0.06086, 0.08245, 0.10209, 0.11975, 0.14135, 0.16294, 0.21202,
+     0.23166, 0.25325, 0.30233, 0.35141, 0.40442, 0.4535, 0.50061, 0.55362, 0.60466, 0.70282, 0.74209},
+    {0.3687, 0.39304, 0.4313, 0.49043, 0.53913, 0.56696, 0.58087, 0.62261, 0.62957, 0.64696, 0.66087,
+     0.64696, 0.62261, 0.5913, 0.51826, 0.4313, 0.3513, 0.25043, 0.17043, 0.10087, 0.0, 0.0},
+};
+
+// Piecewise-linear table lookup of functions_NNPS.cuh:130-150: linear inside
+// the table, extended past either end along its first or last segment.
+double table_lerp(const double *zt, const double *vt, int n, double z) {
+    if (z <= zt[0]) {
+        const double dz = zt[1] - zt[0], dv = vt[1] - vt[0];
+        return vt[0] + (dz == 0.0 ? 0.0 : (z - zt[0]) * (dv / dz));
+    }
+    if (z >= zt[n - 1]) {
+        const double dz = zt[n - 1] - zt[n - 2], dv = vt[n - 1] - vt[n - 2];
+        return vt[n - 2] + (dz == 0.0 ? 0.0 : (z - zt[n - 2]) * (dv / dz));
+    }
+    int lo = 0, hi = n;              // first entry with zt >= z
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (zt[mid] < z) lo = mid + 1; else hi = mid;
+    }
+    const int i = lo > 0 ? lo : 1;
+    const double t = (z - zt[i - 1]) / (zt[i] - zt[i - 1]);
+    return (1.0 - t) * vt[i - 1] + t * vt[i];
+}
+
+}  // namespace
+
+extern "C" int sph_initial_records(const sph_params *p, sph_part1 *P1, int n, const double *k_table, int n_k,
+                                   double l4, double l_ceiling) {
+    using namespace sph;
+    if (!p || (!P1 && n > 0) || n < 0) return SPH_ERR_BAD_ARG;
+    if (p->n_profile < 2 || p->n_profile > SPH_MAX_PROFILE) {
+        set_error("sph_initial_records: the velocity profile needs 2..SPH_MAX_PROFILE points");
+        return SPH_ERR_BAD_ARG;
+    }
+    if (k_table && n_k < 2) { set_error("sph_initial_records: k table needs >= 2 points"); return SPH_ERR_BAD_ARG; }
+    const double *kz = k_table ? k_table : kCaseHK[0];
+    const double *kv = k_table ? k_table + n_k : kCaseHK[1];
+    const int nk = k_table ? n_k : 22;
+    const bool open = p->vii[SPH_VII_OPEN_BOUNDARY] > 0;
+    const bool dim3 = p->vii[SPH_VII_DIM] == 3;
+    const float scale = 0.16f / 0.16f;   // building height 0.16 m, as the reference hard-wires it
+    for (int i = 0; i < n; ++i) {
+        sph_part1 &r = P1[i];
+        r.i_type = 1;
+        r.buffer_type = 0;
+        r.m_ref = r.m;
+        r.uy = 0.0f;
+        r.uz = 0.0f;
+        r.temp = 300.0f;
+        const float zs = scale * r.z;
+        r.ux = (float)table_lerp(p->profile_z, p->profile_u, p->n_profile, zs);
+        r.k_turb = (float)table_lerp(kz, kv, nk, zs);
+        if (r.p_type == 3) r.p_type = 1;
+        if (r.p_type == 0 || r.p_type == 1000) r.rho = 1.225f;
+        const bool moving = r.p_type == 1 || r.p_type == -1;
+        if (open && moving) {
+            // buffer classes; the comparisons are in the record's float
+            // promoted to double, as there
+            if (r.y < p->l_left) { r.buffer_type = 3; r.i_type = 2; }
+            else if (r.y > p->l_right) { r.buffer_type = 4; r.i_type = 2; }
+            else if (r.x >= p->l3 - 1e-6 && r.x < l4 - 1e-6) { r.buffer_type = 2; r.i_type = 2; }
+            else if (r.x < p->l2 - 1e-6) { r.buffer_type = 1; r.i_type = 2; }
+            if (r.z >= l_ceiling && r.y < p->l_left && r.y > p->l_right) r.buffer_type = 5;
+        }
+        if (dim3) {
+            if (moving) {
+                if (r.z < 0) r.ux = 0.0f;
+            } else {
+                r.ux = 0.0f;
+            }
+        }
+    }
+    return SPH_OK;
+}

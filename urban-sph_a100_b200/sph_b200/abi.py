@@ -30,6 +30,7 @@ SYMBOLS = (
     "sph_ml_grad", "sph_ml_predict_samples",
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
     "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
+    "sph_read_solv", "sph_initial_records",
 )
 
 _lib = None
@@ -99,6 +100,8 @@ def lib():
         L.sph_apr.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
         L.sph_set_ib_boxes.argtypes = [vp, vp, i32]
         L.sph_read_deck.argtypes = [ctypes.c_char_p, vp, i32, ctypes.POINTER(i32)]
+        L.sph_read_solv.argtypes = [ctypes.c_char_p, vp, vp, ctypes.POINTER(i32)]
+        L.sph_initial_records.argtypes = [vp, vp, i32, vp, i32, ctypes.c_double, ctypes.c_double]
         L.sph_write_vtk.argtypes = [ctypes.c_char_p, vp, vp, vp, i32, ctypes.POINTER(ctypes.c_char_p), i32]
         _lib = L
     return _lib
@@ -348,3 +351,32 @@ def write_vtk(path, P1, labels, P2=None, P3=None):
     arr = (ctypes.c_char_p * len(labels))(*[l.encode() for l in labels])
     P1 = np.ascontiguousarray(P1, dtype=PART1)
     _check("sph_write_vtk", lib().sph_write_vtk(str(path).encode(), _p(P1), _p(P2), _p(P3), len(P1), arr, len(labels)))
+
+
+def read_solv(path, params=None):
+    """Parameters and plot labels from a solver input file in the reference's format."""
+    p = params.copy() if params is not None else params_init()
+    labels = ctypes.create_string_buffer(400)
+    n = ctypes.c_int32(0)
+    _check("sph_read_solv", lib().sph_read_solv(str(path).encode(), ctypes.byref(p), labels, ctypes.byref(n)))
+    raw = labels.raw
+    return p, [raw[20 * k:20 * k + 20].split(b"\0")[0].decode() for k in range(min(n.value, 20))]
+
+
+CASEH_L4 = 2210.0          # functions_NNPS.cuh:7
+CASEH_L_CEILING = 1.910    # functions_NNPS.cuh:11
+
+
+def initial_records(params, P1, k_table=None, l4=CASEH_L4, l_ceiling=CASEH_L_CEILING):
+    """The reference's host pass over deck records before upload (in a copy)."""
+    P = np.array(P1, dtype=PART1, copy=True)
+    kt = None
+    nk = 0
+    if k_table is not None:
+        z, k = k_table
+        kt = np.ascontiguousarray(np.concatenate([np.asarray(z, np.float64), np.asarray(k, np.float64)]))
+        nk = len(z)
+    _check("sph_initial_records", lib().sph_initial_records(ctypes.byref(params), _p(P), len(P),
+                                                            None if kt is None else _p(kt), nk,
+                                                            float(l4), float(l_ceiling)))
+    return P

@@ -1,0 +1,104 @@
+"""Case runner in the shape of the reference's program.
+
+The reference's main (SOPHIA_gpu.cu:120-141) reads ./input/solv.txt with
+read_solv_input, then ISPH (ISPH.cuh:53-125) reads the particle deck, sets
+the domain and the cell grid, and reserves ``buffersize * num_part`` extra
+records when APR is on; c_initial_inner_outer_particle_single
+(functions_NNPS.cuh:196-373) prepares the deck records on the host; ISPH_Calc (ISPH_Calc.cuh:239-528) starts the step
+counter at floor(time / dt + 0.5) and steps until ``time >= time_end``,
+writing the binary VTK after every step whose counter (taken before the
+step's increment) is a multiple of ``freq_output`` and printing the
+max |u| / max |ftotal| line every ``freq_output`` steps.
+
+``run`` does the same through the C ABI: solver input and deck in the
+reference's formats, one device context, VTK files named
+``fluid_<count>stp.vtk`` in ``out_dir`` with the solver input's
+plot-variables.  Settings the solver input does not carry (the PPE solver
+form, the wall-model and MOST constants, the inflow profile) come from
+``base`` (default: ``params.default_params()``).
+
+    python -m sph_b200.driver solv.txt deck.txt out_dir [--steps N]
+"""
+import argparse
+import math
+import os
+import time as _wall
+
+import numpy as np
+
+from . import abi, params as _params
+from .layout import PART1
+
+
+def setup(solv_path, deck_path, base=None):
+    """Parameters, plot labels and records (with APR headroom) of a case."""
+    p = base.copy() if base is not None else _params.default_params()
+    p, labels = abi.read_solv(solv_path, p)
+    P1 = abi.read_deck(deck_path)
+    abi.domain_setup(p, P1)
+    P1 = abi.initial_records(p, P1)   # ISPH_Calc.cuh:386
+    n = len(P1)
+    extra = int(p.getf("buffersize") * n) if p.geti("apr_solv") else 0   # ISPH.cuh:116
+    if extra > 0:
+        D = np.zeros(extra, dtype=PART1)
+        D["i_type"] = 3
+        for f in ("x", "y", "z", "h", "h_ref", "m", "m_ref", "rho", "vol"):
+            D[f] = P1[f][0]
+        P1 = np.concatenate([P1, D])
+    p.seti("num_part", n)
+    p.seti("num_part2", len(P1))
+    dt = np.float32(p.getf("dt"))
+    p.seti("count", int(math.floor(float(np.float32(p.getf("time")) / dt) + 0.5)))   # ISPH_Calc.cuh:256
+    return p, labels, P1
+
+
+def run(solv_path, deck_path, out_dir=None, base=None, precision=0, max_steps=None, log=print):
+    """Steps a case from its solver input and deck; returns (steps, final records)."""
+    p, labels, P1 = setup(solv_path, deck_path, base)
+    if out_dir is not None:
+        os.makedirs(out_dir, exist_ok=True)
+    freq = max(p.geti("freq_output"), 1)
+    dt = np.float32(p.getf("dt"))
+    t = np.float32(p.getf("time"))
+    t_end = np.float32(p.getf("time_end"))
+    count = p.geti("count")
+    sim = abi.Simulation(p, precision=precision)
+    try:
+        sim.upload(P1)
+        wall0 = _wall.perf_counter()
+        steps = 0
+        while True:
+            sim.step(1)
+            if out_dir is not None and count % freq == 0:
+                Q1, Q2, Q3 = sim.download()
+                abi.write_vtk(os.path.join(out_dir, "fluid_%dstp.vtk" % count), Q1, labels, P2=Q2, P3=Q3)
+            t = np.float32(t + dt)
+            count += 1
+            steps += 1
+            if count % freq == 0 and log is not None:
+                umax, _, fmax = sim.diagnostics()
+                log("Simulation time: %5.2f sec" % t)
+                log("Computing time: %5.2f sec" % (_wall.perf_counter() - wall0))
+                log("%d\t tu_max=%5.2f\tftotal_max=%5.5f" % (count, umax, fmax))
+            if t >= t_end or (max_steps is not None and steps >= max_steps):
+                break
+        P_final, _, _ = sim.download(want=(1,))
+        return steps, P_final
+    finally:
+        sim.close()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("solv")
+    ap.add_argument("deck")
+    ap.add_argument("out_dir")
+    ap.add_argument("--steps", type=int, default=None, help="stop after this many steps")
+    ap.add_argument("--fp64", action="store_true", help="FP64 context instead of FP32")
+    a = ap.parse_args(argv)
+    run(a.solv, a.deck, a.out_dir, precision=1 if a.fp64 else 0, max_steps=a.steps)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
