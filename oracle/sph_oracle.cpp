@@ -42,8 +42,11 @@ struct P {
     int fp_solve() const { return p.vii[12]; }
     int fv_solve() const { return p.vii[13]; }
     int fg_solve() const { return p.vii[14]; }
+    int con_solve() const { return p.vii[15]; }
+    int boussinesq() const { return p.vii[16]; }
     int kgc_solve() const { return p.vii[17]; }
     int turb() const { return p.vii[18]; }
+    int concn_solve() const { return p.vii[19]; }
     int NI() const { return p.vii[24]; }
     int NJ() const { return p.vii[25]; }
     int NK() const { return p.vii[26]; }
@@ -66,6 +69,13 @@ struct P {
 
 const double PI_REF = 3.141592653;      // Parameters.cuh:32
 const double GRAV = 9.810;              // Parameters.cuh:34
+// thermal constants, Parameters.cuh:120-131 (Air_cp is an int literal there)
+const double SOLID_CP = 900.0;
+const int AIR_CP = 1005;
+const double SOLID_K = 1.0;
+const double AIR_K = 0.025;
+const double SOLID_RHO = 2300.0;
+const double TEMPB = 300.0;
 
 // ---- kernel functions, functions_KNL.cuh:2-103 and :326-369 -----------------
 template <class Real>
@@ -175,17 +185,17 @@ struct State {
 
 template <class Real>
 struct P2State {
-    std::vector<Real> rho_ref, SR, x0, y0, z0, ux0, uy0, uz0, temp0;
+    std::vector<Real> rho_ref, SR, x0, y0, z0, ux0, uy0, uz0, temp0, concn0;
     void resize(int n) {
-        for (auto *v : {&rho_ref, &SR, &x0, &y0, &z0, &ux0, &uy0, &uz0, &temp0}) v->assign(n, Real(0));
+        for (auto *v : {&rho_ref, &SR, &x0, &y0, &z0, &ux0, &uy0, &uz0, &temp0, &concn0}) v->assign(n, Real(0));
     }
 };
 
 template <class Real>
 struct P3State {
-    std::vector<Real> ftx, fty, ftz, ft, fpx, fpy, fpz, dtemp, nx, ny, nz, gxx, gyy, gzz, gxy, gyz, gzx;
+    std::vector<Real> ftx, fty, ftz, ft, fpx, fpy, fpz, dtemp, dconcn, nx, ny, nz, gxx, gyy, gzz, gxy, gyz, gzx;
     void reset(int n) {
-        for (auto *v : {&ftx, &fty, &ftz, &ft, &fpx, &fpy, &fpz, &dtemp, &nx, &ny, &nz, &gxx, &gyy,
+        for (auto *v : {&ftx, &fty, &ftz, &ft, &fpx, &fpy, &fpz, &dtemp, &dconcn, &nx, &ny, &nz, &gxx, &gyy,
                         &gzz, &gxy, &gyz, &gzx})
             v->assign(n, Real(0));
     }
@@ -638,17 +648,30 @@ struct Oracle {
         }
     }
 
-    // KERNEL_advection_force3D, functions_PPE.cuh:191-480 (con/concn/boussinesq off)
+    // KERNEL_advection_force3D, functions_PPE.cuh:191-480, with the
+    // conduction / Eulerian temperature term (con_solve), concentration
+    // advection-diffusion (concn_solve) and Boussinesq buoyancy; the literal
+    // types of the reference's expressions are kept (double constants promote
+    // a float expression to double before it is stored).
     void advection(State<Real> &A) {
         const P Q = q();
+        const bool con = Q.con_solve() != 0, cnc = Q.concn_solve() != 0, bsq = Q.boussinesq() != 0;
         for (int i = 0; i < n(); ++i) {
             if (A.i_type[i] > 2 || A.p_type[i] == 1000 || A.p_type[i] <= 0) continue;
             int ptypei = A.p_type[i];
             Real xi = A.x[i], yi = A.y[i], zi = A.z[i], uxi = A.ux[i], uyi = A.uy[i], uzi = A.uz[i];
-            Real hi = A.h[i], mi = A.m[i], rhoi = A.rho[i];
+            Real hi = A.h[i], mi = A.m[i], rhoi = A.rho[i], tempi = A.temp[i];
             Real tmp_A = calc_tmpA(Q, hi);
+            Real kci = 0, cpi = 0, concni = 0, diffi = 0;
+            if (con) {
+                kci = SOLID_K * (ptypei == 0 || ptypei == 1000) + AIR_K * (ptypei == 1 || ptypei == -1);
+                cpi = SOLID_CP * (ptypei == 0 || ptypei == 1000) + AIR_CP * (ptypei == 1 || ptypei == -1);
+            }
+            if (cnc) { concni = A.concn[i]; diffi = 2.0; }
             Real visi = viscosity2<Real>(prm, ptypei) + A.vis_t[i] * rhoi;
+            Real betai = 1.0 / prm.t_ini;    // thermal_expansion, functions_PROP.cuh:203-212
             Real tx = 0, ty = 0, tz = 0, ex = 0, ey = 0, ez = 0;
+            Real eulert = 0, tmp_Rc = 0, tmp_Rd = 0, tmp_temp = 0, tmp_flt = 0;
             const Real Alpha = (float)prm.av_alpha, Beta = (float)prm.av_beta, c0 = (float)prm.av_c0;
             for (int64_t e = nb_off[i]; e < nb_off[i + 1]; ++e) {
                 int j = nb[e];
@@ -659,9 +682,8 @@ struct Oracle {
                 Real tdwij = calc_dwij(Q, tmp_A, hi, tdist);
                 Real tdwx = tdwij * (xi - xj) / tdist, tdwy = tdwij * (yi - yj) / tdist, tdwz = tdwij * (zi - zj) / tdist;
                 if (Q.kgc_solve() == 1) { tdwx = 0; tdwy = 0; tdwz = 0; }
-                (void)twij;
                 int ptypej = A.p_type[j];
-                Real uxj = A.ux[j], uyj = A.uy[j], uzj = A.uz[j], mj = A.m[j], rhoj = A.rho[j];
+                Real uxj = A.ux[j], uyj = A.uy[j], uzj = A.uz[j], mj = A.m[j], rhoj = A.rho[j], tempj = A.temp[j];
                 if (Q.fv_solve() == 1) {
                     Real visj = viscosity2<Real>(prm, ptypej) + A.vis_t[j] * rhoj;
                     Real C_v = (xi - xj) * tdwx + (yi - yj) * tdwy + (zi - zj) * tdwz;
@@ -687,6 +709,35 @@ struct Oracle {
                     ex += (uxi * (uxj - uxi) * tdwx + uyi * (uxj - uxi) * tdwy + uzi * (uxj - uxi) * tdwz) * mj / rhoj * (1 - A.eli[i]);
                     ey += (uxi * (uyj - uyi) * tdwx + uyi * (uyj - uyi) * tdwy + uzi * (uyj - uyi) * tdwz) * mj / rhoj * (1 - A.eli[i]);
                     ez += (uxi * (uzj - uzi) * tdwx + uyi * (uzj - uzi) * tdwy + uzi * (uzj - uzi) * tdwz) * mj / rhoj * (1 - A.eli[i]);
+                    if (con)
+                        eulert -= 2.0 * mj / (rhoi + rhoj) * (tempj - tempi) *
+                                  ((uxi - uxj) * tdwx + (uyi - uyj) * tdwy + (uzi - uzj) * tdwz) * (1 - A.eli[i]);
+                    if (cnc) {
+                        Real concnj = A.concn[j];
+                        tmp_Rd -= (uxi * (concnj - concni) * tdwx + uyi * (concnj - concni) * tdwy +
+                                   uzi * (concnj - concni) * tdwz) * mj / rhoj * (1 - A.eli[i]);
+                    }
+                }
+                if (con) {   // conduction with the uncorrected dW/dr
+                    Real kcj = SOLID_K * (ptypej == 0 || ptypej == 1000) + AIR_K * (ptypej == 1 || ptypej == -1);
+                    Real rhoj_temp = (ptypej == 1 || ptypej == -1) ? rhoj : (Real)SOLID_RHO;
+                    Real mj_temp = mj * rhoj_temp / rhoj;
+                    Real sum_con_H = 4.0 * mj_temp * kcj * kci * (tempi - tempj) * tdwij;
+                    sum_con_H /= (tdist + 1e-10) * rhoi * rhoj_temp * (kci + kcj);
+                    tmp_Rc += sum_con_H;
+                }
+                if (cnc) {
+                    Real concnj = A.concn[j];
+                    Real diffj = 2.0;
+                    Real tmprd = mi * (diffi * rhoi + diffj * rhoj);
+                    tmprd *= ((xi - xj) * tdwx + (yi - yj) * tdwy + (zi - zj) * tdwz);
+                    tmprd /= (rhoi * rhoj * (tdist * tdist + 0.01 * hi * hi));
+                    Real tmprd1 = tmprd * (concni - concnj) * (ptypei == ptypej);
+                    tmp_Rd += tmprd1;
+                }
+                if (bsq) {
+                    tmp_temp += (mj / rhoj) * tempj * twij;
+                    tmp_flt += (mj / rhoj) * twij;
                 }
                 Real uij_xij = (uxi - uxj) * (xi - xj) + (uyi - uyj) * (yi - yj) + (uzi - uzj) * (zi - zj);
                 if (uij_xij < 0) {
@@ -700,8 +751,11 @@ struct Oracle {
                 }
             }
             if (Q.fg_solve()) tz += -GRAV;
+            if (bsq && ptypei > 0 && ptypei < 1000) tz = betai * GRAV * (tmp_temp / tmp_flt - TEMPB);
             S3.ftx[i] = tx - ex; S3.fty[i] = ty - ey; S3.ftz[i] = tz - ez;
             S3.ft[i] = std::sqrt(tx * tx + ty * ty + tz * tz);
+            if (con) S3.dtemp[i] += tmp_Rc / cpi - eulert;
+            if (cnc) S3.dconcn[i] = tmp_Rd;
         }
     }
 
@@ -729,6 +783,12 @@ struct Oracle {
                 S2.ux0[i] = tux0; S2.uy0[i] = tuy0; S2.uz0[i] = tuz0;
             }
             if (ttime == 0) S2.rho_ref[i] = A.rho[i];
+            if (q().con_solve() == 1) S2.temp0[i] = A.temp[i];
+            if (q().concn_solve() == 1) {
+                Real tconcn = A.concn[i];
+                S2.concn0[i] = tconcn;
+                A.concn[i] = tconcn + S3.dconcn[i] * (tdt);
+            }
         }
     }
 
@@ -1273,9 +1333,18 @@ struct Oracle {
                 if ((uxc * uxc + uyc * uyc + uzc * uzc) >= ul * ul) { uxc = tux0; uyc = tuy0; uzc = tuz0; }
                 T.ux[i] = uxc; T.uy[i] = uyc; T.uz[i] = uzc;
             }
-            T.enthalpy[i] = S.enthalpy[i];
-            T.temp[i] = S.temp[i];
-            T.concn[i] = S.concn[i];
+            if (q().con_solve() == 1) {
+                T.temp[i] = S2.temp0[i] + S3.dtemp[i] * tdt * (bt == 0);
+            } else {
+                T.enthalpy[i] = S.enthalpy[i];
+                T.temp[i] = S.temp[i];
+            }
+            if (q().concn_solve() == 1) {
+                T.concn[i] = S2.concn0[i] + S3.dconcn[i] * tdt;
+                if (T.concn[i] < 0.0) T.concn[i] = 0.0;
+            } else {
+                T.concn[i] = S.concn[i];
+            }
             T.pres[i] = S.pres[i]; T.flt_s[i] = S.flt_s[i]; T.m[i] = S.m[i]; T.ncell[i] = S.ncell[i];
             T.h[i] = S.h[i]; T.k_turb[i] = S.k_turb[i]; T.e_turb[i] = S.e_turb[i]; T.eli[i] = S.eli[i];
             T.vol[i] = S.vol[i]; p2_rho_ref[i] = S2.rho_ref[i]; T.vis_t[i] = S.vis_t[i];
@@ -1418,12 +1487,14 @@ struct Oracle {
                 r.SR = S2.SR.empty() ? 0 : S2.SR[i];
                 r.x0 = S2.x0[i]; r.y0 = S2.y0[i]; r.z0 = S2.z0[i];
                 r.ux0 = S2.ux0[i]; r.uy0 = S2.uy0[i]; r.uz0 = S2.uz0[i];
+                r.temp0 = S2.temp0[i]; r.concn0 = S2.concn0[i];
             }
             if (C) {
                 sph_part3 &r = C[i];
                 std::memset(&r, 0, sizeof(r));
                 r.ftotalx = S3.ftx[i]; r.ftotaly = S3.fty[i]; r.ftotalz = S3.ftz[i]; r.ftotal = S3.ft[i];
                 r.fpx = S3.fpx[i]; r.fpy = S3.fpy[i]; r.fpz = S3.fpz[i]; r.dtemp = S3.dtemp[i];
+                r.dconcn = S3.dconcn[i];
                 r.nx = S3.nx[i]; r.ny = S3.ny[i]; r.nz = S3.nz[i];
                 r.inv_cm_xx = S3.gxx[i]; r.inv_cm_yy = S3.gyy[i]; r.inv_cm_zz = S3.gzz[i];
                 r.inv_cm_xy = S3.gxy[i]; r.inv_cm_yz = S3.gyz[i]; r.inv_cm_zx = S3.gzx[i];

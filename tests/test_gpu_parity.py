@@ -118,3 +118,31 @@ def test_fp64_step_without_most_matches_oracle_tightly():
     errs = {f: rel_err(A[f], B[f]) for f in FIELDS}
     bad = {f: e for f, e in errs.items() if e > FP64_TOL}
     assert not bad, bad
+
+
+THERMAL = {"all": (1, 1, 1), "conduction": (1, 0, 0), "boussinesq": (0, 1, 0), "concentration": (0, 0, 1)}
+
+
+@pytest.mark.parametrize("precision,tol", [(layout.PREC_MIXED, FP32_TOL), (layout.PREC_FP64, FP64_TOL)],
+                         ids=["fp32", "fp64"])
+@pytest.mark.parametrize("name", list(THERMAL))
+def test_thermal_step_matches_oracle(name, precision, tol):
+    """Conduction, Boussinesq buoyancy and concentration transport: the
+    oracle is bit-exact against the reference for these switches
+    (tests/test_oracle.py); the CUDA path agrees with it to the step bar
+    (the deck has MOST particles, whose FP32 forcing sets the FP64 bar)."""
+    P, p = decks.thermal_mini(*THERMAL[name])
+    A, A2, A3, B, B2, B3 = _run_pair(P, p, precision, nsteps=3)
+    lim = FP64_MOST_TOL if precision == layout.PREC_FP64 else tol
+    errs = {f: rel_err(A[f], B[f]) for f in FIELDS + ["concn"]}
+    bad = {f: e for f, e in errs.items() if e > lim}
+    assert not bad, bad
+    for f in ("ftotalx", "ftotaly", "ftotalz", "dtemp", "dconcn"):
+        assert rel_err(A3[f], B3[f]) <= stored_tol(B3[f], lim * 10), f
+    for f in ("temp0", "concn0"):
+        assert rel_err(A2[f], B2[f]) <= stored_tol(B2[f], lim), f
+    fluid = B["p_type"] == 1
+    if THERMAL[name][0]:
+        assert np.abs(B3["dtemp"][fluid]).max() > 0
+    if THERMAL[name][2]:
+        assert np.abs(B3["dconcn"][fluid]).max() > 0

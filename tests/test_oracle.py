@@ -91,6 +91,36 @@ def test_step_bit_exact_vs_reference(name):
         assert np.array_equal(R.SP2[f], B2[f]), f
 
 
+def thermal_deck(con=1, bouss=1, concn=1):
+    return decks.thermal_mini(con, bouss, concn)
+
+
+THERMAL = {"all": (1, 1, 1), "conduction": (1, 0, 0), "boussinesq": (0, 1, 0), "concentration": (0, 0, 1)}
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(THERMAL))
+def test_thermal_step_bit_exact_vs_reference(name):
+    P, p = thermal_deck(*THERMAL[name])
+    R = refhost.RefHost(P, p, parallel=False)
+    O = restated.Restated(P, p, 0)
+    for _ in range(3):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, B2, B3 = O.download()
+    for f in FIELDS + ["concn"]:
+        assert np.array_equal(R.P1[f], B[f]), f
+    for f in ("ftotalx", "ftotaly", "ftotalz", "ftotal", "dtemp", "dconcn"):
+        assert np.array_equal(R.P3[f], B3[f]), f
+    for f in ("temp0", "concn0"):
+        assert np.array_equal(R.SP2[f], B2[f]), f
+    fluid = B["p_type"] == 1
+    if THERMAL[name][0]:
+        assert np.abs(B3["dtemp"][fluid]).max() > 0
+    if THERMAL[name][2]:
+        assert np.abs(B3["dconcn"][fluid]).max() > 0
+
+
 @needs_ref
 def test_euler_time_stepping_bit_exact_vs_reference():
     P, p = _deck({})

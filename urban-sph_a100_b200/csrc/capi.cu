@@ -32,6 +32,9 @@ DevParams make_dev_params(const sph_params &p) {
     d.fv_solve = p.vii[SPH_VII_FV_SOLVE];
     d.fg_solve = p.vii[SPH_VII_FG_SOLVE];
     d.kgc_solve = p.vii[SPH_VII_KGC_SOLVE];
+    d.con_solve = p.vii[SPH_VII_CON_SOLVE];
+    d.boussinesq = p.vii[SPH_VII_BOUSSINESQ];
+    d.concn_solve = p.vii[SPH_VII_CONCN_SOLVE];
     d.turb = p.vii[SPH_VII_TURBULENCE];
     d.noslip = p.vii[SPH_VII_NOSLIP_BC];
     d.count = p.vii[SPH_VII_COUNT];

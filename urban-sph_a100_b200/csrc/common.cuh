@@ -33,6 +33,7 @@ void set_error(const char *msg);
 struct DevParams {
     int n, NI, NJ, NK, num_cells;
     int kernel_type, time_type, freq_filt, fp_solve, fv_solve, fg_solve, kgc_solve, turb, noslip;
+    int con_solve, boussinesq, concn_solve;
     int count;
     float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, time, dt_structure;
     double cs_sgs, l2, l3, l_left, l_right, outlet_probe_dx, partner_tol, ghost_tol;

@@ -101,6 +101,9 @@ struct Ctx {
     R4 *ft = nullptr;       // P3: ftotalx, ftotaly, ftotalz, ftotal
     R4 *fp = nullptr;       // P3: fpx, fpy, fpz
     Real *dtemp = nullptr;
+    Real *dconcn = nullptr; // P3: dconcn (concn_solve)
+    Real *temp0 = nullptr;  // SP2: temp0 (con_solve), concn0 (concn_solve)
+    Real *concn0 = nullptr;
     R4 *nrm = nullptr;      // P3: nx, ny, nz
     Real *g6 = nullptr;     // inv_cm: 6 arrays of n (xx, yy, zz, xy, yz, zx)
     // ---- NNPS ----

@@ -56,6 +56,7 @@ __global__ void k_begin_step(Ctx<Real> c) {
     const R4 z = mk4<Real>(0, 0, 0, 0);
     c.u0[i] = z; c.ft[i] = z; c.fp[i] = z; c.nrm[i] = z;
     c.dtemp[i] = 0;
+    c.dconcn[i] = 0; c.temp0[i] = 0; c.concn0[i] = 0;
 }
 
 // KERNEL_clc_IB_normal_vector3D, functions_PREP.cuh:923-1015 (step 0 only)
@@ -380,17 +381,40 @@ __global__ void k_neumann_scatter(const int *rows, int nrows, const Real *in_p, 
 
 // ---------------------------------------------------------------------------
 // KERNEL_advection_force3D, functions_PPE.cuh:191-480: viscous (Cleary or
-// Monaghan), Eulerian convective term, artificial viscosity, gravity
+// Monaghan), Eulerian convective term, artificial viscosity, gravity; with
+// TH the scalar terms of the same pass: conduction and the Eulerian
+// temperature term (con_solve -> dtemp), concentration advection-diffusion
+// (concn_solve -> dconcn) and Boussinesq buoyancy (replaces the z force).
+// Material constants of Parameters.cuh:120-131 and functions_PROP.cuh:192-212.
 // ---------------------------------------------------------------------------
-template <class Real, int FV>
+struct Scalars {
+    const void *temp, *concn;
+    void *dtemp, *dconcn;
+};
+
+__device__ __forceinline__ float th_k(int pt) {      // Solid_k / Air_k
+    return (pt == 0 || pt == 1000) ? 1.0f : ((pt == 1 || pt == -1) ? 0.025f : 0.0f);
+}
+__device__ __forceinline__ float th_cp(int pt) {     // Solid_cp / Air_cp
+    return (pt == 0 || pt == 1000) ? 900.0f : ((pt == 1 || pt == -1) ? 1005.0f : 0.0f);
+}
+
+template <class Real, int FV, int TH>
 __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIST_ARGS,
                                                    const typename V4<Real>::type *__restrict__ u,
                                                    const Real *__restrict__ eli,
-                                                   typename V4<Real>::type *__restrict__ ft, int n) {
+                                                   typename V4<Real>::type *__restrict__ ft, Scalars sc, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 ti = s.ty[i];
     if (ti.x > 2 || ti.w == 1000 || ti.w <= 0) return;
+    const Real *__restrict__ temp = (const Real *)sc.temp;
+    const Real *__restrict__ concn = (const Real *)sc.concn;
+    const bool con = TH && P.con_solve != 0, cnc = TH && P.concn_solve != 0, bsq = TH && P.boussinesq != 0;
+    const Real tempi = TH ? temp[i] : (Real)0;
+    const Real concni = cnc ? concn[i] : (Real)0;
+    const Real kci = con ? (Real)th_k(ti.w) : (Real)0;
+    Real eulert = 0, Rc = 0, Rd = 0, btemp = 0, bflt = 0;
     const int jci = s.jc[i];
     const auto xi = s.pr[i];
     const auto ui = u[i];
@@ -409,8 +433,8 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
         const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
         const Real it = (Real)1 / tdist;
-        Real dw = calc_dwij<Real>(P, tA, hi, tdist);
-        if (kgc) dw = 0;   // Cm is never filled on this path (all zero)
+        const Real dw_raw = calc_dwij<Real>(P, tA, hi, tdist);
+        const Real dw = kgc ? (Real)0 : dw_raw;   // Cm is never filled on this path (all zero)
         const Real dwi = dw * it;
         const Real tdwx = dwi * dx, tdwy = dwi * dy, tdwz = dwi * dz;
         const auto uj = u[j];
@@ -434,11 +458,42 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
             if ((jci & JB_MON0) || (jcj & JB_MON0)) Pij = 0;
             tx += -Pij * tdwx; ty_ += -Pij * tdwy; tz += -Pij * tdwz;
         }
+        Real tempj = 0, concnj = 0;
+        if (TH) { tempj = temp[j]; if (cnc) concnj = concn[j]; }
         if (el < (Real)1) {
             const Real vj = mj.x / mj.y * ((Real)1 - el);
             ex += (ui.x * (-ux) * tdwx + ui.y * (-ux) * tdwy + ui.z * (-ux) * tdwz) * vj;
             ey += (ui.x * (-uy) * tdwx + ui.y * (-uy) * tdwy + ui.z * (-uy) * tdwz) * vj;
             ez += (ui.x * (-uz) * tdwx + ui.y * (-uz) * tdwy + ui.z * (-uz) * tdwz) * vj;
+            if (con)
+                eulert -= (Real)2 * mj.x / (rhoi + mj.y) * (tempj - tempi) * (ux * tdwx + uy * tdwy + uz * tdwz) *
+                          ((Real)1 - el);
+            if (cnc) {
+                const Real dc = concnj - concni;
+                Rd -= (ui.x * dc * tdwx + ui.y * dc * tdwy + ui.z * dc * tdwz) * vj;
+            }
+        }
+        if (TH && (con || cnc)) {
+            const int ptj = s.ty[j].w;
+            if (con) {   // conduction with the uncorrected dW/dr
+                const Real kcj = (Real)th_k(ptj);
+                const Real rhoj_t = (ptj == 1 || ptj == -1) ? mj.y : (Real)2300;
+                const Real mj_t = mj.x * rhoj_t / mj.y;
+                Real q = (Real)4 * mj_t * kcj * kci * (tempi - tempj) * dw_raw;
+                q /= (tdist + (Real)1e-10) * rhoi * rhoj_t * (kci + kcj);
+                Rc += q;
+            }
+            if (cnc) {   // diffusion_coefficient = 2
+                Real d = mi * ((Real)2 * rhoi + (Real)2 * mj.y);
+                d *= (dx * tdwx + dy * tdwy + dz * tdwz);
+                d /= (rhoi * mj.y * (tdist * tdist + (Real)0.01 * hi * hi));
+                Rd += (ti.w == ptj) ? d * (concni - concnj) : (Real)0;
+            }
+        }
+        if (bsq) {
+            const Real vw = mj.x / mj.y * calc_wij<Real>(P, tA, hi, tdist);
+            btemp += vw * tempj;
+            bflt += vw;
         }
         const Real uij_xij = ux * dx + uy * dy + uz * dz;
         if (uij_xij < 0) {
@@ -451,7 +506,13 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
         }
     SELL_LOOP_END
     if (P.fg_solve) tz += (Real)-9.810;
+    if (bsq && ti.w < 1000) tz = (Real)(1.0 / P.t_ini) * (Real)9.810 * (btemp / bflt - (Real)300);   // tempb 300 K
     ft[i] = mk4<Real>(tx - ex, ty_ - ey, tz - ez, sqrt(tx * tx + ty_ * ty_ + tz * tz));
+    if (con) {
+        Real *dtemp = (Real *)sc.dtemp;
+        dtemp[i] += Rc / (Real)th_cp(ti.w) - eulert;
+    }
+    if (cnc) ((Real *)sc.dconcn)[i] = Rd;
 }
 
 // ---------------------------------------------------------------------------
@@ -461,6 +522,7 @@ template <class Real>
 __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::type *u,
                              typename V4<Real>::type *u0, const typename V4<Real>::type *ft,
                              const typename V4<Real>::type *fm, Real *rho_ref, const typename V2<Real>::type *mr,
+                             const Real *temp, Real *temp0, Real *concn, Real *concn0, const Real *dconcn,
                              Real tdt, float ttime, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -484,6 +546,12 @@ __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::typ
     }
     u[i] = ui;
     if (ttime == 0) rho_ref[i] = mr[i].y;
+    if (P.con_solve == 1) temp0[i] = temp[i];
+    if (P.concn_solve == 1) {
+        const Real cc = concn[i];
+        concn0[i] = cc;
+        concn[i] = cc + dconcn[i] * tdt;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -729,6 +797,7 @@ __global__ void k_time_update(Ctx<Real> c, Real tdt, int tcount) {
     ua.w = us.w;   // vis_t
     A.u[i] = ua;
     Real temp = S.temp[i];
+    if (P.con_solve == 1) temp = c.temp0[i] + c.dtemp[i] * tdt * (Real)(t.y == 0);
     if (t.w == 0) {
         const double tt = (double)(tdt * (Real)tcount);
         if (tt >= P.t_start && tt < P.t_con_t) temp = (Real)(P.t_ini + tt * (P.t_con - P.t_ini) / (P.t_con_t - P.t_start));
@@ -736,8 +805,12 @@ __global__ void k_time_update(Ctx<Real> c, Real tdt, int tcount) {
         else temp = (Real)P.t_con;
     }
     A.temp[i] = temp;
-    A.enth[i] = S.enth[i];
+    if (P.con_solve != 1) A.enth[i] = S.enth[i];
     Real concn = S.concn[i];
+    if (P.concn_solve == 1) {
+        concn = c.concn0[i] + c.dconcn[i] * tdt;
+        if (concn < (Real)0) concn = 0;
+    }
     if (c.source[i] == 1) concn += (Real)0.5 * tdt;
     A.concn[i] = concn;
     A.p[i] = S.p[i]; A.flt[i] = S.flt[i]; A.kt[i] = S.kt[i]; A.et[i] = S.et[i];
@@ -897,15 +970,22 @@ int phase_interaction(Ctx<Real> &c) {
         ++c.launches;
     }
     if (tc == 0) SPH_TRY(neumann_pass(c, c.S));
-    if (c.dp.fv_solve == 2)
-        k_advection<Real, 2><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, n);
-    else if (c.dp.fv_solve == 1)
-        k_advection<Real, 1><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, n);
-    else
-        k_advection<Real, 0><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, n);
+    const Scalars sc{c.S.temp, c.S.concn, c.dtemp, c.dconcn};
+    const bool th = c.dp.con_solve != 0 || c.dp.concn_solve != 0 || c.dp.boussinesq != 0;
+    const dim3 ga = grid_for(n, 128);
+    if (th) {
+        if (c.dp.fv_solve == 2) k_advection<Real, 2, 1><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else if (c.dp.fv_solve == 1) k_advection<Real, 1, 1><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else k_advection<Real, 0, 1><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+    } else {
+        if (c.dp.fv_solve == 2) k_advection<Real, 2, 0><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else if (c.dp.fv_solve == 1) k_advection<Real, 1, 0><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else k_advection<Real, 0, 0><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+    }
     ++c.launches;
     if (c.dp.time_type == 1) {
         k_projection<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.ty, c.S.u, c.u0, c.ft, c.S.fm, c.rho_ref_S, c.mr,
+                                                             c.S.temp, c.temp0, c.S.concn, c.concn0, c.dconcn,
                                                              tdt, c.time, n);
         ++c.launches;
     }

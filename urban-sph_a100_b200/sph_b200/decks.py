@@ -21,6 +21,8 @@ before upload, plus the solver parameters.
   ``scale`` shrinks every extent for small cases.
 * ``cube_array`` -- staggered 4 x 4 array of 0.1 m cubes (IBM) in a
   4.8 x 2.4 x 0.8 m channel with two-level APR near the faces.
+* ``thermal_mini`` -- ``caseh_mini`` with the conduction, Boussinesq and
+  concentration switches on and varied temperature / concentration fields.
 * ``cavity``, ``tgv_box``, ``ensemble`` -- the batched-ensemble workload:
   lid-driven cavities and Taylor-Green boxes of 20k-200k particles with Re in
   [100, 2000], seeded.
@@ -139,6 +141,25 @@ def caseh_mini(dx=0.0412, nx=24, ny=12, nz=7, seed=SEED, shuffle=True, **pkw):
         P = P[rng.permutation(len(P))]
     p = default_params(**pkw)
     domain_setup(p, P)
+    return P, p
+
+
+def thermal_mini(con=1, bouss=1, concn=1, seed=11, nx=12, ny=6, nz=5):
+    """caseh_mini with conduction, Boussinesq buoyancy and concentration
+    switched on: a varied temperature (300 K +- 4 K) and concentration field
+    and 20 concentration sources.  Moving walls (p_type 9) become fixed walls:
+    the reference gives p_type 9 zero conductivity and heat capacity
+    (functions_PPE.cuh:233-234), so its temperature rate there is 0/0."""
+    P, p = caseh_mini(nx=nx, ny=ny, nz=nz)
+    rng = np.random.default_rng(seed)
+    P["p_type"][P["p_type"] == 9] = 0
+    P["temp"] = (300.0 + 4.0 * np.sin(7.0 * P["x"]) * np.cos(5.0 * P["z"])
+                 + rng.uniform(-0.5, 0.5, len(P))).astype(np.float32)
+    P["concn"] = rng.uniform(0.0, 1.0, len(P)).astype(np.float32)
+    P["source"][rng.choice(len(P), 20, replace=False)] = 1
+    p.seti("con_solve", con)
+    p.seti("boussinesq_solve", bouss)
+    p.seti("concn_solve", concn)
     return P, p
 
 
