@@ -171,11 +171,24 @@ typedef struct sph_params {
                                 2 p_n - p_(n-1), once two solutions exist     */
     int32_t apr_max_level;   /* APR (vii[35] = 1, every vii[37] steps): target
                                 level log8(m_ref/m) of fluid near IBM markers */
-    int32_t reserved[8];
+    int32_t outlet_bc;       /* pass at the outlet-buffer call sites of the step
+                                (ISPH_Calc.cuh:151, 208): 0 the reference's
+                                KERNEL_donothing_buffer3D; 1 its dormant
+                                KERNEL_open_boundary_extrapolation_buffer3D
+                                (functions_BC.cuh:763-855); 2 its dormant
+                                KERNEL_inout_boundary3D (functions_BC.cuh:1274-1433) */
+    int32_t inlet_recycling; /* 1: the dormant KERNEL_Recycling3D at the end of
+                                the step (ISPH_Calc.cuh:215; functions_BC.cuh:
+                                1857-1941): inlet ux = u* / kappa_vK log(z / z0)
+                                with u* from the MOST particle at the probe    */
+    int32_t reserved[6];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within
                                 which fluid targets apr_max_level [m]          */
+    double  recycle_probe_x, recycle_probe_y;   /* the MOST particle whose u*
+                                feeds inlet recycling: (x - px)^2 + (y - py)^2
+                                < 1e-3 (functions_MOST.cuh:316: 600, 0)        */
 } sph_params;
 
 typedef struct sph_ppe_stats {

@@ -144,6 +144,8 @@ static void launch_snapshot(int n, part1 *P1, F body) {
 }
 
 static int g_threads_parallel = 1;
+static int g_outlet_bc = 0;       // 0 donothing, 1 extrapolation, 2 inout
+static int g_inlet_recycling = 0;
 static int g_stop_after = 1000;   // debugging: phases of ref_step to run
 
 extern "C" {
@@ -153,6 +155,17 @@ int ref_sizeof_part2(void) { return (int)sizeof(part2); }
 int ref_sizeof_part3(void) { return (int)sizeof(part3); }
 
 void ref_set_parallel(int on) { g_threads_parallel = on; }
+
+// Selects the pass run at the outlet-buffer call sites (ISPH_Calc.cuh:151,
+// 208: the shipped KERNEL_donothing_buffer3D or one of the commented-out
+// alternatives) and the commented-out KERNEL_Recycling3D (ISPH_Calc.cuh:215);
+// with reset_probe, clears the u* of the recycling probe (a device global
+// that lives across steps there).
+void ref_set_boundary_variant(int outlet_bc, int inlet_recycling, int reset_probe) {
+    g_outlet_bc = outlet_bc;
+    g_inlet_recycling = inlet_recycling;
+    if (reset_probe) us_update = 0.f;
+}
 void ref_set_stop_after(int k) { g_stop_after = k; }
 
 int ref_num_threads(void) {
@@ -233,6 +246,16 @@ void ref_step(part1 *P1, part1 *SP1, part2 *P2, part2 *SP2, part3 *P3, int *g_id
     // KERNEL_Neumann_boundary3D reads the pressure of its ghost-node partner
     // (functions_BC.cuh:358-364), which may be another Neumann particle being
     // rewritten by the same launch: run it with snapshot semantics when asked.
+    // the extrapolation and inout passes read records the same launch
+    // rewrites (outlet and side buffers): snapshot semantics
+    auto outlet = [&](part1 *A, part2 *B) {
+        if (g_outlet_bc == 1)
+            launch_snapshot(n, A, [&] { KERNEL_open_boundary_extrapolation_buffer3D(g_str, g_end, A, B, P3); });
+        else if (g_outlet_bc == 2)
+            launch_snapshot(n, A, [&] { KERNEL_inout_boundary3D(g_str, g_end, A, B, P3); });
+        else
+            launch(n, par, [&] { KERNEL_donothing_buffer3D(g_str, g_end, A, B, P3); });
+    };
     auto neumann = [&](part1 *A, part2 *B) {
         if (ppe_snapshot)
             launch_snapshot(n, A, [&] { KERNEL_Neumann_boundary3D(g_str, g_end, A, B, P3); });
@@ -280,7 +303,7 @@ void ref_step(part1 *P1, part1 *SP1, part2 *P2, part2 *SP2, part3 *P3, int *g_id
     PHASE(11);
     neumann(SP1, SP2);
     PHASE(12);
-    launch(n, par, [&] { KERNEL_donothing_buffer3D(g_str, g_end, SP1, SP2, P3); });
+    outlet(SP1, SP2);
     PHASE(13);
     launch(n, par, [&] { KERNEL_pressureforce3D(1, g_str, g_end, SP1, SP2, P3); });
     PHASE(14);
@@ -294,11 +317,13 @@ void ref_step(part1 *P1, part1 *SP1, part2 *P2, part2 *SP2, part3 *P3, int *g_id
     PHASE(18);
     neumann(P1, SP2);
     PHASE(19);
-    launch(n, par, [&] { KERNEL_donothing_buffer3D(g_str, g_end, P1, SP2, P3); });
+    outlet(P1, SP2);
     PHASE(20);
     launch(n, par, [&] { KERNEL_periodic_boundary3D(g_str, g_end, P1, SP2, P3); });
     PHASE(21);
     launch(n, par, [&] { KERNEL_freeslip_boundary3D(g_str, g_end, P1, SP2, P3); });
+    PHASE(22);
+    if (g_inlet_recycling == 1) launch(n, par, [&] { KERNEL_Recycling3D(g_str, g_end, P1, SP2, P3); });
 #undef PHASE
 }
 

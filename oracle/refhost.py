@@ -34,6 +34,7 @@ def lib():
         L.ref_nnps.argtypes = [vp] * 8
         L.ref_step.argtypes = [vp] * 9 + [ctypes.c_int, ctypes.c_float, ctypes.c_int]
         L.ref_set_parallel.argtypes = [ctypes.c_int]
+        L.ref_set_boundary_variant.argtypes = [ctypes.c_int] * 3
         L.ref_num_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -55,6 +56,7 @@ class RefHost:
         vii = np.ctypeslib.as_array(self.params.vii).copy()
         vif = np.ctypeslib.as_array(self.params.vif).copy()
         L.ref_set_params(_p(vii), _p(vif))
+        L.ref_set_boundary_variant(int(self.params.outlet_bc), int(self.params.inlet_recycling), 1)
         self.P1 = np.array(P1, copy=True)
         self.SP1 = np.zeros_like(self.P1)
         self.P2 = np.zeros(self.n, dtype=PART2)
@@ -72,6 +74,7 @@ class RefHost:
         vii = np.ctypeslib.as_array(self.params.vii).copy()
         vif = np.ctypeslib.as_array(self.params.vif).copy()
         lib().ref_set_params(_p(vii), _p(vif))
+        lib().ref_set_boundary_variant(int(self.params.outlet_bc), int(self.params.inlet_recycling), 0)
 
     def step(self, nsteps=1, ppe_snapshot=True):
         L = lib()

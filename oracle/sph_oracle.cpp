@@ -237,6 +237,7 @@ struct Oracle {
     bool built = false;
     int count = 0;
     float time = 0.f;
+    float us_update = 0.f;        // u* of the recycling probe (a device global there)
     int pin_row = -1;
     std::vector<int> pins;
     std::vector<int> comp_of;     // rank-one component of each fluid row (-1: none)
@@ -591,6 +592,10 @@ struct Oracle {
             S3.dtemp[i] += 0.5 * shf / (space * rhoi * 1005);
             A.hmz[i] = 0.5 * shf / (space * rhoi * 1005);
             A.f1[i] = u_star; A.f2[i] = theta_star; A.f3[i] = OB_length;
+            // functions_MOST.cuh:316 (probe 600, 0 there)
+            const double dxp = (double)xf[i] - prm.recycle_probe_x;
+            const float dyp = yf[i] - (float)prm.recycle_probe_y;
+            if (dxp * dxp + dyp * dyp < 1e-3) us_update = u_star;
         }
     }
 
@@ -878,6 +883,133 @@ struct Oracle {
                 }
             });
             A.pres[i] = tp; A.ux[i] = tux; A.uy[i] = tuy; A.uz[i] = tuz; A.temp[i] = tt;
+        }
+    }
+
+    // KERNEL_open_boundary_extrapolation_buffer3D, functions_BC.cuh:763-855
+    // (dormant in the shipped step; outlet_bc = 1): an outlet record off the
+    // MOST layer takes the Shepard average of the fluid around its mirror
+    // node across L3 and zero pressure, when that average has weight.  Every
+    // record reads the pre-pass state.
+    void extrapolation(State<Real> &A) {
+        const P Q = q();
+        State<Real> O = A;
+        for (int i = 0; i < n(); ++i) {
+            if (O.buffer_type[i] != 2 || O.most[i] == 1) continue;
+            Real hi = O.h[i];
+            Real tmp_A = calc_tmpA(Q, hi);
+            Real search_range = Q.skappa() * hi;
+            Real xg = 2 * prm.l3 - O.x[i], yg = O.y[i], zg = O.z[i];
+            const float xgf = (float)(2 * prm.l3 - (double)xf[i]);
+            int ic = bin_axis(xgf, Q.xmin(), Q.xmax(), Q.NI());
+            int jc = bin_axis(yf[i], Q.ymin(), Q.ymax(), Q.NJ());
+            int kc = bin_axis(zf[i], Q.zmin(), Q.zmax(), Q.NK());
+            Real tpres = 0, tux = 0, tuy = 0, tuz = 0, tflt = 0;
+            cell_loop(ic, jc, kc, O.ncell[i], [&](int j) {
+                Real tdist = std::sqrt((xg - O.x[j]) * (xg - O.x[j]) + (yg - O.y[j]) * (yg - O.y[j]) + (zg - O.z[j]) * (zg - O.z[j])) - 1e-20;
+                if (O.p_type[j] < 1000 && tdist < search_range) {
+                    Real twij = calc_wij(Q, tmp_A, hi, tdist);
+                    int on = (O.p_type[j] == 1) * (O.most[j] != 1);
+                    Real mj = O.m[j], rhoj = O.rho[j];
+                    tpres += mj / rhoj * O.pres[j] * twij * on;
+                    tux += mj / rhoj * O.ux[j] * twij * on;
+                    tuy += mj / rhoj * O.uy[j] * twij * on;
+                    tuz += mj / rhoj * O.uz[j] * twij * on;
+                    tflt += mj / rhoj * twij * on;
+                }
+            });
+            if (tflt < 1e-6) continue;
+            A.pres[i] = 0.0;
+            A.ux[i] = tux / tflt; A.uy[i] = tuy / tflt; A.uz[i] = tuz / tflt;
+        }
+    }
+
+    // KERNEL_inout_boundary3D, functions_BC.cuh:1274-1433 (dormant;
+    // outlet_bc = 2): side buffers (3, 4) copy u, p and T of the record at
+    // their periodic image (zero when there is none); outlet records are set
+    // so that the interface value at x = L3, a Shepard average of interior
+    // fluid with the pair-averaged h, is the mean of the record and its
+    // mirror: u = 2 u_if - u.  Inlet records are left as they are.  Every
+    // record reads the pre-pass state.
+    void inout(State<Real> &A) {
+        const P Q = q();
+        State<Real> O = A;
+        for (int i = 0; i < n(); ++i) {
+            const int bt = O.buffer_type[i];
+            if (bt == 0 || O.p_type[i] >= 1000) continue;
+            if (bt != 2 && bt != 3 && bt != 4) continue;
+            Real hi = O.h[i];
+            Real search_range = Q.skappa() * hi;
+            const int nc = O.ncell[i];
+            if (bt == 3 || bt == 4) {
+                Real xg = O.x[i], zg = O.z[i];
+                Real yg = (bt == 3) ? (Real)(O.y[i] + prm.l_right - prm.l_left) : (Real)(O.y[i] - prm.l_right + prm.l_left);
+                float ygf = (bt == 3) ? (float)(yf[i] + prm.l_right - prm.l_left) : (float)(yf[i] - prm.l_right + prm.l_left);
+                int ic, jc, kc;
+                search_cell(xf[i], ygf, zf[i], ic, jc, kc);
+                Real tux = 0, tuy = 0, tuz = 0, tp = 0, tt = 0;
+                bool flag = false;
+                for (int z = -nc; z <= nc; z++)
+                    for (int y = -nc; y <= nc; y++)
+                        for (int x = -nc; x <= nc; x++) {
+                            if (flag) continue;
+                            if (ic + x < 0 || ic + x > Q.NI() - 1 || jc + y < 0 || jc + y > Q.NJ() - 1 || kc + z < 0 || kc + z > Q.NK() - 1) continue;
+                            int k = (ic + x) + Q.NI() * (jc + y) + Q.NI() * Q.NJ() * (kc + z);
+                            if (g_str[k] == -1) continue;
+                            for (int j = g_str[k]; j < g_end[k]; j++) {
+                                Real tdist = std::sqrt((xg - O.x[j]) * (xg - O.x[j]) + (yg - O.y[j]) * (yg - O.y[j]) + (zg - O.z[j]) * (zg - O.z[j])) - 1e-20;
+                                if (tdist < 0.001) {
+                                    tux = O.ux[j]; tuy = O.uy[j]; tuz = O.uz[j]; tp = O.pres[j]; tt = O.temp[j];
+                                    flag = true;
+                                }
+                            }
+                        }
+                A.ux[i] = tux; A.uy[i] = tuy; A.uz[i] = tuz; A.pres[i] = tp; A.temp[i] = tt;
+            } else {
+                Real yg = O.y[i], zg = O.z[i];
+                int ic = (int)std::min(std::floor((prm.l3 - (double)Q.xmin()) / (double)Q.dcell()), (double)(Q.NI() - 1));
+                int jc = search_axis(yf[i], Q.ymin(), Q.ymax(), Q.dcell(), Q.NJ());
+                int kc = search_axis(zf[i], Q.zmin(), Q.zmax(), Q.dcell(), Q.NK());
+                if (ic < 0) ic = 0;
+                Real ux_if = 0, uy_if = 0, uz_if = 0, p_if = 0, tflt = 0;
+                cell_loop(ic, jc, kc, nc, [&](int j) {
+                    Real tdist = std::sqrt((prm.l3 - O.x[j]) * (prm.l3 - O.x[j]) + (yg - O.y[j]) * (yg - O.y[j]) + (zg - O.z[j]) * (zg - O.z[j])) - 1e-20;
+                    if (tdist < search_range) {
+                        Real hij = 0.5 * (hi + O.h[j]);
+                        Real tmp_Aij = calc_tmpA(Q, hij);
+                        Real twij = calc_wij(Q, tmp_Aij, hij, tdist);
+                        int on = (O.buffer_type[j] == 0) * (O.p_type[j] == 1);
+                        Real vj = O.m[j] / O.rho[j];
+                        ux_if += O.ux[j] * vj * twij * on;
+                        uy_if += O.uy[j] * vj * twij * on;
+                        uz_if += O.uz[j] * vj * twij * on;
+                        p_if += O.pres[j] * vj * twij * on;
+                        tflt += vj * twij * on;
+                    }
+                });
+                A.ux[i] = -O.ux[i] + 2.0 * ux_if / tflt;
+                A.uy[i] = -O.uy[i] + 2.0 * uy_if / tflt;
+                A.uz[i] = -O.uz[i] + 2.0 * uz_if / tflt;
+                A.pres[i] = -O.pres[i] + 2.0 * p_if / tflt;
+            }
+        }
+    }
+
+    // the pass at the outlet-buffer call sites (ISPH_Calc.cuh:151, 208)
+    void outlet_bc(State<Real> &A) {
+        if (prm.outlet_bc == 1) extrapolation(A);
+        else if (prm.outlet_bc == 2) inout(A);
+        else donothing(A);
+    }
+
+    // KERNEL_Recycling3D, functions_BC.cuh:1857-1941 (dormant; inlet_recycling
+    // = 1, after the last boundary pass, ISPH_Calc.cuh:215).  Its neighbour
+    // search there finds a record whose velocity is then not used; the inlet
+    // takes the log law of the probe's friction velocity.
+    void recycling(State<Real> &A) {
+        for (int i = 0; i < n(); ++i) {
+            if (A.buffer_type[i] != 1 && A.buffer_type[i] != -1) continue;
+            A.ux[i] = (us_update / 0.4) * std::log(A.z[i] / prm.most_z0);
         }
     }
 
@@ -1439,7 +1571,7 @@ struct Oracle {
         PHASE(11);
         neumann(S);
         PHASE(12);
-        donothing(S);
+        outlet_bc(S);
         PHASE(13);
         pressure_force(S);
         PHASE(14);
@@ -1453,11 +1585,13 @@ struct Oracle {
         PHASE(18);
         neumann(S1);
         PHASE(19);
-        donothing(S1);
+        outlet_bc(S1);
         PHASE(20);
         periodic(S1);
         PHASE(21);
         freeslip(S1);
+        PHASE(22);
+        if (prm.inlet_recycling == 1) recycling(S1);
 #undef PHASE
         time = time + Q.dt();
         count = tc + 1;

@@ -146,3 +146,31 @@ def test_thermal_step_matches_oracle(name, precision, tol):
         assert np.abs(B3["dtemp"][fluid]).max() > 0
     if THERMAL[name][2]:
         assert np.abs(B3["dconcn"][fluid]).max() > 0
+
+
+BOUNDARY = {"extrapolation": (layout.OUTLET_EXTRAPOLATION, 0), "inout": (layout.OUTLET_INOUT, 0),
+            "recycling_probe": (layout.OUTLET_DONOTHING, 1), "inout_recycling_probe": (layout.OUTLET_INOUT, 1)}
+
+
+@pytest.mark.parametrize("precision,tol", [(layout.PREC_MIXED, FP32_TOL), (layout.PREC_FP64, FP64_TOL)],
+                         ids=["fp32", "fp64"])
+@pytest.mark.parametrize("name", list(BOUNDARY))
+def test_dormant_boundary_passes_match_oracle(name, precision, tol):
+    """The reference's commented-out open-boundary passes (outlet
+    extrapolation, inflow/outflow, inlet recycling), switched in at their call
+    sites; the oracle is bit-exact against the reference for them
+    (tests/test_oracle.py).  The recycling probe sits on a MOST record of the
+    deck, so its friction velocity drives the inlet."""
+    P, p = decks.caseh_mini(nx=12, ny=12, nz=5)
+    p.outlet_bc, p.inlet_recycling = BOUNDARY[name]
+    if p.inlet_recycling:
+        k = int(np.nonzero(P["MOST_buffer"] == 1)[0][0])
+        p.recycle_probe_x, p.recycle_probe_y = float(P["x"][k]), float(P["y"][k])
+    A, A2, A3, B, B2, B3 = _run_pair(P, p, precision, nsteps=3)
+    lim = FP64_MOST_TOL if precision == layout.PREC_FP64 else tol
+    errs = {f: rel_err(A[f], B[f]) for f in FIELDS}
+    bad = {f: e for f, e in errs.items() if not e <= lim}
+    assert not bad, bad
+    if p.inlet_recycling:
+        inlet = B["buffer_type"] == 1
+        assert np.abs(B["ux"][inlet]).max() > 0

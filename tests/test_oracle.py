@@ -121,6 +121,64 @@ def test_thermal_step_bit_exact_vs_reference(name):
         assert np.abs(B3["dconcn"][fluid]).max() > 0
 
 
+BOUNDARY = {"extrapolation": (layout.OUTLET_EXTRAPOLATION, 0), "inout": (layout.OUTLET_INOUT, 0),
+            "recycling": (layout.OUTLET_DONOTHING, 1), "inout_recycling": (layout.OUTLET_INOUT, 1)}
+
+
+@needs_ref
+@pytest.mark.parametrize("name", list(BOUNDARY))
+def test_dormant_boundary_passes_bit_exact_vs_reference(name):
+    """The reference's commented-out open-boundary kernels, switched in at
+    their call sites, against this oracle."""
+    P, p = decks.caseh_mini(nx=12, ny=12, nz=5)    # inlet, outlet and both side buffers
+    p.outlet_bc, p.inlet_recycling = BOUNDARY[name]
+    R = refhost.RefHost(P, p, parallel=False)
+    O = restated.Restated(P, p, 0)
+    for _ in range(3):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, _, _ = O.download()
+    for f in FIELDS:
+        assert np.array_equal(R.P1[f], B[f], equal_nan=True), f
+    # the variant changed the outcome against the shipped pass
+    q = p.copy()
+    q.outlet_bc, q.inlet_recycling = 0, 0
+    D = restated.Restated(P, q, 0)
+    for _ in range(3):
+        D.step(1, mode=layout.PPE_REF_SWEEP)
+    C, _, _ = D.download()
+    assert not np.array_equal(C["ux"], B["ux"], equal_nan=True)
+
+
+def probe_deck():
+    """The boundary deck plus one MOST record at the reference's hard-wired
+    recycling probe (x = 600, y = 0), so that the probe's friction velocity
+    feeds the inlet."""
+    P, p = decks.caseh_mini(nx=12, ny=12, nz=5)
+    k = int(np.nonzero(P["MOST_buffer"] == 1)[0][0])
+    far = P[k:k + 1].copy()
+    far["x"], far["y"], far["buffer_type"], far["i_type"] = 600.0, 0.0, 0, 1
+    Q = np.concatenate([P, far])
+    decks.domain_setup(p, Q)
+    return Q, p
+
+
+@needs_ref
+def test_recycling_probe_bit_exact_vs_reference():
+    P, p = probe_deck()
+    p.inlet_recycling = 1
+    R = refhost.RefHost(P, p, parallel=False)
+    O = restated.Restated(P, p, 0)
+    for _ in range(2):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, _, _ = O.download()
+    for f in FIELDS:
+        assert np.array_equal(R.P1[f], B[f], equal_nan=True), f
+    inlet = B["buffer_type"] == 1
+    assert np.all(np.isfinite(B["ux"][inlet])) and np.abs(B["ux"][inlet]).max() > 0
+
+
 @needs_ref
 def test_euler_time_stepping_bit_exact_vs_reference():
     P, p = _deck({})

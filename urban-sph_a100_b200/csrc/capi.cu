@@ -35,6 +35,9 @@ DevParams make_dev_params(const sph_params &p) {
     d.con_solve = p.vii[SPH_VII_CON_SOLVE];
     d.boussinesq = p.vii[SPH_VII_BOUSSINESQ];
     d.concn_solve = p.vii[SPH_VII_CONCN_SOLVE];
+    d.outlet_bc = p.outlet_bc;
+    d.inlet_recycling = p.inlet_recycling;
+    d.rp_x = p.recycle_probe_x; d.rp_y = p.recycle_probe_y;
     d.turb = p.vii[SPH_VII_TURBULENCE];
     d.noslip = p.vii[SPH_VII_NOSLIP_BC];
     d.count = p.vii[SPH_VII_COUNT];
@@ -73,6 +76,7 @@ static int check_params(const sph_params &p) {
     if (p.pressure_length != 1.0) { set_error("pressure_length other than 1 is not supported"); return SPH_ERR_UNSUPPORTED; }
     if (p.n_profile < 2 || p.n_profile > SPH_MAX_PROFILE) { set_error("n_profile must be in [2, 32]"); return SPH_ERR_BAD_ARG; }
     if (!(p.vif[SPH_VIF_DT] > 0)) { set_error("dt must be positive"); return SPH_ERR_BAD_ARG; }
+    if (p.outlet_bc < 0 || p.outlet_bc > 2) { set_error("outlet_bc must be 0, 1 or 2"); return SPH_ERR_BAD_ARG; }
     return SPH_OK;
 }
 
@@ -154,6 +158,8 @@ int sph_params_init(sph_params *p) {
     p->ppe_tol = 1e-6;
     p->ppe_pin = 1;
     p->ppe_inner_tol = 1e-3;
+    p->recycle_probe_x = 600.0;   // functions_MOST.cuh:316
+    p->recycle_probe_y = 0.0;
     return SPH_OK;
 }
 

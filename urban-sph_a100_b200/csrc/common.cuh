@@ -34,6 +34,8 @@ struct DevParams {
     int n, NI, NJ, NK, num_cells;
     int kernel_type, time_type, freq_filt, fp_solve, fv_solve, fg_solve, kgc_solve, turb, noslip;
     int con_solve, boussinesq, concn_solve;
+    int outlet_bc, inlet_recycling;
+    double rp_x, rp_y;     // recycling probe
     int count;
     float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, time, dt_structure;
     double cs_sgs, l2, l3, l_left, l_right, outlet_probe_dx, partner_tol, ghost_tol;

@@ -47,6 +47,17 @@ struct SideLists {
     int n_per = 0, n_out = 0;
     int *per_rows = nullptr, *per_partner = nullptr;
     int *out_rows = nullptr, *out_partner = nullptr;
+    // dormant open-boundary variants of the reference (outlet_bc 1 / 2,
+    // inlet_recycling): extrapolation rows (outlet, off the MOST layer) with
+    // the fluid around their mirror node; inout rows, the side buffers first
+    // (partner in io_aux) and then the outlet rows (CSR of the interior fluid
+    // around their interface point); recycling rows (inlet)
+    int n_xo = 0;
+    int *xo_rows = nullptr, *xo_off = nullptr, *xo_nbr = nullptr;
+    int n_ios = 0, n_io = 0;
+    int *io_rows = nullptr, *io_aux = nullptr, *io_off = nullptr, *io_nbr = nullptr;
+    int n_rc = 0;
+    int *rc_rows = nullptr;
     // MOST wall-layer particles and their ghost-node targets
     int n_most = 0;
     int *most_rows = nullptr, *most_off = nullptr, *most_tgt = nullptr;
@@ -105,6 +116,7 @@ struct Ctx {
     Real *temp0 = nullptr;  // SP2: temp0 (con_solve), concn0 (concn_solve)
     Real *concn0 = nullptr;
     R4 *nrm = nullptr;      // P3: nx, ny, nz
+    float *us_update = nullptr;   // u* of the recycling probe, kept across steps
     Real *g6 = nullptr;     // inv_cm: 6 arrays of n (xx, yy, zz, xy, yz, zx)
     // ---- NNPS ----
     int *key = nullptr, *perm = nullptr, *cell_start = nullptr, *cell_fill = nullptr;

@@ -201,6 +201,8 @@ int ctx_allocate(Ctx<Real> &c) {
     SPH_TRY(c.alloc(c.u0, n)); SPH_TRY(c.alloc(c.ft, n)); SPH_TRY(c.alloc(c.fp, n));
     SPH_TRY(c.alloc(c.dtemp, n)); SPH_TRY(c.alloc(c.nrm, n)); SPH_TRY(c.alloc(c.g6, 6 * (size_t)n));
     SPH_TRY(c.alloc(c.dconcn, n)); SPH_TRY(c.alloc(c.temp0, n)); SPH_TRY(c.alloc(c.concn0, n));
+    SPH_TRY(c.alloc(c.us_update, 1));
+    SPH_CUDA_TRY(cudaMemsetAsync(c.us_update, 0, sizeof(float), c.stream));
     SPH_TRY(c.alloc(c.key, n)); SPH_TRY(c.alloc(c.perm, n)); SPH_TRY(c.alloc(c.g_idx, n));
     SPH_TRY(c.alloc(c.cell_start, (size_t)c.num_cells + 2));
     SPH_TRY(c.alloc(c.cell_fill, (size_t)c.num_cells + 2));
@@ -865,6 +867,89 @@ int build_side_lists(Ctx<Real> &c) {
     for (size_t k = 0; k < rows.size(); ++k) aux[rows[k]] = nb[k];
     SPH_CUDA_TRY(cudaMemcpyAsync(c.row_aux, aux.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
+
+    // extrapolation rows, functions_BC.cuh:763-855: outlet records off the
+    // MOST layer; fluid (p_type 1, off the MOST layer) within kappa h_i of the
+    // mirror node (2 L3 - x, y, z), cells by the normalised binning there
+    rows.clear(); off.assign(1, 0); nb.clear();
+    for (int i = 0; i < n; ++i) {
+        if (G.ty[i].y != 2 || G.ty[i].z == 1) continue;
+        rows.push_back(i);
+        const Real xg = (Real)(2 * P.l3 - (double)pr[i].x);
+        const float xgf = (float)(2 * P.l3 - (double)G.pf[i].x);
+        const Real range = (Real)P.skappa * pr[i].w;
+        int ic, jc, kc;
+        G.bin_cell(xgf, G.pf[i].y, G.pf[i].z, ic, jc, kc);
+        G.cell_loop(ic, jc, kc, G.ncell[i], [&](int j) {
+            if (G.ty[j].w != 1 || G.ty[j].z == 1) return;
+            const Real dx = xg - pr[j].x, dy = pr[i].y - pr[j].y, dz = pr[i].z - pr[j].z;
+            const Real d = (Real)(std::sqrt(dx * dx + dy * dy + dz * dz) - 1e-20);
+            if (d < range) nb.push_back(j);
+        });
+        off.push_back((int)nb.size());
+    }
+    L.n_xo = (int)rows.size();
+    SPH_TRY(upload_vec(c, L.xo_rows, rows)); SPH_TRY(upload_vec(c, L.xo_off, off)); SPH_TRY(upload_vec(c, L.xo_nbr, nb));
+
+    // inout rows, functions_BC.cuh:1274-1433: side buffers take the record
+    // at 0.001 of their periodic image (the last one in the first cell that
+    // has one), outlet records the interior fluid (buffer 0, p_type 1)
+    // within kappa h_i of (L3, y, z)
+    {
+        std::vector<int> io_rows, io_aux, io_off(1, 0), io_nb;
+        for (int i = 0; i < n; ++i) {
+            const int bt = G.ty[i].y;
+            if ((bt != 3 && bt != 4) || G.ty[i].w >= 1000) continue;
+            io_rows.push_back(i);
+            const Real yR = (bt == 3) ? (Real)((double)pr[i].y + P.l_right - P.l_left) : (Real)((double)pr[i].y - P.l_right + P.l_left);
+            const float ygf = (bt == 3) ? (float)((double)G.pf[i].y + P.l_right - P.l_left) : (float)((double)G.pf[i].y - P.l_right + P.l_left);
+            int ic, jc, kc;
+            G.search_cell(G.pf[i].x, ygf, G.pf[i].z, ic, jc, kc);
+            const int nc = G.ncell[i];
+            int found = -1;
+            bool flag = false;
+            for (int z = -nc; z <= nc; z++)
+                for (int y = -nc; y <= nc; y++)
+                    for (int x = -nc; x <= nc; x++) {
+                        if (flag) continue;
+                        if (ic + x < 0 || ic + x > P.NI - 1 || jc + y < 0 || jc + y > P.NJ - 1 || kc + z < 0 || kc + z > P.NK - 1) continue;
+                        const int k = (ic + x) + P.NI * (jc + y) + P.NI * P.NJ * (kc + z);
+                        for (int j = G.cs[k]; j < G.cs[k + 1]; j++) {
+                            const Real dx = pr[i].x - pr[j].x, dy = yR - pr[j].y, dz = pr[i].z - pr[j].z;
+                            const Real d = (Real)(std::sqrt(dx * dx + dy * dy + dz * dz) - 1e-20);
+                            if (d < (Real)0.001) { found = j; flag = true; }
+                        }
+                    }
+            io_aux.push_back(found);
+        }
+        L.n_ios = (int)io_rows.size();
+        for (int i = 0; i < n; ++i) {
+            if (G.ty[i].y != 2 || G.ty[i].w >= 1000) continue;
+            io_rows.push_back(i);
+            const Real range = (Real)P.skappa * pr[i].w;
+            int ic = (int)std::min(std::floor((P.l3 - (double)P.xmin) / (double)P.dcell), (double)(P.NI - 1));
+            if (ic < 0) ic = 0;
+            int ic_unused, jc, kc;
+            G.search_cell(G.pf[i].x, G.pf[i].y, G.pf[i].z, ic_unused, jc, kc);
+            G.cell_loop(ic, jc, kc, G.ncell[i], [&](int j) {
+                if (G.ty[j].y != 0 || G.ty[j].w != 1) return;
+                const Real dx = (Real)(P.l3 - (double)pr[j].x), dy = pr[i].y - pr[j].y, dz = pr[i].z - pr[j].z;
+                const Real d = (Real)(std::sqrt(dx * dx + dy * dy + dz * dz) - 1e-20);
+                if (d < range) io_nb.push_back(j);
+            });
+            io_off.push_back((int)io_nb.size());
+        }
+        L.n_io = (int)io_rows.size();
+        SPH_TRY(upload_vec(c, L.io_rows, io_rows)); SPH_TRY(upload_vec(c, L.io_aux, io_aux));
+        SPH_TRY(upload_vec(c, L.io_off, io_off)); SPH_TRY(upload_vec(c, L.io_nbr, io_nb));
+    }
+
+    // recycling rows, functions_BC.cuh:1861: buffer type 1 or -1
+    rows.clear();
+    for (int i = 0; i < n; ++i)
+        if (G.ty[i].y == 1 || G.ty[i].y == -1) rows.push_back(i);
+    L.n_rc = (int)rows.size();
+    SPH_TRY(upload_vec(c, L.rc_rows, rows));
 
     // MOST wall-layer particles and their ghost-node targets, functions_MOST.cuh:262-305
     rows.clear(); off.assign(1, 0); nb.clear();

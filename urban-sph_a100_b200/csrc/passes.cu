@@ -281,7 +281,7 @@ __device__ __forceinline__ double most_Phi_h(float L, float z, float z0h) { retu
 template <class Real>
 __global__ void k_most(DevParams P, SoA<Real> s, const int *rows, const int *off, const int *tgt, int nrows,
                        const typename V4<Real>::type *u, const Real *temp, typename V4<Real>::type *fm,
-                       typename V4<Real>::type *fl, Real *dtemp, int tcount, float tdt) {
+                       typename V4<Real>::type *fl, Real *dtemp, float *us_update, int tcount, float tdt) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nrows) return;
     const int i = rows[k];
@@ -335,6 +335,10 @@ __global__ void k_most(DevParams P, SoA<Real> s, const int *rows, const int *off
     fm[i] = f;
     atomicAdd(&dtemp[i], q);
     fl[i] = mk4<Real>(u_star, theta_star, OB, 0);
+    // the friction velocity at the recycling probe, functions_MOST.cuh:316
+    const double dxp = (double)(float)xi.x - P.rp_x;
+    const float dyp = (float)xi.y - (float)P.rp_y;
+    if (dxp * dxp + (double)(dyp * dyp) < 1e-3) *us_update = u_star;
 }
 
 // ---------------------------------------------------------------------------
@@ -586,6 +590,105 @@ __global__ void k_partner_scatter(const int *rows, int nrows, const typename V4<
     if (k >= nrows) return;
     const int i = rows[k];
     u[i] = ou[k]; p[i] = op[k]; temp[i] = ot[k];
+}
+
+// ---------------------------------------------------------------------------
+// Open-boundary passes the reference ships commented out (gather halves; the
+// scatter is k_partner_scatter, so every row reads the pre-pass state).
+// KERNEL_open_boundary_extrapolation_buffer3D, functions_BC.cuh:763-855:
+// Shepard average of the fluid around the mirror node (2 L3 - x, y, z) and
+// zero pressure, when the average has weight 1e-6 or more.
+// ---------------------------------------------------------------------------
+template <class Real>
+__global__ void k_extrap_gather(DevParams P, SoA<Real> s, const int *rows, const int *off, const int *nbr, int nrows,
+                                const typename V4<Real>::type *u, const Real *p, const Real *temp,
+                                typename V4<Real>::type *ou, Real *op, Real *ot) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    const auto xi = s.pr[i];
+    const Real hi = xi.w;
+    const Real tA = calc_tmpA<Real>(P, hi);
+    const Real xg = (Real)(2.0 * P.l3 - (double)xi.x);
+    Real tp = 0, tx = 0, ty = 0, tz = 0, tf = 0;
+    for (int e = off[k]; e < off[k + 1]; ++e) {
+        const int j = nbr[e];
+        const auto xj = s.pr[j];
+        const Real dx = xg - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
+        const auto mj = s.mr[j];
+        const Real vw = mj.x / mj.y * calc_wij<Real>(P, tA, hi, tdist);
+        const auto uj = u[j];
+        tp += vw * p[j]; tx += vw * uj.x; ty += vw * uj.y; tz += vw * uj.z; tf += vw;
+    }
+    auto ui = u[i];
+    Real pi = p[i];
+    if (tf >= (Real)1e-6) {
+        ui.x = tx / tf; ui.y = ty / tf; ui.z = tz / tf;
+        pi = 0;
+    }
+    ou[k] = ui; op[k] = pi; ot[k] = temp[i];
+}
+
+// KERNEL_inout_boundary3D, functions_BC.cuh:1274-1433: rows [0, nside) copy
+// their periodic partner (zero without one); the outlet rows after them take
+// 2 (interface value) - (own value) for u and p, the interface value being
+// the Shepard average at (L3, y, z) with the pair-averaged h.
+template <class Real>
+__global__ void k_inout_gather(DevParams P, SoA<Real> s, const int *rows, const int *aux, int nside, const int *off,
+                               const int *nbr, int nrows, const typename V4<Real>::type *u, const Real *p,
+                               const Real *temp, typename V4<Real>::type *ou, Real *op, Real *ot) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    auto ui = u[i];
+    if (k < nside) {
+        const int j = aux[k];
+        if (j >= 0) {
+            const auto uj = u[j];
+            ui.x = uj.x; ui.y = uj.y; ui.z = uj.z;
+            op[k] = p[j]; ot[k] = temp[j];
+        } else {
+            ui.x = 0; ui.y = 0; ui.z = 0;
+            op[k] = 0; ot[k] = 0;
+        }
+        ou[k] = ui;
+        return;
+    }
+    const int q = k - nside;
+    const auto xi = s.pr[i];
+    const Real hi = xi.w;
+    Real ax = 0, ay = 0, az = 0, ap = 0, tf = 0;
+    for (int e = off[q]; e < off[q + 1]; ++e) {
+        const int j = nbr[e];
+        const auto xj = s.pr[j];
+        const Real dx = (Real)(P.l3 - (double)xj.x), dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
+        const Real hij = (Real)0.5 * (hi + xj.w);
+        const Real tA = calc_tmpA<Real>(P, hij);
+        const auto mj = s.mr[j];
+        const Real vw = mj.x / mj.y * calc_wij<Real>(P, tA, hij, tdist);
+        const auto uj = u[j];
+        ax += uj.x * vw; ay += uj.y * vw; az += uj.z * vw; ap += p[j] * vw; tf += vw;
+    }
+    ui.x = -ui.x + (Real)2 * ax / tf;
+    ui.y = -ui.y + (Real)2 * ay / tf;
+    ui.z = -ui.z + (Real)2 * az / tf;
+    ou[k] = ui;
+    op[k] = -p[i] + (Real)2 * ap / tf;
+    ot[k] = temp[i];
+}
+
+// KERNEL_Recycling3D, functions_BC.cuh:1857-1941: inlet ux from the log law
+// of the probe's friction velocity (its neighbour search there finds a value
+// that it does not use)
+template <class Real>
+__global__ void k_recycle(DevParams P, SoA<Real> s, const int *rows, int nrows, const float *us_update,
+                          typename V4<Real>::type *u) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nrows) return;
+    const int i = rows[k];
+    u[i].x = (Real)((double)*us_update / 0.4 * log((double)s.pr[i].z / P.most_z0));
 }
 
 // ---------------------------------------------------------------------------
@@ -913,9 +1016,27 @@ static int partner_pass(Ctx<Real> &c, VarSet<Real> &V, const int *rows, const in
     return SPH_OK;
 }
 
+// the pass at the outlet-buffer call sites (ISPH_Calc.cuh:151, 208)
 template <class Real>
 int outlet_pass(Ctx<Real> &c, VarSet<Real> &V) {
-    return partner_pass(c, V, c.L.out_rows, c.L.out_partner, c.L.n_out);
+    const SideLists &L = c.L;
+    if (c.dp.outlet_bc == 0) return partner_pass(c, V, L.out_rows, L.out_partner, L.n_out);
+    const int nrows = c.dp.outlet_bc == 1 ? L.n_xo : L.n_io;
+    if (nrows == 0) return SPH_OK;
+    typename V4<Real>::type *ou; Real *op, *ot;
+    SPH_TRY(scratch_rows(c, ou, op, ot));
+    if (c.dp.outlet_bc == 1) {
+        k_extrap_gather<Real><<<grid_for(nrows, 128), 128, 0, c.stream>>>(c.dp, soa(c), L.xo_rows, L.xo_off, L.xo_nbr, nrows,
+                                                                           V.u, V.p, V.temp, ou, op, ot);
+        k_partner_scatter<Real><<<grid_for(nrows, 128), 128, 0, c.stream>>>(L.xo_rows, nrows, ou, op, ot, V.u, V.p, V.temp);
+    } else {
+        k_inout_gather<Real><<<grid_for(nrows, 128), 128, 0, c.stream>>>(c.dp, soa(c), L.io_rows, L.io_aux, L.n_ios, L.io_off,
+                                                                          L.io_nbr, nrows, V.u, V.p, V.temp, ou, op, ot);
+        k_partner_scatter<Real><<<grid_for(nrows, 128), 128, 0, c.stream>>>(L.io_rows, nrows, ou, op, ot, V.u, V.p, V.temp);
+    }
+    c.launches += 2;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
 }
 
 template <class Real>
@@ -966,7 +1087,7 @@ int phase_interaction(Ctx<Real> &c) {
     }
     if (c.L.n_most > 0) {
         k_most<Real><<<grid_for(c.L.n_most, 128), 128, 0, st>>>(c.dp, soa(c), c.L.most_rows, c.L.most_off, c.L.most_tgt,
-                                                               c.L.n_most, c.S.u, c.S.temp, c.S.fm, c.S.fl, c.dtemp, tc, (float)tdt);
+                                                               c.L.n_most, c.S.u, c.S.temp, c.S.fm, c.S.fl, c.dtemp, c.us_update, tc, (float)tdt);
         ++c.launches;
     }
     if (tc == 0) SPH_TRY(neumann_pass(c, c.S));
@@ -1022,6 +1143,10 @@ int phase_time_update(Ctx<Real> &c) {
     SPH_TRY(outlet_pass(c, c.A));
     SPH_TRY(periodic_pass(c, c.A));
     SPH_TRY(freeslip_pass(c, c.A));
+    if (c.dp.inlet_recycling == 1 && c.L.n_rc > 0) {   // ISPH_Calc.cuh:215
+        k_recycle<Real><<<grid_for(c.L.n_rc, 128), 128, 0, st>>>(c.dp, soa(c), c.L.rc_rows, c.L.n_rc, c.us_update, c.A.u);
+        ++c.launches;
+    }
     SPH_CUDA_TRY(cudaGetLastError());
     c.time = c.time + c.dp.dt;
     c.count += 1;

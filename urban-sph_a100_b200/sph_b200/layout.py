@@ -117,9 +117,12 @@ class SphParams(ctypes.Structure):
         ("ppe_coarse_block", ctypes.c_int32),
         ("ppe_warm_start", ctypes.c_int32),
         ("apr_max_level", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 8),
+        ("outlet_bc", ctypes.c_int32),
+        ("inlet_recycling", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
+        ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
     ]
 
     def seti(self, name, value):
@@ -150,12 +153,16 @@ class PpeStats(ctypes.Structure):
     ]
 
 
-assert ctypes.sizeof(SphParams) == 1272, ctypes.sizeof(SphParams)
+assert ctypes.sizeof(SphParams) == 1288, ctypes.sizeof(SphParams)
+
+OUTLET_DONOTHING = 0      # KERNEL_donothing_buffer3D (the shipped step)
+OUTLET_EXTRAPOLATION = 1  # KERNEL_open_boundary_extrapolation_buffer3D
+OUTLET_INOUT = 2          # KERNEL_inout_boundary3D
 
 
 def params_from_bytes(b):
     """SphParams from stored bytes; fields appended since they were written
-    (apr_zone) read as 0."""
+    (apr_zone, the recycling probe) read as 0."""
     buf = bytearray(ctypes.sizeof(SphParams))
     b = bytes(b)
     buf[:len(b)] = b[:len(buf)]

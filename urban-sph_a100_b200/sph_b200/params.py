@@ -71,6 +71,7 @@ def default_params(dt=1e-4, kernel="Wendland6", turbulence="SSM", viscous=CLEARY
     p.ppe_pin = 1
     p.recompute_gc = 0
     p.ppe_inner_tol = 1e-3
+    p.recycle_probe_x, p.recycle_probe_y = 600.0, 0.0   # functions_MOST.cuh:316
     return p
 
 
