@@ -457,7 +457,7 @@ def main():
                 "initial_residual_mean": statistics.mean(s[5] for s in stats),
                 "not_converged_steps": sum(1 for s in stats if s[4] != 0)},
         "phase_ms": {"interaction": float(ph[1]), "ppe": float(ph[2]), "time_update": float(ph[3])},
-        "roofline": {"bound": "hbm", "kernel": "PPE operator (k_spmv, cached c_ij)" if not args.matrix_free
+        "roofline": {"bound": "hbm", "kernel": "PPE operator (k_spmv_fused: SELL rows + Neumann rows, cached c_ij)" if not args.matrix_free
                      else "PPE operator (k_spmv_mf)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic,

@@ -40,6 +40,7 @@ struct SideLists {
     int *sp_zero = nullptr; int n_sp_zero = 0;   // fluid rows with no marker in range
     // Neumann rows (p_type != 1): CSR of fluid j (p_type 1, buffer 0) in range
     int n_nm = 0;
+    long long nm_nnz = 0;
     int *nm_rows = nullptr, *nm_off = nullptr, *nm_nbr = nullptr;
     int *nm_ghost = nullptr;     // flags: 1 mirror (inlet) row, 2 the pass writes p = 0,
                                  // 4 no fluid in range at all (operator anchor)

@@ -802,6 +802,7 @@ int build_side_lists(Ctx<Real> &c) {
         mir.push_back(flags);
     }
     L.n_nm = (int)rows.size();
+    L.nm_nnz = (long long)nb.size();
     const std::vector<int> nmr = rows, nmo = off;
     SPH_TRY(upload_vec(c, L.nm_rows, rows)); SPH_TRY(upload_vec(c, L.nm_off, off)); SPH_TRY(upload_vec(c, L.nm_nbr, nb));
     SPH_TRY(upload_vec(c, L.nm_ghost, mir));
@@ -977,9 +978,12 @@ int build_side_lists(Ctx<Real> &c) {
         if (t.w == -1) fs.push_back(i);
         // converged-PPE row classes (precedence of the reference's overwrites:
         // outlet copy after Neumann after the PPE sweep)
+        // a record that is both an outlet buffer and a Neumann row (a
+        // free-slip record past L3) is a Neumann row of the operator: the
+        // Neumann application writes it
         if (t.x >= 3) kind[i] = 0;
-        else if (t.y == 2) kind[i] = 3;
         else if (t.w != 1) kind[i] = 2;
+        else if (t.y == 2) kind[i] = 3;
         else kind[i] = 1;
     }
     L.n_fluid = (int)fl.size(); L.n_wall = (int)wl.size(); L.n_fs = (int)fs.size();

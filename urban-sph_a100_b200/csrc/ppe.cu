@@ -196,6 +196,66 @@ __global__ void __launch_bounds__(128) k_ppe_sweep(const int4 *__restrict__ ty, 
 // ---------------------------------------------------------------------------
 // operator y = M x with the cached coefficients (vectors of type V)
 // ---------------------------------------------------------------------------
+// One launch for the whole operator: the Neumann rows (one warp per row over
+// their CSR weights) and the SELL rows (one thread per row) are disjoint row
+// sets, so their blocks are interleaved in one grid and the latency-bound
+// Neumann gathers run beside the bandwidth-bound SELL sweep.  Blocks
+// alternate Neumann / SELL while both kinds remain; the rest are of the
+// larger kind.
+template <class V, class C, class D, class W>
+__global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, const int *__restrict__ kind,
+                                                    const int *__restrict__ aux, LIST_ARGS, const C *__restrict__ coef,
+                                                    const D *__restrict__ diag, const int *__restrict__ comp_id,
+                                                    const double *__restrict__ cmean, const int *__restrict__ nm_rows,
+                                                    const int *__restrict__ nm_off, const int *__restrict__ nm_nb,
+                                                    const W *__restrict__ nm_w, int n_nm, const V *__restrict__ x,
+                                                    V *__restrict__ y, int n) {
+    const int b = blockIdx.x;
+    const int m = min(nb_nm, nb_sell);
+    bool neu;
+    int idx;
+    if (b < 2 * m) { neu = (b & 1) == 0; idx = b >> 1; }
+    else { neu = nb_nm > nb_sell; idx = m + (b - 2 * m); }
+    if (neu) {
+        const int k = idx * 4 + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        if (k >= n_nm) return;   // uniform over the warp
+        const int i = nm_rows[k];
+        const V xi = x[i];
+        const int q0 = nm_off[k], q1 = nm_off[k + 1];
+        double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
+        for (int q = q0 + lane; q < q1; q += 32) s += (double)__ldcs(&nm_w[q]) * (double)(xi - x[__ldcs(&nm_nb[q])]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) y[i] = (q1 > q0) ? (V)s : xi;
+        return;
+    }
+    const int i = idx * 128 + threadIdx.x;
+    if (i >= n) return;
+    const int kd = kind[i];
+    if (kd == 2) return;   // written by the Neumann blocks
+    const V xi = x[i];
+    V yi = xi;   // identity / pinned
+    if (kd == 1) {
+        const long long base = slice_off[i >> 5] + (i & 31);
+        const int cnt = ncnt[i];
+        V s = 0;
+        for (int k = 0; k < cnt; ++k) {
+            const long long e = base + 32LL * k;
+            s += (V)coef[e] * (xi - x[__ldg(&nbr[e])]);   // difference form, as k_spmv
+        }
+        yi = s;
+        if (comp_id) {
+            const int cc = comp_id[i];
+            if (cc >= 0) yi += (V)diag[i] * (V)cmean[cc];
+        }
+    } else if (kd == 3) {
+        const int j = aux[i];
+        if (j >= 0) yi = xi - x[j];
+    }
+    y[i] = yi;
+}
+
 template <class V, class C, class D>
 __global__ void __launch_bounds__(128) k_spmv(const int *__restrict__ kind, const int *__restrict__ aux, LIST_ARGS,
                                               const C *__restrict__ coef, const D *__restrict__ diag,
@@ -520,12 +580,21 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
         ++c.launches;
     }
     if (cached) {
-        if (sizeof(Real) == 4)
-            k_spmv<V, float, Real><<<grid_for(n, 128), 128, 0, c.stream>>>(c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr,
-                                                                          c.coef, c.diag, cid, cmean, x, y, n);
+        // FP32 Neumann weights in the FP32 applications of the mixed form; the
+        // FP64 applications (true residuals) keep the FP64 weights
+        const int nb_nm = div_up((long long)c.L.n_nm, 4), nb_sell = div_up((long long)n, 128);
+        if (sizeof(Real) == 4 && sizeof(V) == 4)
+            k_spmv_fused<V, float, Real, float><<<nb_nm + nb_sell, 128, 0, c.stream>>>(
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, (const float *)c.coef, c.diag, cid, cmean,
+                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.L.n_nm, x, y, n);
+        else if (sizeof(Real) == 4)
+            k_spmv_fused<V, float, Real, double><<<nb_nm + nb_sell, 128, 0, c.stream>>>(
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, (const float *)c.coef, c.diag, cid, cmean,
+                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow, c.L.n_nm, x, y, n);
         else
-            k_spmv<V, double, Real><<<grid_for(n, 128), 128, 0, c.stream>>>(c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr,
-                                                                           c.coef_d, c.diag, cid, cmean, x, y, n);
+            k_spmv_fused<V, double, Real, double><<<nb_nm + nb_sell, 128, 0, c.stream>>>(
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef_d, c.diag, cid, cmean,
+                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow, c.L.n_nm, x, y, n);
     } else {
         k_spmv_mf<Real, V><<<grid_for(n, 128), 128, 0, c.stream>>>(c.dp, c.row_kind, c.row_aux, c.pr, c.mr, c.jc, c.slice_off,
                                                                   c.ncnt, c.nbr, c.g6, c.diag, cid, cmean, x, y, n);
@@ -535,7 +604,7 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
         cudaEventRecord(c.prof_ev[2 * c.prof_pending + 1], c.stream);
         ++c.prof_pending;
     }
-    if (c.L.n_nm > 0) {
+    if (!cached && c.L.n_nm > 0) {
         const int gnm = div_up((long long)c.L.n_nm * 32, 256);
         // FP32 weights in the FP32 applications of the mixed form; the FP64
         // applications (true residuals) keep the FP64 weights
@@ -564,12 +633,16 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
         // per row: kind and list length (4 + 4) + x_i + y_i (Real), with the
         // rank-one term also component id (4) + A_i (Real); per slice of 32
         // rows its offset (8); per stored entry: index (4) + coefficient
-        // (float in the mixed form, double in the FP64 form).  The gathers
-        // x_j are not counted: an ideal kernel serves them from L2.
+        // (float in the mixed form, double in the FP64 form).  The Neumann
+        // rows of the same launch: row index and offset (4 + 4) + x_i + y_i,
+        // per entry index (4) + weight (Real).  The gathers x_j are not
+        // counted: an ideal kernel serves them from L2.
         const double R = (double)sizeof(Real);
         double row = 8.0 + 2.0 * R;
         if (c.n_comp > 0) row += 4.0 + R;
         *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + (double)c.nnz * (4.0 + R);
+        if (c.prm.ppe_matrix_free == 0)
+            *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R) + (double)c.L.nm_nnz * (4.0 + R);
     }
     if (reset) { c.prof_launches = 0; c.prof_ms = 0; }
     return SPH_OK;
