@@ -237,6 +237,9 @@ def main():
     ap.add_argument("--coarse", type=int, default=None,
                     help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; "
                          "default 5 for the canyon, 9 for the cube array)")
+    ap.add_argument("--coarse-mode", default="additive", choices=["additive", "multiplicative"],
+                    help="two-level form: D^-1 r + Z E^-1 Z^T r, or the coarse correction of the residual the "
+                         "Jacobi step leaves (one more operator application per preconditioner call)")
     ap.add_argument("--gmres-restart", type=int, default=0, help="GMRES(m) restart length (0: 40)")
     ap.add_argument("--inner-tol", type=float, default=0.0, help="restarted refinement: inner tolerance (0: 1e-3)")
     ap.add_argument("--warm", default="prev", choices=["prev", "extrap", "learned"],
@@ -280,6 +283,7 @@ def main():
         p.ppe_matrix_free = 1
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2}[args.refinement]
     p.ppe_coarse_block = args.coarse
+    p.ppe_coarse_mode = 1 if args.coarse_mode == "multiplicative" else 0
     p.ppe_gmres_restart = args.gmres_restart
     if args.inner_tol > 0:
         p.ppe_inner_tol = args.inner_tol
@@ -443,8 +447,8 @@ def main():
                    "ppe_refinement": args.refinement,
                    "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",
                                         "learned": "learned per-particle MLP on the previous pressure"}[args.warm],
-                   "ppe_preconditioner": f"jacobi + coarse aggregates of {args.coarse}^3 cells" if args.coarse > 0
-                   else "jacobi",
+                   "ppe_preconditioner": f"jacobi + coarse aggregates of {args.coarse}^3 cells ({args.coarse_mode})"
+                   if args.coarse > 0 else "jacobi",
                    "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": len(P) * layout.PART1.itemsize,

@@ -181,7 +181,12 @@ typedef struct sph_params {
                                 the step (ISPH_Calc.cuh:215; functions_BC.cuh:
                                 1857-1941): inlet ux = u* / kappa_vK log(z / z0)
                                 with u* from the MOST particle at the probe    */
-    int32_t reserved[6];
+    int32_t ppe_coarse_mode; /* with ppe_coarse_block > 0 in the BiCGSTAB forms:
+                                0 additive (D^-1 r + Z E^-1 Z^T r); 1
+                                multiplicative (z = D^-1 r, then z += Z E^-1
+                                Z^T (r - M z): one more operator application
+                                per preconditioner call)                      */
+    int32_t reserved[5];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

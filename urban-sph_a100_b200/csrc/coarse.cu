@@ -204,12 +204,17 @@ __global__ void k_eye(double *A, int m) {
 
 // ---- application ----------------------------------------------------------
 
+// s_I = sum over the rows of aggregate I of r (minus w when given)
 template <class V>
-__global__ void __launch_bounds__(256) k_coarse_restrict(const int *off, const int *rows, const V *r, double *s) {
+__global__ void __launch_bounds__(256) k_coarse_restrict(const int *off, const int *rows, const V *r, const V *w,
+                                                         double *s) {
     __shared__ double sh[8];
     const int I = blockIdx.x;
     double v = 0;
-    for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) v += (double)r[rows[q]];
+    if (w)
+        for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) { const int i = rows[q]; v += (double)(r[i] - w[i]); }
+    else
+        for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) v += (double)r[rows[q]];
     v = block_sum<256>(v, sh);
     if (threadIdx.x == 0) s[I] = v;
 }
@@ -238,10 +243,18 @@ __global__ void k_coarse_add(const int *agg, const double *y, V *z, int n) {
 }
 
 template <class Real, class V>
-void coarse_apply(Ctx<Real> &c, const V *r, V *z) {
+void coarse_restrict_solve(Ctx<Real> &c, const V *r, const V *w) {
+    const int m = c.cg_m;
+    k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, w, c.cg_s);
+    k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_invf, c.cg_s, c.cg_y, m);
+    c.launches += 2;
+}
+
+template <class Real, class V>
+void coarse_apply(Ctx<Real> &c, const V *r, V *z, const V *w) {
     if (c.cg_m <= 0) return;
     const int m = c.cg_m;
-    k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, c.cg_s);
+    k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, w, c.cg_s);
     k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_invf, c.cg_s, c.cg_y, m);
     k_coarse_add<V><<<grid_for(c.n, 256), 256, 0, c.stream>>>(c.cg_agg, c.cg_y, z, c.n);
     c.launches += 3;
@@ -401,8 +414,11 @@ int coarse_build(Ctx<Real> &c) {
 
 template int coarse_build<float>(Ctx<float> &);
 template int coarse_build<double>(Ctx<double> &);
-template void coarse_apply<float, float>(Ctx<float> &, const float *, float *);
-template void coarse_apply<float, double>(Ctx<float> &, const double *, double *);
-template void coarse_apply<double, double>(Ctx<double> &, const double *, double *);
+template void coarse_apply<float, float>(Ctx<float> &, const float *, float *, const float *);
+template void coarse_apply<float, double>(Ctx<float> &, const double *, double *, const double *);
+template void coarse_apply<double, double>(Ctx<double> &, const double *, double *, const double *);
+template void coarse_restrict_solve<float, float>(Ctx<float> &, const float *, const float *);
+template void coarse_restrict_solve<float, double>(Ctx<float> &, const double *, const double *);
+template void coarse_restrict_solve<double, double>(Ctx<double> &, const double *, const double *);
 
 }  // namespace sph

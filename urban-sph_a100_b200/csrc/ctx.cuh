@@ -259,7 +259,10 @@ template <class Real> int ml_set_weights(Ctx<Real> &c, const float *w);
 template <class Real> int ml_get_weights(Ctx<Real> &c, float *w);
 template <class Real> int ml_samples(Ctx<Real> &c, long long first, long long rows, uint16_t *X, float *t, long long *count);
 template <class Real> int ml_predict_samples(Ctx<Real> &c, long long first, int rows, float *y);
-template <class Real, class V> void coarse_apply(Ctx<Real> &c, const V *r, V *z);
+template <class Real, class V> void coarse_apply(Ctx<Real> &c, const V *r, V *z, const V *w = nullptr);
+// the restriction and coarse solve of coarse_apply (c.cg_y = E^-1 Z^T (r - w));
+// the caller adds Z c.cg_y
+template <class Real, class V> void coarse_restrict_solve(Ctx<Real> &c, const V *r, const V *w);
 template <class Real> int phase_time_update(Ctx<Real> &c);
 template <class Real> int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax);
 template <class Real> int gradient_correction(Ctx<Real> &c);

@@ -290,6 +290,29 @@ __global__ void __launch_bounds__(128) k_spmv(const int *__restrict__ kind, cons
     y[i] = yi;
 }
 
+// z += Z y_c (coarse correction) with the per-component mean of the result
+// for the rank-one term of the next operator application (the sums of
+// k_comp_mean, in the same grid and order)
+template <class V, int NC>
+__global__ void k_coarse_add_mean(const int *agg, const double *yc, V *z, const int *comp_id, int n, int ncomp,
+                                  const double *inv, double *partials, unsigned int *counter, double *cmean) {
+    double v[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) v[q] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int a = agg[i];
+        V zi = z[i];
+        if (a >= 0) { zi += (V)yc[a]; z[i] = zi; }
+        const int cc = comp_id[i];
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (cc == q) v[q] += (double)zi;
+    }
+    reduce_finish<NC>(v, partials, counter, [&](double *t) {
+        for (int q = 0; q < ncomp; ++q) cmean[q] = t[q] * inv[q];
+    });
+}
+
 // per-component mean of x over the fluid rows of the singular components:
 // cmean[c] = (1/|u_c|) sum_{i in u_c} x_i, deterministic (block partials)
 // (NC = 1 for the common single-component case, SPH_MAX_COMP otherwise)
@@ -556,7 +579,7 @@ static void prof_drain(Ctx<Real> &c) {
 }
 
 template <class Real, class V>
-static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
+static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_ready = false) {
     const int n = c.n;
     const bool timed = c.prof && sizeof(V) == sizeof(Real);
     if (timed) {
@@ -569,8 +592,8 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached) {
     }
     const int *cid = nullptr;
     double *cmean = c.scal + 40;
-    if (c.n_comp > 0) {
-        cid = c.comp_id;
+    if (c.n_comp > 0) cid = c.comp_id;
+    if (c.n_comp > 0 && !mean_ready) {
         if (c.n_comp == 1)
             k_comp_mean<V, 1><<<red_grid(n), 256, 0, c.stream>>>(c.comp_id, x, n, 1, c.comp_inv, c.red,
                                                                  (unsigned int *)(c.scal + 32), cmean);
@@ -648,6 +671,37 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
     return SPH_OK;
 }
 
+// Two-level preconditioner on r, with z holding D^-1 r on entry: the
+// additive form adds Z E^-1 Z^T r; the multiplicative form corrects the
+// residual that the Jacobi step leaves, z += Z E^-1 Z^T (r - M z), at the
+// cost of one more operator application (tmp receives M z).  With singular
+// components the final add also forms the component means of z for the
+// operator application that follows; returns whether it did.
+template <class Real, class V>
+static bool precond_coarse(Ctx<Real> &c, const V *r, V *z, V *tmp, bool cached) {
+    if (c.cg_m <= 0) return false;
+    const V *w = nullptr;
+    if (c.prm.ppe_coarse_mode == 1) {
+        apply_op<Real, V>(c, z, tmp, cached);
+        w = tmp;
+    }
+    if (c.n_comp <= 0) {
+        coarse_apply<Real, V>(c, r, z, w);
+        return false;
+    }
+    coarse_restrict_solve<Real, V>(c, r, w);
+    unsigned int *counter = (unsigned int *)(c.scal + 32);
+    double *cmean = c.scal + 40;
+    if (c.n_comp == 1)
+        k_coarse_add_mean<V, 1><<<red_grid(c.n), 256, 0, c.stream>>>(c.cg_agg, c.cg_y, z, c.comp_id, c.n, 1, c.comp_inv,
+                                                                    c.red, counter, cmean);
+    else
+        k_coarse_add_mean<V, SPH_MAX_COMP><<<red_grid(c.n), 256, 0, c.stream>>>(c.cg_agg, c.cg_y, z, c.comp_id, c.n,
+                                                                               c.n_comp, c.comp_inv, c.red, counter, cmean);
+    ++c.launches;
+    return true;
+}
+
 // Jacobi-preconditioned BiCGSTAB on M x = b with vectors of type V (the
 // workspace ws holds 9 of them) and FP64 dots; x holds the initial guess.
 // Returns SPH_OK, SPH_NOT_CONVERGED or SPH_ERR_BREAKDOWN (> 20 restarts).
@@ -686,12 +740,12 @@ static int bicgstab_v(Ctx<Real> &c, V *const *ws, V *x, const V *b, double bnorm
         const int check = 4;
         while (it < maxit) {
             k_p_update<V><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
-            coarse_apply<Real, V>(c, p, ph);
-            apply_op<Real, V>(c, ph, v, cached);
+            bool mr = precond_coarse<Real, V>(c, p, ph, v, cached);   // v is free until M ph is written to it
+            apply_op<Real, V>(c, ph, v, cached, mr);
             k_alpha<V><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
             k_s_update<V><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
-            coarse_apply<Real, V>(c, s, sh);
-            apply_op<Real, V>(c, sh, t, cached);
+            mr = precond_coarse<Real, V>(c, s, sh, t, cached);        // t likewise
+            apply_op<Real, V>(c, sh, t, cached, mr);
             k_omega<V><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
             k_xr_update<V><<<G, 256, 0, st>>>(x, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
             c.launches += 5;
@@ -835,12 +889,12 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     const int check = 4;
     while (status != SPH_OK && it < maxit) {
         k_p_update<float><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
-        coarse_apply<Real, float>(c, p, ph);
-        apply_op<Real, float>(c, ph, v, cached);
+        bool mr = precond_coarse<Real, float>(c, p, ph, v, cached);
+        apply_op<Real, float>(c, ph, v, cached, mr);
         k_alpha<float><<<G, 256, 0, st>>>(rh, v, n, c.red, counter, c.scal);
         k_s_update<float><<<G, 256, 0, st>>>(r, v, s, sh, dinv, n, c.scal);
-        coarse_apply<Real, float>(c, s, sh);
-        apply_op<Real, float>(c, sh, t, cached);
+        mr = precond_coarse<Real, float>(c, s, sh, t, cached);
+        apply_op<Real, float>(c, sh, t, cached, mr);
         k_omega<float><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
         k_xr_update<float><<<G, 256, 0, st>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
         c.launches += 5;

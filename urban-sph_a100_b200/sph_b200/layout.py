@@ -119,7 +119,8 @@ class SphParams(ctypes.Structure):
         ("apr_max_level", ctypes.c_int32),
         ("outlet_bc", ctypes.c_int32),
         ("inlet_recycling", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("ppe_coarse_mode", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
         ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
