@@ -256,40 +256,6 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
     y[i] = yi;
 }
 
-template <class V, class C, class D>
-__global__ void __launch_bounds__(128) k_spmv(const int *__restrict__ kind, const int *__restrict__ aux, LIST_ARGS,
-                                              const C *__restrict__ coef, const D *__restrict__ diag,
-                                              const int *__restrict__ comp_id, const double *__restrict__ cmean,
-                                              const V *__restrict__ x, V *__restrict__ y, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int kd = kind[i];
-    const V xi = x[i];
-    V yi = xi;   // identity / pinned; Neumann rows are applied by k_spmv_neumann
-    if (kd == 1) {
-        // A_i x_i - sum_j c_ij x_j with A_i = sum_j c_ij (k_ppe_rows), evaluated
-        // as sum_j c_ij (x_i - x_j): the differences of nearby values are exact,
-        // so a smooth x does not lose (L/h)^2 digits to cancellation, which
-        // in FP32 would stall the Krylov iteration on the smooth modes
-        const long long base = slice_off[i >> 5] + (i & 31);
-        const int cnt = ncnt[i];
-        V s = 0;
-        for (int k = 0; k < cnt; ++k) {
-            const long long e = base + 32LL * k;
-            s += (V)coef[e] * (xi - x[__ldg(&nbr[e])]);
-        }
-        yi = s;
-        if (comp_id) {
-            const int cc = comp_id[i];
-            if (cc >= 0) yi += (V)diag[i] * (V)cmean[cc];   // A_i * mean: beside the spectrum
-        }
-    } else if (kd == 3) {
-        const int j = aux[i];
-        if (j >= 0) yi = xi - x[j];
-    }
-    y[i] = yi;
-}
-
 // z += Z y_c (coarse correction) with the per-component mean of the result
 // for the rank-one term of the next operator application (the sums of
 // k_comp_mean, in the same grid and order)
