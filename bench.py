@@ -240,10 +240,15 @@ def main():
     ap.add_argument("--coarse-mode", default="additive", choices=["additive", "multiplicative"],
                     help="two-level form: D^-1 r + Z E^-1 Z^T r, or the coarse correction of the residual the "
                          "Jacobi step leaves (one more operator application per preconditioner call)")
+    ap.add_argument("--pair-h", default=None, choices=["ref", "avg"],
+                    help="smoothing length of a pair in the pressure system: h_i as the reference's KERNEL_PPE3D "
+                         "(ref), or (h_i + h_j)/2, its commented-out multi-resolution form (avg); default avg with "
+                         "--apr, else ref")
     ap.add_argument("--gmres-restart", type=int, default=0, help="GMRES(m) restart length (0: 40)")
     ap.add_argument("--inner-tol", type=float, default=0.0, help="restarted refinement: inner tolerance (0: 1e-3)")
-    ap.add_argument("--warm", default="prev", choices=["prev", "extrap", "learned"],
-                    help="PPE start vector: previous pressure, linear extrapolation in time, or the learned "
+    ap.add_argument("--warm", default="prev", choices=["prev", "scaled", "extrap", "learned"],
+                    help="PPE start vector: previous pressure, previous pressure times its residual-minimising factor, linear "
+                         "extrapolation in time, or the learned "
                          "per-particle network (trained on this run's warm-up solves)")
     ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres"],
                     help="mixed_ir form: FP64 reliable updates, or refinement restarting the FP32 solver")
@@ -284,10 +289,13 @@ def main():
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2}[args.refinement]
     p.ppe_coarse_block = args.coarse
     p.ppe_coarse_mode = 1 if args.coarse_mode == "multiplicative" else 0
+    if args.pair_h is None:
+        args.pair_h = "avg" if args.apr else "ref"
+    p.ppe_pair_h = 1 if args.pair_h == "avg" else 0
     p.ppe_gmres_restart = args.gmres_restart
     if args.inner_tol > 0:
         p.ppe_inner_tol = args.inner_tol
-    p.ppe_warm_start = 1 if args.warm == "extrap" else 0
+    p.ppe_warm_start = {"extrap": 1, "scaled": 3}.get(args.warm, 0)
     n = len(P)
     sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
     if boxes is not None:
@@ -445,7 +453,9 @@ def main():
                    "ppe": args.mode, "ppe_tol": 1e-6,
                    "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
                    "ppe_refinement": args.refinement,
+                   "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],
                    "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",
+                                        "scaled": "previous pressure times its residual-minimising factor",
                                         "learned": "learned per-particle MLP on the previous pressure"}[args.warm],
                    "ppe_preconditioner": f"jacobi + coarse aggregates of {args.coarse}^3 cells ({args.coarse_mode})"
                    if args.coarse > 0 else "jacobi",

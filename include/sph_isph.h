@@ -168,7 +168,10 @@ typedef struct sph_params {
                                 B x B x B NNPS cells (additive two-level)      */
     int32_t ppe_warm_start;  /* start vector of the converged solves: 0 previous
                                 pressure; 1 linear extrapolation in time,
-                                2 p_n - p_(n-1), once two solutions exist     */
+                                2 p_n - p_(n-1), once two solutions exist;
+                                3 the previous pressure times the factor that
+                                minimises the FP64 residual (so the start
+                                residual never exceeds that of a zero start) */
     int32_t apr_max_level;   /* APR (vii[35] = 1, every vii[37] steps): target
                                 level log8(m_ref/m) of fluid near IBM markers */
     int32_t outlet_bc;       /* pass at the outlet-buffer call sites of the step
@@ -186,7 +189,13 @@ typedef struct sph_params {
                                 multiplicative (z = D^-1 r, then z += Z E^-1
                                 Z^T (r - M z): one more operator application
                                 per preconditioner call)                      */
-    int32_t reserved[5];
+    int32_t ppe_pair_h;      /* smoothing length of a pair in the pressure
+                                system (rows, right-hand side, operator): 0 h_i
+                                as KERNEL_PPE3D uses it; 1 (h_i + h_j) / 2, the
+                                multi-resolution form that KERNEL_PPE3D keeps
+                                commented out (functions_PPE.cuh:113-116) and
+                                KERNEL_pressureforce3D uses (:598-602)         */
+    int32_t reserved[4];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

@@ -1032,7 +1032,13 @@ struct Oracle {
             Real xj = A.x[j], yj = A.y[j], zj = A.z[j], uxj = A.ux[j], uyj = A.uy[j], uzj = A.uz[j];
             Real rhoj = A.rho[j], mj = A.m[j];
             Real tdist = std::sqrt((xi - xj) * (xi - xj) + (yi - yj) * (yi - yj) + (zi - zj) * (zi - zj)) + 1e-20;
-            Real tdwij = calc_dwij_pressure(Q, tmp_A, hi, tdist);
+            Real tdwij;
+            if (prm.ppe_pair_h == 1) {   // functions_PPE.cuh:113-116 (commented out there)
+                Real hij = 0.5 * (hi + prm.pressure_length * A.h[j]);
+                tdwij = calc_dwij_pressure(Q, calc_tmpA(Q, hij), hij, tdist);
+            } else {
+                tdwij = calc_dwij_pressure(Q, tmp_A, hi, tdist);
+            }
             Real tdwx = tdwij * (xi - xj) / tdist, tdwy = tdwij * (yi - yj) / tdist, tdwz = tdwij * (zi - zj) / tdist;
             Real tdwxc = gc11 * tdwx + gc12 * tdwy + gc31 * tdwz;
             Real tdwyc = gc12 * tdwx + gc22 * tdwy + gc23 * tdwz;

@@ -157,3 +157,37 @@ def test_coarse_block_too_small_is_rejected(deck):
         sim.step(1)
     assert e.value.status == -7
     sim.close()
+
+
+def _two_level_deck():
+    """caseh_mini with the smoothing length of the channel's downstream half
+    (0.3 m < x, before the outlet block at L3) raised by half, so that pairs
+    across the level interface have h_i != h_j."""
+    P, p = decks.caseh_mini(nx=14, ny=8, nz=5)
+    P = P.copy()
+    far = (P["x"] > np.float32(0.3)) & (P["x"] < np.float32(5.0))
+    P["h"][far] *= np.float32(1.5)
+    P["h_ref"][far] = P["h"][far]
+    decks.domain_setup(p, P)
+    return P, p
+
+
+def test_pair_averaged_h_matches_oracle():
+    """ppe_pair_h = 1 (the reference's commented-out multi-resolution form of
+    the pressure rows): FP64 BiCGSTAB against the oracle with the same
+    option, the matrix-free operator against the cached one, and a pressure
+    different from the h_i form on a deck with two smoothing lengths."""
+    P, p = _two_level_deck()
+    q = p.copy()
+    q.ppe_pair_h = 1
+    A, stats = _gpu_step(P, q, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8)
+    assert stats[-1].status == 0 and stats[-1].rel_residual <= 1e-8
+    O = restated.Restated(P, q, 1)
+    st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-10, maxit=5000)
+    assert st == 0
+    B, _, _ = O.download()
+    assert rel_err(A["pres"], B["pres"]) <= PRES_TOL_FP64
+    M, s2 = _gpu_step(P, q, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8, matrix_free=True)
+    assert s2[-1].status == 0 and rel_err(M["pres"], A["pres"]) <= 1e-6
+    R, s3 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8)
+    assert s3[-1].status == 0 and rel_err(R["pres"], A["pres"]) > 1e-4

@@ -36,6 +36,7 @@ DevParams make_dev_params(const sph_params &p) {
     d.boussinesq = p.vii[SPH_VII_BOUSSINESQ];
     d.concn_solve = p.vii[SPH_VII_CONCN_SOLVE];
     d.outlet_bc = p.outlet_bc;
+    d.ppe_pair_h = p.ppe_pair_h;
     d.inlet_recycling = p.inlet_recycling;
     d.rp_x = p.recycle_probe_x; d.rp_y = p.recycle_probe_y;
     d.turb = p.vii[SPH_VII_TURBULENCE];

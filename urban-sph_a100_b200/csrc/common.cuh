@@ -35,6 +35,7 @@ struct DevParams {
     int kernel_type, time_type, freq_filt, fp_solve, fv_solve, fg_solve, kgc_solve, turb, noslip;
     int con_solve, boussinesq, concn_solve;
     int outlet_bc, inlet_recycling;
+    int ppe_pair_h;        // 1: pair-averaged h in the pressure system
     double rp_x, rp_y;     // recycling probe
     int count;
     float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, time, dt_structure;

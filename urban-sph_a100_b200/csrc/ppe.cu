@@ -123,7 +123,13 @@ __global__ void __launch_bounds__(128) k_ppe_rows(DevParams P, const float4 *__r
             const auto mj = mr[j];
             const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
-            const Real dw = calc_dwij_pressure<Real>(P, tA, hi, tdist);
+            Real dw;
+            if (P.ppe_pair_h == 1) {   // the multi-resolution form, functions_PPE.cuh:113-116
+                const Real hij = (Real)0.5 * (hi + (Real)(P.pressure_length * (double)xj.w));
+                dw = calc_dwij_pressure<Real>(P, calc_tmpA<Real>(P, hij), hij, tdist);
+            } else {
+                dw = calc_dwij_pressure<Real>(P, tA, hi, tdist);
+            }
             const Real tdx = dw * dx / tdist, tdy = dw * dy / tdist, tdz = dw * dz / tdist;
             const Real cx = gc11 * tdx + gc12 * tdy + gc31 * tdz;
             const Real cy = gc12 * tdx + gc22 * tdy + gc23 * tdz;
@@ -330,7 +336,13 @@ __global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restr
             const auto mj = mr[j];
             const Real dx = xp.x - xj.x, dy = xp.y - xj.y, dz = xp.z - xj.z;
             const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
-            const Real dw = calc_dwij_pressure<Real>(P, tA, hi, tdist);
+            Real dw;
+            if (P.ppe_pair_h == 1) {   // the multi-resolution form, functions_PPE.cuh:113-116
+                const Real hij = (Real)0.5 * (hi + (Real)(P.pressure_length * (double)xj.w));
+                dw = calc_dwij_pressure<Real>(P, calc_tmpA<Real>(P, hij), hij, tdist);
+            } else {
+                dw = calc_dwij_pressure<Real>(P, tA, hi, tdist);
+            }
             const Real tdx = dw * dx / tdist, tdy = dw * dy / tdist, tdz = dw * dz / tdist;
             const Real cx = gc11 * tdx + gc12 * tdy + gc31 * tdz;
             const Real cy = gc12 * tdx + gc22 * tdy + gc23 * tdz;
@@ -605,6 +617,23 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
                                                                  x, y);
         ++c.launches;
     }
+}
+
+// start vector a x with a = (b, y) / (y, y), y = M x: the multiple of x with
+// the smallest residual (x unchanged when y = 0)
+__global__ void k_start_factor(const double *b, const double *y, int n, double *partials, unsigned int *counter,
+                               double *scal) {
+    double d[2] = {0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d[0] += b[i] * y[i];
+        d[1] += y[i] * y[i];
+    }
+    reduce_finish<2>(d, partials, counter, [&](double *t) { scal[SC_ALPHA] = t[1] > 0 ? t[0] / t[1] : 1.0; });
+}
+
+__global__ void k_scale_start(double *x, int n, const double *scal) {
+    const double a = scal[SC_ALPHA];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= a;
 }
 
 // y = M x with FP64 vectors and the context's cached or matrix-free operator
@@ -1232,6 +1261,12 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         if (history) SPH_TRY(ml_prepare(c, (const Real *)b, learned || c.ml_every > 0));
         if (extrap) SPH_TRY(ml_extrapolate(c, xd));
         if (learned) SPH_TRY(ml_warm_start(c, bd, xd, rd));
+        if (!learned && c.prm.ppe_warm_start == 3) {
+            apply_op<Real, double>(c, xd, rd, cached);
+            k_start_factor<<<G, 256, 0, st>>>(bd, rd, n, c.red, counter, c.scal);
+            k_scale_start<<<G, 256, 0, st>>>(xd, n, c.scal);
+            c.launches += 2;
+        }
         const double tol = c.prm.ppe_tol > 0 ? c.prm.ppe_tol : 1e-6;
         const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
         int status = SPH_OK, iters = 0, restarts = 0, refinements = 0;

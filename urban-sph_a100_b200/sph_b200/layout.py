@@ -120,7 +120,8 @@ class SphParams(ctypes.Structure):
         ("outlet_bc", ctypes.c_int32),
         ("inlet_recycling", ctypes.c_int32),
         ("ppe_coarse_mode", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("ppe_pair_h", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
         ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
