@@ -336,7 +336,9 @@ def main():
                    "train_s": train_s, "train_loss": loss, "epochs": 6, "batch": 4096}
         for _ in range(2):
             sim.step(1)
+        ml_weights = sim.ml_get_weights()
     else:
+        ml_weights = None
         for _ in range(args.warmup):
             sim.step(1)
 
@@ -387,7 +389,7 @@ def main():
     # ---- other forms on the same deck, rank 0 only ----
     sim.close()
 
-    def timed_form(precision, mode, coarse, steps):
+    def timed_form(precision, mode, coarse, steps, keep=False):
         q = p.copy()
         q.ppe_mode = mode
         q.ppe_coarse_block = coarse
@@ -408,20 +410,55 @@ def main():
         g1.record()
         torch.cuda.synchronize()
         dms = g0.elapsed_time(g1)
+        state = sd.download(want=(1,))[0] if keep else None
         sd.close()
-        return {"value": n * steps / (dms / 1e3), "ms_per_step": dms / steps, "steps": steps,
-                "ppe_ms": statistics.mean(d[2] for d in dstats),
-                "ppe_iterations": statistics.mean(d[0] for d in dstats),
-                "rel_residual_max": max(d[1] for d in dstats)}
+        out = {"value": n * steps / (dms / 1e3), "ms_per_step": dms / steps, "steps": steps,
+               "ppe_ms": statistics.mean(d[2] for d in dstats),
+               "ppe_iterations": statistics.mean(d[0] for d in dstats),
+               "rel_residual_max": max(d[1] for d in dstats)}
+        if keep:
+            out["_state"] = state
+        return out
 
-    fp64 = fp64_same = sweep = None
+    def error_vs(ref_state, steps):
+        """The chosen form run from the same start for the same number of
+        steps as the FP64 form, and its relative error against it over the
+        fluid particles (L2 and max norms)."""
+        if ref_state is None:
+            return None
+        q = p.copy()
+        if ml_weights is not None:   # the learned form with this run's trained network
+            q.ppe_mode = layout.PPE_LEARNED
+        sd = abi.Simulation(q, precision=layout.PREC_MIXED, device=local)
+        if boxes is not None:
+            sd.set_ib_boxes(boxes)
+        if ml_weights is not None:
+            sd.ml_set_weights(ml_weights)
+        sd.upload(P)
+        for _ in range(steps):
+            sd.step(1)
+        A = sd.download(want=(1,))[0]
+        sd.close()
+        B = ref_state
+        fl = (B["i_type"] < 3) & (B["p_type"] == 1)
+        ua = np.stack([A[f][fl] for f in ("ux", "uy", "uz")]).astype(np.float64)
+        ub = np.stack([B[f][fl] for f in ("ux", "uy", "uz")]).astype(np.float64)
+        pa, pb = A["pres"][fl].astype(np.float64), B["pres"][fl].astype(np.float64)
+        return {"steps": steps, "particles": int(fl.sum()),
+                "u_rel_l2": float(np.linalg.norm(ua - ub) / np.linalg.norm(ub)),
+                "u_rel_max": float(np.abs(ua - ub).max() / np.abs(ub).max()),
+                "p_rel_l2": float(np.linalg.norm(pa - pb) / np.linalg.norm(pb)),
+                "p_rel_max": float(np.abs(pa - pb).max() / np.abs(pb).max())}
+
+    fp64 = fp64_same = sweep = err64 = None
     if rank == 0:
         kd = max(3, args.steps // 4)
         fp64_mode = layout.PPE_GMRES if args.fp64_mode == "gmres" else layout.PPE_BICGSTAB
         if not args.no_fp64:
             # the plain form: FP64 throughout, Jacobi-preconditioned Krylov
-            fp64 = timed_form(layout.PREC_FP64, fp64_mode, 0, kd)
+            fp64 = timed_form(layout.PREC_FP64, fp64_mode, 0, kd, keep=True)
             fp64.update({"solver": args.fp64_mode + " + jacobi", "ppe_tol": 1e-6})
+            err64 = error_vs(fp64.pop("_state"), kd + 2)
             if args.coarse > 0:
                 # FP64 with this run's preconditioner: isolates the precision change
                 fp64_same = timed_form(layout.PREC_FP64, layout.PPE_BICGSTAB, args.coarse, kd)
@@ -477,6 +514,7 @@ def main():
                      "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": op_bytes, "launch_ms": per_launch_ms, "launches": op_n},
         "plain_fp64": fp64,
+        "error_vs_plain_fp64": err64,
         "fp64_same_preconditioner": fp64_same,
         "learned_warm_start": learned,
         "reference_step_semantics": sweep,
