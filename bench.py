@@ -179,6 +179,103 @@ def run_ensemble(args, rank, world, local):
     return 0
 
 
+def run_transfer(args, rank, world, local):
+    """Learned warm start across decks: the network is trained on the
+    pressure solves of the urban canyon (dx = 0.01 m) and starts the solves
+    of the cube-array geometry at dx = 0.0075 m.  Three forms from the same
+    start on the array: the mixed form with the previous pressure as start
+    vector, the same with the learned start, and the plain FP64 form (Jacobi
+    BiCGSTAB), which judges both."""
+    import numpy as np
+    import torch
+    from sph_b200 import abi, decks, layout
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    t_all = time.perf_counter()
+    # ---- training on the canyon's solves ----
+    P, p = decks.canyon(scale=1.0)
+    p.ppe_mode, p.ppe_tol, p.ppe_coarse_block = layout.PPE_MIXED_IR, 1e-6, 5
+    sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
+    sim.upload(P)
+    every = max(1, len(P) * args.train_solves // 1900000)
+    sim.ml_collect(every)
+    for _ in range(args.train_solves):
+        sim.step(1)
+    sim.ml_collect(0)
+    nsamp = int(lib_sample_count(sim))
+    t0 = time.perf_counter()
+    loss = sim.ml_train(epochs=6, batch=4096, lr=1e-3, seed=20261203)
+    train_s = time.perf_counter() - t0
+    w = sim.ml_get_weights()
+    sim.close()
+    # ---- the array geometry at the finer spacing ----
+    Pa, pa, boxes = decks.cube_array(scale=args.scale, dx=args.dx)
+    pa.ppe_tol = 1e-6
+    n = int((Pa["i_type"] < 3).sum())
+    coarse = args.coarse if args.coarse is not None else 12
+
+    def form(precision, mode, cb, weights, steps):
+        q = pa.copy()
+        q.ppe_mode, q.ppe_coarse_block = mode, cb
+        sd = abi.Simulation(q, precision=precision, device=local)
+        sd.set_ib_boxes(boxes)
+        if weights is not None:
+            sd.ml_set_weights(weights)
+        sd.upload(Pa)
+        for _ in range(2):
+            sd.step(1)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        st = []
+        g0.record()
+        for _ in range(steps):
+            s_ = sd.step(1)
+            st.append((s_.iterations, s_.rel_residual, s_.solve_ms, s_.initial_residual, s_.status))
+        g1.record()
+        torch.cuda.synchronize()
+        ms = g0.elapsed_time(g1)
+        A = sd.download(want=(1,))[0]
+        sd.close()
+        return A, {"value": n * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                   "ppe_iterations": float(np.mean([x[0] for x in st])),
+                   "rel_residual_max": float(max(x[1] for x in st)),
+                   "ppe_ms": float(np.mean([x[2] for x in st])),
+                   "initial_residual_mean": float(np.mean([x[3] for x in st])),
+                   "not_converged_steps": sum(1 for x in st if x[4] != 0)}
+
+    k = args.steps
+    Ap, prev = form(layout.PREC_MIXED, layout.PPE_MIXED_IR, coarse, None, k)
+    Al, lrn = form(layout.PREC_MIXED, layout.PPE_LEARNED, coarse, w, k)
+    A64, plain = form(layout.PREC_FP64, layout.PPE_BICGSTAB, 0, None, k)
+    fl = (A64["i_type"] < 3) & (A64["p_type"] == 1)
+
+    def err(A):
+        ua = np.stack([A[f][fl] for f in ("ux", "uy", "uz")]).astype(np.float64)
+        ub = np.stack([A64[f][fl] for f in ("ux", "uy", "uz")]).astype(np.float64)
+        pa_, pb = A["pres"][fl].astype(np.float64), A64["pres"][fl].astype(np.float64)
+        return {"u_rel_l2": float(np.linalg.norm(ua - ub) / np.linalg.norm(ub)),
+                "p_rel_l2": float(np.linalg.norm(pa_ - pb) / np.linalg.norm(pb))}
+
+    prev["error_vs_plain_fp64"] = err(Ap)
+    lrn["error_vs_plain_fp64"] = err(Al)
+    out = {"metric": METRIC, "value": lrn["value"], "unit": METRIC, "n_gpus": 1, "steps": k,
+           "warmup": 2, "ms_per_step": lrn["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+           "config": {"workload": f"learned warm start trained on the urban canyon (dx 0.01 m, {args.train_solves} "
+                                  f"solves) applied to the 4x4 cube array at dx {args.dx} m",
+                      "particles": n, "scale": args.scale, "coarse": coarse},
+           "training": {"solves": args.train_solves, "samples": nsamp, "every_kth_fluid_row": every,
+                        "loss": loss, "train_s": train_s},
+           "mixed_learned": lrn, "mixed_previous_pressure": prev, "plain_fp64": plain,
+           "iterations_saved_per_step": prev["ppe_iterations"] - lrn["ppe_iterations"],
+           "learned_vs_plain_fp64": lrn["value"] / plain["value"],
+           "wall_s": time.perf_counter() - t_all}
+    print(json.dumps(out))
+    return 0
+
+
 def lib_sample_count(sim):
     import ctypes
     from sph_b200 import abi
@@ -223,9 +320,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--config", default="canyon", choices=["canyon", "array", "ensemble"],
+    ap.add_argument("--config", default="canyon", choices=["canyon", "array", "ensemble", "transfer"],
                     help="canyon: the urban-canyon step (default); array: 4x4 cube array with two-level APR; "
-                         "ensemble: 64 seeded cavity / Taylor-Green cases of 20k-200k particles stepped together")
+                         "ensemble: 64 seeded cavity / Taylor-Green cases of 20k-200k particles stepped together; "
+                         "transfer: the learned start trained on the canyon's solves, applied to the cube array")
+    ap.add_argument("--dx", type=float, default=0.0075, help="transfer config: particle spacing of the cube array")
+    ap.add_argument("--train-solves", type=int, default=40, help="transfer config: canyon solves sampled for training")
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--apr", action="store_true",
                     help="array config: two-level APR near the faces before timing (default: uniform resolution)")
@@ -260,6 +360,8 @@ def main():
         return run_reference(args, rank, world)
     if args.config == "ensemble":
         return run_ensemble(args, rank, world, local)
+    if args.config == "transfer":
+        return run_transfer(args, rank, world, local)
     if args.warmup < 3:
         args.warmup = 3
 

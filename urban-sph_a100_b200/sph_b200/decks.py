@@ -269,7 +269,8 @@ def cube_array(scale=1.0, dx=0.01, seed=SEED, ustar=0.3, z0=0.01, cs=0.12, dt=2e
     (P, params, boxes) with boxes an (ncube, 6) array for sph_set_ib_boxes."""
     rng = np.random.default_rng(seed)
     f = np.float32
-    nx, ny, nz = (int(round(480 * scale)), int(round(240 * scale)), int(round(80 * scale)))
+    # the 4.8 x 2.4 x 0.8 m channel (times scale) at spacing dx
+    nx, ny, nz = (int(round(4.8 * scale / dx)), int(round(2.4 * scale / dx)), int(round(0.8 * scale / dx)))
     nx, ny, nz = max(nx, 40), max(ny, 24), max(nz, 16)
     xs = (np.arange(nx) + 0.5) * dx
     ys = (np.arange(ny) + 0.5) * dx - 0.5 * ny * dx
