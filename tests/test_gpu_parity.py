@@ -48,6 +48,12 @@ def _decks():
     out = [("caseh_mini", decks.caseh_mini())]
     out.append(("caseh_ddf_monaghan", decks.caseh_mini(turbulence="DDF", viscous=layout.MONAGHAN, seed=7)))
     out.append(("canyon_small", decks.canyon(scale=0.12)))
+    # the other kernel functions of functions_KNL.cuh and Euler time stepping
+    for k in ("Gaussian", "Quintic", "Quartic", "Wendland2", "Wendland4"):
+        out.append(("caseh_" + k.lower(), decks.caseh_mini(nx=12, ny=6, nz=5, kernel=k)))
+    P, p = decks.caseh_mini(nx=12, ny=6, nz=5)
+    p.seti("time_type", layout.EULER)
+    out.append(("caseh_euler", (P, p)))
     return out
 
 

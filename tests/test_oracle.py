@@ -32,6 +32,9 @@ VARIANTS = {
     "ddf_monaghan": dict(turbulence="DDF", viscous=layout.MONAGHAN),
     "wendland2": dict(kernel="Wendland2"),
     "quartic_laminar": dict(kernel="Quartic", turbulence="Laminar"),
+    "gaussian": dict(kernel="Gaussian"),
+    "quintic": dict(kernel="Quintic"),
+    "wendland4": dict(kernel="Wendland4"),
     "no_slip_off": dict(noslip=0),
 }
 
