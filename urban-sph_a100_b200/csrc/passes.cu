@@ -142,6 +142,8 @@ __global__ void __launch_bounds__(128) k_grad_corr(DevParams P, SoA<Real> s, LIS
 // ---------------------------------------------------------------------------
 // KERNEL_clc_prep3D, functions_PREP.cuh:287-488 (Shepard filter, strain rate,
 // SSM / DDF sub-grid viscosity, reference density)
+// Algorithmic flops per pair with a fluid neighbour (Wendland-6, filter and
+// LES on; +, -, *, / and sqrt counted 1 each from the loop below): ~110.
 // ---------------------------------------------------------------------------
 template <class Real>
 __global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ g6,
@@ -385,7 +387,9 @@ __global__ void k_neumann_scatter(const int *rows, int nrows, const Real *in_p, 
 
 // ---------------------------------------------------------------------------
 // KERNEL_advection_force3D, functions_PPE.cuh:191-480: viscous (Cleary or
-// Monaghan), Eulerian convective term, artificial viscosity, gravity; with
+// Monaghan), Eulerian convective term, artificial viscosity, gravity (~113
+// flops per pair for Cleary with the Eulerian term, the artificial
+// viscosity on about half the pairs, counted as for k_prep); with
 // TH the scalar terms of the same pass: conduction and the Eulerian
 // temperature term (con_solve -> dtemp), concentration advection-diffusion
 // (concn_solve -> dconcn) and Boussinesq buoyancy (replaces the z force).
@@ -737,7 +741,8 @@ __global__ void k_copy_rows(const int *rows, int nrows, const typename V4<Real>:
 }
 
 // ---------------------------------------------------------------------------
-// KERNEL_pressureforce3D, functions_PPE.cuh:482-647 (h_ij = (h_i+h_j)/2)
+// KERNEL_pressureforce3D, functions_PPE.cuh:482-647 (h_ij = (h_i+h_j)/2);
+// ~50 flops per pair (counted as for k_prep)
 // ---------------------------------------------------------------------------
 template <class Real>
 __global__ void __launch_bounds__(128) k_pressure_force(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ p,

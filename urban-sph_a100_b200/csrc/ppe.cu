@@ -152,7 +152,8 @@ __global__ void __launch_bounds__(128) k_ppe_rows(DevParams P, const float4 *__r
     diag[i] = Aij;
 }
 
-// the right-hand side of later steps from the cached pair vectors
+// the right-hand side of later steps from the cached pair vectors (9 flops
+// and 16 bytes of stored entry per pair: bandwidth bound)
 // g_ij = m_j/rho_j * 2 rho_i rho_j / (rho_i + rho_j) * G_i grad W_ij (the
 // particles, masses and densities do not change between steps)
 template <class Real>
