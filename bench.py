@@ -329,8 +329,8 @@ def main():
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--apr", action="store_true",
                     help="array config: two-level APR near the faces before timing (default: uniform resolution)")
-    ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "gmres", "ref_sweep"])
-    ap.add_argument("--fp64-mode", default="bicgstab", choices=["gmres", "bicgstab"])
+    ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "gmres", "idrs", "ref_sweep"])
+    ap.add_argument("--fp64-mode", default="bicgstab", choices=["gmres", "bicgstab", "idrs"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--matrix-free", action="store_true")
@@ -350,7 +350,8 @@ def main():
                     help="PPE start vector: previous pressure, previous pressure times its residual-minimising factor, linear "
                          "extrapolation in time, or the learned "
                          "per-particle network (trained on this run's warm-up solves)")
-    ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres"],
+    ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres",
+                                                                  "restart-idrs"],
                     help="mixed_ir form: FP64 reliable updates, or refinement restarting the FP32 solver")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -383,12 +384,12 @@ def main():
     if args.coarse is None:
         args.coarse = 9 if args.config == "array" else 5
     mode = {"mixed_ir": layout.PPE_MIXED_IR, "bicgstab": layout.PPE_BICGSTAB, "gmres": layout.PPE_GMRES,
-            "ref_sweep": layout.PPE_REF_SWEEP}[args.mode]
+            "idrs": layout.PPE_IDRS, "ref_sweep": layout.PPE_REF_SWEEP}[args.mode]
     p.ppe_mode = mode
     p.ppe_tol = 1e-6
     if args.matrix_free:
         p.ppe_matrix_free = 1
-    p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2}[args.refinement]
+    p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2, "restart-idrs": 3}[args.refinement]
     p.ppe_coarse_block = args.coarse
     p.ppe_coarse_mode = 1 if args.coarse_mode == "multiplicative" else 0
     if args.pair_h is None:

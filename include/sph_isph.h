@@ -59,6 +59,10 @@ extern "C" {
 #define SPH_PPE_LEARNED    3  /* MIXED_IR warm-started by the per-particle net   */
 #define SPH_PPE_GMRES      4  /* restarted GMRES(m) in the context's precision,
                                  FP64 reductions                              */
+#define SPH_PPE_IDRS       5  /* IDR(4) (biorthogonal variant, right
+                                 preconditioned) in the context's precision,
+                                 FP64 reductions; iterations count operator
+                                 applications (a BiCGSTAB iteration is two)  */
 
 /* ---- particle records: class_Cuda_Particle_Array.cuh:11-112, Real=float --- */
 typedef struct sph_part1 {
@@ -160,9 +164,9 @@ typedef struct sph_params {
     int32_t ppe_matrix_free; /* 1: PPE operator recomputes c_ij at every
                                 application instead of reading the cache      */
     int32_t ppe_gmres_restart;   /* GMRES restart length (0: 40, max 64)       */
-    int32_t ppe_refinement;  /* MIXED_IR: 0 reliable updates (default); 1 / 2
+    int32_t ppe_refinement;  /* MIXED_IR: 0 reliable updates (default); 1 / 2 / 3
                                 iterative refinement restarting FP32 GMRES /
-                                BiCGSTAB at every correction                   */
+                                BiCGSTAB / IDR(4) at every correction          */
     int32_t ppe_coarse_block;    /* BiCGSTAB preconditioner: 0 Jacobi; B > 0
                                 adds a coarse correction on aggregates of
                                 B x B x B NNPS cells (additive two-level)      */

@@ -191,3 +191,29 @@ def test_pair_averaged_h_matches_oracle():
     assert s2[-1].status == 0 and rel_err(M["pres"], A["pres"]) <= 1e-6
     R, s3 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8)
     assert s3[-1].status == 0 and rel_err(R["pres"], A["pres"]) > 1e-4
+
+
+def test_fp64_idrs_matches_oracle(deck):
+    """IDR(4) in the FP64 form (with the two-level preconditioner) converges
+    to the oracle's FP64 BiCGSTAB pressure."""
+    P, p = deck
+    A, stats = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_IDRS, 1e-8, coarse=2)
+    assert stats[-1].status == 0 and stats[-1].rel_residual <= 1e-8, (stats[-1].rel_residual, stats[-1].iterations)
+    O = restated.Restated(P, p, 1)
+    st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-10, maxit=5000)
+    assert st == 0
+    B, _, _ = O.download()
+    assert rel_err(A["pres"], B["pres"]) <= PRES_TOL_FP64
+
+
+def test_mixed_refinement_with_idrs_matches_fp64(deck):
+    """Refinement restarting FP32 IDR(4) (ppe_refinement = 3) reaches the
+    tolerance and the velocity of the FP64 form."""
+    P, p = deck
+    q = p.copy()
+    q.ppe_refinement = 3
+    A, s1 = _gpu_step(P, q, layout.PREC_MIXED, layout.PPE_MIXED_IR, 1e-6, coarse=2)
+    B, s2 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-9, coarse=2)
+    assert s1[-1].status == 0 and s1[-1].rel_residual <= 1e-6
+    for f in ("ux", "uy", "uz"):
+        assert rel_err(A[f], B[f]) <= MIXED_TOL, f

@@ -155,6 +155,8 @@ struct Ctx {
     double *gm_h = nullptr;       // GMRES Hessenberg column / coefficients (device)
     void *gm_ws_r = nullptr;      // GMRES workspace in the context precision
     void *gm_ws_d = nullptr;      // GMRES workspace with FP64 vectors (FP32 context)
+    void *idr_ws_r = nullptr;     // IDR(s) workspace in the context precision
+    void *idr_ws_f = nullptr;     // IDR(s) workspace with FP32 vectors (inner solves of the refinement)
     double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
     float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
     sph_ppe_stats last_ppe = {};

@@ -930,6 +930,321 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
 }
 
 // ---------------------------------------------------------------------------
+// IDR(s), the biorthogonal variant of van Gijzen & Sonneveld ("Algorithm
+// 913: an elegant IDR(s) variant that efficiently exploits
+// bi-orthogonality properties", ACM TOMS 38, 2011), right preconditioned
+// with the Jacobi / two-level preconditioner, s = 4.  One operator
+// application per step and s + 1 per cycle; the shadow space P is s
+// orthonormalised seeded random vectors.  The small s x s lower-triangular
+// system, the step scalars and the convergence flag live on the device
+// (IdrWs::sc); the host reads the residual once per cycle.
+// ---------------------------------------------------------------------------
+#define IDR_S 4
+enum { IS_M = 0, IS_F = IDR_S * IDR_S, IS_C = IS_F + IDR_S, IS_OM = IS_C + IDR_S, IS_RR, IS_FLAG, IS_TOL2, IS_COUNT };
+
+template <class V>
+struct IdrWs {
+    V *P = nullptr, *G = nullptr, *U = nullptr;   // s columns of n each
+    V *r = nullptr, *v = nullptr, *z = nullptr, *t = nullptr, *tmp = nullptr, *dinv = nullptr;
+    double *sc = nullptr;
+};
+
+// c[k..s) from M[k..s, k..s) c = f[k..s) (lower triangular)
+__global__ void k_idr_c(double *sc, int k) {
+    if (threadIdx.x || blockIdx.x || sc[IS_FLAG] != 0) return;
+    const double *M = sc + IS_M, *f = sc + IS_F;
+    double *cc = sc + IS_C;
+    for (int i = k; i < IDR_S; ++i) {
+        double t = f[i];
+        for (int j = k; j < i; ++j) t -= M[i * IDR_S + j] * cc[j];
+        cc[i] = t / M[i * IDR_S + i];
+    }
+}
+
+// v = r - sum_{j >= k} c_j G_j ; z = dinv v
+template <class V>
+__global__ void k_idr_v(const V *r, const V *G, const V *dinv, const double *sc, int k, V *v, V *z, int n) {
+    if (sc[IS_FLAG] != 0) return;
+    V cc[IDR_S];
+#pragma unroll
+    for (int j = 0; j < IDR_S; ++j) cc[j] = (V)sc[IS_C + j];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        V a = r[i];
+#pragma unroll
+        for (int j = 0; j < IDR_S; ++j)
+            if (j >= k) a -= cc[j] * G[(size_t)j * n + i];
+        v[i] = a;
+        z[i] = dinv[i] * a;
+    }
+}
+
+// U_k = sum_{j >= k} c_j U_j + om z
+template <class V>
+__global__ void k_idr_u(V *U, const V *z, const double *sc, int k, int n) {
+    if (sc[IS_FLAG] != 0) return;
+    V cc[IDR_S];
+#pragma unroll
+    for (int j = 0; j < IDR_S; ++j) cc[j] = (V)sc[IS_C + j];
+    const V om = (V)sc[IS_OM];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        V a = om * z[i];
+#pragma unroll
+        for (int j = 0; j < IDR_S; ++j)
+            if (j >= k) a += cc[j] * U[(size_t)j * n + i];
+        U[(size_t)k * n + i] = a;
+    }
+}
+
+// alpha = (P_i, G_k) / M_ii, then G_k -= alpha G_i, U_k -= alpha U_i (two kernels)
+template <class V>
+__global__ void k_idr_alpha(const V *Pi, const V *Gk, int i, int n, double *partials, unsigned int *counter,
+                            double *sc, double *out) {
+    if (sc[IS_FLAG] != 0) return;
+    double d[1] = {0};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) d[0] += (double)Pi[q] * (double)Gk[q];
+    reduce_finish<1>(d, partials, counter, [&](double *t) { *out = t[0] / sc[IS_M + i * IDR_S + i]; });
+}
+
+template <class V>
+__global__ void k_idr_axpy2(V *Gk, const V *Gi, V *Uk, const V *Ui, const double *sc, const double *alpha, int n) {
+    if (sc[IS_FLAG] != 0) return;
+    const V a = (V)*alpha;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        Gk[q] -= a * Gi[q];
+        Uk[q] -= a * Ui[q];
+    }
+}
+
+// M[j][k] = (P_j, G_k) for j >= k
+template <class V>
+__global__ void k_idr_mcol(const V *P, const V *Gk, int k, int n, double *partials, unsigned int *counter, double *sc) {
+    if (sc[IS_FLAG] != 0) return;
+    double d[IDR_S];
+#pragma unroll
+    for (int j = 0; j < IDR_S; ++j) d[j] = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const double g = (double)Gk[q];
+#pragma unroll
+        for (int j = 0; j < IDR_S; ++j)
+            if (j >= k) d[j] += (double)P[(size_t)j * n + q] * g;
+    }
+    reduce_finish<IDR_S>(d, partials, counter, [&](double *t) {
+        for (int j = k; j < IDR_S; ++j) sc[IS_M + j * IDR_S + k] = t[j];
+    });
+}
+
+// beta = f_k / M_kk ; r -= beta G_k ; x += beta U_k ; then f_j -= beta M_jk (j > k),
+// rr = (r, r) and the convergence / breakdown flag
+template <class V>
+__global__ void k_idr_step(V *r, V *x, const V *Gk, const V *Uk, int k, int n, double *partials, unsigned int *counter,
+                           double *sc) {
+    if (sc[IS_FLAG] != 0) return;
+    const double mkk = sc[IS_M + k * IDR_S + k];
+    const double beta = mkk != 0 ? sc[IS_F + k] / mkk : 0.0;
+    const V bv = (V)beta;
+    double d[1] = {0};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const V rq = r[q] - bv * Gk[q];
+        r[q] = rq;
+        x[q] += bv * Uk[q];
+        d[0] += (double)rq * (double)rq;
+    }
+    reduce_finish<1>(d, partials, counter, [&](double *t) {
+        for (int j = k + 1; j < IDR_S; ++j) sc[IS_F + j] -= beta * sc[IS_M + j * IDR_S + k];
+        sc[IS_RR] = t[0];
+        if (mkk == 0.0 || !isfinite(t[0])) sc[IS_FLAG] = 2;
+        else if (t[0] <= sc[IS_TOL2]) sc[IS_FLAG] = 1;
+    });
+}
+
+// om = (t, r) / (t, t), enlarged to keep |cos(t, r)| >= 0.7
+template <class V>
+__global__ void k_idr_om(const V *t, const V *r, int n, double *partials, unsigned int *counter, double *sc) {
+    if (sc[IS_FLAG] != 0) return;
+    double d[2] = {0, 0};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        d[0] += (double)t[q] * (double)r[q];
+        d[1] += (double)t[q] * (double)t[q];
+    }
+    reduce_finish<2>(d, partials, counter, [&](double *tt) {
+        if (!(tt[1] > 0)) { sc[IS_FLAG] = 2; return; }
+        double om = tt[0] / tt[1];
+        const double rho = fabs(tt[0]) / (sqrt(tt[1]) * sqrt(sc[IS_RR]));
+        if (rho < 0.7 && rho > 0) om *= 0.7 / rho;
+        sc[IS_OM] = om;
+    });
+}
+
+// x += om z ; r -= om t ; rr ; flag
+template <class V>
+__global__ void k_idr_xr(V *x, V *r, const V *z, const V *t, int n, double *partials, unsigned int *counter, double *sc) {
+    if (sc[IS_FLAG] != 0) return;
+    const V om = (V)sc[IS_OM];
+    double d[1] = {0};
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        x[q] += om * z[q];
+        const V rq = r[q] - om * t[q];
+        r[q] = rq;
+        d[0] += (double)rq * (double)rq;
+    }
+    reduce_finish<1>(d, partials, counter, [&](double *tt) {
+        sc[IS_RR] = tt[0];
+        if (!isfinite(tt[0])) sc[IS_FLAG] = 2;
+        else if (tt[0] <= sc[IS_TOL2]) sc[IS_FLAG] = 1;
+    });
+}
+
+// f = P^T r
+template <class V>
+__global__ void k_idr_f(const V *P, const V *r, int n, double *partials, unsigned int *counter, double *sc) {
+    if (sc[IS_FLAG] != 0) return;
+    double d[IDR_S];
+#pragma unroll
+    for (int j = 0; j < IDR_S; ++j) d[j] = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const double rq = (double)r[q];
+#pragma unroll
+        for (int j = 0; j < IDR_S; ++j) d[j] += (double)P[(size_t)j * n + q] * rq;
+    }
+    reduce_finish<IDR_S>(d, partials, counter, [&](double *t) {
+        for (int j = 0; j < IDR_S; ++j) sc[IS_F + j] = t[j];
+    });
+}
+
+// z = d * r
+template <class V>
+__global__ void k_mul(const V *d, const V *r, V *z, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = d[i] * r[i];
+}
+
+// r = b - y
+template <class V>
+__global__ void k_idr_res(const V *b, const V *y, V *r, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r[i] = b[i] - y[i];
+}
+
+// sc: M = I, om = 1, flag 0, tol2
+__global__ void k_idr_init(double *sc, double tol2) {
+    if (threadIdx.x || blockIdx.x) return;
+    for (int q = 0; q < IS_COUNT; ++q) sc[q] = 0;
+    for (int j = 0; j < IDR_S; ++j) sc[IS_M + j * IDR_S + j] = 1;
+    sc[IS_OM] = 1;
+    sc[IS_TOL2] = tol2;
+}
+
+template <class Real, class V>
+static int idr_ws(Ctx<Real> &c, IdrWs<V> &w) {
+    const size_t n = (size_t)c.n;
+    SPH_TRY(c.alloc(w.P, IDR_S * n)); SPH_TRY(c.alloc(w.G, IDR_S * n)); SPH_TRY(c.alloc(w.U, IDR_S * n));
+    SPH_TRY(c.alloc(w.r, n)); SPH_TRY(c.alloc(w.v, n)); SPH_TRY(c.alloc(w.z, n)); SPH_TRY(c.alloc(w.t, n));
+    SPH_TRY(c.alloc(w.tmp, n)); SPH_TRY(c.alloc(w.dinv, n)); SPH_TRY(c.alloc(w.sc, 64));
+    // shadow space: s seeded random vectors, orthonormalised (modified
+    // Gram-Schmidt in FP64 on the host)
+    std::vector<double> Ph(IDR_S * n);
+    unsigned long long st = 0x9E3779B97F4A7C15ULL;
+    for (size_t q = 0; q < Ph.size(); ++q) {
+        st ^= st << 13; st ^= st >> 7; st ^= st << 17;   // xorshift64
+        Ph[q] = ((double)(st >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+    }
+    for (int j = 0; j < IDR_S; ++j) {
+        double *pj = Ph.data() + (size_t)j * n;
+        for (int i = 0; i < j; ++i) {
+            const double *pi = Ph.data() + (size_t)i * n;
+            double d = 0;
+            for (size_t q = 0; q < n; ++q) d += pi[q] * pj[q];
+            for (size_t q = 0; q < n; ++q) pj[q] -= d * pi[q];
+        }
+        double nn = 0;
+        for (size_t q = 0; q < n; ++q) nn += pj[q] * pj[q];
+        nn = 1.0 / std::sqrt(nn);
+        for (size_t q = 0; q < n; ++q) pj[q] *= nn;
+    }
+    std::vector<V> Pv(Ph.begin(), Ph.end());
+    SPH_CUDA_TRY(cudaMemcpyAsync(w.P, Pv.data(), sizeof(V) * Pv.size(), cudaMemcpyHostToDevice, c.stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return SPH_OK;
+}
+
+// IDR(s) on M x = b; x holds the initial guess.  iters counts operator
+// applications.  Returns SPH_OK, SPH_NOT_CONVERGED or SPH_ERR_BREAKDOWN.
+template <class Real, class V>
+static int idrs(Ctx<Real> &c, IdrWs<V> &w, V *x, const V *b, double bnorm2, double tol, int maxit, bool cached,
+                int *iters, double *relres) {
+    const int n = c.n;
+    cudaStream_t st = c.stream;
+    const int G = red_grid(n);
+    unsigned int *counter = (unsigned int *)(c.scal + 32);
+    const double tol2 = tol * tol * bnorm2;
+    double *alpha = w.sc + IS_COUNT;
+    k_dinv<V, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, w.dinv, n);
+    ++c.launches;
+    int mv = 0, restarts = 0, status = SPH_NOT_CONVERGED;
+    *relres = 1;
+    while (true) {
+        // (re)start: r = b - M x, M = I, G = U = 0, om = 1, f = P^T r
+        apply_op<Real, V>(c, x, w.t, cached);
+        k_idr_res<V><<<G, 256, 0, st>>>(b, w.t, w.r, n);
+        k_idr_init<<<1, 1, 0, st>>>(w.sc, tol2);
+        k_norm2<V><<<G, 256, 0, st>>>(w.r, n, c.red, counter, w.sc, IS_RR);
+        SPH_CUDA_TRY(cudaMemsetAsync(w.G, 0, sizeof(V) * IDR_S * (size_t)n, st));
+        SPH_CUDA_TRY(cudaMemsetAsync(w.U, 0, sizeof(V) * IDR_S * (size_t)n, st));
+        k_idr_f<V><<<G, 256, 0, st>>>(w.P, w.r, n, c.red, counter, w.sc);
+        c.launches += 4;
+        SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, w.sc, sizeof(double) * IS_COUNT, cudaMemcpyDeviceToHost, st));
+        SPH_CUDA_TRY(cudaStreamSynchronize(st));
+        double rr = c.red_host[IS_RR];
+        *relres = std::sqrt(rr / bnorm2);
+        if (c.init_relres < 0) c.init_relres = *relres;
+        if (rr <= tol2) { status = SPH_OK; break; }
+        if (mv >= maxit) break;
+        bool restart = false;
+        while (mv < maxit) {
+            for (int k = 0; k < IDR_S; ++k) {
+                V *Gk = w.G + (size_t)k * n, *Uk = w.U + (size_t)k * n;
+                k_idr_c<<<1, 1, 0, st>>>(w.sc, k);
+                k_idr_v<V><<<G, 256, 0, st>>>(w.r, w.G, w.dinv, w.sc, k, w.v, w.z, n);
+                c.launches += 2;
+                precond_coarse<Real, V>(c, w.v, w.z, w.tmp, cached);
+                k_idr_u<V><<<G, 256, 0, st>>>(w.U, w.z, w.sc, k, n);
+                ++c.launches;
+                apply_op<Real, V>(c, Uk, Gk, cached);
+                for (int i = 0; i < k; ++i) {
+                    k_idr_alpha<V><<<G, 256, 0, st>>>(w.P + (size_t)i * n, Gk, i, n, c.red, counter, w.sc, alpha);
+                    k_idr_axpy2<V><<<G, 256, 0, st>>>(Gk, w.G + (size_t)i * n, Uk, w.U + (size_t)i * n, w.sc, alpha, n);
+                    c.launches += 2;
+                }
+                k_idr_mcol<V><<<G, 256, 0, st>>>(w.P, Gk, k, n, c.red, counter, w.sc);
+                k_idr_step<V><<<G, 256, 0, st>>>(w.r, x, Gk, Uk, k, n, c.red, counter, w.sc);
+                c.launches += 2;
+                ++mv;
+            }
+            // the (s+1)-th step: z = M^-1 r, t = M z, om, x += om z, r -= om t
+            k_mul<V><<<G, 256, 0, st>>>(w.dinv, w.r, w.z, n);
+            ++c.launches;
+            precond_coarse<Real, V>(c, w.r, w.z, w.tmp, cached);
+            apply_op<Real, V>(c, w.z, w.t, cached);
+            k_idr_om<V><<<G, 256, 0, st>>>(w.t, w.r, n, c.red, counter, w.sc);
+            k_idr_xr<V><<<G, 256, 0, st>>>(x, w.r, w.z, w.t, n, c.red, counter, w.sc);
+            k_idr_f<V><<<G, 256, 0, st>>>(w.P, w.r, n, c.red, counter, w.sc);
+            c.launches += 3;
+            ++mv;
+            SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, w.sc, sizeof(double) * IS_COUNT, cudaMemcpyDeviceToHost, st));
+            SPH_CUDA_TRY(cudaStreamSynchronize(st));
+            const double flag = c.red_host[IS_FLAG];
+            rr = c.red_host[IS_RR];
+            *relres = std::sqrt(rr / bnorm2);
+            if (flag == 1) { status = SPH_OK; break; }
+            if (flag == 2) { restart = true; break; }
+        }
+        if (status == SPH_OK || !restart || mv >= maxit) break;
+        if (++restarts > 20) { status = SPH_ERR_BREAKDOWN; break; }
+    }
+    SPH_CUDA_TRY(cudaGetLastError());
+    *iters = mv;
+    return status;
+}
+
+// ---------------------------------------------------------------------------
 // restarted GMRES(m), right Jacobi preconditioning, classical Gram-Schmidt
 // with a conditional second pass, FP64 dot products; the Hessenberg matrix,
 // its Givens rotations and the small triangular solve live on the host
@@ -1289,8 +1604,28 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             }
             return (GmresWs<Real, double> *)c.gm_ws_d;
         };
+        auto idr_r = [&]() -> IdrWs<Real> * {
+            if (!c.idr_ws_r) {
+                auto *w = new IdrWs<Real>();
+                if (idr_ws(c, *w) < 0) { delete w; return nullptr; }
+                c.idr_ws_r = w;
+            }
+            return (IdrWs<Real> *)c.idr_ws_r;
+        };
+        auto idr_f = [&]() -> IdrWs<float> * {
+            if (!c.idr_ws_f) {
+                auto *w = new IdrWs<float>();
+                if (idr_ws(c, *w) < 0) { delete w; return nullptr; }
+                c.idr_ws_f = w;
+            }
+            return (IdrWs<float> *)c.idr_ws_f;
+        };
         const bool trace = getenv("SPH_TRACE_PPE") != nullptr;
-        if (sizeof(Real) == 8) {
+        if (sizeof(Real) == 8 && mode == SPH_PPE_IDRS) {
+            IdrWs<Real> *w = idr_r();
+            if (!w) return SPH_ERR_OUT_OF_MEMORY;
+            status = idrs<Real, Real>(c, *w, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres);
+        } else if (sizeof(Real) == 8) {
             // plain form: the whole solve in FP64
             if (mode != SPH_PPE_GMRES)
                 status = bicgstab<Real>(c, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres, &restarts);
@@ -1299,13 +1634,17 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
                 if (!w) return SPH_ERR_OUT_OF_MEMORY;
                 status = gmres<Real, Real>(c, *w, (Real *)xd, (const Real *)bd, bb, tol, maxit, cached, &iters, &relres);
             }
-        } else if (mode == SPH_PPE_BICGSTAB || mode == SPH_PPE_GMRES) {
+        } else if (mode == SPH_PPE_BICGSTAB || mode == SPH_PPE_GMRES || mode == SPH_PPE_IDRS) {
             // FP32 vectors throughout, FP64 reductions
             k_cast<double, float><<<grid_for(n, 256), 256, 0, st>>>(xd, c.xf, n);
             k_cast<double, float><<<grid_for(n, 256), 256, 0, st>>>(bd, c.bf, n);
             c.launches += 2;
             if (mode == SPH_PPE_BICGSTAB) {
                 status = bicgstab<Real>(c, (Real *)c.xf, (const Real *)c.bf, bb, tol, maxit, cached, &iters, &relres, &restarts);
+            } else if (mode == SPH_PPE_IDRS) {
+                IdrWs<float> *w = idr_f();
+                if (!w) return SPH_ERR_OUT_OF_MEMORY;
+                status = idrs<Real, float>(c, *w, c.xf, c.bf, bb, tol, maxit, cached, &iters, &relres);
             } else {
                 GmresWs<Real, Real> *w = ws_r();
                 if (!w) return SPH_ERR_OUT_OF_MEMORY;
@@ -1335,6 +1674,8 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             const double inner_tol = c.prm.ppe_inner_tol > 0 ? c.prm.ppe_inner_tol : 1e-3;
             GmresWs<Real, Real> *w = c.prm.ppe_refinement == 1 ? ws_r() : nullptr;
             if (c.prm.ppe_refinement == 1 && !w) return SPH_ERR_OUT_OF_MEMORY;
+            IdrWs<float> *wi = c.prm.ppe_refinement == 3 ? idr_f() : nullptr;
+            if (c.prm.ppe_refinement == 3 && !wi) return SPH_ERR_OUT_OF_MEMORY;
             status = SPH_NOT_CONVERGED;
             for (refinements = 0; refinements < 50; ++refinements) {
                 apply_op<Real, double>(c, xd, rd, cached);
@@ -1352,6 +1693,8 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
                 const int st_in = c.prm.ppe_refinement == 1
                                       ? gmres<Real, Real>(c, *w, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters,
                                                           cached, &it_in, &rel_in)
+                                  : c.prm.ppe_refinement == 3
+                                      ? idrs<Real, float>(c, *wi, ef, rf, rr, inner_tol, maxit - iters, cached, &it_in, &rel_in)
                                       : bicgstab<Real>(c, (Real *)ef, (const Real *)rf, rr, inner_tol, maxit - iters, cached,
                                                        &it_in, &rel_in, &rs_in);
                 restarts += rs_in;
@@ -1402,8 +1745,12 @@ template <class Real>
 void release_solver_ws(Ctx<Real> &c) {
     delete (GmresWs<Real, Real> *)c.gm_ws_r;
     delete (GmresWs<Real, double> *)c.gm_ws_d;
+    delete (IdrWs<Real> *)c.idr_ws_r;
+    delete (IdrWs<float> *)c.idr_ws_f;
     c.gm_ws_r = nullptr;
     c.gm_ws_d = nullptr;
+    c.idr_ws_r = nullptr;
+    c.idr_ws_f = nullptr;
 }
 
 #define INST(R) template int phase_ppe<R>(Ctx<R> &, sph_ppe_stats *); \

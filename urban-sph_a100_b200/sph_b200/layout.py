@@ -72,7 +72,7 @@ CLEARY, MONAGHAN = 1, 2
 KGC = 1
 
 PREC_MIXED, PREC_FP64 = 0, 1
-PPE_REF_SWEEP, PPE_BICGSTAB, PPE_MIXED_IR, PPE_LEARNED, PPE_GMRES = 0, 1, 2, 3, 4
+PPE_REF_SWEEP, PPE_BICGSTAB, PPE_MIXED_IR, PPE_LEARNED, PPE_GMRES, PPE_IDRS = 0, 1, 2, 3, 4, 5
 
 MAX_PROFILE = 32
 
