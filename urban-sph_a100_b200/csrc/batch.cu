@@ -7,9 +7,10 @@
 // together.  The number of workers, i.e. how many cases are in flight at
 // once, is chosen by sph_batch_autotune from timed probe steps.
 //
-// A case's step is not captured as one CUDA graph: the Krylov solver tests
-// convergence on the host every few iterations, which a graph cannot
-// express without device-side control flow.
+// A case's step is not one CUDA graph: the Krylov solver tests convergence
+// on the host every few iterations.  The iterations between two tests are
+// one graph (captured once per context and replayed, ppe.cu), since every
+// case runs on its own stream.
 #include <algorithm>
 #include <atomic>
 #include <chrono>

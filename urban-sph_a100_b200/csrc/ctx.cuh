@@ -157,6 +157,8 @@ struct Ctx {
     void *gm_ws_d = nullptr;      // GMRES workspace with FP64 vectors (FP32 context)
     void *idr_ws_r = nullptr;     // IDR(s) workspace in the context precision
     void *idr_ws_f = nullptr;     // IDR(s) workspace with FP32 vectors (inner solves of the refinement)
+    void *kgraph = nullptr;       // CUDA graph of the mixed BiCGSTAB's iterations between host checks
+    bool kgraph_off = false;      // capture failed once: launch the kernels one by one
     double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
     float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
     sph_ppe_stats last_ppe = {};

@@ -798,6 +798,32 @@ static int bicgstab_fp64(Ctx<Real> &c, double *x, const double *b, double bnorm2
 // ---------------------------------------------------------------------------
 #define RELIABLE_DELTA 0.1
 
+// The iterations between two host checks, captured once as a CUDA graph and
+// replayed: one graph launch instead of about 60 kernel launches, which
+// matters for the small cases of an ensemble, whose kernels last a few
+// microseconds.  Only contexts on their own stream use it (the legacy
+// default stream cannot be captured).  The key holds every pointer and size
+// the captured launches use; a change (new lists, a rebuilt preconditioner,
+// reallocated work space) recaptures.
+struct KrylovGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uintptr_t> key;
+    long long nodes = 0;
+};
+
+template <class Real>
+static std::vector<uintptr_t> krylov_graph_key(Ctx<Real> &c, float *const *ws, const float *xlo) {
+    std::vector<uintptr_t> k;
+    for (int q = 0; q < 9; ++q) k.push_back((uintptr_t)ws[q]);
+    const void *ptrs[] = {xlo, c.scal, c.red, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, c.diag,
+                          c.comp_id, c.comp_inv, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.cg_off, c.cg_rows,
+                          c.cg_s, c.cg_y, c.cg_invf, c.cg_agg};
+    for (const void *q : ptrs) k.push_back((uintptr_t)q);
+    const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode};
+    for (long long q : sizes) k.push_back((uintptr_t)q);
+    return k;
+}
+
 // r = (float)(b - y); x_lo = 0; rho = (rh, r), rr = ||b - y||^2 (FP64);
 // beta is rescaled to the replaced rho so the next direction stays conjugate
 template <class V>
@@ -883,7 +909,7 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     if (trace) fprintf(stderr, "RU start relres %.3e\n", *relres);
     if (rr <= tol2) status = SPH_OK;
     const int check = 4;
-    while (status != SPH_OK && it < maxit) {
+    auto iteration = [&]() {
         k_p_update<float><<<G, 256, 0, st>>>(p, ph, r, v, dinv, n, c.scal);
         bool mr = precond_coarse<Real, float>(c, p, ph, v, cached);
         apply_op<Real, float>(c, ph, v, cached, mr);
@@ -894,7 +920,51 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
         k_omega<float><<<G, 256, 0, st>>>(t, s, n, c.red, counter, c.scal);
         k_xr_update<float><<<G, 256, 0, st>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
         c.launches += 5;
-        ++it;
+    };
+    // `check` iterations as one graph launch; false: run them one launch at a time
+    auto graph_chunk = [&]() -> bool {
+        if (c.kgraph_off || st == nullptr || c.prof || !cached) return false;
+        auto *g = (KrylovGraph *)c.kgraph;
+        if (!g) { g = new KrylovGraph(); c.kgraph = g; }
+        std::vector<uintptr_t> key = krylov_graph_key(c, ws, xlo);
+        if (!g->exec || g->key != key) {
+            if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
+            const long long l0 = c.launches;
+            cudaGraph_t graph = nullptr;
+            if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                cudaGetLastError();
+                c.kgraph_off = true;
+                return false;
+            }
+            for (int q = 0; q < check; ++q) iteration();
+            const cudaError_t e1 = cudaStreamEndCapture(st, &graph);
+            const cudaError_t e2 = e1 == cudaSuccess ? cudaGraphInstantiate(&g->exec, graph, 0) : e1;
+            if (graph) cudaGraphDestroy(graph);
+            g->nodes = c.launches - l0;
+            c.launches = l0;
+            if (e2 != cudaSuccess) {
+                cudaGetLastError();
+                g->exec = nullptr;
+                c.kgraph_off = true;
+                return false;
+            }
+            g->key = key;
+        }
+        if (cudaGraphLaunch(g->exec, st) != cudaSuccess) {
+            cudaGetLastError();
+            c.kgraph_off = true;
+            return false;
+        }
+        c.launches += g->nodes;
+        return true;
+    };
+    while (status != SPH_OK && it < maxit) {
+        if (it % check == 0 && it + check <= maxit && graph_chunk()) {
+            it += check;
+        } else {
+            iteration();
+            ++it;
+        }
         if (it % check != 0 && it < maxit) continue;
         SPH_TRY(read_scal());
         const double flag = c.red_host[SC_FLAG];
@@ -1747,6 +1817,12 @@ void release_solver_ws(Ctx<Real> &c) {
     delete (GmresWs<Real, double> *)c.gm_ws_d;
     delete (IdrWs<Real> *)c.idr_ws_r;
     delete (IdrWs<float> *)c.idr_ws_f;
+    if (c.kgraph) {
+        auto *g = (KrylovGraph *)c.kgraph;
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        delete g;
+        c.kgraph = nullptr;
+    }
     c.gm_ws_r = nullptr;
     c.gm_ws_d = nullptr;
     c.idr_ws_r = nullptr;
