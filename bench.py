@@ -34,6 +34,8 @@ METRIC = "particle-steps/s"
 WORKLOAD = "urban canyon 2.4x1.2x0.6 m, dx=0.01 m: 240x120x60 fluid + floor walls + free-slip ceiling + IBM cube, neutral MOST, SSM Cs=0.12"
 WORKLOAD_ARRAY = ("staggered 4x4 array of 0.1 m IBM cubes at 0.3 m pitch in a 4.8x2.4x0.8 m channel, dx=0.01 m, "
                   "uniform resolution (--apr: two-level APR within 0.1 m of the faces), neutral MOST, SSM Cs=0.12")
+WORKLOAD_TGV = ("triply periodic Taylor-Green vortex: {n}^3 particles, dx=1/{n} m in a 1 m cube with 3 layers of "
+                "periodic ghosts, h=1.3dx, Wendland C6, rho=1000, nu=1e-3, U0=1 m/s, CFL 0.1")
 
 
 def peaks():
@@ -320,13 +322,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--config", default="canyon", choices=["canyon", "array", "ensemble", "transfer"],
+    ap.add_argument("--config", default="canyon", choices=["canyon", "array", "ensemble", "transfer", "tgv"],
                     help="canyon: the urban-canyon step (default); array: 4x4 cube array with two-level APR; "
                          "ensemble: 64 seeded cavity / Taylor-Green cases of 20k-200k particles stepped together; "
                          "transfer: the learned start trained on the canyon's solves, applied to the cube array")
     ap.add_argument("--dx", type=float, default=0.0075, help="transfer config: particle spacing of the cube array")
     ap.add_argument("--train-solves", type=int, default=40, help="transfer config: canyon solves sampled for training")
     ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--tol", type=float, default=None, help="PPE tolerance (default 1e-6; tgv config 1e-8)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="precision of the timed form (mixed: FP32 fields and Krylov vectors, FP64 refinement)")
     ap.add_argument("--apr", action="store_true",
                     help="array config: two-level APR near the faces before timing (default: uniform resolution)")
     ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "gmres", "idrs", "ref_sweep"])
@@ -379,14 +384,18 @@ def main():
     boxes = None
     if args.config == "array":
         P, p, boxes = decks.cube_array(scale=args.scale, apr=args.apr)
+    elif args.config == "tgv":
+        P, p = decks.tgv_periodic(n=int(round(64 * args.scale)))
     else:
         P, p = decks.canyon(scale=args.scale)
     if args.coarse is None:
-        args.coarse = 9 if args.config == "array" else 5
+        args.coarse = {"array": 9, "tgv": 4}.get(args.config, 5)
+    if args.tol is None:
+        args.tol = 1e-8 if args.config == "tgv" else 1e-6
     mode = {"mixed_ir": layout.PPE_MIXED_IR, "bicgstab": layout.PPE_BICGSTAB, "gmres": layout.PPE_GMRES,
             "idrs": layout.PPE_IDRS, "ref_sweep": layout.PPE_REF_SWEEP}[args.mode]
     p.ppe_mode = mode
-    p.ppe_tol = 1e-6
+    p.ppe_tol = args.tol
     if args.matrix_free:
         p.ppe_matrix_free = 1
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2, "restart-idrs": 3}[args.refinement]
@@ -399,8 +408,10 @@ def main():
     if args.inner_tol > 0:
         p.ppe_inner_tol = args.inner_tol
     p.ppe_warm_start = {"extrap": 1, "scaled": 3}.get(args.warm, 0)
-    n = len(P)
-    sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
+    # particle-steps count particles, not the periodic ghost records
+    n = int((P["buffer_type"] != layout.BUFFER_PERIODIC_GHOST).sum())
+    prec = layout.PREC_FP64 if args.precision == "fp64" else layout.PREC_MIXED
+    sim = abi.Simulation(p, precision=prec, device=local)
     if boxes is not None:
         sim.set_ib_boxes(boxes)
     sim.upload(P)
@@ -543,7 +554,7 @@ def main():
         A = sd.download(want=(1,))[0]
         sd.close()
         B = ref_state
-        fl = (B["i_type"] < 3) & (B["p_type"] == 1)
+        fl = (B["i_type"] < 3) & (B["p_type"] == 1) & (B["buffer_type"] != layout.BUFFER_PERIODIC_GHOST)
         ua = np.stack([A[f][fl] for f in ("ux", "uy", "uz")]).astype(np.float64)
         ub = np.stack([B[f][fl] for f in ("ux", "uy", "uz")]).astype(np.float64)
         pa, pb = A["pres"][fl].astype(np.float64), B["pres"][fl].astype(np.float64)
@@ -560,12 +571,12 @@ def main():
         if not args.no_fp64:
             # the plain form: FP64 throughout, Jacobi-preconditioned Krylov
             fp64 = timed_form(layout.PREC_FP64, fp64_mode, 0, kd, keep=True)
-            fp64.update({"solver": args.fp64_mode + " + jacobi", "ppe_tol": 1e-6})
+            fp64.update({"solver": args.fp64_mode + " + jacobi", "ppe_tol": args.tol})
             err64 = error_vs(fp64.pop("_state"), kd + 2)
             if args.coarse > 0:
                 # FP64 with this run's preconditioner: isolates the precision change
                 fp64_same = timed_form(layout.PREC_FP64, layout.PPE_BICGSTAB, args.coarse, kd)
-                fp64_same.update({"solver": f"bicgstab + coarse {args.coarse}", "ppe_tol": 1e-6})
+                fp64_same.update({"solver": f"bicgstab + coarse {args.coarse}", "ppe_tol": args.tol})
         # the reference's own step semantics (one PPE sweep) on the same deck
         sweep = timed_form(layout.PREC_MIXED, layout.PPE_REF_SWEEP, 0, kd)
         for k in ("ppe_iterations", "rel_residual_max"):
@@ -587,10 +598,13 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD if args.config == "canyon" else WORKLOAD_ARRAY,
-                   "particles": n, "apr": apr, "scale": args.scale, "precision": "mixed FP32/FP64",
-                   "ppe": args.mode, "ppe_tol": 1e-6,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": {"canyon": WORKLOAD, "array": WORKLOAD_ARRAY}.get(
+                       args.config, WORKLOAD_TGV.format(n=int(round(64 * args.scale)))),
+                   "particles": n, "apr": apr, "scale": args.scale,
+                   "precision": "mixed FP32/FP64" if args.precision == "mixed" else "FP64",
+                   "ppe": args.mode, "ppe_tol": args.tol,
                    "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
                    "ppe_refinement": args.refinement,
                    "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],

@@ -207,7 +207,17 @@ typedef struct sph_params {
     double  recycle_probe_x, recycle_probe_y;   /* the MOST particle whose u*
                                 feeds inlet recycling: (x - px)^2 + (y - py)^2
                                 < 1e-3 (functions_MOST.cuh:316: 600, 0)        */
+    double  periodic_box[6]; /* x0,x1,y0,y1,z0,z1 of a periodic box (new work:
+                                the reference's only periodicity is the y copy
+                                of functions_BC.cuh:1015-1154).  A record with
+                                buffer_type SPH_BUFFER_PERIODIC_GHOST copies u,
+                                p and T from the record at its position
+                                wrapped into the box (|d| < partner_tol), after
+                                the periodic-y copy at each of its call sites;
+                                in the pressure system it is a copy row.      */
 } sph_params;
+
+#define SPH_BUFFER_PERIODIC_GHOST 7
 
 typedef struct sph_ppe_stats {
     int32_t status;          /* SPH_OK / SPH_NOT_CONVERGED / error             */

@@ -831,6 +831,36 @@ struct Oracle {
                     }
             A.ux[i] = tux; A.uy[i] = tuy; A.uz[i] = tuz; A.pres[i] = tp; A.temp[i] = tt;
         }
+        // ghosts of the periodic box (new work, no reference counterpart):
+        // u, p and T of the record at the wrapped position, after the y copy
+        const State<Real> O2 = A;
+        for (int i = 0; i < n(); ++i) {
+            if (O2.buffer_type[i] != SPH_BUFFER_PERIODIC_GHOST) continue;
+            const int j = ghost_partner(O2, i);
+            A.ux[i] = j >= 0 ? O2.ux[j] : 0; A.uy[i] = j >= 0 ? O2.uy[j] : 0; A.uz[i] = j >= 0 ? O2.uz[j] : 0;
+            A.pres[i] = j >= 0 ? O2.pres[j] : 0; A.temp[i] = j >= 0 ? O2.temp[j] : 0;
+        }
+    }
+
+    // partner of a periodic-box ghost: the record (not a ghost) within
+    // partner_tol of the ghost's position wrapped into the box, x - L
+    // floor((x - x0) / L) per axis with x1 > x0, in double; the last match
+    // in cell order
+    int ghost_partner(const State<Real> &A, int i) const {
+        const float v[3] = {xf[i], yf[i], zf[i]};
+        double w[3];
+        for (int a = 0; a < 3; ++a) {
+            const double lo = prm.periodic_box[2 * a], len = prm.periodic_box[2 * a + 1] - lo;
+            w[a] = (len > 0) ? (double)v[a] - len * std::floor(((double)v[a] - lo) / len) : (double)v[a];
+        }
+        int ic, jc, kc, found = -1;
+        search_cell((float)w[0], (float)w[1], (float)w[2], ic, jc, kc);
+        cell_loop(ic, jc, kc, 1, [&](int j) {
+            if (A.buffer_type[j] == SPH_BUFFER_PERIODIC_GHOST) return;
+            const double dx = w[0] - (double)xf[j], dy = w[1] - (double)yf[j], dz = w[2] - (double)zf[j];
+            if (std::sqrt(dx * dx + dy * dy + dz * dz) < prm.partner_tol) found = j;
+        });
+        return found;
     }
 
     // KERNEL_freeslip_boundary3D, functions_BC.cuh:1156-1271
@@ -1077,7 +1107,7 @@ struct Oracle {
     // reference's overwrites): 0 identity, 1 fluid, 2 Neumann, 3 outlet copy.
     int row_class(const State<Real> &A, int i) const {
         if (A.i_type[i] >= 3) return 0;
-        if (A.buffer_type[i] == 2) return 3;
+        if (A.buffer_type[i] == 2 || A.buffer_type[i] == SPH_BUFFER_PERIODIC_GHOST) return 3;
         if (A.p_type[i] != 1) return 2;
         return 1;
     }
@@ -1105,7 +1135,7 @@ struct Oracle {
                 continue;
             }
             if (rc == 3) {
-                int partner = outlet_partner(A, i);
+                int partner = A.buffer_type[i] == SPH_BUFFER_PERIODIC_GHOST ? ghost_partner(A, i) : outlet_partner(A, i);
                 ci.push_back(i); va.push_back(1.0);
                 if (partner >= 0) { ci.push_back(partner); va.push_back(-1.0); }
                 continue;

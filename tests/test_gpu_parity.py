@@ -54,6 +54,8 @@ def _decks():
     P, p = decks.caseh_mini(nx=12, ny=6, nz=5)
     p.seti("time_type", layout.EULER)
     out.append(("caseh_euler", (P, p)))
+    # triply periodic box with periodic ghost records
+    out.append(("tgv_periodic", decks.tgv_periodic(n=8)))
     return out
 
 

@@ -217,3 +217,40 @@ def test_mixed_refinement_with_idrs_matches_fp64(deck):
     assert s1[-1].status == 0 and s1[-1].rel_residual <= 1e-6
     for f in ("ux", "uy", "uz"):
         assert rel_err(A[f], B[f]) <= MIXED_TOL, f
+
+
+def _tgv_amplitude(A):
+    it = A["buffer_type"] != layout.BUFFER_PERIODIC_GHOST
+    k = 2 * np.pi
+    x, y, z = (A[c][it].astype(np.float64) for c in "xyz")
+    ua = np.sin(k * x) * np.cos(k * y) * np.cos(k * z)
+    return float((A["ux"][it] * ua).sum() / (ua * ua).sum())
+
+
+@pytest.mark.parametrize("coarse", [0, 2], ids=["jacobi", "two_level"])
+def test_tgv_fp64_bicgstab_matches_oracle(coarse):
+    """Triply periodic box (ghost rows are copy rows, the operator is
+    singular): the FP64 solve matches the oracle's pressure and velocity."""
+    P, p = decks.tgv_periodic(n=12)
+    A, stats = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8, nsteps=2, coarse=coarse)
+    for s in stats:
+        assert s.status == 0 and s.rel_residual <= 1e-8, (s.rel_residual, s.iterations)
+    O = restated.Restated(P, p, 1)
+    for _ in range(2):
+        st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-10, maxit=5000)
+        assert st == 0
+    B, _, _ = O.download()
+    assert rel_err(A["pres"], B["pres"]) <= PRES_TOL_FP64
+    for f in ("ux", "uy", "uz"):
+        assert rel_err(A[f], B[f]) <= PRES_TOL_FP64, f
+
+
+def test_tgv_mixed_decay_rate():
+    """The mixed form on the Taylor-Green box decays as exp(-3 nu k^2 t)
+    (Re = 20, 16^3 lattice, 20 steps) like the oracle's FP64 step."""
+    P, p = decks.tgv_periodic(n=16, nu=0.05)
+    A, stats = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_BICGSTAB, 1e-6, nsteps=20, coarse=2)
+    assert all(s.status == 0 for s in stats)
+    t = 20 * p.getf("dt")
+    want = np.exp(-3 * 0.05 * (2 * np.pi) ** 2 * t)
+    assert abs(_tgv_amplitude(A) / want - 1) < 1e-2

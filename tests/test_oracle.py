@@ -346,3 +346,65 @@ def test_bf16_rounding_of_the_oracle():
     import mlp
     x = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 0.0], np.float32)
     assert np.array_equal(mlp.round_bf16(x), np.array([1.0, 1.0, 1.0078125, -3.140625, 0.0], np.float32))
+
+
+def _tgv_amplitude(B):
+    it = B["buffer_type"] != layout.BUFFER_PERIODIC_GHOST
+    k = 2 * np.pi
+    x, y, z = (B[c][it].astype(np.float64) for c in "xyz")
+    ua = np.sin(k * x) * np.cos(k * y) * np.cos(k * z)
+    return float((B["ux"][it] * ua).sum() / (ua * ua).sum())
+
+
+def test_periodic_ghosts_copy_their_partners():
+    # every ghost of the triply periodic box holds the state of the interior
+    # record at its wrapped position after the step
+    P, p = decks.tgv_periodic(n=8)
+    O = restated.Restated(P, p, 1)
+    st, rel, it = O.step(2, mode=layout.PPE_BICGSTAB, tol=1e-8, maxit=4000)
+    assert st == 0 and rel <= 1e-8
+    B, _, _ = O.download()
+    g = B["buffer_type"] == layout.BUFFER_PERIODIC_GHOST
+    assert g.sum() == 14 ** 3 - 8 ** 3
+    key = lambda s: [tuple(r) for r in np.round(np.mod(np.stack([B[c][s] for c in "xyz"], 1).astype(np.float64), 1.0) * 16).astype(int)]
+    inner = dict(zip(key(~g), np.nonzero(~g)[0]))
+    src = np.array([inner[k] for k in key(g)])
+    for f in ("ux", "uy", "uz", "pres"):
+        assert np.array_equal(B[f][g], B[f][src]), f
+
+
+def test_taylor_green_decay_rate():
+    # u = U0 sin x cos y cos z decays as exp(-3 nu k^2 t) at low Reynolds
+    # number (Re = 20 here); the oracle's converged FP64 step follows it to
+    # within 1 % over 20 steps on a 16^3 lattice
+    P, p = decks.tgv_periodic(n=16, nu=0.05)
+    O = restated.Restated(P, p, 1)
+    for _ in range(20):
+        st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-8, maxit=4000)
+        assert st == 0
+    B, _, _ = O.download()
+    t = 20 * p.getf("dt")
+    want = np.exp(-3 * 0.05 * (2 * np.pi) ** 2 * t)
+    assert abs(_tgv_amplitude(B) / want - 1) < 1e-2
+
+
+def test_taylor_green_pressure_converges_to_analytic():
+    # the projection pressure of one step approaches the Taylor-Green pressure
+    # rho U0^2 / 16 (cos 2x + cos 2y)(cos 2z + 2) with resolution
+    k = 2 * np.pi
+    out = []
+    for n in (8, 16):
+        P, p = decks.tgv_periodic(n=n)
+        O = restated.Restated(P, p, 1)
+        st, rel, it = O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-8, maxit=4000)
+        assert st == 0
+        B, _, _ = O.download()
+        it = B["buffer_type"] != layout.BUFFER_PERIODIC_GHOST
+        x, y, z = (B[c][it].astype(np.float64) for c in "xyz")
+        pa = 1000 / 16 * (np.cos(2 * k * x) + np.cos(2 * k * y)) * (np.cos(2 * k * z) + 2)
+        pn = B["pres"][it].astype(np.float64)
+        pa -= pa.mean()
+        pn -= pn.mean()
+        out.append(((pn * pa).sum() / np.sqrt((pn * pn).sum() * (pa * pa).sum()), np.abs(pn - pa).max()))
+    assert out[1][0] > 0.999 and out[0][0] > 0.99
+    assert out[1][1] < 0.6 * out[0][1]

@@ -39,6 +39,7 @@ DevParams make_dev_params(const sph_params &p) {
     d.ppe_pair_h = p.ppe_pair_h;
     d.inlet_recycling = p.inlet_recycling;
     d.rp_x = p.recycle_probe_x; d.rp_y = p.recycle_probe_y;
+    for (int a = 0; a < 6; ++a) d.periodic_box[a] = p.periodic_box[a];
     d.turb = p.vii[SPH_VII_TURBULENCE];
     d.noslip = p.vii[SPH_VII_NOSLIP_BC];
     d.count = p.vii[SPH_VII_COUNT];

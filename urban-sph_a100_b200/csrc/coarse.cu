@@ -270,9 +270,10 @@ int coarse_build(Ctx<Real> &c) {
     const int n = c.n;
     cudaStream_t st = c.stream;
     // host copies of what the aggregation needs
-    std::vector<int> kind(n), ncnt(n), comp(n, -1);
+    std::vector<int> kind(n), ncnt(n), comp(n, -1), aux(n);
     std::vector<float4> pos(n);
     SPH_CUDA_TRY(cudaMemcpyAsync(kind.data(), c.row_kind, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaMemcpyAsync(aux.data(), c.row_aux, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaMemcpyAsync(ncnt.data(), c.ncnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaMemcpyAsync(pos.data(), c.pf, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
     if (c.n_comp > 0) SPH_CUDA_TRY(cudaMemcpyAsync(comp.data(), c.comp_id, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
@@ -282,17 +283,22 @@ int coarse_build(Ctx<Real> &c) {
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
 
     // aggregates: blocks of B^3 cells of the binning grid, numbered in order
-    // of their first row (rows ascending), identity and pinned rows excluded
+    // of their first row (rows ascending), identity and pinned rows excluded.
+    // A copy row (outlet partner, periodic ghost) joins its partner's block,
+    // so that every coarse vector satisfies the copy rows exactly: a ghost
+    // and the interior record it mirrors across the box share an aggregate.
     const DevParams &P = c.dp;
     const int NBx = (P.NI + B - 1) / B, NBy = (P.NJ + B - 1) / B, NBz = (P.NK + B - 1) / B;
     std::vector<int> block_agg((size_t)NBx * NBy * NBz, -1), agg(n, -1), size;
+    auto member = [&](int k) { return kind[k] == 1 || kind[k] == 2 || kind[k] == 3; };
     int m = 0;
     for (int i = 0; i < n; ++i) {
-        const int kd = kind[i];
-        if (kd != 1 && kd != 2 && kd != 3) continue;
-        const int bx = bin_axis(pos[i].x, P.xmin, P.xmax, P.NI) / B;
-        const int by = bin_axis(pos[i].y, P.ymin, P.ymax, P.NJ) / B;
-        const int bz = bin_axis(pos[i].z, P.zmin, P.zmax, P.NK) / B;
+        if (!member(i)) continue;
+        int src = i;
+        if (kind[i] == 3 && aux[i] >= 0 && aux[i] < n && member(aux[i])) src = aux[i];
+        const int bx = bin_axis(pos[src].x, P.xmin, P.xmax, P.NI) / B;
+        const int by = bin_axis(pos[src].y, P.ymin, P.ymax, P.NJ) / B;
+        const int bz = bin_axis(pos[src].z, P.zmin, P.zmax, P.NK) / B;
         int &a = block_agg[((size_t)bz * NBy + by) * NBx + bx];
         if (a < 0) { a = m++; size.push_back(0); }
         agg[i] = a;

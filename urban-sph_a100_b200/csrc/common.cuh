@@ -37,6 +37,7 @@ struct DevParams {
     int outlet_bc, inlet_recycling;
     int ppe_pair_h;        // 1: pair-averaged h in the pressure system
     double rp_x, rp_y;     // recycling probe
+    double periodic_box[6];   // x0,x1,y0,y1,z0,z1 of the periodic box (ghost partners)
     int count;
     float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, time, dt_structure;
     double cs_sgs, l2, l3, l_left, l_right, outlet_probe_dx, partner_tol, ghost_tol;

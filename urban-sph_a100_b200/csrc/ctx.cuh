@@ -44,10 +44,12 @@ struct SideLists {
     int *nm_rows = nullptr, *nm_off = nullptr, *nm_nbr = nullptr;
     int *nm_ghost = nullptr;     // flags: 1 mirror (inlet) row, 2 the pass writes p = 0,
                                  // 4 no fluid in range at all (operator anchor)
-    // partners of periodic (buffer 3/4) and outlet (buffer 2) particles
-    int n_per = 0, n_out = 0;
+    // partners of periodic (buffer 3/4), outlet (buffer 2) and periodic-box
+    // ghost (buffer 7) particles
+    int n_per = 0, n_out = 0, n_gh = 0;
     int *per_rows = nullptr, *per_partner = nullptr;
     int *out_rows = nullptr, *out_partner = nullptr;
+    int *gh_rows = nullptr, *gh_partner = nullptr;
     // dormant open-boundary variants of the reference (outlet_bc 1 / 2,
     // inlet_recycling): extrapolation rows (outlet, off the MOST layer) with
     // the fluid around their mirror node; inout rows, the side buffers first
@@ -133,7 +135,7 @@ struct Ctx {
     // ---- PPE ----
     Real *diag = nullptr;         // A_i of fluid rows
     int *row_kind = nullptr;      // 0 identity, 1 fluid, 2 Neumann, 3 outlet copy, 4 pinned
-    int *row_aux = nullptr;       // outlet partner of kind-3 rows, -1 otherwise
+    int *row_aux = nullptr;       // partner of kind-3 rows (outlet copy, periodic ghost), -1 otherwise
     int n_pins = 0;               // rows pinned to p = 0 (one per unanchored component)
     int n_comp = 0;               // components carrying the rank-one mean-pressure term
     int *comp_id = nullptr;       // component of each fluid row (-1: none)

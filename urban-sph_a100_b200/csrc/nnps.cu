@@ -484,6 +484,16 @@ struct HostGrid {
     }
 };
 
+// a position wrapped into the periodic box (axes with x1 > x0), in double:
+// v - L floor((v - x0) / L)
+static inline void periodic_wrap(const double *box, float x, float y, float z, double *w) {
+    const float v[3] = {x, y, z};
+    for (int a = 0; a < 3; ++a) {
+        const double lo = box[2 * a], len = box[2 * a + 1] - box[2 * a];
+        w[a] = (len > 0) ? (double)v[a] - len * std::floor(((double)v[a] - lo) / len) : (double)v[a];
+    }
+}
+
 static inline float hdist(float xi, float yi, float zi, float xj, float yj, float zj) {
     volatile float dx = xi - xj, dy = yi - yj, dz = zi - zj;
     volatile float a = dx * dx, b = dy * dy, cc = dz * dz;
@@ -574,8 +584,9 @@ static int null_components(Ctx<Real> &c, std::vector<int> &kind, const std::vect
         k_cc_fluid<<<grid_for(n, 128), 128, 0, st>>>(c.row_kind, c.jc, c.slice_off, c.ncnt, c.nbr, label, flag, n);
         if (c.L.n_nm) k_cc_csr<<<grid_for(c.L.n_nm, 128), 128, 0, st>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.L.n_nm, label, flag);
         if (c.L.n_out) k_cc_pairs<<<grid_for(c.L.n_out, 128), 128, 0, st>>>(c.L.out_rows, c.L.out_partner, c.L.n_out, label, flag);
+        if (c.L.n_gh) k_cc_pairs<<<grid_for(c.L.n_gh, 128), 128, 0, st>>>(c.L.gh_rows, c.L.gh_partner, c.L.n_gh, label, flag);
         k_cc_jump<<<grid_for(n, 256), 256, 0, st>>>(label, n);
-        c.launches += 4;
+        c.launches += 4 + (c.L.n_gh ? 1 : 0);
         SPH_CUDA_TRY(cudaMemcpyAsync(&changed, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
         ++rounds;
@@ -846,6 +857,28 @@ int build_side_lists(Ctx<Real> &c) {
     L.n_per = (int)rows.size();
     SPH_TRY(upload_vec(c, L.per_rows, rows)); SPH_TRY(upload_vec(c, L.per_partner, nb));
 
+    // ghosts of the periodic box (buffer 7): the record at the ghost's
+    // position wrapped into the box, |d| < partner_tol, ghosts excluded; the
+    // last match in cell order wins, as in the outlet search below
+    std::vector<int> gh_rows, gh_nb;
+    for (int i = 0; i < n; ++i) {
+        if (G.ty[i].y != SPH_BUFFER_PERIODIC_GHOST) continue;
+        gh_rows.push_back(i);
+        double w[3];
+        periodic_wrap(P.periodic_box, G.pf[i].x, G.pf[i].y, G.pf[i].z, w);
+        int ic, jc, kc;
+        G.search_cell((float)w[0], (float)w[1], (float)w[2], ic, jc, kc);
+        int found = -1;
+        G.cell_loop(ic, jc, kc, 1, [&](int j) {
+            if (G.ty[j].y == SPH_BUFFER_PERIODIC_GHOST) return;
+            const double dx = w[0] - (double)G.pf[j].x, dy = w[1] - (double)G.pf[j].y, dz = w[2] - (double)G.pf[j].z;
+            if (std::sqrt(dx * dx + dy * dy + dz * dz) < P.partner_tol) found = j;
+        });
+        gh_nb.push_back(found);
+    }
+    L.n_gh = (int)gh_rows.size();
+    SPH_TRY(upload_vec(c, L.gh_rows, gh_rows)); SPH_TRY(upload_vec(c, L.gh_partner, gh_nb));
+
     // outlet partners, functions_BC.cuh:673-761
     rows.clear(); nb.clear();
     for (int i = 0; i < n; ++i) {
@@ -866,6 +899,7 @@ int build_side_lists(Ctx<Real> &c) {
     SPH_TRY(upload_vec(c, L.out_rows, rows)); SPH_TRY(upload_vec(c, L.out_partner, nb));
     aux.assign(n, -1);
     for (size_t k = 0; k < rows.size(); ++k) aux[rows[k]] = nb[k];
+    for (size_t k = 0; k < gh_rows.size(); ++k) aux[gh_rows[k]] = gh_nb[k];
     SPH_CUDA_TRY(cudaMemcpyAsync(c.row_aux, aux.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
 
@@ -977,13 +1011,13 @@ int build_side_lists(Ctx<Real> &c) {
         if (t.x <= 2 && t.w <= 0 && t.w == 0) wl.push_back(i);
         if (t.w == -1) fs.push_back(i);
         // converged-PPE row classes (precedence of the reference's overwrites:
-        // outlet copy after Neumann after the PPE sweep)
-        // a record that is both an outlet buffer and a Neumann row (a
-        // free-slip record past L3) is a Neumann row of the operator: the
-        // Neumann application writes it
+        // outlet copy after Neumann after the PPE sweep).  A record that is
+        // both an outlet buffer and a Neumann row (a free-slip record past L3)
+        // is a copy row, as the outlet copy overwrites the Neumann value; a
+        // periodic-box ghost is a copy row too
         if (t.x >= 3) kind[i] = 0;
+        else if (t.y == 2 || t.y == SPH_BUFFER_PERIODIC_GHOST) kind[i] = 3;
         else if (t.w != 1) kind[i] = 2;
-        else if (t.y == 2) kind[i] = 3;
         else kind[i] = 1;
     }
     L.n_fluid = (int)fl.size(); L.n_wall = (int)wl.size(); L.n_fs = (int)fs.size();

@@ -1044,9 +1044,12 @@ int outlet_pass(Ctx<Real> &c, VarSet<Real> &V) {
     return SPH_OK;
 }
 
+// the periodic-y copy (functions_BC.cuh:1015-1154), then the ghosts of a
+// periodic box, which copy the record at their wrapped position
 template <class Real>
 int periodic_pass(Ctx<Real> &c, VarSet<Real> &V) {
-    return partner_pass(c, V, c.L.per_rows, c.L.per_partner, c.L.n_per);
+    SPH_TRY(partner_pass(c, V, c.L.per_rows, c.L.per_partner, c.L.n_per));
+    return partner_pass(c, V, c.L.gh_rows, c.L.gh_partner, c.L.n_gh);
 }
 
 template <class Real>

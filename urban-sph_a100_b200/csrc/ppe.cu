@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         const int lane = threadIdx.x & 31;
         if (k >= n_nm) return;   // uniform over the warp
         const int i = nm_rows[k];
+        if (kind[i] != 2) return;   // an outlet copy row written by the SELL blocks
         const V xi = x[i];
         const int q0 = nm_off[k], q1 = nm_off[k + 1];
         double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
@@ -373,13 +374,15 @@ __global__ void __launch_bounds__(128) k_spmv_mf(DevParams P, const int *__restr
 // rows do not act as point Dirichlet anchors; the pass still writes p = 0.
 // One warp per row: the lanes read the row's CSR entries coalesced.
 template <class V, class W>
-__global__ void __launch_bounds__(256) k_spmv_neumann(const int *__restrict__ rows, const int *__restrict__ off,
-                                                      const int *__restrict__ nb, const W *__restrict__ w,
-                                                      int nrows, const V *__restrict__ x, V *__restrict__ y) {
+__global__ void __launch_bounds__(256) k_spmv_neumann(const int *__restrict__ kind, const int *__restrict__ rows,
+                                                      const int *__restrict__ off, const int *__restrict__ nb,
+                                                      const W *__restrict__ w, int nrows, const V *__restrict__ x,
+                                                      V *__restrict__ y) {
     const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (k >= nrows) return;   // uniform over the warp
     const int i = rows[k];
+    if (kind[i] != 2) return;   // an outlet copy row (the row operator wrote it)
     const V xi = x[i];
     const int q0 = off[k], q1 = off[k + 1];
     double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
@@ -611,11 +614,11 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
         // FP32 weights in the FP32 applications of the mixed form; the FP64
         // applications (true residuals) keep the FP64 weights
         if (sizeof(Real) == 4 && sizeof(V) == 4)
-            k_spmv_neumann<V, float><<<gnm, 256, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.L.n_nm,
-                                                                x, y);
+            k_spmv_neumann<V, float><<<gnm, 256, 0, c.stream>>>(c.row_kind, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf,
+                                                                c.L.n_nm, x, y);
         else
-            k_spmv_neumann<V, double><<<gnm, 256, 0, c.stream>>>(c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow, c.L.n_nm,
-                                                                 x, y);
+            k_spmv_neumann<V, double><<<gnm, 256, 0, c.stream>>>(c.row_kind, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow,
+                                                                 c.L.n_nm, x, y);
         ++c.launches;
     }
 }

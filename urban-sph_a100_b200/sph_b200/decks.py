@@ -29,7 +29,7 @@ before upload, plus the solver parameters.
 """
 import numpy as np
 
-from .layout import PART1
+from .layout import BUFFER_PERIODIC_GHOST, PART1
 from .params import CASEH_PROFILE_U, CASEH_PROFILE_Z, default_params, domain_setup, set_profile
 
 SEED = 20261203
@@ -423,6 +423,44 @@ def tgv_box(n=30, dx=0.01, re=1000.0, seed=SEED, **kw):
     """Taylor-Green initial field in a walled box (the reference's NNPS has
     no triply periodic mode)."""
     return _box_case(n, dx, re, False, seed, kw)
+
+
+def tgv_periodic(n=64, h_coeff=1.3, kernel="Wendland6", rho=1000.0, nu=1e-3, u0=1.0, seed=SEED, shuffle=True, **kw):
+    """Triply periodic Taylor-Green vortex: n^3 particles cell-centred in the
+    unit cube (dx = 1/n, h = h_coeff dx), u = U0 sin x cos y cos z,
+    v = -U0 cos x sin y cos z, w = 0 with the coordinates mapped to
+    [0, 2 pi), density rho, kinematic viscosity nu, dt = 0.1 dx / U0
+    (CFL 0.1), and the Taylor-Green pressure of that field.  Three layers of
+    periodic ghosts (buffer_type 7) surround the cube, enough for the kernel
+    support kappa h = 2.6 dx."""
+    rng = np.random.default_rng(seed)
+    f = np.float32
+    dx = 1.0 / n
+    c = (np.arange(-3, n + 3) + 0.5) * dx
+    x, y, z = _grid(c, c, c)
+    P = _records(x, y, z)
+    P["p_type"] = 1
+    ghost = (x < 0) | (x > 1) | (y < 0) | (y > 1) | (z < 0) | (z > 1)
+    P["buffer_type"][ghost] = BUFFER_PERIODIC_GHOST
+    _common_fields(P, dx, h_coeff=h_coeff, rho=rho)
+    k = 2 * np.pi
+    xd, yd, zd = x.astype(np.float64), y.astype(np.float64), z.astype(np.float64)
+    P["ux"] = (u0 * np.sin(k * xd) * np.cos(k * yd) * np.cos(k * zd)).astype(f)
+    P["uy"] = (-u0 * np.cos(k * xd) * np.sin(k * yd) * np.cos(k * zd)).astype(f)
+    P["pres"] = (rho * u0 * u0 / 16.0 * (np.cos(2 * k * xd) + np.cos(2 * k * yd)) * (np.cos(2 * k * zd) + 2.0)).astype(f)
+    if shuffle:
+        P = P[rng.permutation(len(P))]
+    p = default_params(dt=0.1 * dx / u0, kernel=kernel, turbulence="Laminar", open_boundary=0, noslip=0, **kw)
+    p.visc_fluid = nu * rho
+    p.rho_air = rho
+    p.l2, p.l3, p.l_left, p.l_right = -1e9, 1e9, -1e9, 1e9
+    for a, v in enumerate((0.0, 1.0, 0.0, 1.0, 0.0, 1.0)):
+        p.periodic_box[a] = v
+    p.partner_tol = 1e-3 * dx
+    p.setf("u_limit", 20.0 * u0)
+    p.setf("time_end", 1e9)
+    domain_setup(p, P)
+    return P, p
 
 
 def ensemble(ncase=64, nmin=20000, nmax=200000, dx=0.01, seed=SEED, **kw):

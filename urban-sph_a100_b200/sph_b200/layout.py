@@ -125,6 +125,7 @@ class SphParams(ctypes.Structure):
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
         ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
+        ("periodic_box", ctypes.c_double * 6),
     ]
 
     def seti(self, name, value):
@@ -155,7 +156,9 @@ class PpeStats(ctypes.Structure):
     ]
 
 
-assert ctypes.sizeof(SphParams) == 1288, ctypes.sizeof(SphParams)
+assert ctypes.sizeof(SphParams) == 1336, ctypes.sizeof(SphParams)
+
+BUFFER_PERIODIC_GHOST = 7   # buffer_type of a periodic ghost (sph_params.periodic_box)
 
 OUTLET_DONOTHING = 0      # KERNEL_donothing_buffer3D (the shipped step)
 OUTLET_EXTRAPOLATION = 1  # KERNEL_open_boundary_extrapolation_buffer3D
@@ -164,7 +167,7 @@ OUTLET_INOUT = 2          # KERNEL_inout_boundary3D
 
 def params_from_bytes(b):
     """SphParams from stored bytes; fields appended since they were written
-    (apr_zone, the recycling probe) read as 0."""
+    (apr_zone, the recycling probe, the periodic box) read as 0."""
     buf = bytearray(ctypes.sizeof(SphParams))
     b = bytes(b)
     buf[:len(b)] = b[:len(buf)]
