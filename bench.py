@@ -19,6 +19,7 @@ Multi-GPU: the step is a one-GPU path; N ranks run N independent replicas
 (weak scaling, no collective in the step).
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -411,7 +412,10 @@ def main():
     # particle-steps count particles, not the periodic ghost records
     n = int((P["buffer_type"] != layout.BUFFER_PERIODIC_GHOST).sum())
     prec = layout.PREC_FP64 if args.precision == "fp64" else layout.PREC_MIXED
-    sim = abi.Simulation(p, precision=prec, device=local)
+    # the context's own stream: the Krylov iterations between host checks
+    # replay as a CUDA graph (the legacy default stream cannot be captured)
+    stream = torch.cuda.Stream(device=local)
+    sim = abi.Simulation(p, precision=prec, device=local, stream=ctypes.c_void_p(stream.cuda_stream))
     if boxes is not None:
         sim.set_ib_boxes(boxes)
     sim.upload(P)
@@ -468,12 +472,12 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     stats, phases = [], []
-    e0.record()
+    e0.record(stream)
     for _ in range(args.steps):
         s = sim.step(1)
         stats.append((s.iterations, s.refinements, s.rel_residual, s.solve_ms, s.status, s.initial_residual))
         phases.append(sim.phase_ms().copy())
-    e1.record()
+    e1.record(stream)
     torch.cuda.synchronize()
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
@@ -490,12 +494,12 @@ def main():
     t0 = time.perf_counter()
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
-    f0.record()
+    f0.record(stream)
     for _ in range(ke):
         sim.upload_state(host)
         sim.step(1)
         sim.download_into(host)
-    f1.record()
+    f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
     e2e, e2e_ms = replicas.throughput(n, ke, e2e_ms, device="cuda")

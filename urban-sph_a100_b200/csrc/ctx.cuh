@@ -177,6 +177,8 @@ struct Ctx {
     bool prof = false;
     cudaEvent_t *prof_ev = nullptr;   // 512 events, created on first use
     int prof_pending = 0;
+    cudaEvent_t *cap_ev = nullptr;    // while a Krylov graph is captured: its timing events
+    int cap_n = 0, cap_max = 0;       // timed applications captured, room for
     long long prof_launches = 0;
     double prof_ms = 0;
     double *red = nullptr;        // block partial sums

@@ -564,7 +564,12 @@ template <class Real, class V>
 static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_ready = false) {
     const int n = c.n;
     const bool timed = c.prof && sizeof(V) == sizeof(Real);
-    if (timed) {
+    // inside a graph capture the timing events become event-record nodes of
+    // the graph (read after each replay)
+    const bool cap_timed = timed && c.cap_ev && c.cap_n < c.cap_max;
+    if (cap_timed) {
+        cudaEventRecordWithFlags(c.cap_ev[2 * c.cap_n], c.stream, cudaEventRecordExternal);
+    } else if (timed && !c.cap_ev) {
         if (c.prof_pending == 256) prof_drain(c);
         if (!c.prof_ev) {
             c.prof_ev = new cudaEvent_t[512];
@@ -605,7 +610,10 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
                                                                   c.ncnt, c.nbr, c.g6, c.diag, cid, cmean, x, y, n);
     }
     ++c.launches;
-    if (timed) {
+    if (cap_timed) {
+        cudaEventRecordWithFlags(c.cap_ev[2 * c.cap_n + 1], c.stream, cudaEventRecordExternal);
+        ++c.cap_n;
+    } else if (timed && !c.cap_ev) {
         cudaEventRecord(c.prof_ev[2 * c.prof_pending + 1], c.stream);
         ++c.prof_pending;
     }
@@ -812,6 +820,13 @@ struct KrylovGraph {
     cudaGraphExec_t exec = nullptr;
     std::vector<uintptr_t> key;
     long long nodes = 0;
+    // with live operator timing on: a start / end event per operator
+    // application, recorded by event nodes of the graph
+    std::vector<cudaEvent_t> ev;
+    int n_timed = 0;
+    ~KrylovGraph() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
 };
 
 template <class Real>
@@ -822,7 +837,7 @@ static std::vector<uintptr_t> krylov_graph_key(Ctx<Real> &c, float *const *ws, c
                           c.comp_id, c.comp_inv, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.cg_off, c.cg_rows,
                           c.cg_s, c.cg_y, c.cg_invf, c.cg_agg};
     for (const void *q : ptrs) k.push_back((uintptr_t)q);
-    const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode};
+    const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode, c.prof ? 1 : 0};
     for (long long q : sizes) k.push_back((uintptr_t)q);
     return k;
 }
@@ -926,12 +941,16 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
     };
     // `check` iterations as one graph launch; false: run them one launch at a time
     auto graph_chunk = [&]() -> bool {
-        if (c.kgraph_off || st == nullptr || c.prof || !cached) return false;
+        if (c.kgraph_off || st == nullptr || !cached) return false;
         auto *g = (KrylovGraph *)c.kgraph;
         if (!g) { g = new KrylovGraph(); c.kgraph = g; }
         std::vector<uintptr_t> key = krylov_graph_key(c, ws, xlo);
         if (!g->exec || g->key != key) {
             if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
+            if (c.prof && g->ev.empty()) {
+                g->ev.resize(4 * check);   // two applications per iteration
+                for (auto &e : g->ev) cudaEventCreate(&e);
+            }
             const long long l0 = c.launches;
             cudaGraph_t graph = nullptr;
             if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
@@ -939,7 +958,11 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
                 c.kgraph_off = true;
                 return false;
             }
+            if (c.prof) { c.cap_ev = g->ev.data(); c.cap_n = 0; c.cap_max = 2 * check; }
             for (int q = 0; q < check; ++q) iteration();
+            g->n_timed = c.prof ? c.cap_n : 0;
+            c.cap_ev = nullptr;
+            c.cap_n = c.cap_max = 0;
             const cudaError_t e1 = cudaStreamEndCapture(st, &graph);
             const cudaError_t e2 = e1 == cudaSuccess ? cudaGraphInstantiate(&g->exec, graph, 0) : e1;
             if (graph) cudaGraphDestroy(graph);
@@ -959,6 +982,21 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
             return false;
         }
         c.launches += g->nodes;
+        if (g->n_timed > 0) {
+            // operator times of this replay (the host waits for the chunk's
+            // scalars right after it anyway)
+            prof_drain(c);
+            cudaEventSynchronize(g->ev[2 * g->n_timed - 1]);
+            for (int k = 0; k < g->n_timed; ++k) {
+                float ms = 0;
+                if (cudaEventElapsedTime(&ms, g->ev[2 * k], g->ev[2 * k + 1]) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                c.prof_ms += ms;
+                ++c.prof_launches;
+            }
+        }
         return true;
     };
     while (status != SPH_OK && it < maxit) {
