@@ -340,6 +340,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--matrix-free", action="store_true")
+    ap.add_argument("--wide-index", action="store_true",
+                    help="pressure operator on 32-bit neighbour indices instead of the 16-bit codes")
     ap.add_argument("--coarse", type=int, default=None,
                     help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; "
                          "default 5 for the canyon, 9 for the cube array)")
@@ -399,6 +401,7 @@ def main():
     p.ppe_tol = args.tol
     if args.matrix_free:
         p.ppe_matrix_free = 1
+    p.ppe_wide_index = 1 if args.wide_index else 0
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2, "restart-idrs": 3}[args.refinement]
     p.ppe_coarse_block = args.coarse
     p.ppe_coarse_mode = 1 if args.coarse_mode == "multiplicative" else 0
@@ -609,7 +612,8 @@ def main():
                    "particles": n, "apr": apr, "scale": args.scale,
                    "precision": "mixed FP32/FP64" if args.precision == "mixed" else "FP64",
                    "ppe": args.mode, "ppe_tol": args.tol,
-                   "ppe_operator": "matrix-free" if args.matrix_free else "cached c_ij",
+                   "ppe_operator": "matrix-free" if args.matrix_free else
+                   ("cached c_ij, 32-bit neighbour indices" if args.wide_index else "cached c_ij, 16-bit neighbour codes"),
                    "ppe_refinement": args.refinement,
                    "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],
                    "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",

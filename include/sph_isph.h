@@ -199,7 +199,15 @@ typedef struct sph_params {
                                 multi-resolution form that KERNEL_PPE3D keeps
                                 commented out (functions_PPE.cuh:113-116) and
                                 KERNEL_pressureforce3D uses (:598-602)         */
-    int32_t reserved[4];
+    int32_t ppe_wide_index;  /* 1: the pressure operator reads the 32-bit
+                                neighbour indices; 0 (default): 16-bit codes
+                                (cell plane of the entry, offset from the
+                                plane's first reachable record) wherever every
+                                row searches at most two cells around its own
+                                and every offset is below 8192 -- same
+                                entries, same order, same results, fewer
+                                bytes                                         */
+    int32_t reserved[3];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

@@ -290,3 +290,34 @@ def test_graph_replay_with_live_timing_matches_stream_launches(deck):
     # two timed applications per iteration (graph chunks run whole chunks of
     # four, the solve stops counting at convergence)
     assert out[2][2] >= 2 * its and out[2][3] > 0
+
+
+@pytest.mark.parametrize("name", ["caseh_mini", "tgv_periodic", "canyon_small"])
+def test_16bit_neighbour_codes_give_identical_steps(name):
+    """The pressure operator reading 16-bit neighbour codes (default) visits
+    the same entries in the same order as with 32-bit indices
+    (ppe_wide_index = 1): the mixed and FP64 steps are bit-identical, and the
+    operator's algorithmic bytes show which form ran."""
+    P, p = {"caseh_mini": lambda: decks.caseh_mini(nx=14, ny=8, nz=5),
+            "tgv_periodic": lambda: decks.tgv_periodic(n=10),
+            "canyon_small": lambda: decks.canyon(scale=0.12)}[name]()
+    for precision in (layout.PREC_MIXED, layout.PREC_FP64):
+        out = []
+        for wide in (0, 1):
+            q = p.copy()
+            q.ppe_mode = layout.PPE_MIXED_IR
+            q.ppe_tol = 1e-6
+            q.ppe_coarse_block = 2
+            q.ppe_wide_index = wide
+            sim = abi.Simulation(q, precision=precision)
+            sim.upload(P)
+            st = [sim.step(1) for _ in range(2)]
+            _, _, nbytes = sim.operator_stats(reset=True)
+            A, _, _ = sim.download()
+            sim.close()
+            assert all(s.status == 0 for s in st)
+            out.append((A, [s.iterations for s in st], nbytes))
+        assert out[0][2] < out[1][2]
+        assert out[0][1] == out[1][1]
+        for f in ("ux", "uy", "uz", "pres"):
+            assert np.array_equal(out[0][0][f], out[1][0][f]), (precision, f)

@@ -53,7 +53,7 @@ __global__ void k_coef_absmax(const int *kind, const long long *slice_off, const
     double m = 0;
     if (i < n && kind[i] == 1) {
         const long long base = slice_off[i >> 5] + (i & 31);
-        for (int k = 0; k < ncnt[i]; ++k) m = fmax(m, fabs((double)coef[base + 32LL * k]));
+        for (int k = 0; k < ncnt[i]; ++k) m = fmax(m, fabs((double)coef[sell4(base - (i & 31), i & 31, k)]));
     }
     if (m > 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) k_coarse_assemble(
             const int cnt = ncnt[i];
             for (int k = 0; k < cnt; ++k) {
                 const long long e = base + 32LL * k;
-                couple(nbr[e], (double)coef[e]);
+                couple(nbr[e], (double)coef[sell4(base - (i & 31), i & 31, k)]);
             }
             const int cc = comp_id ? comp_id[i] : -1;
 #pragma unroll

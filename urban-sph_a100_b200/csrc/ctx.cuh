@@ -131,6 +131,13 @@ struct Ctx {
     int *nbr = nullptr;
     long long nnz = 0, nnz_padded = 0;
     long long nbr_cap = 0;
+    // the same list as 16-bit codes for the pressure operator (plane_cell in
+    // common.cuh): valid when every row searches at most two cells around
+    // its own and every offset fits in 13 bits
+    uint16_t *nbr16 = nullptr;
+    int *row_cell = nullptr;      // cell index of the row's first x-run cell (dy = dz = 0)
+    int row_cell_cap = 0;
+    bool list16 = false;
     SideLists L;
     // ---- PPE ----
     Real *diag = nullptr;         // A_i of fluid rows

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) k_ml_residual(const int *__restrict__ kin
         double s = 0;
         for (int k = 0; k < cnt; ++k) {
             const long long e = base + 32LL * k;
-            s += (double)coef[e] * ((double)p[i] - (double)p[nbr[e]]);
+            s += (double)coef[sell4(base - (i & 31), i & 31, k)] * ((double)p[i] - (double)p[nbr[e]]);
         }
         r = (float)((double)b[i] - s);
         const double a = (double)diag[i];
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256) k_ml_features(const int *__restrict__ kin
         for (int k = 0; k < cnt; ++k) {
             const long long e = base + 32LL * k;
             const int j = nbr[e];
-            const float w = (float)coef[e] * ia;
+            const float w = (float)coef[sell4(base - (i & 31), i & 31, k)] * ia;
             const bool fl = kind[j] == 1;
             const float qj[5] = {fl ? dd[j] * isd : 0.f, fl ? rr[j] * isr : 0.f, fl ? (float)b[j] * isb : 0.f,
                                  (pold[j] - pbar) * isp, pprev ? (pold[j] - pprev[j]) * isd : 0.f};

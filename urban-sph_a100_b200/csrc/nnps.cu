@@ -400,15 +400,20 @@ static int regather(Ctx<Real> &c, T *arr, void *scratch) {
 // kept when sqrt(r2) < search_kappa * fmax(h_i, h_j) in FP32
 // (functions_PPE.cuh:96-100; the +-1e-20 of the individual kernels does not
 // change an FP32 comparison with a positive radius).
+// The fill pass also writes the 16-bit codes of the pressure operator
+// (nbr16, row_cell; flag16 set when a row cannot be coded: a search radius
+// beyond two cells, or an offset beyond 8191 in its cell plane).
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restrict__ pf,
                                               const int4 *__restrict__ ty, const int *__restrict__ ncell,
                                               const int *__restrict__ cs, int *__restrict__ ncnt,
                                               const long long *__restrict__ slice_off, int *__restrict__ nbr,
-                                              int n) {
+                                              uint16_t *__restrict__ nbr16, int *__restrict__ row_cell,
+                                              int *__restrict__ flag16, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int cnt = 0;
+    if (FILL && nbr16) row_cell[i] = 0;
     if (ty[i].x != 3) {
         const float4 xi = pf[i];
         const int ic = search_axis(xi.x, P.xmin, P.xmax, P.dcell, P.NI);
@@ -418,6 +423,11 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
         const int x0 = max(ic - nc, 0), x1 = min(ic + nc, P.NI - 1);
         long long base = 0;
         if (FILL) base = slice_off[i >> 5] + (i & 31);
+        const int rc = P.NI * jc + P.NI * P.NJ * kc + x0;
+        if (FILL && nbr16) {
+            row_cell[i] = rc;
+            if (nc > 2) atomicOr(flag16, 1);
+        }
         for (int dz = -nc; dz <= nc; ++dz) {
             const int zz = kc + dz;
             if (zz < 0 || zz > P.NK - 1) continue;
@@ -427,11 +437,20 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
                 if (x0 > x1) continue;
                 const int kb = P.NI * yy + P.NI * P.NJ * zz;
                 const int s = cs[kb + x0], e = cs[kb + x1 + 1];
+                const int s16 = (FILL && nbr16) ? cs[plane_cell(rc, dz, P.NI, P.NI * P.NJ, P.num_cells + 1)] : 0;
                 for (int j = s; j < e; ++j) {
                     const float4 xj = pf[j];
                     const float r = dist_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z);
                     if (r < __fmul_rn(P.skappa, fmaxf(xi.w, xj.w))) {
-                        if (FILL) nbr[base + (long long)cnt * 32] = j;
+                        if (FILL) {
+                            nbr[base + (long long)cnt * 32] = j;
+                            if (nbr16) {
+                                const int off = j - s16;
+                                if (off < 0 || off > (int)kCodeMask) atomicOr(flag16, 2);
+                                nbr16[sell4(slice_off[i >> 5], i & 31, cnt)] =
+                                    (uint16_t)(((unsigned)(dz + 2) << kCodeShift) | ((unsigned)off & kCodeMask));
+                            }
+                        }
                         ++cnt;
                     }
                 }
@@ -441,7 +460,8 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
     if (!FILL) ncnt[i] = cnt;
 }
 
-// slice width (max count of the 32 particles of a slice) * 32
+// slice width (max count of the 32 particles of a slice, rounded up to a
+// multiple of four) * 32
 __global__ void k_slice_width(const int *ncnt, long long *w, int n, int nslices) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslices) return;
@@ -450,7 +470,7 @@ __global__ void k_slice_width(const int *ncnt, long long *w, int n, int nslices)
         const int i = s * 32 + l;
         if (i < n) m = max(m, ncnt[i]);
     }
-    w[s] = (long long)m * 32;
+    w[s] = (long long)((m + 3) & ~3) * 32;   // a multiple of four entries per row (sell4)
 }
 
 // ---------------------------------------------------------------------------
@@ -1090,7 +1110,8 @@ int nnps_build(Ctx<Real> &c) {
     SPH_TRY(regather(c, c.rho_ref_A, scratch));
 
     // neighbour lists: count, slice widths, offsets, fill
-    k_list<false><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, nullptr, nullptr, n);
+    k_list<false><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, nullptr, nullptr,
+                                                    nullptr, nullptr, nullptr, n);
     const int nslices = (n + 31) / 32;
     long long *w = (long long *)scratch;
     k_slice_width<<<grid_for(nslices, 256), 256, 0, st>>>(c.ncnt, w, n, nslices);
@@ -1102,15 +1123,28 @@ int nnps_build(Ctx<Real> &c) {
     SPH_CUDA_TRY(cudaMemcpyAsync(&total, c.slice_off + nslices, sizeof(long long), cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
     c.nnz_padded = total;
-    if (c.nbr && c.nbr_cap < total) c.release(c.nbr);
+    if (c.nbr && c.nbr_cap < total) { c.release(c.nbr); c.release(c.nbr16); }
+    const bool want16 = c.prm.ppe_wide_index == 0;
+    if (!want16) c.release(c.nbr16);
     if (!c.nbr) { SPH_TRY(c.alloc(c.nbr, (size_t)std::max(total, 1LL))); c.nbr_cap = std::max(total, 1LL); }
-    k_list<true><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, c.slice_off, c.nbr, n);
+    if (want16 && !c.nbr16) SPH_TRY(c.alloc(c.nbr16, (size_t)c.nbr_cap));
+    if (want16 && c.row_cell_cap < n) {
+        c.release(c.row_cell);
+        SPH_TRY(c.alloc(c.row_cell, (size_t)std::max(n, 1)));
+        c.row_cell_cap = std::max(n, 1);
+    }
+    SPH_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+    k_list<true><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, c.slice_off, c.nbr,
+                                                   want16 ? c.nbr16 : nullptr, c.row_cell, err, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     {
         std::vector<int> hc(n);
+        int flag16 = 0;
         SPH_CUDA_TRY(cudaMemcpyAsync(hc.data(), c.ncnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+        SPH_CUDA_TRY(cudaMemcpyAsync(&flag16, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
+        c.list16 = want16 && flag16 == 0;
         long long s = 0;
         for (int v : hc) s += v;
         c.nnz = s;

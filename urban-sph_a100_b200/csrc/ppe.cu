@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(128) k_ppe_rows(DevParams P, const float4 *__r
         } else if (gb) {
             gb[e] = 0; gb[nnzp + e] = 0; gb[2 * nnzp + e] = 0;
         }
-        if (coef) coef[e] = (C)c;
+        if (coef) coef[sell4(slice_off[i >> 5], i & 31, k)] = (C)c;
     }
     b[i] = (bx + by + bz) / tdt;
     diag[i] = Aij;
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(128) k_ppe_sweep(const int4 *__restrict__ ty, 
     for (int k = 0; k < cnt; ++k) {
         const long long e = base + 32LL * k;
         const int j = __ldg(&nbr[e]);
-        s += (Real)coef[e] * (p[j] - p0[j]);
+        s += (Real)coef[sell4(slice_off[i >> 5], i & 31, k)] * (p[j] - p0[j]);
     }
     pout[i] = p0[i] + (b[i] + s) / diag[i];
 }
@@ -209,9 +209,39 @@ __global__ void __launch_bounds__(128) k_ppe_sweep(const int4 *__restrict__ ty, 
 // Neumann gathers run beside the bandwidth-bound SELL sweep.  Blocks
 // alternate Neumann / SELL while both kinds remain; the rest are of the
 // larger kind.
-template <class V, class C, class D, class W>
+//
+// The coefficients are read four entries at a time (sell4 layout): one
+// 16-byte load per four FP32 coefficients, then the four gathers, which
+// halves the load requests of the stream against one entry per load.
+// L16: the neighbours are 16-bit codes (cell plane dz of the entry, offset
+// from that plane's first reachable record; plane_cell in common.cuh), four
+// per 8-byte load, instead of 32-bit indices.  A row's five plane starts
+// come from the cell-start array (cache resident) once per row, and a
+// select chain picks one per entry.  Both forms visit the entries of the
+// 32-bit list in its order, so their sums are identical.
+template <class C>
+__device__ __forceinline__ void load_coef4(const C *p, C (&a)[4]);
+template <>
+__device__ __forceinline__ void load_coef4<float>(const float *p, float (&a)[4]) {
+    const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+    a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void load_coef4<double>(const double *p, double (&a)[4]) {
+    const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 w = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    a[0] = v.x; a[1] = v.y; a[2] = w.x; a[3] = w.y;
+}
+struct List16 {
+    const uint16_t *code;
+    const int *row_cell, *cs;
+    int NI, NINJ, cs_max;
+};
+
+template <class V, class C, class D, class W, bool L16>
 __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, const int *__restrict__ kind,
-                                                    const int *__restrict__ aux, LIST_ARGS, const C *__restrict__ coef,
+                                                    const int *__restrict__ aux, LIST_ARGS, List16 l16,
+                                                    const C *__restrict__ coef,
                                                     const D *__restrict__ diag, const int *__restrict__ comp_id,
                                                     const double *__restrict__ cmean, const int *__restrict__ nm_rows,
                                                     const int *__restrict__ nm_off, const int *__restrict__ nm_nb,
@@ -245,12 +275,42 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
     const V xi = x[i];
     V yi = xi;   // identity / pinned
     if (kd == 1) {
-        const long long base = slice_off[i >> 5] + (i & 31);
+        const long long sb = slice_off[i >> 5];
+        const int lane = i & 31;
         const int cnt = ncnt[i];
         V s = 0;
-        for (int k = 0; k < cnt; ++k) {
-            const long long e = base + 32LL * k;
-            s += (V)coef[e] * (xi - x[__ldg(&nbr[e])]);   // difference form, as k_spmv
+        int b0 = 0, b1 = 0, b2 = 0, b3 = 0, b4 = 0;
+        if (L16) {
+            const int rc = l16.row_cell[i];
+            auto start = [&](int dz) { return __ldg(&l16.cs[plane_cell(rc, dz, l16.NI, l16.NINJ, l16.cs_max)]); };
+            b0 = start(-2); b1 = start(-1); b2 = start(0); b3 = start(1); b4 = start(2);
+        }
+        for (int k = 0; k < cnt; k += 4) {
+            const long long e4 = sell4(sb, lane, k);
+            C a[4];
+            load_coef4<C>(coef + e4, a);
+            int j[4];
+            if (L16) {
+                const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(l16.code + e4));
+                const unsigned cc[4] = {q.x & 0xffffu, q.x >> 16, q.y & 0xffffu, q.y >> 16};
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const unsigned r = cc[t] >> kCodeShift;
+                    int b = b0;
+                    b = r == 1 ? b1 : b; b = r == 2 ? b2 : b; b = r == 3 ? b3 : b; b = r == 4 ? b4 : b;
+                    j[t] = b + (int)(cc[t] & kCodeMask);
+                }
+            } else {
+                const long long e = sb + lane + 32LL * k;
+#pragma unroll
+                for (int t = 0; t < 4; ++t) j[t] = (k + t < cnt) ? __ldg(&nbr[e + 32 * t]) : 0;
+            }
+            V xj[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) xj[t] = (k + t < cnt) ? x[j[t]] : xi;
+#pragma unroll
+            for (int t = 0; t < 4; ++t)   // difference form, entries in list order
+                if (k + t < cnt) s += (V)a[t] * (xi - xj[t]);
         }
         yi = s;
         if (comp_id) {
@@ -593,18 +653,25 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
         // FP32 Neumann weights in the FP32 applications of the mixed form; the
         // FP64 applications (true residuals) keep the FP64 weights
         const int nb_nm = div_up((long long)c.L.n_nm, 4), nb_sell = div_up((long long)n, 128);
+        const List16 l16{c.nbr16, c.row_cell, c.cell_start, c.dp.NI, c.dp.NI * c.dp.NJ, c.num_cells + 1};
+#define SPMV_FUSED(C_, W_, COEF, NMW)                                                                              \
+    do {                                                                                                       \
+        if (c.list16)                                                                                          \
+            k_spmv_fused<V, C_, Real, W_, true><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                        \
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, c.diag, cid, cmean, \
+                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                                   \
+        else                                                                                                   \
+            k_spmv_fused<V, C_, Real, W_, false><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                       \
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, c.diag, cid, cmean, \
+                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                                   \
+    } while (0)
         if (sizeof(Real) == 4 && sizeof(V) == 4)
-            k_spmv_fused<V, float, Real, float><<<nb_nm + nb_sell, 128, 0, c.stream>>>(
-                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, (const float *)c.coef, c.diag, cid, cmean,
-                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.L.n_nm, x, y, n);
+            SPMV_FUSED(float, float, (const float *)c.coef, c.nm_owf);
         else if (sizeof(Real) == 4)
-            k_spmv_fused<V, float, Real, double><<<nb_nm + nb_sell, 128, 0, c.stream>>>(
-                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, (const float *)c.coef, c.diag, cid, cmean,
-                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow, c.L.n_nm, x, y, n);
+            SPMV_FUSED(float, double, (const float *)c.coef, c.nm_ow);
         else
-            k_spmv_fused<V, double, Real, double><<<nb_nm + nb_sell, 128, 0, c.stream>>>(
-                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef_d, c.diag, cid, cmean,
-                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_ow, c.L.n_nm, x, y, n);
+            SPMV_FUSED(double, double, c.coef_d, c.nm_ow);
+#undef SPMV_FUSED
     } else {
         k_spmv_mf<Real, V><<<grid_for(n, 128), 128, 0, c.stream>>>(c.dp, c.row_kind, c.row_aux, c.pr, c.mr, c.jc, c.slice_off,
                                                                   c.ncnt, c.nbr, c.g6, c.diag, cid, cmean, x, y, n);
@@ -662,15 +729,19 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
     if (bytes) {
         // per row: kind and list length (4 + 4) + x_i + y_i (Real), with the
         // rank-one term also component id (4) + A_i (Real); per slice of 32
-        // rows its offset (8); per stored entry: index (4) + coefficient
-        // (float in the mixed form, double in the FP64 form).  The Neumann
-        // rows of the same launch: row index and offset (4 + 4) + x_i + y_i,
-        // per entry index (4) + weight (Real).  The gathers x_j are not
-        // counted: an ideal kernel serves them from L2.
+        // rows its offset (8); per stored entry: index (4, or 2 for the
+        // 16-bit codes, which add the row's cell (4) per row and the cell
+        // starts once) + coefficient (float in the mixed form, double in
+        // the FP64 form).  The Neumann rows of the same launch: row index
+        // and offset (4 + 4) + x_i + y_i, per entry index (4) + weight
+        // (Real).  The gathers x_j are not counted: an ideal kernel serves
+        // them from L2.
         const double R = (double)sizeof(Real);
-        double row = 8.0 + 2.0 * R;
+        const bool l16 = c.list16 && c.prm.ppe_matrix_free == 0;
+        double row = 8.0 + 2.0 * R + (l16 ? 4.0 : 0.0);
         if (c.n_comp > 0) row += 4.0 + R;
-        *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + (double)c.nnz * (4.0 + R);
+        *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + (double)c.nnz * ((l16 ? 2.0 : 4.0) + R);
+        if (l16) *bytes += 4.0 * ((double)c.num_cells + 2.0);
         if (c.prm.ppe_matrix_free == 0)
             *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R) + (double)c.L.nm_nnz * (4.0 + R);
     }
@@ -835,9 +906,10 @@ static std::vector<uintptr_t> krylov_graph_key(Ctx<Real> &c, float *const *ws, c
     for (int q = 0; q < 9; ++q) k.push_back((uintptr_t)ws[q]);
     const void *ptrs[] = {xlo, c.scal, c.red, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, c.diag,
                           c.comp_id, c.comp_inv, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.cg_off, c.cg_rows,
-                          c.cg_s, c.cg_y, c.cg_invf, c.cg_agg};
+                          c.cg_s, c.cg_y, c.cg_invf, c.cg_agg, c.nbr16, c.row_cell, c.cell_start};
     for (const void *q : ptrs) k.push_back((uintptr_t)q);
-    const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode, c.prof ? 1 : 0};
+    const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode, c.prof ? 1 : 0, c.list16 ? 1 : 0,
+                               c.num_cells};
     for (long long q : sizes) k.push_back((uintptr_t)q);
     return k;
 }
