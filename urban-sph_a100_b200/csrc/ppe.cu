@@ -238,6 +238,38 @@ struct List16 {
     int NI, NINJ, cs_max;
 };
 
+// one group of four entries of a row: the coefficients in one load, the
+// neighbours from four 16-bit codes (plane starts in the thread's column of
+// the shared table) or from the 32-bit list; GUARD only for the row's last,
+// partly filled group
+template <bool L16, bool GUARD, class V, class C>
+__device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane, const C *__restrict__ coef,
+                                          const uint16_t *__restrict__ code, const int *__restrict__ nbr,
+                                          const int *plane_start, const V *__restrict__ x, V xi, V &s) {
+    const long long e4 = sell4(sb, lane, k);
+    C a[4];
+    load_coef4<C>(coef + e4, a);
+    int j[4];
+    if (L16) {
+        const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(code + e4));
+        const unsigned cc[4] = {q.x & 0xffffu, q.x >> 16, q.y & 0xffffu, q.y >> 16};
+        // the padding entries of a last group hold no code: not decoded
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            j[t] = (!GUARD || k + t < cnt) ? plane_start[128 * (cc[t] >> kCodeShift)] + (int)(cc[t] & kCodeMask) : 0;
+    } else {
+        const long long e = sb + lane + 32LL * k;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) j[t] = (!GUARD || k + t < cnt) ? __ldg(&nbr[e + 32 * t]) : 0;
+    }
+    V xj[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) xj[t] = (!GUARD || k + t < cnt) ? x[j[t]] : xi;
+#pragma unroll
+    for (int t = 0; t < 4; ++t)   // difference form, entries in list order
+        if (!GUARD || k + t < cnt) s += (V)a[t] * (xi - xj[t]);
+}
+
 template <class V, class C, class D, class W, bool L16>
 __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, const int *__restrict__ kind,
                                                     const int *__restrict__ aux, LIST_ARGS, List16 l16,
@@ -279,39 +311,20 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         const int lane = i & 31;
         const int cnt = ncnt[i];
         V s = 0;
-        int b0 = 0, b1 = 0, b2 = 0, b3 = 0, b4 = 0;
+        // the row's five plane starts, in this thread's column (no other
+        // thread reads it, so no barrier)
+        __shared__ int plane_tab[5 * 128];
+        int *ps = plane_tab + threadIdx.x;
         if (L16) {
             const int rc = l16.row_cell[i];
-            auto start = [&](int dz) { return __ldg(&l16.cs[plane_cell(rc, dz, l16.NI, l16.NINJ, l16.cs_max)]); };
-            b0 = start(-2); b1 = start(-1); b2 = start(0); b3 = start(1); b4 = start(2);
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+                ps[128 * q] = __ldg(&l16.cs[plane_cell(rc, q - 2, l16.NI, l16.NINJ, l16.cs_max)]);
         }
-        for (int k = 0; k < cnt; k += 4) {
-            const long long e4 = sell4(sb, lane, k);
-            C a[4];
-            load_coef4<C>(coef + e4, a);
-            int j[4];
-            if (L16) {
-                const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(l16.code + e4));
-                const unsigned cc[4] = {q.x & 0xffffu, q.x >> 16, q.y & 0xffffu, q.y >> 16};
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    const unsigned r = cc[t] >> kCodeShift;
-                    int b = b0;
-                    b = r == 1 ? b1 : b; b = r == 2 ? b2 : b; b = r == 3 ? b3 : b; b = r == 4 ? b4 : b;
-                    j[t] = b + (int)(cc[t] & kCodeMask);
-                }
-            } else {
-                const long long e = sb + lane + 32LL * k;
-#pragma unroll
-                for (int t = 0; t < 4; ++t) j[t] = (k + t < cnt) ? __ldg(&nbr[e + 32 * t]) : 0;
-            }
-            V xj[4];
-#pragma unroll
-            for (int t = 0; t < 4; ++t) xj[t] = (k + t < cnt) ? x[j[t]] : xi;
-#pragma unroll
-            for (int t = 0; t < 4; ++t)   // difference form, entries in list order
-                if (k + t < cnt) s += (V)a[t] * (xi - xj[t]);
-        }
+        const int full = cnt & ~3;
+        int k = 0;
+        for (; k < full; k += 4) quad_step<L16, false, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s);
+        if (k < cnt) quad_step<L16, true, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s);
         yi = s;
         if (comp_id) {
             const int cc = comp_id[i];
