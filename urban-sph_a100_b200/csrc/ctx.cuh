@@ -156,6 +156,12 @@ struct Ctx {
     bool coef_valid = false;
     Real *ppe_gb = nullptr;       // cached rhs pair vectors g_ij (3 x SELL arrays)
     Real *vis_stage = nullptr;    // staging of the LES viscosity in the prep pass
+    // time-invariant parts of the prep pass (particles never move): per row
+    // the filter sum and the LES length sum, per pair the strain weights
+    // V_j G_i grad W_ij (three SELL arrays); rebuilt with the lists or g6
+    Real *prep_row = nullptr, *prep_w = nullptr;
+    long long prep_cap = 0;
+    bool prep_valid = false;
     double *ib_boxes = nullptr;   // obstacle boxes for the IB normals (NULL: params.ib_box)
     int n_ib_boxes = 0;
     // Krylov workspace

@@ -235,6 +235,7 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     c.uploaded = true;
     c.built = false;
     c.gc_valid = false;
+    c.prep_valid = false;
     c.coef_valid = false;
     return SPH_OK;
 }
@@ -1154,6 +1155,7 @@ int nnps_build(Ctx<Real> &c) {
     c.release(scr);
     c.built = true;
     c.gc_valid = false;
+    c.prep_valid = false;
     c.coef_valid = false;
     return SPH_OK;
 }

@@ -141,15 +141,21 @@ __global__ void __launch_bounds__(128) k_grad_corr(DevParams P, SoA<Real> s, LIS
 
 // ---------------------------------------------------------------------------
 // KERNEL_clc_prep3D, functions_PREP.cuh:287-488 (Shepard filter, strain rate,
-// SSM / DDF sub-grid viscosity, reference density)
-// Algorithmic flops per pair with a fluid neighbour (Wendland-6, filter and
-// LES on; +, -, *, / and sqrt counted 1 each from the loop below): ~110.
+// SSM / DDF sub-grid viscosity, reference density), in two parts.
+// Particles never move, so the filter sum sum V_j W_ij, the LES length sum
+// sum r^2 W_ij V_j and the strain weights V_j G_i grad W_ij of every pair
+// are the same at every step (G_i = g6 while it is not recomputed):
+// k_prep_cache computes them once per neighbour build (the reference's
+// radius test against kappa h_i, fluid neighbours for the strain), and
+// k_prep_cached evaluates the step's part, the strain rate from the
+// velocities: 12 bytes of stored weights and ~15 flops per pair instead of
+// ~110 flops.  The sums are those of the reference up to the order of two
+// FP multiplications per pair (V_j (u_ji . G grad W) as (u_ji . V_j G grad W)).
 // ---------------------------------------------------------------------------
 template <class Real>
-__global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ g6,
-                                              const typename V4<Real>::type *__restrict__ u, Real *__restrict__ flt,
-                                              Real *__restrict__ vis_out, Real *__restrict__ kt, Real *__restrict__ et,
-                                              Real *__restrict__ SR, Real *__restrict__ rho_ref, int tcount, Real tdt, int n) {
+__global__ void __launch_bounds__(128) k_prep_cache(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ g6,
+                                                    Real *__restrict__ prow, Real *__restrict__ pw, long long nnzp,
+                                                    int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 ti = s.ty[i];
@@ -157,49 +163,73 @@ __global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARG
     const size_t N = (size_t)n;
     const float4 fi = s.pf[i];
     const auto xi = s.pr[i];
-    const auto ui = u[i];
-    const auto mri = s.mr[i];
     const Real gc11 = g6[i], gc22 = g6[N + i], gc33 = g6[2 * N + i], gc12 = g6[3 * N + i], gc23 = g6[4 * N + i], gc31 = g6[5 * N + i];
     const Real hi = xi.w;
     const Real tA = calc_tmpA<Real>(P, hi);
-    const bool filt = (tcount % P.freq_filt) == 0;
-    const bool les = P.fv_solve != 0 && P.turb != 0;
     Real tmp_flt = 0, tmp_sigma = 0;
-    Real st11 = 0, st12 = 0, st22 = 0, st23 = 0, st31 = 0, st33 = 0;
     SELL_LOOP_BEGIN(i)
+        const long long e = sbase_ + 32LL * k_;
+        Real wx = 0, wy = 0, wz = 0;
         const float4 fj = s.pf[j];
-        if (!within_hi(P, fi, fj)) continue;
-        const auto xj = s.pr[j];
-        const auto mj = s.mr[j];
-        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
-        const Real w = calc_wij<Real>(P, tA, hi, tdist);
-        const Real vj = mj.x / mj.y;
-        if (filt) tmp_flt += vj * w;
-        if (les) {
+        if (within_hi(P, fi, fj)) {
+            const auto xj = s.pr[j];
+            const auto mj = s.mr[j];
+            const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+            const Real w = calc_wij<Real>(P, tA, hi, tdist);
+            const Real vj = mj.x / mj.y;
+            tmp_flt += vj * w;
             tmp_sigma += tdist * tdist * w * vj;
             if (s.jc[j] & JB_PT1) {
                 const Real dwi = calc_dwij<Real>(P, tA, hi, tdist) / tdist;
                 const Real tdwx = dwi * dx, tdwy = dwi * dy, tdwz = dwi * dz;
-                const Real cx = gc11 * tdwx + gc12 * tdwy + gc31 * tdwz;
-                const Real cy = gc12 * tdwx + gc22 * tdwy + gc23 * tdwz;
-                const Real cz = gc31 * tdwx + gc23 * tdwy + gc33 * tdwz;
-                const auto uj = u[j];
-                const Real ux = uj.x - ui.x, uy = uj.y - ui.y, uz = uj.z - ui.z;
-                st11 += vj * ux * cx;
-                st12 += (Real)0.5 * vj * (ux * cy + uy * cx);
-                st22 += vj * uy * cy;
-                st23 += (Real)0.5 * vj * (uy * cz + uz * cy);
-                st31 += (Real)0.5 * vj * (ux * cz + uz * cx);
-                st33 += vj * uz * cz;
+                wx = vj * (gc11 * tdwx + gc12 * tdwy + gc31 * tdwz);
+                wy = vj * (gc12 * tdwx + gc22 * tdwy + gc23 * tdwz);
+                wz = vj * (gc31 * tdwx + gc23 * tdwy + gc33 * tdwz);
             }
         }
+        pw[e] = wx; pw[nnzp + e] = wy; pw[2 * nnzp + e] = wz;
     SELL_LOOP_END
+    prow[i] = tmp_flt;
+    prow[N + i] = tmp_sigma;
+}
+
+template <class Real>
+__global__ void __launch_bounds__(128) k_prep_cached(DevParams P, const int4 *__restrict__ ty, LIST_ARGS,
+                                                     const Real *__restrict__ prow, const Real *__restrict__ pw,
+                                                     long long nnzp, const typename V4<Real>::type *__restrict__ u,
+                                                     const typename V2<Real>::type *__restrict__ mr,
+                                                     const typename V4<Real>::type *__restrict__ pr,
+                                                     Real *__restrict__ flt, Real *__restrict__ vis_out,
+                                                     Real *__restrict__ kt, Real *__restrict__ et, Real *__restrict__ SR,
+                                                     Real *__restrict__ rho_ref, int tcount, Real tdt, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
+    const size_t N = (size_t)n;
+    const bool filt = (tcount % P.freq_filt) == 0;
+    const bool les = P.fv_solve != 0 && P.turb != 0;
     if (les) {
+        const auto ui = u[i];
+        const Real hi = pr[i].w;
+        Real st11 = 0, st12 = 0, st22 = 0, st23 = 0, st31 = 0, st33 = 0;
+        SELL_LOOP_BEGIN(i)
+            const long long e = sbase_ + 32LL * k_;
+            const Real cx = __ldcs(&pw[e]), cy = __ldcs(&pw[nnzp + e]), cz = __ldcs(&pw[2 * nnzp + e]);
+            const auto uj = u[j];
+            const Real ux = uj.x - ui.x, uy = uj.y - ui.y, uz = uj.z - ui.z;
+            st11 += ux * cx;
+            st12 += (Real)0.5 * (ux * cy + uy * cx);
+            st22 += uy * cy;
+            st23 += (Real)0.5 * (uy * cz + uz * cy);
+            st31 += (Real)0.5 * (ux * cz + uz * cx);
+            st33 += uz * cz;
+        SELL_LOOP_END
         Real tmp_SR = 2 * (st11 * st11 + st22 * st22 + st33 * st33 + 2 * st12 * st12 + 2 * st31 * st31 + 2 * st23 * st23);
         tmp_SR = sqrt(tmp_SR);
         SR[i] = tmp_SR;
-        tmp_sigma = sqrt((Real)0.3333 * tmp_sigma);
+        const Real tmp_sigma = sqrt((Real)0.3333 * prow[N + i]);
         const Real cl = (tmp_sigma > hi) ? tmp_sigma : hi;
         const int bt = ti.y;
         if (P.turb == 4) {
@@ -207,7 +237,7 @@ __global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARG
             if (bt != 1) vis_out[i] = v;
         } else if (P.turb == 5) {
             Real ki = kt[i] > 0 ? kt[i] : (Real)0;
-            const Real nui = u[i].w;
+            const Real nui = ui.w;
             const Real pp = nui * tmp_SR * tmp_SR;
             const Real eps = (Real)0.93 * ki * sqrt(ki) / cl;     // Ce_sgs, Parameters.cuh:133
             ki += (pp - eps) * tdt;
@@ -216,8 +246,8 @@ __global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARG
             if (bt != 1) { vis_out[i] = v; kt[i] = ki; et[i] = eps; }
         }
     }
-    if (tcount == 0) rho_ref[i] = mri.y;
-    if (filt) flt[i] = tmp_flt;
+    if (tcount == 0) rho_ref[i] = mr[i].y;
+    if (filt) flt[i] = prow[i];
 }
 
 // vis_t lives in u.w; the LES result is staged and merged so that neighbours
@@ -978,6 +1008,7 @@ int gradient_correction(Ctx<Real> &c) {
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     c.gc_valid = true;
+    c.prep_valid = false;   // the strain weights hold G_i
     return SPH_OK;
 }
 
@@ -1082,8 +1113,23 @@ int phase_interaction(Ctx<Real> &c) {
     // prep / LES
     if (!c.vis_stage) SPH_TRY(c.alloc(c.vis_stage, n));
     Real *vis_stage = c.vis_stage;   // LES viscosity staged until every row has read the old one
-    k_prep<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
-                                                   c.S.et, c.SR, c.rho_ref_S, tc, tdt, n);
+    if (!c.prep_valid) {
+        const long long nnzp = c.nnz_padded;
+        if (c.prep_cap < nnzp) {
+            c.release(c.prep_w);
+            SPH_TRY(c.alloc(c.prep_w, (size_t)(3 * nnzp)));
+            c.prep_cap = nnzp;
+        }
+        c.release(c.prep_row);
+        SPH_TRY(c.alloc(c.prep_row, 2 * (size_t)n));
+        SPH_CUDA_TRY(cudaMemsetAsync(c.prep_row, 0, sizeof(Real) * 2 * (size_t)n, st));
+        k_prep_cache<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.prep_row, c.prep_w, nnzp, n);
+        ++c.launches;
+        c.prep_valid = true;
+    }
+    k_prep_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, LIST(c), c.prep_row, c.prep_w, c.nnz_padded, c.S.u,
+                                                          c.mr, c.pr, c.S.flt, vis_stage, c.S.kt, c.S.et, c.SR,
+                                                          c.rho_ref_S, tc, tdt, n);
     ++c.launches;
     if (c.dp.fv_solve != 0 && (c.dp.turb == 4 || c.dp.turb == 5)) {
         k_merge_vis<Real><<<grid_for(n, 256), 256, 0, st>>>(c.S.u, vis_stage, c.ty, n);
