@@ -150,6 +150,7 @@ int apr_split(Ctx<Real> &c, int *n_split, int *n_wanted) {
         c.built = false;   // new particle set: NNPS and everything built on it again
         c.gc_valid = false;
         c.prep_valid = false;
+        c.pforce_valid = false;
         c.coef_valid = false;
         c.cg_valid = false;
         c.ml_have_prev = false;

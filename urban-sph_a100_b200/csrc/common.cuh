@@ -84,6 +84,14 @@ template <class T> struct V2;
 template <> struct V2<float> { typedef float2 type; };
 template <> struct V2<double> { typedef double2 type; };
 
+// streaming (evict-first) loads of a Real4 read once per pass
+__device__ __forceinline__ float4 ld_stream(const float4 *p) { return __ldcs(p); }
+__device__ __forceinline__ double4 ld_stream(const double4 *p) {
+    const double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
 template <class T> __host__ __device__ inline typename V4<T>::type mk4(T a, T b, T c, T d) {
     typename V4<T>::type v; v.x = a; v.y = b; v.z = c; v.w = d; return v;
 }

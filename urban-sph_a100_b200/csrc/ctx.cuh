@@ -162,6 +162,10 @@ struct Ctx {
     Real *prep_row = nullptr, *prep_w = nullptr;
     long long prep_cap = 0;
     bool prep_valid = false;
+    // time-invariant part of the pressure force per pair: g_ij (3) and rho_j
+    typename V4<Real>::type *pforce_w = nullptr;
+    long long pforce_cap = 0;
+    bool pforce_valid = false;
     double *ib_boxes = nullptr;   // obstacle boxes for the IB normals (NULL: params.ib_box)
     int n_ib_boxes = 0;
     // Krylov workspace

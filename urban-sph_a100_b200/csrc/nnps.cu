@@ -236,6 +236,7 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     c.built = false;
     c.gc_valid = false;
     c.prep_valid = false;
+    c.pforce_valid = false;
     c.coef_valid = false;
     return SPH_OK;
 }
@@ -1156,6 +1157,7 @@ int nnps_build(Ctx<Real> &c) {
     c.built = true;
     c.gc_valid = false;
     c.prep_valid = false;
+    c.pforce_valid = false;
     c.coef_valid = false;
     return SPH_OK;
 }

@@ -771,39 +771,64 @@ __global__ void k_copy_rows(const int *rows, int nrows, const typename V4<Real>:
 }
 
 // ---------------------------------------------------------------------------
-// KERNEL_pressureforce3D, functions_PPE.cuh:482-647 (h_ij = (h_i+h_j)/2);
-// ~50 flops per pair (counted as for k_prep)
+// KERNEL_pressureforce3D, functions_PPE.cuh:482-647 (h_ij = (h_i+h_j)/2), in
+// two parts.  The pair term is -2 m_j (p_i rho_j + p_j rho_i) /
+// ((rho_i rho_j)(rho_i + rho_j)) dW(r, h_ij) / r x_ij; everything but the
+// pressures is fixed while particles do not move, so k_pforce_cache stores
+// g_ij = -2 m_j / ((rho_i rho_j)(rho_i + rho_j)) dW / r x_ij and rho_j per
+// pair (one Real4, zero for markers and with the gradient correction's
+// dW = 0) once per neighbour build, and k_pressure_force_cached sums
+// (p_i rho_j + p_j rho_i) g_ij: one Real4 and the p_j gathers per pair
+// instead of ~50 flops.  Same sums up to the grouping of the products.
 // ---------------------------------------------------------------------------
 template <class Real>
-__global__ void __launch_bounds__(128) k_pressure_force(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ p,
-                                                        const Real *__restrict__ pres0,
-                                                        typename V4<Real>::type *__restrict__ fp, int n) {
+__global__ void __launch_bounds__(128) k_pforce_cache(DevParams P, SoA<Real> s, LIST_ARGS,
+                                                      typename V4<Real>::type *__restrict__ pw, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 ti = s.ty[i];
     if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0 || ti.y != 0) return;
     const auto xi = s.pr[i];
-    const auto mri = s.mr[i];
-    const Real hi = xi.w, rhoi = mri.y, pi = p[i] - pres0[i];
+    const Real hi = xi.w, rhoi = s.mr[i].y;
     const bool kgc = P.kgc_solve == 1;
-    const bool uniform_hint = true;
-    Real tA_ii = calc_tmpA<Real>(P, hi);
-    Real tx = 0, ty_ = 0, tz = 0;
-    if (P.fp_solve) {
-        SELL_LOOP_BEGIN(i)
-            if (!(s.jc[j] & JB_LT1000)) continue;
+    const Real tA_ii = calc_tmpA<Real>(P, hi);
+    SELL_LOOP_BEGIN(i)
+        const long long e = sbase_ + 32LL * k_;
+        const auto mj = s.mr[j];
+        Real gx = 0, gy = 0, gz = 0;
+        if (s.jc[j] & JB_LT1000) {
             const auto xj = s.pr[j];
             const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
             const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
             const Real hij = (Real)0.5 * (hi + xj.w);
-            const Real tA = (uniform_hint && xj.w == hi) ? tA_ii : calc_tmpA<Real>(P, hij);
+            const Real tA = (xj.w == hi) ? tA_ii : calc_tmpA<Real>(P, hij);
             Real dw = calc_dwij<Real>(P, tA, hij, tdist);
             if (kgc) dw = 0;
-            const auto mj = s.mr[j];
+            const Real c = (Real)-2 * mj.x / ((rhoi * mj.y) * (rhoi + mj.y)) * dw / tdist;
+            gx = c * dx; gy = c * dy; gz = c * dz;
+        }
+        pw[e] = mk4<Real>(gx, gy, gz, mj.y);
+    SELL_LOOP_END
+}
+
+template <class Real>
+__global__ void __launch_bounds__(128) k_pressure_force_cached(DevParams P, const int4 *__restrict__ ty,
+                                                               const typename V2<Real>::type *__restrict__ mr, LIST_ARGS,
+                                                               const typename V4<Real>::type *__restrict__ pw,
+                                                               const Real *__restrict__ p, const Real *__restrict__ pres0,
+                                                               typename V4<Real>::type *__restrict__ fp, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0 || ti.y != 0) return;
+    const Real rhoi = mr[i].y, pi = p[i] - pres0[i];
+    Real tx = 0, ty_ = 0, tz = 0;
+    if (P.fp_solve) {
+        SELL_LOOP_BEGIN(i)
+            const auto g = ld_stream(&pw[sbase_ + 32LL * k_]);
             const Real pj = p[j] - pres0[j];
-            const Real Cp = (Real)-2 * mj.x * (pi * mj.y + pj * rhoi) / ((rhoi * mj.y) * (rhoi + mj.y));
-            const Real f = Cp * dw / tdist;
-            tx += f * dx; ty_ += f * dy; tz += f * dz;
+            const Real c = pi * g.w + pj * rhoi;
+            tx += c * g.x; ty_ += c * g.y; tz += c * g.z;
         SELL_LOOP_END
     }
     fp[i] = mk4<Real>(tx, ty_, tz, 0);
@@ -1175,7 +1200,19 @@ int phase_time_update(Ctx<Real> &c) {
     cudaStream_t st = c.stream;
     const int n = c.n;
     const Real tdt = (Real)c.dp.dt;
-    k_pressure_force<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.p, c.pres0, c.fp, n);
+    if (!c.pforce_valid) {
+        const long long nnzp = c.nnz_padded;
+        if (c.pforce_cap < nnzp) {
+            c.release(c.pforce_w);
+            SPH_TRY(c.alloc(c.pforce_w, (size_t)nnzp));
+            c.pforce_cap = nnzp;
+        }
+        k_pforce_cache<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.pforce_w, n);
+        ++c.launches;
+        c.pforce_valid = true;
+    }
+    k_pressure_force_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, c.mr, LIST(c), c.pforce_w, c.S.p,
+                                                                    c.pres0, c.fp, n);
     ++c.launches;
     if (c.L.n_mk > 0) {
         k_ibm_force<Real><<<grid_for(c.L.n_mk, 128), 128, 0, st>>>(c.dp, soa(c), c.L.mk_rows, c.L.mk_off, c.L.mk_nbr,
