@@ -207,7 +207,13 @@ typedef struct sph_params {
                                 and every offset is below 8192 -- same
                                 entries, same order, same results, fewer
                                 bytes                                         */
-    int32_t reserved[3];
+    int32_t recompute_pairs; /* 1: the prep pass and the pressure force evaluate
+                                their pair terms every step, as the reference
+                                does; 0 (default): their time-invariant pair
+                                factors are stored at the neighbour build (the
+                                particles never move) when they fit with a
+                                tenth of the device memory to spare          */
+    int32_t reserved[2];
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

@@ -182,3 +182,35 @@ def test_dormant_boundary_passes_match_oracle(name, precision, tol):
     if p.inlet_recycling:
         inlet = B["buffer_type"] == 1
         assert np.abs(B["ux"][inlet]).max() > 0
+
+
+@pytest.mark.parametrize("precision,tol", [(layout.PREC_MIXED, FP32_TOL), (layout.PREC_FP64, FP64_TOL)],
+                         ids=["fp32", "fp64"])
+def test_stored_pair_factors_match_full_evaluation(precision, tol):
+    """The prep pass and the pressure force with their time-invariant pair
+    factors stored at the neighbour build (default) against the same passes
+    evaluating every pair term each step (recompute_pairs = 1, the
+    reference's way), and switching between the two inside a run."""
+    P, p = decks.caseh_mini(turbulence="DDF", seed=5)
+    out = []
+    for rp in (0, 1):
+        q = p.copy()
+        q.ppe_mode = layout.PPE_REF_SWEEP
+        q.recompute_pairs = rp
+        sim = abi.Simulation(q, precision=precision)
+        sim.upload(P)
+        for _ in range(2):
+            sim.step(1)
+        q2 = q.copy()
+        q2.recompute_pairs = 1 - rp
+        sim.set_params(q2)
+        sim.step(1)
+        A, A2, A3 = sim.download()
+        sim.close()
+        out.append((A, A2, A3))
+    (A, A2, A3), (B, B2, B3) = out
+    for f in FIELDS:
+        assert rel_err(A[f], B[f]) <= tol, f
+    for f in ("fpx", "fpy", "fpz"):
+        assert rel_err(A3[f], B3[f]) <= stored_tol(B3[f], tol * 10), f
+    assert rel_err(A2["SR"], B2["SR"]) <= stored_tol(B2["SR"], tol * 10)

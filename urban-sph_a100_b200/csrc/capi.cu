@@ -268,6 +268,18 @@ int sph_set_params(sph_ctx *ctx, const sph_params *p) {
             return SPH_ERR_BAD_ARG;
         }
         const int recompute = (p->ppe_pin != c->prm.ppe_pin);
+        // the stored pair factors (correction matrix, pressure coefficients,
+        // prep and pressure-force factors) follow the kernel function and
+        // the pair forms
+        const sph_params &o = c->prm;
+        if (p->vii[SPH_VII_KERNEL_TYPE] != o.vii[SPH_VII_KERNEL_TYPE] || p->vif[SPH_VIF_KAPPA] != o.vif[SPH_VIF_KAPPA] ||
+            p->vii[SPH_VII_KGC_SOLVE] != o.vii[SPH_VII_KGC_SOLVE] || p->pressure_length != o.pressure_length ||
+            p->ppe_pair_h != o.ppe_pair_h || p->recompute_pairs != o.recompute_pairs) {
+            c->gc_valid = false;
+            c->coef_valid = false;
+            c->prep_valid = false;
+            c->pforce_valid = false;
+        }
         c->prm = *p;
         c->dp = make_dev_params(*p);
         if (recompute && c->built) return build_side_lists(*c);

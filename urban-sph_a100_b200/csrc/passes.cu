@@ -250,6 +250,83 @@ __global__ void __launch_bounds__(128) k_prep_cached(DevParams P, const int4 *__
     if (filt) flt[i] = prow[i];
 }
 
+// The prep pass evaluated in full every step: used when the device has no
+// room for the cached weights.
+template <class Real>
+__global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ g6,
+                                              const typename V4<Real>::type *__restrict__ u, Real *__restrict__ flt,
+                                              Real *__restrict__ vis_out, Real *__restrict__ kt, Real *__restrict__ et,
+                                              Real *__restrict__ SR, Real *__restrict__ rho_ref, int tcount, Real tdt, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
+    const size_t N = (size_t)n;
+    const float4 fi = s.pf[i];
+    const auto xi = s.pr[i];
+    const auto ui = u[i];
+    const auto mri = s.mr[i];
+    const Real gc11 = g6[i], gc22 = g6[N + i], gc33 = g6[2 * N + i], gc12 = g6[3 * N + i], gc23 = g6[4 * N + i], gc31 = g6[5 * N + i];
+    const Real hi = xi.w;
+    const Real tA = calc_tmpA<Real>(P, hi);
+    const bool filt = (tcount % P.freq_filt) == 0;
+    const bool les = P.fv_solve != 0 && P.turb != 0;
+    Real tmp_flt = 0, tmp_sigma = 0;
+    Real st11 = 0, st12 = 0, st22 = 0, st23 = 0, st31 = 0, st33 = 0;
+    SELL_LOOP_BEGIN(i)
+        const float4 fj = s.pf[j];
+        if (!within_hi(P, fi, fj)) continue;
+        const auto xj = s.pr[j];
+        const auto mj = s.mr[j];
+        const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+        const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) + (Real)1e-20;
+        const Real w = calc_wij<Real>(P, tA, hi, tdist);
+        const Real vj = mj.x / mj.y;
+        if (filt) tmp_flt += vj * w;
+        if (les) {
+            tmp_sigma += tdist * tdist * w * vj;
+            if (s.jc[j] & JB_PT1) {
+                const Real dwi = calc_dwij<Real>(P, tA, hi, tdist) / tdist;
+                const Real tdwx = dwi * dx, tdwy = dwi * dy, tdwz = dwi * dz;
+                const Real cx = gc11 * tdwx + gc12 * tdwy + gc31 * tdwz;
+                const Real cy = gc12 * tdwx + gc22 * tdwy + gc23 * tdwz;
+                const Real cz = gc31 * tdwx + gc23 * tdwy + gc33 * tdwz;
+                const auto uj = u[j];
+                const Real ux = uj.x - ui.x, uy = uj.y - ui.y, uz = uj.z - ui.z;
+                st11 += vj * ux * cx;
+                st12 += (Real)0.5 * vj * (ux * cy + uy * cx);
+                st22 += vj * uy * cy;
+                st23 += (Real)0.5 * vj * (uy * cz + uz * cy);
+                st31 += (Real)0.5 * vj * (ux * cz + uz * cx);
+                st33 += vj * uz * cz;
+            }
+        }
+    SELL_LOOP_END
+    if (les) {
+        Real tmp_SR = 2 * (st11 * st11 + st22 * st22 + st33 * st33 + 2 * st12 * st12 + 2 * st31 * st31 + 2 * st23 * st23);
+        tmp_SR = sqrt(tmp_SR);
+        SR[i] = tmp_SR;
+        tmp_sigma = sqrt((Real)0.3333 * tmp_sigma);
+        const Real cl = (tmp_sigma > hi) ? tmp_sigma : hi;
+        const int bt = ti.y;
+        if (P.turb == 4) {
+            const Real v = (Real)(P.cs_sgs * P.cs_sgs) * cl * cl * tmp_SR;
+            if (bt != 1) vis_out[i] = v;
+        } else if (P.turb == 5) {
+            Real ki = kt[i] > 0 ? kt[i] : (Real)0;
+            const Real nui = u[i].w;
+            const Real pp = nui * tmp_SR * tmp_SR;
+            const Real eps = (Real)0.93 * ki * sqrt(ki) / cl;     // Ce_sgs, Parameters.cuh:133
+            ki += (pp - eps) * tdt;
+            ki = (ki > (Real)1e-4) ? ki : (Real)1e-4;
+            const Real v = (Real)0.1 * cl * sqrt(ki);              // Ck_sgs, Parameters.cuh:132
+            if (bt != 1) { vis_out[i] = v; kt[i] = ki; et[i] = eps; }
+        }
+    }
+    if (tcount == 0) rho_ref[i] = mri.y;
+    if (filt) flt[i] = tmp_flt;
+}
+
 // vis_t lives in u.w; the LES result is staged and merged so that neighbours
 // read the step-start value (the reference reads nu_j only in the unused Tk term)
 template <class Real>
@@ -834,6 +911,43 @@ __global__ void __launch_bounds__(128) k_pressure_force_cached(DevParams P, cons
     fp[i] = mk4<Real>(tx, ty_, tz, 0);
 }
 
+// The pressure force evaluated in full every step: used when the device has
+// no room for the cached pair factors.
+template <class Real>
+__global__ void __launch_bounds__(128) k_pressure_force(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ p,
+                                                        const Real *__restrict__ pres0,
+                                                        typename V4<Real>::type *__restrict__ fp, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 ti = s.ty[i];
+    if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0 || ti.y != 0) return;
+    const auto xi = s.pr[i];
+    const auto mri = s.mr[i];
+    const Real hi = xi.w, rhoi = mri.y, pi = p[i] - pres0[i];
+    const bool kgc = P.kgc_solve == 1;
+    const bool uniform_hint = true;
+    Real tA_ii = calc_tmpA<Real>(P, hi);
+    Real tx = 0, ty_ = 0, tz = 0;
+    if (P.fp_solve) {
+        SELL_LOOP_BEGIN(i)
+            if (!(s.jc[j] & JB_LT1000)) continue;
+            const auto xj = s.pr[j];
+            const Real dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const Real tdist = sqrt(dx * dx + dy * dy + dz * dz) - (Real)1e-20;
+            const Real hij = (Real)0.5 * (hi + xj.w);
+            const Real tA = (uniform_hint && xj.w == hi) ? tA_ii : calc_tmpA<Real>(P, hij);
+            Real dw = calc_dwij<Real>(P, tA, hij, tdist);
+            if (kgc) dw = 0;
+            const auto mj = s.mr[j];
+            const Real pj = p[j] - pres0[j];
+            const Real Cp = (Real)-2 * mj.x * (pi * mj.y + pj * rhoi) / ((rhoi * mj.y) * (rhoi + mj.y));
+            const Real f = Cp * dw / tdist;
+            tx += f * dx; ty_ += f * dy; tz += f * dz;
+        SELL_LOOP_END
+    }
+    fp[i] = mk4<Real>(tx, ty_, tz, 0);
+}
+
 // ---------------------------------------------------------------------------
 // IBM_force_interpolation3D (functions_IBM.cuh:342-490) and
 // IBM_spreading_interpolation3D (functions_IBM.cuh:492-613)
@@ -1027,6 +1141,18 @@ static SoA<Real> soa(Ctx<Real> &c) {
 
 #define LIST(c) (c).slice_off, (c).ncnt, (c).nbr
 
+// whether `bytes` more of device memory leave a tenth of the device free
+// (the per-pair caches of the prep pass and the pressure force are an
+// optimisation: without room the passes evaluate their pair terms in full)
+static bool cache_fits(size_t bytes) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return bytes + tot / 10 <= fr;
+}
+
 template <class Real>
 int gradient_correction(Ctx<Real> &c) {
     k_grad_corr<Real><<<grid_for(c.n, 128), 128, 0, c.stream>>>(c.dp, soa(c), LIST(c), c.g6, c.n);
@@ -1142,19 +1268,29 @@ int phase_interaction(Ctx<Real> &c) {
         const long long nnzp = c.nnz_padded;
         if (c.prep_cap < nnzp) {
             c.release(c.prep_w);
-            SPH_TRY(c.alloc(c.prep_w, (size_t)(3 * nnzp)));
-            c.prep_cap = nnzp;
+            c.prep_cap = 0;
         }
         c.release(c.prep_row);
-        SPH_TRY(c.alloc(c.prep_row, 2 * (size_t)n));
-        SPH_CUDA_TRY(cudaMemsetAsync(c.prep_row, 0, sizeof(Real) * 2 * (size_t)n, st));
-        k_prep_cache<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.prep_row, c.prep_w, nnzp, n);
-        ++c.launches;
-        c.prep_valid = true;
+        const size_t need = (c.prep_w ? 0 : sizeof(Real) * 3 * (size_t)nnzp) + sizeof(Real) * 2 * (size_t)n;
+        if (!c.prm.recompute_pairs && cache_fits(need)) {
+            if (!c.prep_w) {
+                SPH_TRY(c.alloc(c.prep_w, (size_t)(3 * nnzp)));
+                c.prep_cap = nnzp;
+            }
+            SPH_TRY(c.alloc(c.prep_row, 2 * (size_t)n));
+            SPH_CUDA_TRY(cudaMemsetAsync(c.prep_row, 0, sizeof(Real) * 2 * (size_t)n, st));
+            k_prep_cache<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.prep_row, c.prep_w, nnzp, n);
+            ++c.launches;
+            c.prep_valid = true;
+        }
     }
-    k_prep_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, LIST(c), c.prep_row, c.prep_w, c.nnz_padded, c.S.u,
-                                                          c.mr, c.pr, c.S.flt, vis_stage, c.S.kt, c.S.et, c.SR,
-                                                          c.rho_ref_S, tc, tdt, n);
+    if (c.prep_valid)
+        k_prep_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, LIST(c), c.prep_row, c.prep_w, c.nnz_padded,
+                                                              c.S.u, c.mr, c.pr, c.S.flt, vis_stage, c.S.kt, c.S.et, c.SR,
+                                                              c.rho_ref_S, tc, tdt, n);
+    else
+        k_prep<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
+                                                       c.S.et, c.SR, c.rho_ref_S, tc, tdt, n);
     ++c.launches;
     if (c.dp.fv_solve != 0 && (c.dp.turb == 4 || c.dp.turb == 5)) {
         k_merge_vis<Real><<<grid_for(n, 256), 256, 0, st>>>(c.S.u, vis_stage, c.ty, n);
@@ -1204,15 +1340,23 @@ int phase_time_update(Ctx<Real> &c) {
         const long long nnzp = c.nnz_padded;
         if (c.pforce_cap < nnzp) {
             c.release(c.pforce_w);
-            SPH_TRY(c.alloc(c.pforce_w, (size_t)nnzp));
-            c.pforce_cap = nnzp;
+            c.pforce_cap = 0;
         }
-        k_pforce_cache<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.pforce_w, n);
-        ++c.launches;
-        c.pforce_valid = true;
+        if (!c.prm.recompute_pairs && (c.pforce_w || cache_fits(sizeof(typename V4<Real>::type) * (size_t)nnzp))) {
+            if (!c.pforce_w) {
+                SPH_TRY(c.alloc(c.pforce_w, (size_t)nnzp));
+                c.pforce_cap = nnzp;
+            }
+            k_pforce_cache<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.pforce_w, n);
+            ++c.launches;
+            c.pforce_valid = true;
+        }
     }
-    k_pressure_force_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, c.mr, LIST(c), c.pforce_w, c.S.p,
-                                                                    c.pres0, c.fp, n);
+    if (c.pforce_valid)
+        k_pressure_force_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, c.mr, LIST(c), c.pforce_w, c.S.p,
+                                                                        c.pres0, c.fp, n);
+    else
+        k_pressure_force<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.p, c.pres0, c.fp, n);
     ++c.launches;
     if (c.L.n_mk > 0) {
         k_ibm_force<Real><<<grid_for(c.L.n_mk, 128), 128, 0, st>>>(c.dp, soa(c), c.L.mk_rows, c.L.mk_off, c.L.mk_nbr,
