@@ -1147,6 +1147,11 @@ int nnps_build(Ctx<Real> &c) {
         SPH_CUDA_TRY(cudaMemcpyAsync(&flag16, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
         c.list16 = want16 && flag16 == 0;
+        if (!c.list16) {   // codes that cannot be used: their memory goes back
+            c.release(c.nbr16);
+            c.release(c.row_cell);
+            c.row_cell_cap = 0;
+        }
         long long s = 0;
         for (int v : hc) s += v;
         c.nnz = s;
