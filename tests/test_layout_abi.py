@@ -33,6 +33,18 @@ def test_header_struct_sizes(tmp_path):
     assert int(out[5]) == layout.SphParams.ppe_tol.offset
 
 
+def test_every_params_field_at_the_header_offset(tmp_path):
+    # the ctypes mirror and the C struct agree field by field, not only in size
+    names = [f for f, _ in layout.SphParams._fields_]
+    body = "".join('printf("%%zu\\n", offsetof(sph_params, %s));' % f for f in names)
+    src = tmp_path / "off.c"
+    src.write_text('#include "sph_isph.h"\n#include <stdio.h>\n#include <stddef.h>\nint main(){' + body + '}')
+    exe = tmp_path / "off"
+    subprocess.check_call(["gcc", "-I" + os.path.dirname(HEADER), str(src), "-o", str(exe)])
+    out = [int(v) for v in subprocess.check_output([str(exe)]).decode().split()]
+    assert out == [getattr(layout.SphParams, f).offset for f in names]
+
+
 def test_library_loads_and_exports_every_symbol():
     L = abi.lib()
     declared = set()
