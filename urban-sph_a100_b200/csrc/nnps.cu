@@ -629,8 +629,11 @@ static int null_components(Ctx<Real> &c, std::vector<int> &kind, const std::vect
             if (ty[i].y == 0) cand[lab[i]] = std::max(cand[lab[i]], i);
         }
     }
+    // a Neumann row without fluid in range is an identity row of the operator
+    // (an anchor); a Neumann candidate that is a copy row anchors only
+    // without partner (above), as in the oracle
     for (size_t k = 0; k < nm_rows.size(); ++k)
-        if (nm_flags[k] & 4) anchored[lab[nm_rows[k]]] = 1;
+        if ((nm_flags[k] & 4) && kind[nm_rows[k]] == 2) anchored[lab[nm_rows[k]]] = 1;
     c.n_pins = 0;
     c.n_comp = 0;
     for (int r = 0; r < n; ++r) {
