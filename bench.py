@@ -127,6 +127,27 @@ def cpu_baseline(steps):
             "seconds": dt}
 
 
+def cpu_baseline_tgv(steps):
+    """The Taylor-Green box on the host: the reference has no triply periodic
+    mode, so the CPU restatement of its step (the oracle, FP64, one thread,
+    Jacobi-BiCGSTAB to 1e-8) is timed on a bounded sample of the deck."""
+    import restated
+    from sph_b200 import decks, layout
+    n = 32
+    P, p = decks.tgv_periodic(n=n)
+    O = restated.Restated(P, p, 1)
+    O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-8, maxit=4000)   # untimed first step
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-8, maxit=4000)
+    dt = time.perf_counter() - t0
+    return {"value": n ** 3 * steps / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"Taylor-Green box at {n}^3 particles (dx = 1/{n} m, same physics), {steps} steps of the "
+                      f"CPU restatement of the step in FP64 with Jacobi-BiCGSTAB to 1e-8 after one untimed step; "
+                      f"the reference itself has no triply periodic mode",
+            "seconds": dt}
+
+
 def run_ensemble(args, rank, world, local):
     """Batched ensemble: every rank steps its own seeded set of cases."""
     import numpy as np
@@ -648,7 +669,7 @@ def main():
     if fp64:
         out["mixed_vs_fp64"] = value / fp64["value"] if fp64["value"] else None
     if world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(steps=4)
+        out["cpu_baseline"] = cpu_baseline_tgv(steps=4) if args.config == "tgv" else cpu_baseline(steps=4)
     print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
