@@ -71,3 +71,39 @@ def test_taylor_green_cpu_baseline_line():
     b = bench.cpu_baseline_tgv(1)
     assert b["kind"] == "port" and b["cores"] == 1 and b["unit"] == bench.METRIC
     assert b["value"] > 0 and b["seconds"] > 0 and "32^3" in b["sample"]
+
+
+def _state(u, p, n_extra_ghosts=0):
+    from sph_b200 import layout
+    import numpy as np
+    n = len(u) + n_extra_ghosts
+    S = np.zeros(n, dtype=layout.PART1)
+    S["i_type"] = 1
+    S["p_type"] = 1
+    S["ux"][:len(u)], S["uy"][:len(u)], S["uz"][:len(u)] = np.asarray(u, np.float32).T
+    S["pres"][:len(p)] = p
+    S["buffer_type"][len(u):] = layout.BUFFER_PERIODIC_GHOST
+    S["ux"][len(u):] = 99.0
+    return S
+
+
+def test_form_error_counts_u_limit_decisions_apart():
+    import numpy as np
+    u_ref = [[1.0, 0.0, 0.0]] * 8 + [[1.0, -0.59, 0.0]]
+    u_new = [[1.0 + 1e-6, 0.0, 0.0]] * 8 + [[0.62, 19.97, 0.0]]   # one particle accepted at the limit
+    p = np.linspace(1.0, 2.0, 9)
+    B, A = _state(u_ref, p, n_extra_ghosts=3), _state(u_new, p, n_extra_ghosts=3)
+    e = bench.form_error(A, B, 20.0)
+    assert e["particles"] == 9                       # ghosts excluded
+    assert e["u_limit_decided_differently"] == 1
+    assert e["u_rel_l2"] > 1.0
+    assert abs(e["u_rel_l2_other_particles"] - 1e-6) < 1e-7
+    assert e["p_rel_l2"] == 0.0 and e["p_rel_max"] == 0.0
+
+
+def test_form_error_of_equal_states_is_zero():
+    import numpy as np
+    u = np.random.default_rng(1).normal(size=(50, 3))
+    S = _state(u, np.ones(50))
+    e = bench.form_error(S, S.copy(), 20.0)
+    assert e["u_rel_l2"] == 0.0 and e["u_limit_decided_differently"] == 0 and e["u_rel_l2_other_particles"] == 0.0
