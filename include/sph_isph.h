@@ -461,11 +461,13 @@ int64_t sph_batch_particles(sph_batch *b);
  * which every GPU that loads this library holds until the process exits.
  * Limits: n <= SPH_NOALLOC_MAX_PARTICLES and num_cells + 2 <=
  * SPH_NOALLOC_MAX_CELLS; larger inputs return SPH_ERR_BAD_ARG.  The first
- * call on a device looks up that array's device address, so make it before
- * any stream capture.  All calls on a device share the array: calls that
- * overlap on the GPU (other streams, other host threads) race.  The call
- * waits for its stream before it returns, to report a cell of more than
- * 4096 particles (SPH_ERR_UNSUPPORTED).  It calls no cudaMalloc or cudaFree. */
+ * call on a device looks up that array's device address.  All calls on a
+ * device share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race.  Every call ends by copying two flags to host
+ * memory and waiting for its stream, to report a cell of more than 4096
+ * particles (SPH_ERR_UNSUPPORTED); so do not make it while any stream of the
+ * device is being captured into a CUDA graph.  It calls no cudaMalloc or
+ * cudaFree. */
 #define SPH_NOALLOC_MAX_PARTICLES 262144
 #define SPH_NOALLOC_MAX_CELLS     524288
 int sph_nnps_sort_noalloc(const sph_params *params, const float *d_x, const float *d_y, const float *d_z,

@@ -327,30 +327,36 @@ __global__ void k_sort_small(const int *cell_start, int *perm, int *big, int *nb
     for (int a = 0; a < len; ++a) perm[s + a] = v[a];
 }
 
-// one block per long segment: bitonic sort of up to 4096 indices in shared memory
+// bitonic sort of up to 4096 indices in shared memory, one long segment per
+// block at a time; the blocks stride over the list of long segments, so a
+// small fixed grid (kSortBigGrid) serves any count
+constexpr int kSortBigGrid = 296;
 __global__ void k_sort_big(const int *cell_start, int *perm, const int *big, const int *nbig, int *err) {
     __shared__ int sv[4096];
-    if (blockIdx.x >= (unsigned)*nbig) return;
-    const int c = big[blockIdx.x];
-    const int s = cell_start[c], len = cell_start[c + 1] - s;
-    if (len > 4096) { if (threadIdx.x == 0) atomicExch(err, 1); return; }
-    int m = 1;
-    while (m < len) m <<= 1;
-    for (int a = threadIdx.x; a < m; a += blockDim.x) sv[a] = (a < len) ? perm[s + a] : 0x7fffffff;
-    __syncthreads();
-    for (int k = 2; k <= m; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int a = threadIdx.x; a < m; a += blockDim.x) {
-                const int b = a ^ j;
-                if (b > a) {
-                    const bool up = (a & k) == 0;
-                    const int x = sv[a], y = sv[b];
-                    if ((x > y) == up) { sv[a] = y; sv[b] = x; }
+    const int nb = *nbig;
+    for (int q = blockIdx.x; q < nb; q += gridDim.x) {
+        const int c = big[q];
+        const int s = cell_start[c], len = cell_start[c + 1] - s;
+        if (len > 4096) { if (threadIdx.x == 0) atomicExch(err, 1); continue; }
+        int m = 1;
+        while (m < len) m <<= 1;
+        for (int a = threadIdx.x; a < m; a += blockDim.x) sv[a] = (a < len) ? perm[s + a] : 0x7fffffff;
+        __syncthreads();
+        for (int k = 2; k <= m; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int a = threadIdx.x; a < m; a += blockDim.x) {
+                    const int b = a ^ j;
+                    if (b > a) {
+                        const bool up = (a & k) == 0;
+                        const int x = sv[a], y = sv[b];
+                        if ((x > y) == up) { sv[a] = y; sv[b] = x; }
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
-        }
-    for (int a = threadIdx.x; a < len; a += blockDim.x) perm[s + a] = sv[a];
+        for (int a = threadIdx.x; a < len; a += blockDim.x) perm[s + a] = sv[a];
+        __syncthreads();   // sv is refilled by the next segment
+    }
 }
 
 __global__ void k_sorted_keys(const int *key, const int *perm, int *g_idx, int n) {
@@ -364,20 +370,11 @@ __global__ void k_gather(const T *src, T *dst, const int *perm, int n) {
     if (s < n) dst[s] = src[perm[s]];
 }
 
-__global__ void k_float_of_href(const float4 *dummy, float *out, const float *src, int n) {
-    (void)dummy;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = src[i];
-}
-
 template <class Real>
 __global__ void k_href_to_float(const Real *h_ref, float *out, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (float)h_ref[i];
 }
-
-template <class T>
-static int gather_inplace(Ctx<T> &, void *, int) { return SPH_OK; }
 
 // gathers one device array by `perm` through a scratch buffer
 template <class Real, class T>
@@ -1090,15 +1087,14 @@ int nnps_build(Ctx<Real> &c) {
     SPH_CUDA_TRY(cudaMemsetAsync(c.cell_fill, 0, sizeof(int) * ((size_t)NC + 2), st));
     k_scatter<<<grid_for(n, 256), 256, 0, st>>>(c.key, c.cell_start, c.cell_fill, drank, c.perm, NC, n);
     k_sort_small<<<grid_for(NC, 256), 256, 0, st>>>(c.cell_start, c.perm, big, nbig, NC);
-    k_sort_big<<<NC > 0 ? std::min(NC, 65535) : 1, 256, 0, st>>>(c.cell_start, c.perm, big, nbig, err);
+    k_sort_big<<<kSortBigGrid, 256, 0, st>>>(c.cell_start, c.perm, big, nbig, err);
     k_sorted_keys<<<grid_for(n, 256), 256, 0, st>>>(c.key, c.perm, c.g_idx, n);
     c.launches += 4;
     SPH_CUDA_TRY(cudaGetLastError());
-    int herr = 0, hbig = 0;
+    int herr = 0;
     SPH_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SPH_CUDA_TRY(cudaMemcpyAsync(&hbig, nbig, sizeof(int), cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
-    if (herr || hbig > 65535) { set_error("nnps: a cell holds more than 4096 particles"); return SPH_ERR_UNSUPPORTED; }
+    if (herr) { set_error("nnps: a cell holds more than 4096 particles"); return SPH_ERR_UNSUPPORTED; }
 
     // reorder every per-particle array (KERNEL_reorder, functions_NNPS.cuh:840-843)
     SPH_TRY(regather(c, c.pf, scratch));
@@ -1352,7 +1348,7 @@ extern "C" int sph_nnps_sort_noalloc(const sph_params *params, const float *d_x,
         SPH_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)NC + 2), st));
         k_scatter<<<grid_for(n, 256), 256, 0, st>>>(key, cs, cnt, drank, d_p_idx, NC, n);
         k_sort_small<<<grid_for(NC, 256), 256, 0, st>>>(cs, d_p_idx, big, nbig, NC);
-        k_sort_big<<<std::min(NC, 65535), 256, 0, st>>>(cs, d_p_idx, big, nbig, err);
+        k_sort_big<<<kSortBigGrid, 256, 0, st>>>(cs, d_p_idx, big, nbig, err);
         k_sorted_keys<<<grid_for(n, 256), 256, 0, st>>>(key, d_p_idx, d_g_idx, n);
         SPH_CUDA_TRY(cudaGetLastError());
     }
@@ -1361,7 +1357,7 @@ extern "C" int sph_nnps_sort_noalloc(const sph_params *params, const float *d_x,
     int flags[3] = {0, 0, 0};   // nbig, pad, err
     SPH_CUDA_TRY(cudaMemcpyAsync(flags, nbig, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
-    if (flags[2] || flags[0] > 65535) {
+    if (flags[2]) {
         set_error("sph_nnps_sort_noalloc: a cell holds more than 4096 particles");
         return SPH_ERR_UNSUPPORTED;
     }
