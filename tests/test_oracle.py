@@ -58,6 +58,43 @@ def test_nnps_bit_exact_vs_reference(name):
     assert np.array_equal(g_end, oe)
 
 
+def _domain_decks():
+    yield "caseh_mini", decks.caseh_mini()[0], decks.caseh_mini()[1]
+    P, p = decks.canyon(scale=0.3)
+    yield "canyon_0.3", P, p
+    P, p, _ = decks.cube_array(scale=0.2)
+    yield "cube_array_0.2", P, p
+    P, p = decks.tgv_periodic(n=16)
+    yield "tgv_16", P, p
+    P, p = decks.nnps_stress()
+    yield "nnps_stress", P, p
+
+
+@needs_ref
+def test_domain_setup_equals_reference_host_setup():
+    """sph_domain_setup against the reference's own host set-up (find_minmax,
+    function_init.cuh:678-708; dcell and NI/NJ/NK, ISPH.cuh:88-97;
+    clc_num_cells, functions_NNPS.cuh:534-546) on five decks: every grid
+    slot of k_vii / k_vif bit-identical."""
+    from sph_b200 import abi
+    L = refhost.lib()
+    for name, P, p in _domain_decks():
+        c = p.copy()
+        abi.domain_setup(c, P)
+        vii = np.ctypeslib.as_array(p.vii).copy()
+        vif = np.ctypeslib.as_array(p.vif).copy()
+        L.ref_set_params(vii.ctypes.data_as(ctypes.c_void_p), vif.ctypes.data_as(ctypes.c_void_p))
+        Q = np.ascontiguousarray(P.copy())
+        L.ref_domain_setup(Q.ctypes.data_as(ctypes.c_void_p), len(Q))
+        L.ref_get_params(vii.ctypes.data_as(ctypes.c_void_p), vif.ctypes.data_as(ctypes.c_void_p))
+        for slot in ("NI", "NJ", "NK", "num_cells", "num_part"):
+            assert c.geti(slot) == int(vii[getattr(layout, "VII")[slot]]), (name, slot)
+        for slot in ("x_min", "x_max", "y_min", "y_max", "z_min", "z_max", "dcell", "search_kappa"):
+            a = np.float32(c.getf(slot))
+            b = np.float32(vif[getattr(layout, "VIF")[slot]])
+            assert a.tobytes() == b.tobytes(), (name, slot, a, b)
+
+
 @needs_ref
 def test_nnps_bit_exact_vs_reference_on_stress_deck():
     # dummies, a 150-particle cell, duplicates, records on the domain maximum
