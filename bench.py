@@ -1,19 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 ISPH step on the urban-canyon workload.
+"""Benchmark of the B200 ISPH step.
+
+Default workload: the staggered 4x4 cube array (4.8 x 2.4 x 0.8 m, base
+dx = 0.01 m) with two-level APR within 0.1 m of the cube faces, stepped in
+the mixed-precision form with the learned PPE warm start, against the plain
+FP64 form (Jacobi-BiCGSTAB) timed in the same run.  --config canyon / tgv /
+ensemble / transfer select the other workloads.
 
 One JSON line on rank 0:
-  metric  particle-steps/s: particles x steps / device time of the full step
-          (interaction passes, PPE converged to ||b-Ap||/||b|| <= 1e-6 with
-          FP32 BiCGSTAB inside FP64 refinement, time update); NNPS runs at
-          step 0 inside the warm-up (the reference runs it only at step 0,
-          ISPH_Calc.cuh:23-52, because particles never move).
+  metric  particle-steps/s: active particles x steps / device time of the
+          full step (interaction passes, PPE converged to ||b-Ap||/||b|| <=
+          1e-6 with FP32 BiCGSTAB and FP64 reliable updates, time update);
+          NNPS runs at step 0 inside the warm-up (the reference runs it only
+          at step 0, ISPH_Calc.cuh:23-52, because particles never move).
   e2e     the same step through the C ABI with host buffers: every step
           uploads the particle records (part1, pinned host memory), runs the
           step and downloads the records again.
   roofline of the dominant kernel (the PPE operator), from live CUDA-event
           timing of its launches inside the timed region.
+  plain_fp64 / error_vs_plain_fp64  the plain FP64 form on the same deck and
+          the chosen form's velocity and pressure error against it.
+  nnps_bit_exact  cell hash, permutation, cell ranges and neighbour lists of
+          the timed deck against the CPU oracle.
   cpu_baseline  the reference's own step compiled for the host cores
-          (oracle/_ref), timed on a bounded sample of the same deck.
+          (oracle/_ref), timed on a bounded sample of the config's deck.
 With --impl reference only the reference arm runs (rank 0).
 Multi-GPU: the step is a one-GPU path; N ranks run N independent replicas
 (weak scaling, no collective in the step).
@@ -33,8 +43,13 @@ sys.path[:0] = [os.path.join(ROOT, "urban-sph_a100_b200"), os.path.join(ROOT, "o
 
 METRIC = "particle-steps/s"
 WORKLOAD = "urban canyon 2.4x1.2x0.6 m, dx=0.01 m: 240x120x60 fluid + floor walls + free-slip ceiling + IBM cube, neutral MOST, SSM Cs=0.12"
-WORKLOAD_ARRAY = ("staggered 4x4 array of 0.1 m IBM cubes at 0.3 m pitch in a 4.8x2.4x0.8 m channel, dx=0.01 m, "
-                  "uniform resolution (--apr: two-level APR within 0.1 m of the faces), neutral MOST, SSM Cs=0.12")
+WORKLOAD_ARRAY = ("staggered 4x4 array of 0.1 m IBM cubes at 0.3 m pitch in a 4.8x2.4x0.8 m channel, base dx=0.01 m, "
+                  "{res}, SSM Cs=0.12, log-law inflow u*=0.3 m/s z0=0.01 m with a seeded 5% perturbation; MOST runs "
+                  "neutral: with the stable L=100 m surface temperature difference the reference's Obukhov-length "
+                  "Newton iteration (functions_MOST.cuh:205-245) returns NaN at the low-wind wall-layer records of "
+                  "this deck, in the reference's own kernel as here")
+RES_APR = "two-level APR (ratio 2, children at dx/2) within 0.1 m of the cube faces"
+RES_UNIFORM = "uniform resolution"
 WORKLOAD_TGV = ("triply periodic Taylor-Green vortex: {n}^3 particles, dx=1/{n} m in a 1 m cube with 3 layers of "
                 "periodic ghosts, h=1.3dx, Wendland C6, rho=1000, nu=1e-3, U0=1 m/s, CFL 0.1")
 
@@ -106,14 +121,29 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(steps):
-    """The reference's own step on the host cores, bounded sample of the deck."""
-    import numpy as np
-    import refhost
+def reference_sample(config):
+    """The bounded deck on which the reference's own host step is timed, and
+    its description.  The reference compiles no APR and runs one in-place
+    PPE sweep per step (ISPH_Calc.cuh:137-154), so its sample is the
+    uniform-resolution deck of the config at reduced extent."""
     from sph_b200 import decks
+    if config == "array":
+        P, p, _ = decks.cube_array(scale=0.2)
+        what = (f"uniform-resolution cube array at scale 0.2 ({len(P)} particles; the reference compiles no APR), "
+                f"the reference's step: one in-place PPE sweep, no converged solve")
+    else:
+        P, p = decks.canyon(scale=0.3)
+        what = (f"canyon deck at scale 0.3 ({len(P)} particles), the reference's step: one in-place PPE sweep, "
+                f"no converged solve")
+    return P, p, what
+
+
+def cpu_baseline(steps, config="canyon"):
+    """The reference's own step on the host cores, bounded sample of the deck."""
+    import refhost
     if not refhost.available():
         return None
-    P, p = decks.canyon(scale=0.3)
+    P, p, what = reference_sample(config)
     R = refhost.RefHost(P, p, parallel=True)
     R.step(1)   # step 0: NNPS + first step (untimed)
     t0 = time.perf_counter()
@@ -121,10 +151,68 @@ def cpu_baseline(steps):
     dt = time.perf_counter() - t0
     cores = int(refhost.lib().ref_num_threads())
     return {"value": len(P) * steps / dt, "unit": METRIC, "cores": cores, "kind": "reference",
-            "sample": f"canyon deck at scale 0.3 ({len(P)} particles), {steps} steps of the reference "
-                      f"step (one in-place PPE sweep) after its step-0 NNPS, host build of the "
-                      f"reference kernels with the reference's own hard-wired Case-H constants",
+            "sample": f"{what}; {steps} steps after its step-0 NNPS, host build of the reference kernels "
+                      f"(oracle/_ref) with its hard-wired Case-H constants",
             "seconds": dt}
+
+
+def cpu_converged_port(local, steps=1):
+    """Like-for-like CPU work: the CPU restatement of the step in FP64 with
+    Jacobi-BiCGSTAB to 1e-6 (the plain form) on the refined cube array at
+    scale 0.1, split by the GPU's APR passes; one thread."""
+    import restated
+    from sph_b200 import abi, decks, layout
+    P, p, boxes = decks.cube_array(scale=0.1, apr=True)
+    p.ppe_pair_h = 1
+    sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
+    sim.set_ib_boxes(boxes)
+    sim.upload(P)
+    for _ in range(16):
+        if sim.apr()[0] == 0:
+            break
+    P, _, _ = sim.download()
+    sim.close()
+    n = int((P["i_type"] < 3).sum())
+    q = p.copy()
+    q.ppe_tol = 1e-6
+    O = restated.Restated(P, q, 1)
+    O.step(1, mode=layout.PPE_BICGSTAB, tol=1e-6, maxit=40000)    # NNPS and the first step, untimed
+    t0 = time.perf_counter()
+    st = O.step(steps, mode=layout.PPE_BICGSTAB, tol=1e-6, maxit=40000)
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"refined cube array at scale 0.1 ({n} active particles, one cube), {steps} step(s) of the "
+                      f"CPU restatement in FP64 with Jacobi-BiCGSTAB to 1e-6 after one untimed step "
+                      f"({st[2]} iterations in the last)",
+            "seconds": dt}
+
+
+def nnps_check(P, p, boxes, local):
+    """Cell hash, sort permutation, cell start/end and the neighbour lists of
+    the timed deck (the records as the timed context held them after the
+    APR passes) from a fresh context, against the CPU oracle on the same
+    records: bit-exact or not."""
+    import numpy as np
+    import restated
+    from sph_b200 import abi, layout
+    t0 = time.perf_counter()
+    sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
+    if boxes is not None:
+        sim.set_ib_boxes(boxes)
+    sim.upload(P)
+    sim.nnps()
+    g = sim.export_nnps()
+    off, lst = sim.neighbors()
+    sim.close()
+    O = restated.Restated(P, p, 0)
+    O.nnps()
+    og = O.export_nnps()
+    arrays = all(np.array_equal(a, b) for a, b in zip(g, og))
+    ooff, olst = O.neighbors()
+    del O
+    lists = bool(np.array_equal(off, ooff) and np.array_equal(lst, olst))
+    return {"nnps_arrays": bool(arrays), "neighbour_lists": lists, "bit_exact": bool(arrays and lists),
+            "records": int(len(P)), "list_entries": int(len(lst)), "seconds": time.perf_counter() - t0}
 
 
 def form_error(A, B, u_limit):
@@ -342,8 +430,7 @@ def run_reference(args, rank, world):
     if not refhost.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsophia_ref.so not built"}))
         return 0
-    from sph_b200 import decks
-    P, p = decks.canyon(scale=0.3)
+    P, p, what = reference_sample(args.config)
     R = refhost.RefHost(P, p, parallel=True)
     for _ in range(max(args.warmup, 1)):
         R.step(1)
@@ -356,9 +443,10 @@ def run_reference(args, rank, world):
            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "impl": "reference",
-           "config": {"workload": WORKLOAD, "sample_particles": len(P), "scale": 0.3},
+           "config": {"workload": {"canyon": WORKLOAD}.get(args.config, WORKLOAD_ARRAY.format(res=RES_APR)),
+                      "sample_particles": len(P)},
            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
-                            "sample": f"canyon deck at scale 0.3 ({len(P)} particles) per step"},
+                            "sample": f"{what}; per step, host build of the reference kernels (oracle/_ref)"},
            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -371,8 +459,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--config", default="canyon", choices=["canyon", "array", "ensemble", "transfer", "tgv"],
-                    help="canyon: the urban-canyon step (default); array: 4x4 cube array with two-level APR; "
+    ap.add_argument("--config", default="array", choices=["canyon", "array", "ensemble", "transfer", "tgv"],
+                    help="array: 4x4 cube array with two-level APR, the mixed + learned form against the plain "
+                         "FP64 form (default); canyon: the urban-canyon step; "
                          "ensemble: 64 seeded cavity / Taylor-Green cases of 20k-200k particles stepped together; "
                          "transfer: the learned start trained on the canyon's solves, applied to the cube array")
     ap.add_argument("--dx", type=float, default=0.0075, help="transfer config: particle spacing of the cube array")
@@ -381,12 +470,14 @@ def main():
     ap.add_argument("--tol", type=float, default=None, help="PPE tolerance (default 1e-6; tgv config 1e-8)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the timed form (mixed: FP32 fields and Krylov vectors, FP64 refinement)")
-    ap.add_argument("--apr", action="store_true",
-                    help="array config: two-level APR near the faces before timing (default: uniform resolution)")
+    ap.add_argument("--apr", action=argparse.BooleanOptionalAction, default=True,
+                    help="array config: two-level APR near the faces before timing (--no-apr: uniform resolution)")
     ap.add_argument("--mode", default="mixed_ir", choices=["mixed_ir", "bicgstab", "gmres", "idrs", "ref_sweep"])
     ap.add_argument("--fp64-mode", default="bicgstab", choices=["gmres", "bicgstab", "idrs"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-nnps-check", action="store_true",
+                    help="array config: skip the NNPS / neighbour-list comparison with the CPU oracle")
     ap.add_argument("--matrix-free", action="store_true")
     ap.add_argument("--wide-index", action="store_true",
                     help="pressure operator on 32-bit neighbour indices instead of the 16-bit codes")
@@ -402,10 +493,11 @@ def main():
                          "--apr, else ref")
     ap.add_argument("--gmres-restart", type=int, default=0, help="GMRES(m) restart length (0: 40)")
     ap.add_argument("--inner-tol", type=float, default=0.0, help="restarted refinement: inner tolerance (0: 1e-3)")
-    ap.add_argument("--warm", default="prev", choices=["prev", "scaled", "extrap", "learned"],
+    ap.add_argument("--warm", default=None, choices=["prev", "scaled", "extrap", "learned"],
                     help="PPE start vector: previous pressure, previous pressure times its residual-minimising factor, linear "
                          "extrapolation in time, or the learned "
-                         "per-particle network (trained on this run's warm-up solves)")
+                         "per-particle network (trained on this run's warm-up solves); default learned for the "
+                         "array config, previous pressure otherwise")
     ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres",
                                                                   "restart-idrs"],
                     help="mixed_ir form: FP64 reliable updates, or refinement restarting the FP32 solver")
@@ -421,6 +513,10 @@ def main():
         return run_transfer(args, rank, world, local)
     if args.warmup < 3:
         args.warmup = 3
+    if args.config != "array":
+        args.apr = False
+    if args.warm is None:
+        args.warm = "learned" if args.config == "array" else "prev"
 
     import numpy as np
     import torch
@@ -534,6 +630,7 @@ def main():
     ms = e0.elapsed_time(e1)
     launches = sim.launches() - l0
     op_n, op_ms, op_bytes = sim.operator_stats(reset=True)
+    _, op_index_bytes = sim.operator_bytes()
     sim.profile(False)
     value, ms = replicas.throughput(n, args.steps, ms, device="cuda")
 
@@ -637,18 +734,27 @@ def main():
 
     hbm, peak_kind = peaks()
     per_launch_ms = op_ms / max(op_n, 1)
-    achieved = op_bytes / (per_launch_ms / 1e3) / 1e9 if op_n else 0.0
-    nc = ncu_traffic("ppe_operator_canyon.json")
+    # the roofline counts per-row fields and 4 B per stored neighbour index
+    # (sph_operator_bytes' index rule); the stored-layout figure (cached
+    # coefficients and 16-bit codes streamed per launch) is reported beside it
+    achieved = op_index_bytes / (per_launch_ms / 1e3) / 1e9 if op_n else 0.0
+    achieved_stored = op_bytes / (per_launch_ms / 1e3) / 1e9 if op_n else 0.0
+    # DRAM bytes per launch from the committed ncu capture of this config's
+    # operator on a smaller deck, scaled by the stored bytes of a launch
+    # (rows, stored entries and Neumann entries grow together)
+    nc = ncu_traffic(f"ppe_operator_{args.config}.json")
     traffic = None
-    if nc and abs(nc.get("particles", 0) - n) <= 1 and "dram_bytes_per_launch" in nc:
-        traffic = nc["dram_bytes_per_launch"]
+    if nc and "measured_at" in nc and nc.get("apr", False) == bool(args.apr):
+        m = nc["measured_at"]
+        traffic = m["traffic_over_algorithmic"] * op_bytes
     ph = np.mean(np.array(phases), axis=0) if phases else np.zeros(4)
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
         "data": "synthetic",
-        "config": {"workload": {"canyon": WORKLOAD, "array": WORKLOAD_ARRAY}.get(
+        "config": {"workload": {"canyon": WORKLOAD,
+                                "array": WORKLOAD_ARRAY.format(res=RES_APR if args.apr else RES_UNIFORM)}.get(
                        args.config, WORKLOAD_TGV.format(n=int(round(64 * args.scale)))),
                    "particles": n, "apr": apr, "scale": args.scale,
                    "precision": "mixed FP32/FP64" if args.precision == "mixed" else "FP64",
@@ -678,7 +784,13 @@ def main():
                      else "PPE operator (k_spmv_mf)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_kind": peak_kind, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": op_bytes, "launch_ms": per_launch_ms, "launches": op_n},
+                     "algorithmic_bytes_per_launch": op_index_bytes,
+                     "bytes_rule": "per row its fields read and written, per stored neighbour its 4-byte index",
+                     "stored_layout": {"bytes_per_launch": op_bytes, "achieved": achieved_stored,
+                                       "frac": achieved_stored / hbm,
+                                       "rule": "what the launch streams: 16-bit codes or 32-bit indices plus the "
+                                               "cached coefficient per entry, Neumann weights, code tables"},
+                     "launch_ms": per_launch_ms, "launches": op_n},
         "plain_fp64": fp64,
         "error_vs_plain_fp64": err64,
         "fp64_same_preconditioner": fp64_same,
@@ -688,8 +800,12 @@ def main():
     }
     if fp64:
         out["mixed_vs_fp64"] = value / fp64["value"] if fp64["value"] else None
+    if args.config == "array" and not args.no_nnps_check:
+        out["nnps_bit_exact"] = nnps_check(P, p, boxes, local)
     if world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline_tgv(steps=4) if args.config == "tgv" else cpu_baseline(steps=4)
+        out["cpu_baseline"] = cpu_baseline_tgv(steps=4) if args.config == "tgv" else cpu_baseline(4, args.config)
+        if args.config == "array":
+            out["cpu_converged_port"] = cpu_converged_port(local)
     print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()

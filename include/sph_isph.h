@@ -335,6 +335,13 @@ int64_t sph_launch_count(sph_ctx *ctx);
  * `reset` clears the counters after reading. */
 int sph_profile(sph_ctx *ctx, int enable);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
+/* Algorithmic bytes of one operator launch in two accountings: `stored` is
+ * the figure of sph_operator_stats (what the launch's layout streams,
+ * including the cached coefficients and code tables); `index_rule` counts
+ * per row the fields read and written for it, per slice its offset and 4
+ * bytes per stored neighbour index (SELL and Neumann rows), and no stored
+ * coefficient.  Either pointer may be NULL. */
+int sph_operator_bytes(sph_ctx *ctx, double *stored, double *index_rule);
 
 /* ---- files in the reference's formats (host code) -------------------------
  * sph_read_deck reads a particle deck in the format of read_input

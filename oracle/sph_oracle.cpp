@@ -345,22 +345,34 @@ struct Oracle {
         kc = search_axis(z, Q.zmin(), Q.zmax(), Q.dcell(), Q.NK());
     }
 
+    // rows are independent: a counting pass and a filling pass, each over
+    // rows in parallel, give the same list as one serial pass
     void build_lists() {
         const P Q = q();
         const int N = n();
         nb_off.assign(N + 1, 0);
-        nb.clear();
-        for (int i = 0; i < N; ++i) {
-            nb_off[i] = (int64_t)nb.size();
-            if (S1.i_type[i] == 3) continue;   // not in any cell, never a neighbour
+        auto visit = [&](int i, auto &&emit) {
+            if (S1.i_type[i] == 3) return;   // not in any cell, never a neighbour
             int ic, jc, kc;
             search_cell(xf[i], yf[i], zf[i], ic, jc, kc);
             cell_loop(ic, jc, kc, S1.ncell[i], [&](int j) {
                 float tdist = std::sqrt(d2f(xf[i], yf[i], zf[i], xf[j], yf[j], zf[j]));
-                if (tdist < Q.skappa() * std::fmax(hf[i], hf[j])) nb.push_back(j);
+                if (tdist < Q.skappa() * std::fmax(hf[i], hf[j])) emit(j);
             });
+        };
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int i = 0; i < N; ++i) {
+            int64_t c = 0;
+            visit(i, [&](int) { ++c; });
+            nb_off[i + 1] = c;
         }
-        nb_off[N] = (int64_t)nb.size();
+        for (int i = 0; i < N; ++i) nb_off[i + 1] += nb_off[i];
+        nb.assign((size_t)nb_off[N], 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (int i = 0; i < N; ++i) {
+            int64_t e = nb_off[i];
+            visit(i, [&](int j) { nb[(size_t)e++] = j; });
+        }
     }
 
     // ---- passes ----------------------------------------------------------------

@@ -425,6 +425,11 @@ int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double
                     operator_stats(*ctx->d, launches, total_ms, bytes_per_launch, reset));
 }
 
+int sph_operator_bytes(sph_ctx *ctx, double *stored, double *index_rule) {
+    if (!ctx) return SPH_ERR_BAD_ARG;
+    return DISPATCH(ctx, operator_bytes(*ctx->f, stored, index_rule), operator_bytes(*ctx->d, stored, index_rule));
+}
+
 // ---- learned warm start (learned.cu) ------------------------------------------
 int sph_ml_collect(sph_ctx *ctx, int every) {
     if (!ctx || every < 0) return SPH_ERR_BAD_ARG;

@@ -298,6 +298,7 @@ template <class Real> int freeslip_pass(Ctx<Real> &c, VarSet<Real> &V);
 template <class Real> int build_side_lists(Ctx<Real> &c);
 template <class Real> void release_solver_ws(Ctx<Real> &c);
 template <class Real> int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *bytes, int reset);
+template <class Real> int operator_bytes(Ctx<Real> &c, double *stored, double *index_rule);
 
 // launch helper: grid for n threads
 inline dim3 grid_for(long long n, int block) { return dim3((unsigned)((n + block - 1) / block)); }

@@ -762,6 +762,27 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
     return SPH_OK;
 }
 
+// Bytes of one operator launch in two accountings.  `stored`: what the
+// launch's layout streams (the operator_stats figure).  `index_rule`: per row
+// the fields read and written for it (kind, list length, x_i, y_i; component
+// id and A_i with the rank-one term), per slice its offset, and 4 bytes per
+// stored neighbour index, for the SELL rows and the Neumann rows alike --
+// stored coefficients, the 16-bit code tables and the Neumann weights are
+// not counted, since a kernel that recomputes them from the positions needs
+// none of them.
+template <class Real>
+int operator_bytes(Ctx<Real> &c, double *stored, double *index_rule) {
+    if (stored) SPH_TRY(operator_stats(c, nullptr, nullptr, stored, 0));
+    if (index_rule) {
+        const double R = (double)sizeof(Real);
+        double row = 8.0 + 2.0 * R;
+        if (c.n_comp > 0) row += 4.0 + R;
+        *index_rule = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + 4.0 * (double)c.nnz +
+                      (double)c.L.n_nm * (8.0 + 2.0 * R) + 4.0 * (double)c.L.nm_nnz;
+    }
+    return SPH_OK;
+}
+
 // Two-level preconditioner on r, with z holding D^-1 r on entry: the
 // additive form adds Z E^-1 Z^T r; the multiplicative form corrects the
 // residual that the Jacobi step leaves, z += Z E^-1 Z^T (r - M z), at the
@@ -1958,6 +1979,7 @@ void release_solver_ws(Ctx<Real> &c) {
 #define INST(R) template int phase_ppe<R>(Ctx<R> &, sph_ppe_stats *); \
     template void release_solver_ws<R>(Ctx<R> &); \
     template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int); \
+    template int operator_bytes<R>(Ctx<R> &, double *, double *); \
     template void ppe_apply_fp64<R>(Ctx<R> &, const double *, double *);
 INST(float)
 INST(double)

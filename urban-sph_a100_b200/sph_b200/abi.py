@@ -25,7 +25,7 @@ SYMBOLS = (
     "sph_upload", "sph_upload_state", "sph_download", "sph_nnps", "sph_nnps_export",
     "sph_neighbors_export", "sph_interaction", "sph_ppe", "sph_time_update", "sph_step",
     "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_status_string",
-    "sph_last_error", "sph_profile", "sph_operator_stats", "sph_nnps_sort_noalloc",
+    "sph_last_error", "sph_profile", "sph_operator_stats", "sph_operator_bytes", "sph_nnps_sort_noalloc",
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
@@ -79,6 +79,7 @@ def lib():
         L.sph_profile.argtypes = [vp, i32]
         L.sph_operator_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double), i32]
+        L.sph_operator_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.sph_nnps_sort_noalloc.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
         f32p = ctypes.POINTER(ctypes.c_float)
         L.sph_ml_collect.argtypes = [vp, i32]
@@ -285,6 +286,13 @@ class Simulation:
         _check("sph_operator_stats", lib().sph_operator_stats(self.h, ctypes.byref(n), ctypes.byref(ms),
                                                               ctypes.byref(by), 1 if reset else 0))
         return n.value, ms.value, by.value
+
+    def operator_bytes(self):
+        """(stored, index_rule) bytes of one operator launch."""
+        a = ctypes.c_double(0)
+        b = ctypes.c_double(0)
+        _check("sph_operator_bytes", lib().sph_operator_bytes(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
 
 class Batch:
