@@ -187,6 +187,63 @@ def cpu_converged_port(local, steps=1):
             "seconds": dt}
 
 
+REF_CUDA = os.path.join(ROOT, "baseline", "_ref", "sophia_gpu_sm100a")
+REF_VTK_DIR = "CaseH_n10_DDF(WL6,dt=2.5e-5,KGC,IBM_WM)"   # functions_OUTPUT.cuh:142
+
+
+def ref_cuda_inputs(run_dir, P, p, steps):
+    """The files the reference's program reads (SOPHIA_gpu.cu:124-129,
+    ISPH.cuh:59): ./input/solv.txt for `steps` steps from t = 0 with output
+    only at step 0, an empty ./input/data.txt (no property tables) and the
+    deck ./input/CaseH_n10.txt; plus the VTK directory its writer expects."""
+    from sph_b200 import driver
+    os.makedirs(os.path.join(run_dir, "input"), exist_ok=True)
+    os.makedirs(os.path.join(run_dir, REF_VTK_DIR), exist_ok=True)
+    q = p.copy()
+    dt = float(q.getf("dt"))
+    q.setf("time", 0.0)
+    q.setf("time_end", dt * (steps - 0.5))
+    q.seti("freq_output", 100000000)
+    driver.write_solv(os.path.join(run_dir, "input", "solv.txt"), q, labels=("velocity", "pressure"))
+    open(os.path.join(run_dir, "input", "data.txt"), "w").close()
+    driver.write_deck(os.path.join(run_dir, "input", "CaseH_n10.txt"), P)
+
+
+def ref_cuda_baseline(config, warmup, steps):
+    """The reference's own CUDA program recompiled for sm_100a
+    (baseline/build_ref_cuda.py), run on this config's deck in its file
+    formats; wall clock of `steps` steps after `warmup` (the patched timer,
+    a device synchronise on both sides).  Its step is the reference's: one
+    PPE sweep, every launch followed by cudaDeviceSynchronize."""
+    if not os.path.exists(REF_CUDA):
+        return {"unavailable": "baseline/_ref/sophia_gpu_sm100a not built (python baseline/build_ref_cuda.py)"}
+    from sph_b200 import decks
+    if config == "array":
+        P, p, _ = decks.cube_array(scale=1.0)
+        what = "uniform-resolution cube array at full size (the reference compiles no APR)"
+    else:
+        P, p = decks.canyon(scale=1.0)
+        what = "urban canyon at full size"
+    with tempfile.TemporaryDirectory() as run_dir:
+        t0 = time.perf_counter()
+        ref_cuda_inputs(run_dir, P, p, warmup + steps)
+        t_files = time.perf_counter() - t0
+        env = dict(os.environ, SOPHIA_WARMUP=str(warmup))
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_CUDA, "1"], cwd=run_dir, env=env, capture_output=True, text=True, timeout=1800)
+        t_run = time.perf_counter() - t0
+    line = [x for x in r.stdout.splitlines() if x.startswith("SOPHIA_TIMED")]
+    if r.returncode != 0 or not line:
+        return {"unavailable": f"reference program exit {r.returncode}: " + (r.stderr or r.stdout)[-300:]}
+    kv = dict(x.split("=") for x in line[-1].split()[1:])
+    k, sec = int(kv["steps"]), float(kv["seconds"])
+    return {"value": len(P) * k / sec, "unit": METRIC, "ms_per_step": 1e3 * sec / k, "steps": k, "warmup": warmup,
+            "particles": int(len(P)), "dtype": "f32",
+            "sample": f"{what}; the reference's step (one PPE sweep) as shipped, Case-H constants, recompiled "
+                      f"for sm_100a; wall clock with a device synchronise on both sides",
+            "input_files_s": t_files, "process_s": t_run}
+
+
 def nnps_check(P, p, boxes, local):
     """Cell hash, sort permutation, cell start/end and the neighbour lists of
     the timed deck (the records as the timed context held them after the
@@ -476,6 +533,8 @@ def main():
     ap.add_argument("--fp64-mode", default="bicgstab", choices=["gmres", "bicgstab", "idrs"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true",
+                    help="skip the reference's own CUDA program (baseline/_ref) on the config's deck")
     ap.add_argument("--no-nnps-check", action="store_true",
                     help="array config: skip the NNPS / neighbour-list comparison with the CPU oracle")
     ap.add_argument("--matrix-free", action="store_true")
@@ -802,6 +861,8 @@ def main():
         out["mixed_vs_fp64"] = value / fp64["value"] if fp64["value"] else None
     if args.config == "array" and not args.no_nnps_check:
         out["nnps_bit_exact"] = nnps_check(P, p, boxes, local)
+    if world == 1 and not args.no_ref_cuda and args.config in ("array", "canyon"):
+        out["ref_cuda_baseline"] = ref_cuda_baseline(args.config, 2, 5)
     if world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline_tgv(steps=4) if args.config == "tgv" else cpu_baseline(4, args.config)
         if args.config == "array":

@@ -87,3 +87,42 @@ def test_run_writes_reference_vtk_series(tmp_path):
     data = (out / "fluid_2stp.vtk").read_bytes()
     assert b"POINTS\t%d\tfloat" % alive.sum() in data
     assert any("tu_max" in line for line in log)
+
+
+def test_written_deck_and_solver_input_read_back(tmp_path):
+    """write_deck / write_solv produce files that the readers pinned to the
+    reference's own parser give back unchanged: the deck's records and every
+    k_vii / k_vif slot the solver input carries."""
+    import refhost
+    P, p = decks.canyon(scale=0.12)
+    p.setf("time_end", 0.0123)
+    p.seti("freq_output", 77)
+    deck = tmp_path / "deck.txt"
+    solv = tmp_path / "solv.txt"
+    driver.write_deck(deck, P)
+    driver.write_solv(solv, p)
+    Q = abi.read_deck(deck)
+    assert len(Q) == len(P)
+    for c in ("x", "y", "z", "ux", "uy", "uz", "m", "p_type", "h", "temp", "pres", "rho", "h_ref", "m_ref"):
+        assert np.array_equal(Q[c], P[c]), c
+    q, labels = abi.read_solv(solv, decks.default_params())
+    for slot in ("dim", "kernel_type", "time_type", "open_boundary", "fp_solve", "fv_solve", "fg_solve",
+                 "kgc_solve", "turbulence_model", "noslip_bc", "apr_solv", "freq_filt", "freq_output"):
+        assert q.geti(slot) == p.geti(slot), slot
+    for slot in ("kappa", "dt", "time", "time_end", "u_limit", "buffersize"):
+        assert np.float32(q.getf(slot)) == np.float32(p.getf(slot)), slot
+    assert labels == ["velocity", "pressure", "p_type"]
+    if refhost.available():
+        import ctypes
+        L = refhost.lib()
+        L.ref_read_solv.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p]
+        vii = np.zeros(64, np.int32)
+        vif = np.zeros(32, np.float32)
+        buf = ctypes.create_string_buffer(400)
+        L.ref_read_solv(str(solv).encode(), vii.ctypes.data_as(ctypes.c_void_p),
+                        vif.ctypes.data_as(ctypes.c_void_p), buf)
+        from sph_b200 import layout
+        for slot in ("dim", "kernel_type", "time_type", "open_boundary", "turbulence_model", "freq_output"):
+            assert int(vii[layout.VII[slot]]) == p.geti(slot), slot
+        for slot in ("dt", "time_end", "u_limit"):
+            assert vif[layout.VIF[slot]] == np.float32(p.getf(slot)), slot

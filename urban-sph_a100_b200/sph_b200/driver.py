@@ -30,6 +30,65 @@ from . import abi, params as _params
 from .layout import PART1
 
 
+# deck columns: the variable codes read_input (function_init.cuh:522-548)
+# understands for the fields a deck carries
+DECK_CODES = (1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 26, 27)
+_DECK_FIELDS = {1: "x", 2: "y", 3: "z", 4: "ux", 5: "uy", 6: "uz", 7: "m", 8: "p_type", 9: "h", 10: "temp",
+                11: "pres", 12: "rho", 26: "h_ref", 27: "m_ref"}
+
+
+def write_deck(path, P1):
+    """Writes records in the particle-deck format of read_input: a line of
+    tab-separated variable codes, then one line per record (p_type as an
+    integer, every other value with nine significant digits, enough to
+    round-trip an FP32 value)."""
+    cols = [_DECK_FIELDS[c] for c in DECK_CODES]
+    with open(path, "w") as f:
+        f.write("\t".join(str(c) for c in DECK_CODES) + "\n")
+        data = [np.asarray(P1[c]) for c in cols]
+        for k in range(len(P1)):
+            f.write("\t".join(str(int(v[k])) if c == "p_type" else "%.9g" % float(v[k])
+                              for c, v in zip(cols, data)) + "\n")
+
+
+_KERNEL_NAMES = {0: "Gaussian", 1: "Quintic", 2: "Quartic", 3: "Wendland2", 4: "Wendland4", 5: "Wendland6"}
+_TURB_NAMES = {0: "Laminar", 1: "k-lm", 2: "k-e", 3: "HB", 4: "SSM", 5: "DDF"}
+
+
+def write_solv(path, p, labels=("velocity", "pressure", "p_type")):
+    """Writes the keywords of read_solv_input (function_init.cuh:166-463)
+    that carry p's solver settings: kernel, time integration, open
+    boundary, force switches, turbulence model, no-slip walls, APR switch
+    and buffer size, kappa, time step, start and end time, filter and
+    output frequencies, plot variables and the velocity limit."""
+    yes = lambda v: "YES" if v else "NO"
+    lines = [
+        "solver_type : ISPH",
+        "dimension(1/2/3): %d" % p.geti("dim"),
+        "kernel type : %s" % _KERNEL_NAMES[p.geti("kernel_type")],
+        "time integration : %s" % ("Predictor_Corrector" if p.geti("time_type") == 1 else "Euler"),
+        "open boundary type: %s" % {1: "OPEN", 2: "PERIODIC"}.get(p.geti("open_boundary"), "NO"),
+        "pressure-force : %s" % yes(p.geti("fp_solve")),
+        "viscous-force : %s" % {1: "Cleary", 2: "Monaghan"}.get(p.geti("fv_solve"), "NO"),
+        "turbulence-model : %s" % _TURB_NAMES[p.geti("turbulence_model")],
+        "gravitational-force : %s" % yes(p.geti("fg_solve")),
+        "kernel-gradient-correction : %s" % yes(p.geti("kgc_solve")),
+        "noslip_boundary : %s" % yes(p.geti("noslip_bc")),
+        "APR_solve : %s" % ("Cell" if p.geti("apr_solv") else "NO"),
+        "Buffersize: %.9g" % p.getf("buffersize"),
+        "kappa: %.9g" % p.getf("kappa"),
+        "time-step : %.9g" % p.getf("dt"),
+        "start-time : %.9g" % p.getf("time"),
+        "end-time : %.9g" % p.getf("time_end"),
+        "filtering : %d" % max(p.geti("freq_filt"), 1),
+        "plot-output : %d" % max(p.geti("freq_output"), 1),
+        "plot-variables: %d %s" % (len(labels), " ".join(labels)),
+        "velocity-limit : %.9g" % p.getf("u_limit"),
+    ]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 def setup(solv_path, deck_path, base=None):
     """Parameters, plot labels and records (with APR headroom) of a case."""
     p = base.copy() if base is not None else _params.default_params()
