@@ -384,15 +384,29 @@ int sph_write_vtk(const char *path, const sph_part1 *P1, const sph_part2 *P2, co
 int sph_set_ib_boxes(sph_ctx *ctx, const double *boxes, int nbox);
 
 /* ---- adaptive particle refinement ----------------------------------------
- * One 3-D splitting pass (functions_APR.cuh:270-652, cell-based APR, which the
- * shipped reference does not compile): every cell splits the first fluid
- * particle whose target level exceeds its level log8(m_ref/m) by >= 0.75
- * into eight children (m/8, vol/8, h/2 with vii[36]) written into free
- * dummy records (i_type 3) the deck reserves; the parent becomes a dummy.
+ * One pass of the reference's cell-based 3-D APR, which the shipped reference
+ * does not compile (KERNEL_APR_condition3D_cell, functions_APR.cuh:270-403;
+ * Cell_index, functions_APR_etc.cuh:5-20; KERNEL_cell_APR_3D,
+ * functions_APR.cuh:406-652).  Per cell, the first particle whose target
+ * level M exceeds its level log(m_ref/m)/log(8) by >= 0.75 splits into eight
+ * children (m/8, vol/8, h/2 with vii[36], its family) written from 8 records
+ * past the first free dummy record (i_type 3) the deck reserves; the parent
+ * becomes a dummy.  Otherwise a complete family of eight whose members
+ * exceed M by more than 0.3 merges into one record (sums of m and vol, means
+ * of position, velocity and pressure, h = h_ref cbrt(m/m_ref) with vii[36];
+ * the reference's 2-D merge, KERNEL_cell_APR_2D, functions_APR.cuh:119-186,
+ * in 3-D) written to the tail records.  M is apr_max_level for fluid in NNPS
+ * cells within apr_zone of an IBM marker's cell, 0 elsewhere; families (the
+ * reference's blood_index) start as record index + 1 at the first pass.
  * Runs by itself every vii[37] steps when vii[35] = 1.  *n_split: cells
  * split; *n_wanted: cells that asked (more than the free records allow when
  * larger).  The next step rebuilds NNPS and the operators. */
 int sph_apr(sph_ctx *ctx, int32_t *n_split, int32_t *n_wanted);
+/* The APR state per record in the current (sorted) order: family (the
+ * reference's blood_index; 0 before the first pass) and target level (its
+ * M_num), and the families merged by the last pass.  Any pointer may be
+ * NULL.  Synchronises. */
+int sph_apr_state(sph_ctx *ctx, int32_t *family, float *target, int32_t *n_merged);
 
 /* ---- learned warm start of the pressure solve -----------------------------
  * No counterpart in the reference (it runs one pressure sweep per step).  A

@@ -98,3 +98,52 @@ class RefHost:
         L.ref_nnps(_p(P1), _p(P2), _p(SP1), _p(SP2), _p(self.g_idx), _p(self.p_idx),
                    _p(self.g_str), _p(self.g_end))
         return SP1, self.g_idx.copy(), self.p_idx.copy(), self.g_str.copy(), self.g_end.copy()
+
+
+APR_LIB_PATH = os.path.join(HERE, "_ref", "libsophia_ref_apr.so")
+_apr_lib = None
+
+
+def apr_available():
+    return os.path.exists(APR_LIB_PATH)
+
+
+def apr_lib():
+    """The reference's APR kernels compiled for the host (ref_apr_shim.cpp)."""
+    global _apr_lib
+    if _apr_lib is None:
+        L = ctypes.CDLL(APR_LIB_PATH)
+        vp = ctypes.c_void_p
+        L.refapr_set_params.argtypes = [vp, vp]
+        L.refapr_condition.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, vp, vp]
+        L.refapr_split.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, vp]
+        _apr_lib = L
+    return _apr_lib
+
+
+def ref_apr_pass(P, g_str, g_end, params, target, family, first_free):
+    """The reference's condition, numbering and split on a sorted state:
+    returns (apr_cond, apr_cell, records after the split, M_num, blood_index)."""
+    L = apr_lib()
+    vii = np.ctypeslib.as_array(params.vii).copy()
+    vif = np.ctypeslib.as_array(params.vif).copy()
+    L.refapr_set_params(_p(vii), _p(vif))
+    n = len(P)
+    nc = params.geti("num_cells")
+    R = np.ascontiguousarray(P.copy())
+    M = np.ascontiguousarray(target, np.float32)
+    B = np.ascontiguousarray(family, np.int32)
+    gs = np.ascontiguousarray(g_str, np.int32)
+    ge = np.ascontiguousarray(g_end, np.int32)
+    cond = np.zeros(n, np.int32)
+    cell = np.zeros(nc, np.int32)
+    L.refapr_condition(_p(R), n, _p(M), _p(B), _p(gs), _p(ge), _p(cond), _p(cell))
+    Mo = np.zeros(n, np.float32)
+    Bo = np.zeros(n, np.int32)
+    # KERNEL_cell_APR_3D writes children up to first_free + 8 * (splits + 1)
+    # without a bound: refuse states without that room
+    if first_free + 8 * (int((cell > 0).sum()) + 1) > n:
+        raise ValueError("not enough free records for the reference's split")
+    num_part = params.geti("num_part")
+    L.refapr_split(_p(R), n, int(first_free - num_part), _p(gs), _p(ge), _p(Mo), _p(Bo))
+    return cond, cell, R, Mo, Bo

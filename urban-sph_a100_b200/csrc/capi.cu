@@ -474,15 +474,24 @@ int sph_ml_predict_samples(sph_ctx *ctx, int64_t first, int32_t rows, float *y) 
 
 int sph_apr(sph_ctx *ctx, int32_t *n_split, int32_t *n_wanted) {
     if (!ctx) return SPH_ERR_BAD_ARG;
-    int a = 0, b = 0;
+    int a = 0, b = 0, m = 0;
     auto go = [&](auto *c) -> int {
         SPH_TRY(ensure_built(*c));
-        return apr_split(*c, &a, &b);
+        return apr_pass(*c, &a, &b, &m);
     };
     const int st = DISPATCH(ctx, go(ctx->f), go(ctx->d));
     if (n_split) *n_split = a;
     if (n_wanted) *n_wanted = b;
     return st;
+}
+
+int sph_apr_state(sph_ctx *ctx, int32_t *family, float *target, int32_t *n_merged) {
+    if (!ctx) return SPH_ERR_BAD_ARG;
+    auto go = [&](auto *c) -> int {
+        if (n_merged) *n_merged = c->apr_last_merged;
+        return apr_state(*c, family, target);
+    };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
 }
 
 int sph_set_ib_boxes(sph_ctx *ctx, const double *boxes, int nbox) {

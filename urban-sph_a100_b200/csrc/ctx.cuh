@@ -221,6 +221,12 @@ struct Ctx {
     int ml_nfluid = 0, ml_phase = 0;
     float *ml_part = nullptr, *ml_lpart = nullptr;        // per-block gradient / loss partials
     int ml_part_cap = 0;
+    // APR (apr.cu): family (the reference's blood_index) and target level
+    // (its M_num) per record, sorted with the records; allocated at the
+    // first pass
+    int *apr_family = nullptr;
+    float *apr_target = nullptr;
+    int apr_last_merged = 0;
     R4 *sc_u = nullptr;           // pass scratch
     Real *sc_p = nullptr, *sc_t = nullptr;
 
@@ -271,7 +277,8 @@ template <class Real> int neighbors_export(Ctx<Real> &c, int64_t *off, int32_t *
 template <class Real> int phase_interaction(Ctx<Real> &c);
 template <class Real> int phase_ppe(Ctx<Real> &c, sph_ppe_stats *st);
 template <class Real> int coarse_build(Ctx<Real> &c);
-template <class Real> int apr_split(Ctx<Real> &c, int *n_split, int *n_wanted);
+template <class Real> int apr_pass(Ctx<Real> &c, int *n_split, int *n_wanted, int *n_merged);
+template <class Real> int apr_state(Ctx<Real> &c, int32_t *family, float *target);
 template <class Real> int ml_prepare(Ctx<Real> &c, const Real *b, bool features);
 template <class Real> int ml_extrapolate(Ctx<Real> &c, double *x);
 template <class Real> int ml_warm_start(Ctx<Real> &c, const double *b, double *x, double *tmp);

@@ -232,6 +232,8 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     SPH_CUDA_TRY(cudaGetLastError());
     c.count = c.prm.vii[SPH_VII_COUNT];
     c.time = c.prm.vif[SPH_VIF_TIME];
+    c.release(c.apr_family);   // new records: APR families start again
+    c.release(c.apr_target);
     c.uploaded = true;
     c.built = false;
     c.gc_valid = false;
@@ -1109,6 +1111,7 @@ int nnps_build(Ctx<Real> &c) {
     SPH_TRY(regather(c, A.fb, scratch)); SPH_TRY(regather(c, A.fm, scratch)); SPH_TRY(regather(c, A.fl, scratch));
     SPH_TRY(regather(c, A.concn, scratch)); SPH_TRY(regather(c, A.enth, scratch));
     SPH_TRY(regather(c, c.rho_ref_A, scratch));
+    SPH_TRY(regather(c, c.apr_family, scratch)); SPH_TRY(regather(c, c.apr_target, scratch));
 
     // neighbour lists: count, slice widths, offsets, fill
     k_list<false><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, nullptr, nullptr,

@@ -1388,7 +1388,7 @@ int phase_time_update(Ctx<Real> &c) {
     // APR every freq_apr steps (vii[35] = 1: cell-based)
     const int freq_apr = c.prm.vii[SPH_VII_FREQ_APR];
     if (c.prm.vii[SPH_VII_APR_SOLV] == 1 && freq_apr > 0 && c.count % freq_apr == 0)
-        SPH_TRY(apr_split(c, nullptr, nullptr));
+        SPH_TRY(apr_pass(c, nullptr, nullptr, nullptr));
     return SPH_OK;
 }
 

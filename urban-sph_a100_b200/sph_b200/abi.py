@@ -29,7 +29,7 @@ SYMBOLS = (
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
-    "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
+    "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_apr_state", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
     "sph_read_solv", "sph_initial_records",
 )
 
@@ -99,6 +99,7 @@ def lib():
         L.sph_batch_particles.argtypes = [vp]
         L.sph_batch_particles.restype = i64
         L.sph_apr.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+        L.sph_apr_state.argtypes = [vp, vp, vp, ctypes.POINTER(i32)]
         L.sph_set_ib_boxes.argtypes = [vp, vp, i32]
         L.sph_read_deck.argtypes = [ctypes.c_char_p, vp, i32, ctypes.POINTER(i32)]
         L.sph_read_solv.argtypes = [ctypes.c_char_p, vp, vp, ctypes.POINTER(i32)]
@@ -239,6 +240,14 @@ class Simulation:
         return a.value, b.value
 
     # ---- learned warm start ----
+
+    def apr_state(self):
+        """(family, target level, families merged by the last pass) per record."""
+        fam = np.zeros(self.n, np.int32)
+        tgt = np.zeros(self.n, np.float32)
+        nm = ctypes.c_int32(0)
+        _check("sph_apr_state", lib().sph_apr_state(self.h, _p(fam), _p(tgt), ctypes.byref(nm)))
+        return fam, tgt, nm.value
     def ml_collect(self, every):
         _check("sph_ml_collect", lib().sph_ml_collect(self.h, int(every)))
 
