@@ -557,6 +557,9 @@ def main():
                          "extrapolation in time, or the learned "
                          "per-particle network (trained on this run's warm-up solves); default learned for the "
                          "array config, previous pressure otherwise")
+    ap.add_argument("--start-proj", default="none", choices=["none", "galerkin", "ls"],
+                    help="start vector projected on [previous pressure change, coarse correction of the start "
+                         "residual, network prediction with --warm learned]: Galerkin or least squares")
     ap.add_argument("--refinement", default="reliable", choices=["reliable", "restart-bicgstab", "restart-gmres",
                                                                   "restart-idrs"],
                     help="mixed_ir form: FP64 reliable updates, or refinement restarting the FP32 solver")
@@ -615,6 +618,8 @@ def main():
     if args.inner_tol > 0:
         p.ppe_inner_tol = args.inner_tol
     p.ppe_warm_start = {"extrap": 1, "scaled": 3}.get(args.warm, 0)
+    if args.start_proj != "none":
+        p.ppe_warm_start = 4 if args.start_proj == "galerkin" else 5
     # particle-steps count particles, not the periodic ghost records
     n = int((P["buffer_type"] != layout.BUFFER_PERIODIC_GHOST).sum())
     prec = layout.PREC_FP64 if args.precision == "fp64" else layout.PREC_MIXED
@@ -822,6 +827,7 @@ def main():
                    ("cached c_ij, 32-bit neighbour indices" if args.wide_index else "cached c_ij, 16-bit neighbour codes"),
                    "ppe_refinement": args.refinement,
                    "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],
+                   "ppe_start_projection": args.start_proj,
                    "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",
                                         "scaled": "previous pressure times its residual-minimising factor",
                                         "learned": "learned per-particle MLP on the previous pressure"}[args.warm],

@@ -214,6 +214,9 @@ struct Ctx {
     float *ml_pprev = nullptr;                            // p_old of the previous step
     bool ml_have_prev = false;
     double *ml_zd = nullptr, *ml_wd = nullptr;            // predicted change and its image
+    double *ml_W = nullptr, *ml_MW = nullptr, *ml_r0 = nullptr;   // subspace start: columns, images, r0
+    double *ml_subred = nullptr;                          // its reduction partials and small system
+    unsigned int *ml_subcnt = nullptr;
     __nv_bfloat16 *ml_SX = nullptr;                       // collected samples
     float *ml_St = nullptr;
     long long ml_cap = 0, ml_count = 0;
@@ -282,6 +285,8 @@ template <class Real> int apr_state(Ctx<Real> &c, int32_t *family, float *target
 template <class Real> int ml_prepare(Ctx<Real> &c, const Real *b, bool features);
 template <class Real> int ml_extrapolate(Ctx<Real> &c, double *x);
 template <class Real> int ml_warm_start(Ctx<Real> &c, const double *b, double *x, double *tmp);
+template <class Real> int ml_subspace_start(Ctx<Real> &c, const double *b, double *x, double *tmp, bool with_net,
+                                            bool galerkin);
 template <class Real> int ml_finish_step(Ctx<Real> &c);
 template <class Real> void ppe_apply_fp64(Ctx<Real> &c, const double *x, double *y);
 template <class Real> int ml_collect(Ctx<Real> &c, const double *xnew);

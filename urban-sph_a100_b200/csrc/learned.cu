@@ -589,6 +589,144 @@ int ml_warm_start(Ctx<Real> &c, const double *b, double *x, double *tmp) {
     return SPH_OK;
 }
 
+// ---- subspace start ---------------------------------------------------------
+// x0 = p_old + W y over up to three columns: the previous step's pressure
+// change (p_old - p_old of the step before), the coarse correction of the
+// start residual (Z E^-1 Z^T r0) and the network's predicted change; y solves
+// the projected system, Galerkin (W^T M W) y = W^T r0 or least squares
+// (MW)^T (MW) y = (MW)^T r0.
+constexpr int ML_SUB = 3;
+
+__global__ void k_ml_hist_dir(const int *kind, const float *pold, const float *pprev, double *w, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) w[i] = kind[i] == 1 ? (double)pold[i] - (double)pprev[i] : 0.0;
+}
+
+__global__ void k_ml_resid(const double *b, const double *mx, double *r, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = b[i] - mx[i];
+}
+
+// the k x k projected matrix and right-hand side (12 sums at most)
+__global__ void __launch_bounds__(256) k_ml_sub_dots(const double *W, const double *MW, const double *r, int k,
+                                                     int galerkin, int n, double *partials, unsigned int *counter,
+                                                     double *out) {
+    double v[ML_SUB * ML_SUB + ML_SUB];
+#pragma unroll
+    for (int q = 0; q < ML_SUB * ML_SUB + ML_SUB; ++q) v[q] = 0;
+    const size_t ns = (size_t)n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double a[ML_SUB], m[ML_SUB];
+#pragma unroll
+        for (int q = 0; q < ML_SUB; ++q) {
+            a[q] = q < k ? (galerkin ? W[q * ns + i] : MW[q * ns + i]) : 0.0;
+            m[q] = q < k ? MW[q * ns + i] : 0.0;
+        }
+        const double ri = r[i];
+#pragma unroll
+        for (int p = 0; p < ML_SUB; ++p) {
+#pragma unroll
+            for (int q = 0; q < ML_SUB; ++q) v[p * ML_SUB + q] += a[p] * m[q];
+            v[ML_SUB * ML_SUB + p] += a[p] * ri;
+        }
+    }
+    ml_reduce<ML_SUB * ML_SUB + ML_SUB>(v, partials, counter, [&](double *t) {
+        for (int q = 0; q < ML_SUB * ML_SUB + ML_SUB; ++q) out[q] = t[q];
+    });
+}
+
+// y of the k x k system by Gaussian elimination with partial pivoting (one
+// thread); a pivot below 1e-14 of the largest diagonal entry drops that
+// column (y = 0 for it)
+__global__ void k_ml_sub_solve(double *sys, int k) {
+    if (threadIdx.x || blockIdx.x) return;
+    double A[ML_SUB][ML_SUB], g[ML_SUB], y[ML_SUB];
+    int col[ML_SUB];
+    double dmax = 0;
+    for (int p = 0; p < k; ++p) {
+        for (int q = 0; q < k; ++q) A[p][q] = sys[p * ML_SUB + q];
+        g[p] = sys[ML_SUB * ML_SUB + p];
+        dmax = fmax(dmax, fabs(A[p][p]));
+        col[p] = 1;
+    }
+    for (int p = 0; p < k; ++p) {
+        int piv = p;
+        for (int q = p + 1; q < k; ++q)
+            if (fabs(A[q][p]) > fabs(A[piv][p])) piv = q;
+        if (!(fabs(A[piv][p]) > 1e-14 * dmax)) { col[p] = 0; continue; }
+        if (piv != p) {
+            for (int q = 0; q < k; ++q) { const double t = A[p][q]; A[p][q] = A[piv][q]; A[piv][q] = t; }
+            const double t = g[p]; g[p] = g[piv]; g[piv] = t;
+        }
+        for (int q = p + 1; q < k; ++q) {
+            const double f = A[q][p] / A[p][p];
+            for (int r = p; r < k; ++r) A[q][r] -= f * A[p][r];
+            g[q] -= f * g[p];
+        }
+    }
+    for (int p = k - 1; p >= 0; --p) {
+        if (!col[p]) { y[p] = 0; continue; }
+        double t = g[p];
+        for (int q = p + 1; q < k; ++q) t -= A[p][q] * y[q];
+        y[p] = t / A[p][p];
+        if (!isfinite(y[p])) y[p] = 0;
+    }
+    for (int p = 0; p < ML_SUB; ++p) sys[ML_SUB * ML_SUB + ML_SUB + p] = p < k ? y[p] : 0.0;
+}
+
+__global__ void k_ml_sub_update(const double *W, const double *y, int k, double *x, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double t = x[i];
+    for (int q = 0; q < k; ++q) t += y[q] * W[(size_t)q * n + i];
+    x[i] = t;
+}
+
+template <class Real>
+int ml_subspace_start(Ctx<Real> &c, const double *b, double *x, double *tmp, bool with_net, bool galerkin) {
+    const int n = c.n;
+    cudaStream_t st = c.stream;
+    if (!c.ml_W) {
+        SPH_TRY(c.alloc(c.ml_W, (size_t)ML_SUB * n));
+        SPH_TRY(c.alloc(c.ml_MW, (size_t)ML_SUB * n));
+        SPH_TRY(c.alloc(c.ml_r0, (size_t)n));
+        SPH_TRY(c.alloc(c.ml_subred, (size_t)(ML_SUB * ML_SUB + ML_SUB) * 1184 + 32));
+        SPH_TRY(c.alloc(c.ml_subcnt, 1));
+        SPH_CUDA_TRY(cudaMemsetAsync(c.ml_subcnt, 0, sizeof(unsigned int), st));
+    }
+    ppe_apply_fp64(c, x, tmp);
+    k_ml_resid<<<grid_for(n, 256), 256, 0, st>>>(b, tmp, c.ml_r0, n);
+    ++c.launches;
+    int k = 0;
+    if (c.ml_have_prev) {
+        k_ml_hist_dir<<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.ml_pold, c.ml_pprev, c.ml_W + (size_t)k * n, n);
+        ++c.launches;
+        ++k;
+    }
+    if (c.cg_m > 0) {
+        double *w = c.ml_W + (size_t)k * n;
+        SPH_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(double) * n, st));
+        coarse_apply<Real, double>(c, c.ml_r0, w);
+        ++k;
+    }
+    if (with_net) {
+        k_ml_infer<<<div_up(n, 128), 256, 0, st>>>(c.ml_X, nullptr, c.ml_w1b, c.ml_w2b, c.ml_w, c.ml_y, n);
+        k_ml_dir<<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.ml_y, (MlScal *)c.ml_sc, c.ml_W + (size_t)k * n, n);
+        c.launches += 2;
+        ++k;
+    }
+    if (k == 0) return SPH_OK;
+    for (int q = 0; q < k; ++q) ppe_apply_fp64(c, c.ml_W + (size_t)q * n, c.ml_MW + (size_t)q * n);
+    const int G = std::max(1, std::min((n + 255) / 256, 1184));
+    double *sys = c.ml_subred + (size_t)(ML_SUB * ML_SUB + ML_SUB) * 1184;
+    k_ml_sub_dots<<<G, 256, 0, st>>>(c.ml_W, c.ml_MW, c.ml_r0, k, galerkin ? 1 : 0, n, c.ml_subred, c.ml_subcnt, sys);
+    k_ml_sub_solve<<<1, 32, 0, st>>>(sys, k);
+    k_ml_sub_update<<<grid_for(n, 256), 256, 0, st>>>(c.ml_W, sys + ML_SUB * ML_SUB + ML_SUB, k, x, n);
+    c.launches += 3;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
 // samples of a converged solve: every k-th fluid row, offset rotating per step
 template <class Real>
 int ml_collect(Ctx<Real> &c, const double *xnew) {
@@ -791,6 +929,7 @@ int ml_predict_samples(Ctx<Real> &c, long long first, int rows, float *y) {
     template int ml_prepare<R>(Ctx<R> &, const R *, bool);                                               \
     template int ml_extrapolate<R>(Ctx<R> &, double *);                                                  \
     template int ml_warm_start<R>(Ctx<R> &, const double *, double *, double *);                         \
+    template int ml_subspace_start<R>(Ctx<R> &, const double *, double *, double *, bool, bool);         \
     template int ml_finish_step<R>(Ctx<R> &);                                                            \
     template int ml_collect<R>(Ctx<R> &, const double *);                                                \
     template int ml_grad<R>(Ctx<R> &, long long, int, float *, float *);                                 \

@@ -1790,10 +1790,12 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         c.init_relres = -1;
         const bool learned = mode == SPH_PPE_LEARNED && c.ml_ready;
         const bool extrap = c.prm.ppe_warm_start == 1;
-        const bool history = learned || c.ml_every > 0 || extrap;
+        const bool subspace = c.prm.ppe_warm_start == 4 || c.prm.ppe_warm_start == 5;
+        const bool history = learned || c.ml_every > 0 || extrap || subspace;
         if (history) SPH_TRY(ml_prepare(c, (const Real *)b, learned || c.ml_every > 0));
         if (extrap) SPH_TRY(ml_extrapolate(c, xd));
-        if (learned) SPH_TRY(ml_warm_start(c, bd, xd, rd));
+        if (subspace) SPH_TRY(ml_subspace_start(c, bd, xd, rd, learned, c.prm.ppe_warm_start == 4));
+        else if (learned) SPH_TRY(ml_warm_start(c, bd, xd, rd));
         if (!learned && c.prm.ppe_warm_start == 3) {
             apply_op<Real, double>(c, xd, rd, cached);
             k_start_factor<<<G, 256, 0, st>>>(bd, rd, n, c.red, counter, c.scal);
