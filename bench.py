@@ -156,7 +156,7 @@ def cpu_baseline(steps, config="canyon"):
             "seconds": dt}
 
 
-def cpu_converged_port(local, steps=1):
+def cpu_converged_port(local, steps=1, pforce_form=1):
     """Like-for-like CPU work: the CPU restatement of the step in FP64 with
     Jacobi-BiCGSTAB to 1e-6 (the plain form) on the refined cube array at
     scale 0.1, split by the GPU's APR passes; one thread."""
@@ -164,6 +164,7 @@ def cpu_converged_port(local, steps=1):
     from sph_b200 import abi, decks, layout
     P, p, boxes = decks.cube_array(scale=0.1, apr=True)
     p.ppe_pair_h = 1
+    p.pressure_force_form = pforce_form
     sim = abi.Simulation(p, precision=layout.PREC_MIXED, device=local)
     sim.set_ib_boxes(boxes)
     sim.upload(P)
@@ -557,6 +558,9 @@ def main():
                          "extrapolation in time, or the learned "
                          "per-particle network (trained on this run's warm-up solves); default learned for the "
                          "array config, previous pressure otherwise")
+    ap.add_argument("--pforce-form", default=None, choices=["active", "difference"],
+                    help="pressure-force pair term: the reference's active form, or its commented-out difference "
+                         "form (no force from a constant pressure); default difference with APR, else active")
     ap.add_argument("--start-proj", default="none", choices=["none", "galerkin", "ls"],
                     help="start vector projected on [previous pressure change, coarse correction of the start "
                          "residual, network prediction with --warm learned]: Galerkin or least squares")
@@ -614,6 +618,9 @@ def main():
     if args.pair_h is None:
         args.pair_h = "avg" if args.apr else "ref"
     p.ppe_pair_h = 1 if args.pair_h == "avg" else 0
+    if args.pforce_form is None:
+        args.pforce_form = "difference" if args.apr else "active"
+    p.pressure_force_form = 1 if args.pforce_form == "difference" else 0
     p.ppe_gmres_restart = args.gmres_restart
     if args.inner_tol > 0:
         p.ppe_inner_tol = args.inner_tol
@@ -828,6 +835,9 @@ def main():
                    "ppe_refinement": args.refinement,
                    "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],
                    "ppe_start_projection": args.start_proj,
+                   "pressure_force": {"active": "the reference's active pair term (Monaghan variation)",
+                                      "difference": "the reference's commented-out difference form "
+                                                    "-m_j (p_j - p_i) / (rho_i rho_j)"}[args.pforce_form],
                    "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",
                                         "scaled": "previous pressure times its residual-minimising factor",
                                         "learned": "learned per-particle MLP on the previous pressure"}[args.warm],
@@ -872,7 +882,7 @@ def main():
     if world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline_tgv(steps=4) if args.config == "tgv" else cpu_baseline(4, args.config)
         if args.config == "array":
-            out["cpu_converged_port"] = cpu_converged_port(local)
+            out["cpu_converged_port"] = cpu_converged_port(local, pforce_form=p.pressure_force_form)
     print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()

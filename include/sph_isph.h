@@ -213,7 +213,17 @@ typedef struct sph_params {
                                 factors are stored at the neighbour build (the
                                 particles never move) when they fit with a
                                 tenth of the device memory to spare          */
-    int32_t reserved[2];
+    int32_t pressure_force_form; /* pair term of the pressure force
+                                (KERNEL_pressureforce3D, functions_PPE.cuh:
+                                620-627): 0 (default) the reference's active
+                                "Monaghan variation" -2 m_j ((p_i + Pb) rho_j +
+                                (p_j + Pb) rho_i) / ((rho_i rho_j)(rho_i +
+                                rho_j)), Pb = 0; 1 its commented-out difference
+                                form -m_j (p_j - p_i) / (rho_i rho_j) (the
+                                "pressure stabilization (KDH)" line with its
+                                stabilisation term zero), which exerts no force
+                                for a constant pressure                       */
+    int32_t reserved;
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

@@ -14,19 +14,21 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libsophia_ref.so")
 
-_lib = None
+# host builds of the reference: as shipped (None), and with the pressure
+# force's commented-out difference form in place of its active line ("dp")
+VARIANTS = {None: LIB_PATH, "dp": os.path.join(HERE, "_ref", "libsophia_ref_dp.so")}
+_libs = {}
 
 
-def available():
-    return os.path.exists(LIB_PATH)
+def available(variant=None):
+    return os.path.exists(VARIANTS[variant])
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise FileNotFoundError(f"{LIB_PATH} not built (make -C oracle ref)")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(variant=None):
+    if variant not in _libs:
+        if not available(variant):
+            raise FileNotFoundError(f"{VARIANTS[variant]} not built (make -C oracle ref ref_dp)")
+        L = ctypes.CDLL(VARIANTS[variant])
         vp = ctypes.c_void_p
         L.ref_set_params.argtypes = [vp, vp]
         L.ref_get_params.argtypes = [vp, vp]
@@ -36,8 +38,8 @@ def lib():
         L.ref_set_parallel.argtypes = [ctypes.c_int]
         L.ref_set_boundary_variant.argtypes = [ctypes.c_int] * 3
         L.ref_num_threads.restype = ctypes.c_int
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def _p(a):
@@ -47,9 +49,9 @@ def _p(a):
 class RefHost:
     """Reference step on the host, one instance per deck."""
 
-    def __init__(self, P1, params, parallel=True):
+    def __init__(self, P1, params, parallel=True, variant=None):
         from sph_b200.layout import PART2, PART3
-        L = lib()
+        self.L = L = lib(variant)
         self.params = params.copy()
         self.n = len(P1)
         L.ref_set_parallel(1 if parallel else 0)
@@ -73,11 +75,11 @@ class RefHost:
     def _load_params(self):
         vii = np.ctypeslib.as_array(self.params.vii).copy()
         vif = np.ctypeslib.as_array(self.params.vif).copy()
-        lib().ref_set_params(_p(vii), _p(vif))
-        lib().ref_set_boundary_variant(int(self.params.outlet_bc), int(self.params.inlet_recycling), 0)
+        self.L.ref_set_params(_p(vii), _p(vif))
+        self.L.ref_set_boundary_variant(int(self.params.outlet_bc), int(self.params.inlet_recycling), 0)
 
     def step(self, nsteps=1, ppe_snapshot=True):
-        L = lib()
+        L = self.L
         self._load_params()
         for _ in range(nsteps):
             L.ref_step(_p(self.P1), _p(self.SP1), _p(self.P2), _p(self.SP2), _p(self.P3),
@@ -89,7 +91,7 @@ class RefHost:
 
     def nnps(self):
         """Step-0 NNPS only (ISPH_Calc.cuh:20-45) on a copy of P1."""
-        L = lib()
+        L = self.L
         self._load_params()
         P1 = np.array(self.P1, copy=True)
         P2 = np.array(self.P2, copy=True)

@@ -1481,7 +1481,11 @@ struct Oracle {
                 if (Q.kgc_solve() == 1) { tdwx = 0; tdwy = 0; tdwz = 0; }
                 Real mj = A.m[j], rhoj = A.rho[j], pj = A.pres[j] - A.pres0[j];
                 if (Q.fp_solve()) {
-                    Real C_p = -2.0 * mj / (rhoi * rhoj) * ((pi + 0.0) * rhoj + (pj + 0.0) * rhoi) / (rhoi + rhoj);
+                    // pressure_force_form 1: the commented-out difference form
+                    // of functions_PPE.cuh:626 with its stabilisation term zero
+                    Real C_p = prm.pressure_force_form == 1
+                                   ? -mj * (pj - pi) / (rhoi * rhoj)
+                                   : -2.0 * mj / (rhoi * rhoj) * ((pi + 0.0) * rhoj + (pj + 0.0) * rhoi) / (rhoi + rhoj);
                     tx += C_p * tdwx; ty += C_p * tdwy; tz += C_p * tdwz;
                 }
             }

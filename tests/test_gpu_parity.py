@@ -56,6 +56,10 @@ def _decks():
     out.append(("caseh_euler", (P, p)))
     # triply periodic box with periodic ghost records
     out.append(("tgv_periodic", decks.tgv_periodic(n=8)))
+    # the pressure force's difference form (pressure_force_form 1)
+    P, p = decks.canyon(scale=0.12)
+    p.pressure_force_form = 1
+    out.append(("canyon_difference_form", (P, p)))
     return out
 
 
@@ -184,14 +188,17 @@ def test_dormant_boundary_passes_match_oracle(name, precision, tol):
         assert np.abs(B["ux"][inlet]).max() > 0
 
 
+@pytest.mark.parametrize("form", [0, 1], ids=["active_form", "difference_form"])
 @pytest.mark.parametrize("precision,tol", [(layout.PREC_MIXED, FP32_TOL), (layout.PREC_FP64, FP64_TOL)],
                          ids=["fp32", "fp64"])
-def test_stored_pair_factors_match_full_evaluation(precision, tol):
+def test_stored_pair_factors_match_full_evaluation(precision, tol, form):
     """The prep pass and the pressure force with their time-invariant pair
     factors stored at the neighbour build (default) against the same passes
     evaluating every pair term each step (recompute_pairs = 1, the
-    reference's way), and switching between the two inside a run."""
+    reference's way), and switching between the two inside a run; with the
+    pressure force's active pair term and its difference form."""
     P, p = decks.caseh_mini(turbulence="DDF", seed=5)
+    p.pressure_force_form = form
     out = []
     for rp in (0, 1):
         q = p.copy()

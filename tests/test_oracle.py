@@ -131,6 +131,28 @@ def test_step_bit_exact_vs_reference(name):
         assert np.array_equal(R.SP2[f], B2[f]), f
 
 
+@pytest.mark.skipif(not refhost.available("dp"), reason="reference host build (difference form) absent")
+def test_difference_form_pressure_force_bit_exact_vs_reference():
+    """pressure_force_form = 1 against the reference compiled with its own
+    commented-out difference form in place of the active pair term."""
+    P, p = _deck(VARIANTS["ssm_cleary_w6"])
+    p.pressure_force_form = 1
+    R = refhost.RefHost(P, p, parallel=False, variant="dp")
+    O = restated.Restated(P, p, 0)
+    for _ in range(3):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, B2, B3 = O.download()
+    for f in FIELDS:
+        assert np.array_equal(R.P1[f], B[f]), f
+    for f in ("fpx", "fpy", "fpz", "ftotalx", "ftotal"):
+        assert np.array_equal(R.P3[f], B3[f]), f
+    # and the form changes the force: the shipped build differs
+    S = refhost.RefHost(P, p, parallel=False)
+    S.step(3)
+    assert not np.array_equal(S.P3["fpx"], B3["fpx"])
+
+
 def thermal_deck(con=1, bouss=1, concn=1):
     return decks.thermal_mini(con, bouss, concn)
 

@@ -37,6 +37,7 @@ DevParams make_dev_params(const sph_params &p) {
     d.concn_solve = p.vii[SPH_VII_CONCN_SOLVE];
     d.outlet_bc = p.outlet_bc;
     d.ppe_pair_h = p.ppe_pair_h;
+    d.pforce_form = p.pressure_force_form;
     d.inlet_recycling = p.inlet_recycling;
     d.rp_x = p.recycle_probe_x; d.rp_y = p.recycle_probe_y;
     for (int a = 0; a < 6; ++a) d.periodic_box[a] = p.periodic_box[a];
@@ -79,6 +80,9 @@ static int check_params(const sph_params &p) {
     if (p.n_profile < 2 || p.n_profile > SPH_MAX_PROFILE) { set_error("n_profile must be in [2, 32]"); return SPH_ERR_BAD_ARG; }
     if (!(p.vif[SPH_VIF_DT] > 0)) { set_error("dt must be positive"); return SPH_ERR_BAD_ARG; }
     if (p.outlet_bc < 0 || p.outlet_bc > 2) { set_error("outlet_bc must be 0, 1 or 2"); return SPH_ERR_BAD_ARG; }
+    if (p.pressure_force_form < 0 || p.pressure_force_form > 1) {
+        set_error("pressure_force_form must be 0 or 1"); return SPH_ERR_BAD_ARG;
+    }
     return SPH_OK;
 }
 
@@ -274,7 +278,8 @@ int sph_set_params(sph_ctx *ctx, const sph_params *p) {
         const sph_params &o = c->prm;
         if (p->vii[SPH_VII_KERNEL_TYPE] != o.vii[SPH_VII_KERNEL_TYPE] || p->vif[SPH_VIF_KAPPA] != o.vif[SPH_VIF_KAPPA] ||
             p->vii[SPH_VII_KGC_SOLVE] != o.vii[SPH_VII_KGC_SOLVE] || p->pressure_length != o.pressure_length ||
-            p->ppe_pair_h != o.ppe_pair_h || p->recompute_pairs != o.recompute_pairs) {
+            p->ppe_pair_h != o.ppe_pair_h || p->recompute_pairs != o.recompute_pairs ||
+            p->pressure_force_form != o.pressure_force_form) {
             c->gc_valid = false;
             c->coef_valid = false;
             c->prep_valid = false;

@@ -857,6 +857,10 @@ __global__ void k_copy_rows(const int *rows, int nrows, const typename V4<Real>:
 // dW = 0) once per neighbour build, and k_pressure_force_cached sums
 // (p_i rho_j + p_j rho_i) g_ij: one Real4 and the p_j gathers per pair
 // instead of ~50 flops.  Same sums up to the grouping of the products.
+// With pressure_force_form 1 the pair term is the reference's commented-out
+// difference form -m_j (p_j - p_i) / (rho_i rho_j) dW / r x_ij: the cache
+// then holds g_ij = -m_j / (rho_i^2 rho_j) dW / r x_ij and -rho_i, so the same
+// cached sum (p_i g.w + p_j rho_i) g_ij gives it.
 // ---------------------------------------------------------------------------
 template <class Real>
 __global__ void __launch_bounds__(128) k_pforce_cache(DevParams P, SoA<Real> s, LIST_ARGS,
@@ -881,10 +885,12 @@ __global__ void __launch_bounds__(128) k_pforce_cache(DevParams P, SoA<Real> s, 
             const Real tA = (xj.w == hi) ? tA_ii : calc_tmpA<Real>(P, hij);
             Real dw = calc_dwij<Real>(P, tA, hij, tdist);
             if (kgc) dw = 0;
-            const Real c = (Real)-2 * mj.x / ((rhoi * mj.y) * (rhoi + mj.y)) * dw / tdist;
+            // difference form: (p_i (-rho_i) + p_j rho_i) g with g = -m_j / (rho_i^2 rho_j) dW / r x_ij
+            const Real c = P.pforce_form == 1 ? -mj.x / ((rhoi * mj.y) * rhoi) * dw / tdist
+                                              : (Real)-2 * mj.x / ((rhoi * mj.y) * (rhoi + mj.y)) * dw / tdist;
             gx = c * dx; gy = c * dy; gz = c * dz;
         }
-        pw[e] = mk4<Real>(gx, gy, gz, mj.y);
+        pw[e] = mk4<Real>(gx, gy, gz, P.pforce_form == 1 ? -rhoi : mj.y);
     SELL_LOOP_END
 }
 
@@ -940,7 +946,8 @@ __global__ void __launch_bounds__(128) k_pressure_force(DevParams P, SoA<Real> s
             if (kgc) dw = 0;
             const auto mj = s.mr[j];
             const Real pj = p[j] - pres0[j];
-            const Real Cp = (Real)-2 * mj.x * (pi * mj.y + pj * rhoi) / ((rhoi * mj.y) * (rhoi + mj.y));
+            const Real Cp = P.pforce_form == 1 ? -mj.x * (pj - pi) / (rhoi * mj.y)
+                                               : (Real)-2 * mj.x * (pi * mj.y + pj * rhoi) / ((rhoi * mj.y) * (rhoi + mj.y));
             const Real f = Cp * dw / tdist;
             tx += f * dx; ty_ += f * dy; tz += f * dz;
         SELL_LOOP_END
