@@ -150,15 +150,16 @@ def numbering(flag):
 
 
 def execute(P, g_str, g_end, p, target, family, cond, num, first_free):
-    """Split and merge with the capacity rule of the CUDA pass; returns
+    """Split and merge with the capacity rule of the CUDA pass (children
+    while they fit, then merged records at the tail while they stay past the
+    children, both in cell order); returns
     (records, target, family, cells split, families merged)."""
     n = len(P)
     pos = int((num > 0).sum())
     neg = int((num < 0).sum())
     nfree = n - first_free
-    do_merge = 0 < neg <= nfree
-    tail = neg if do_merge else 0
-    max_split = max(0, min(pos, (nfree - tail - 8) // 8))
+    max_split = max(0, min(pos, (nfree - 8) // 8))
+    min_slot = first_free + 8 * (max_split + 1) if max_split > 0 else first_free
     Q = P.copy()
     T = np.array(target, np.float32, copy=True)
     F = np.array(family, np.int32, copy=True)
@@ -194,7 +195,7 @@ def execute(P, g_str, g_end, p, target, family, cond, num, first_free):
                     Q["h"][dst] = f32(0.5 * float(P["h"][j]))
             Q["i_type"][j] = 3
             continue
-        if not do_merge:
+        if n + q < min_slot:
             continue
         js = [j for j in range(s, e) if cond[j] == -1]
         if not js:

@@ -41,7 +41,8 @@
 // The free records are the dummies the deck reserves: after NNPS they form
 // the segment [cell_start[num_cells], n) of the sorted arrays.  A pass whose
 // children and merged records do not fit splits the cells in cell order
-// while they fit and skips the merges.  The particle set then changes, so the
+// while their children fit, then merges the cells in cell order while their
+// records at the tail stay past the children.  The particle set then changes, so the
 // next step rebuilds NNPS, lists, side lists and the PPE operator.
 #include <algorithm>
 #include <cmath>
@@ -164,10 +165,11 @@ __device__ void copy_record(Ctx<Real> &c, const float *target, float *target_w, 
 
 // KERNEL_cell_APR_3D: the split of the marked particle of every splitting
 // cell (number[k] > 0, at most max_split of them) and the merge of the
-// marked family member of every merging cell (number[k] < 0) when do_merge
+// marked family member of every merging cell (number[k] < 0) whose record
+// n + number[k] lies at or past min_slot
 template <class Real>
 __global__ void k_apr_execute(Ctx<Real> c, const int *number, const int *apr_cond, float *target, int *family,
-                              int first_free, int max_split, int do_merge, int h_change, int *merged) {
+                              int first_free, int max_split, int min_slot, int h_change, int *merged) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= c.num_cells) return;
     const int q = number[k];
@@ -209,7 +211,7 @@ __global__ void k_apr_execute(Ctx<Real> c, const int *number, const int *apr_con
         c.ty[j] = t;
         return;
     }
-    if (!do_merge) return;
+    if (c.n + q < min_slot) return;
     int j = -1;
     for (int a = s; a < e; ++a)
         if (apr_cond[a] == -1) { j = a; break; }
@@ -323,16 +325,17 @@ int apr_pass(Ctx<Real> &c, int *n_split, int *n_wanted, int *n_merged) {
         else if (hf[k] < 0) num[k] = -(++neg);
     }
     const int first_free = cs[0], nfree = n - first_free;
-    // merged records fill the tail; children start 8 records past the first free one
-    const int do_merge = (neg > 0 && neg <= nfree) ? 1 : 0;
-    const int tail = do_merge ? neg : 0;
-    const int max_split = std::max(0, std::min(pos, (nfree - tail - 8) / 8));
+    // children start 8 records past the first free one; merged records go to
+    // the tail, counting down, while they stay past the children
+    const int max_split = std::max(0, std::min(pos, (nfree - 8) / 8));
+    const int min_slot = max_split > 0 ? first_free + 8 * (max_split + 1) : first_free;
+    const int do_merge = (neg > 0 && n - 1 >= min_slot) ? 1 : 0;
     if (n_wanted) *n_wanted = pos;
     int hmerged = 0;
     if (max_split > 0 || do_merge) {
         SPH_CUDA_TRY(cudaMemcpyAsync(number, num.data(), sizeof(int) * NC, cudaMemcpyHostToDevice, st));
         k_apr_execute<Real><<<grid_for(NC, 256), 256, 0, st>>>(c, number, cond, c.apr_target, c.apr_family, first_free,
-                                                               max_split, do_merge, c.prm.vii[SPH_VII_H_CHANGE], merged);
+                                                               max_split, min_slot, c.prm.vii[SPH_VII_H_CHANGE], merged);
         ++c.launches;
         SPH_CUDA_TRY(cudaGetLastError());
         SPH_CUDA_TRY(cudaMemcpyAsync(&hmerged, merged, sizeof(int), cudaMemcpyDeviceToHost, st));
