@@ -561,6 +561,8 @@ def main():
     ap.add_argument("--pforce-form", default=None, choices=["active", "difference"],
                     help="pressure-force pair term: the reference's active form, or its commented-out difference "
                          "form (no force from a constant pressure); default difference with APR, else active")
+    ap.add_argument("--coef-half", action="store_true",
+                    help="FP32 operator applications read row-scaled FP16 coefficients (ppe_coef_half)")
     ap.add_argument("--start-proj", default="none", choices=["none", "galerkin", "ls"],
                     help="start vector projected on [previous pressure change, coarse correction of the start "
                          "residual, network prediction with --warm learned]: Galerkin or least squares")
@@ -612,6 +614,7 @@ def main():
     if args.matrix_free:
         p.ppe_matrix_free = 1
     p.ppe_wide_index = 1 if args.wide_index else 0
+    p.ppe_coef_half = 1 if args.coef_half else 0
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2, "restart-idrs": 3}[args.refinement]
     p.ppe_coarse_block = args.coarse
     p.ppe_coarse_mode = 1 if args.coarse_mode == "multiplicative" else 0
@@ -726,13 +729,15 @@ def main():
     # ---- other forms on the same deck, rank 0 only ----
     sim.close()
 
-    def timed_form(precision, mode, coarse, steps, keep=False):
+    def timed_form(precision, mode, coarse, steps, keep=False, weights=None):
         q = p.copy()
         q.ppe_mode = mode
         q.ppe_coarse_block = coarse
         sd = abi.Simulation(q, precision=precision, device=local)
         if boxes is not None:
             sd.set_ib_boxes(boxes)
+        if weights is not None:
+            sd.ml_set_weights(weights)
         sd.upload(P)
         for _ in range(2):
             sd.step(1)
@@ -780,7 +785,7 @@ def main():
         out.update(form_error(A, ref_state, p.getf("u_limit")))
         return out
 
-    fp64 = fp64_same = sweep = err64 = None
+    fp64 = fp64_same = sweep = err64 = learned_vs_prev = None
     if rank == 0:
         kd = max(3, args.steps // 4)
         fp64_mode = layout.PPE_GMRES if args.fp64_mode == "gmres" else layout.PPE_BICGSTAB
@@ -793,6 +798,14 @@ def main():
                 # FP64 with this run's preconditioner: isolates the precision change
                 fp64_same = timed_form(layout.PREC_FP64, layout.PPE_BICGSTAB, args.coarse, kd)
                 fp64_same.update({"solver": f"bicgstab + coarse {args.coarse}", "ppe_tol": args.tol})
+        if ml_weights is not None:
+            # the learned start against the previous pressure, same start, same steps
+            prev_same = timed_form(layout.PREC_MIXED, layout.PPE_MIXED_IR, args.coarse, kd)
+            learned_same = timed_form(layout.PREC_MIXED, layout.PPE_LEARNED, args.coarse, kd, weights=ml_weights)
+            learned_vs_prev = {"steps": kd, "previous_pressure": prev_same, "learned": learned_same,
+                               "iterations_saved_per_step": prev_same["ppe_iterations"] -
+                               learned_same["ppe_iterations"],
+                               "ms_saved_per_step": prev_same["ms_per_step"] - learned_same["ms_per_step"]}
         # the reference's own step semantics (one PPE sweep) on the same deck
         sweep = timed_form(layout.PREC_MIXED, layout.PPE_REF_SWEEP, 0, kd)
         for k in ("ppe_iterations", "rel_residual_max"):
@@ -831,7 +844,8 @@ def main():
                    "precision": "mixed FP32/FP64" if args.precision == "mixed" else "FP64",
                    "ppe": args.mode, "ppe_tol": args.tol,
                    "ppe_operator": "matrix-free" if args.matrix_free else
-                   ("cached c_ij, 32-bit neighbour indices" if args.wide_index else "cached c_ij, 16-bit neighbour codes"),
+                   ("cached c_ij, 32-bit neighbour indices" if args.wide_index else "cached c_ij, 16-bit neighbour codes")
+                   + (", FP16 row-scaled c_ij in the FP32 applications" if args.coef_half else ""),
                    "ppe_refinement": args.refinement,
                    "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],
                    "ppe_start_projection": args.start_proj,
@@ -870,6 +884,7 @@ def main():
         "error_vs_plain_fp64": err64,
         "fp64_same_preconditioner": fp64_same,
         "learned_warm_start": learned,
+        "learned_vs_previous_pressure": learned_vs_prev,
         "reference_step_semantics": sweep,
         "clocks": ck,
     }

@@ -223,7 +223,14 @@ typedef struct sph_params {
                                 "pressure stabilization (KDH)" line with its
                                 stabilisation term zero), which exerts no force
                                 for a constant pressure                       */
-    int32_t reserved;
+    int32_t ppe_coef_half;   /* 1: the FP32 operator applications of the mixed
+                                form read the cached coefficients as FP16,
+                                each row's c_ij divided by the row's largest
+                                |c_ij| (one FP32 scale per row): 2 bytes per
+                                stored entry instead of 4.  The FP64
+                                applications (true residuals, the solution
+                                the tolerance is checked on) keep the FP32
+                                coefficients                                  */
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

@@ -32,8 +32,9 @@ def rel_err(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
 
 
-def _gpu_step(P, p, precision, mode, tol, nsteps=1, matrix_free=False, coarse=0):
+def _gpu_step(P, p, precision, mode, tol, nsteps=1, matrix_free=False, coarse=0, coef_half=0):
     q = p.copy()
+    q.ppe_coef_half = coef_half
     q.ppe_mode = mode
     q.ppe_tol = tol
     q.ppe_max_iter = 4000
@@ -137,6 +138,21 @@ def test_mixed_coarse_reaches_tolerance_and_matches_fp64(deck):
     P, p = deck
     A, st32 = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_MIXED_IR, 1e-6, nsteps=2, coarse=2)
     for s in st32:
+        assert s.status == 0 and s.rel_residual <= 1e-6, (s.rel_residual, s.iterations, s.refinements)
+    B, _ = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_GMRES, 1e-9, nsteps=2)
+    assert rel_err(A["pres"], B["pres"]) <= MIXED_PRES_TOL
+    for f in ("ux", "uy", "uz"):
+        assert rel_err(A[f], B[f]) <= MIXED_TOL, f
+
+
+@pytest.mark.parametrize("coarse", [0, 2], ids=["jacobi", "two_level"])
+def test_fp16_coefficients_reach_tolerance_and_match_fp64(deck, coarse):
+    """ppe_coef_half: the FP32 applications read FP16 row-scaled c_ij; the
+    FP64 true residuals keep the FP32 coefficients, so the solve still ends
+    at ||b - Ap|| <= 1e-6 ||b|| and the step stays within the mixed form's bar."""
+    P, p = deck
+    A, st = _gpu_step(P, p, layout.PREC_MIXED, layout.PPE_MIXED_IR, 1e-6, nsteps=2, coarse=coarse, coef_half=1)
+    for s in st:
         assert s.status == 0 and s.rel_residual <= 1e-6, (s.rel_residual, s.iterations, s.refinements)
     B, _ = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_GMRES, 1e-9, nsteps=2)
     assert rel_err(A["pres"], B["pres"]) <= MIXED_PRES_TOL

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -154,6 +155,9 @@ struct Ctx {
     float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
     double *coef_d = nullptr;     // cached c_ij, FP64 form
     bool coef_valid = false;
+    __half *coef_h = nullptr;     // c_ij / (row's max |c_ij|) in FP16 (ppe_coef_half), mixed form
+    float *coef_rs = nullptr;     // the row scales
+    bool coef_h_valid = false;
     Real *ppe_gb = nullptr;       // cached rhs pair vectors g_ij (3 x SELL arrays)
     Real *vis_stage = nullptr;    // staging of the LES viscosity in the prep pass
     // time-invariant parts of the prep pass (particles never move): per row

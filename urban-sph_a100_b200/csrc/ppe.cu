@@ -232,6 +232,18 @@ __device__ __forceinline__ void load_coef4<double>(const double *p, double (&a)[
     const double2 w = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
     a[0] = v.x; a[1] = v.y; a[2] = w.x; a[3] = w.y;
 }
+template <>
+__device__ __forceinline__ void load_coef4<__half>(const __half *p, __half (&a)[4]) {
+    const uint2 v = __ldcs(reinterpret_cast<const uint2 *>(p));
+    a[0] = __ushort_as_half((unsigned short)(v.x & 0xffffu));
+    a[1] = __ushort_as_half((unsigned short)(v.x >> 16));
+    a[2] = __ushort_as_half((unsigned short)(v.y & 0xffffu));
+    a[3] = __ushort_as_half((unsigned short)(v.y >> 16));
+}
+template <class V, class C>
+__device__ __forceinline__ V coef_to(C a) { return (V)a; }
+template <>
+__device__ __forceinline__ float coef_to<float, __half>(__half a) { return __half2float(a); }
 struct List16 {
     const uint16_t *code;
     const int *row_cell, *cs;
@@ -267,13 +279,13 @@ __device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane
     for (int t = 0; t < 4; ++t) xj[t] = (!GUARD || k + t < cnt) ? x[j[t]] : xi;
 #pragma unroll
     for (int t = 0; t < 4; ++t)   // difference form, entries in list order
-        if (!GUARD || k + t < cnt) s += (V)a[t] * (xi - xj[t]);
+        if (!GUARD || k + t < cnt) s += coef_to<V, C>(a[t]) * (xi - xj[t]);
 }
 
 template <class V, class C, class D, class W, bool L16>
 __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, const int *__restrict__ kind,
                                                     const int *__restrict__ aux, LIST_ARGS, List16 l16,
-                                                    const C *__restrict__ coef,
+                                                    const C *__restrict__ coef, const float *__restrict__ rowscale,
                                                     const D *__restrict__ diag, const int *__restrict__ comp_id,
                                                     const double *__restrict__ cmean, const int *__restrict__ nm_rows,
                                                     const int *__restrict__ nm_off, const int *__restrict__ nm_nb,
@@ -325,7 +337,7 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         int k = 0;
         for (; k < full; k += 4) quad_step<L16, false, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s);
         if (k < cnt) quad_step<L16, true, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s);
-        yi = s;
+        yi = rowscale ? s * (V)rowscale[i] : s;
         if (comp_id) {
             const int cc = comp_id[i];
             if (cc >= 0) yi += (V)diag[i] * (V)cmean[cc];
@@ -335,6 +347,28 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         if (j >= 0) yi = xi - x[j];
     }
     y[i] = yi;
+}
+
+// FP16 copy of the cached FP32 coefficients of the fluid rows, each row
+// divided by its largest |c_ij| (kept as an FP32 row scale, 1 for rows
+// without entries); the padding of a row's last group of four is zeroed
+__global__ void __launch_bounds__(128) k_coef_half(const int *__restrict__ kind, const long long *__restrict__ slice_off,
+                                                   const int *__restrict__ ncnt, const float *__restrict__ coef,
+                                                   __half *__restrict__ ch, float *__restrict__ rs, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (kind[i] != 1) { rs[i] = 1.f; return; }
+    const long long sb = slice_off[i >> 5];
+    const int lane = i & 31, cnt = ncnt[i], padded = (cnt + 3) & ~3;
+    float mx = 0.f;
+    for (int k = 0; k < cnt; ++k) mx = fmaxf(mx, fabsf(coef[sell4(sb, lane, k)]));
+    const float scale = mx > 0.f ? mx : 1.f;
+    const float inv = 1.f / scale;
+    for (int k = 0; k < padded; ++k) {
+        const long long e = sell4(sb, lane, k);
+        ch[e] = __float2half_rn(k < cnt ? coef[e] * inv : 0.f);
+    }
+    rs[i] = scale;
 }
 
 // z += Z y_c (coarse correction) with the per-component mean of the result
@@ -667,23 +701,25 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
         // FP64 applications (true residuals) keep the FP64 weights
         const int nb_nm = div_up((long long)c.L.n_nm, 4), nb_sell = div_up((long long)n, 128);
         const List16 l16{c.nbr16, c.row_cell, c.cell_start, c.dp.NI, c.dp.NI * c.dp.NJ, c.num_cells + 1};
-#define SPMV_FUSED(C_, W_, COEF, NMW)                                                                              \
+#define SPMV_FUSED(C_, W_, COEF, RS, NMW)                                                                          \
     do {                                                                                                       \
         if (c.list16)                                                                                          \
             k_spmv_fused<V, C_, Real, W_, true><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                        \
-                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, c.diag, cid, cmean, \
-                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                                   \
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, RS, c.diag, cid,   \
+                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                            \
         else                                                                                                   \
             k_spmv_fused<V, C_, Real, W_, false><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                       \
-                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, c.diag, cid, cmean, \
-                c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                                   \
+                nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, RS, c.diag, cid,   \
+                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                            \
     } while (0)
-        if (sizeof(Real) == 4 && sizeof(V) == 4)
-            SPMV_FUSED(float, float, (const float *)c.coef, c.nm_owf);
+        if (sizeof(Real) == 4 && sizeof(V) == 4 && c.prm.ppe_coef_half && c.coef_h_valid)
+            SPMV_FUSED(__half, float, c.coef_h, c.coef_rs, c.nm_owf);
+        else if (sizeof(Real) == 4 && sizeof(V) == 4)
+            SPMV_FUSED(float, float, (const float *)c.coef, nullptr, c.nm_owf);
         else if (sizeof(Real) == 4)
-            SPMV_FUSED(float, double, (const float *)c.coef, c.nm_ow);
+            SPMV_FUSED(float, double, (const float *)c.coef, nullptr, c.nm_ow);
         else
-            SPMV_FUSED(double, double, c.coef_d, c.nm_ow);
+            SPMV_FUSED(double, double, c.coef_d, nullptr, c.nm_ow);
 #undef SPMV_FUSED
     } else {
         k_spmv_mf<Real, V><<<grid_for(n, 128), 128, 0, c.stream>>>(c.dp, c.row_kind, c.row_aux, c.pr, c.mr, c.jc, c.slice_off,
@@ -751,9 +787,11 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
         // them from L2.
         const double R = (double)sizeof(Real);
         const bool l16 = c.list16 && c.prm.ppe_matrix_free == 0;
-        double row = 8.0 + 2.0 * R + (l16 ? 4.0 : 0.0);
+        const bool half = sizeof(Real) == 4 && c.prm.ppe_coef_half && c.coef_h_valid && c.prm.ppe_matrix_free == 0;
+        double row = 8.0 + 2.0 * R + (l16 ? 4.0 : 0.0) + (half ? 4.0 : 0.0);
         if (c.n_comp > 0) row += 4.0 + R;
-        *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + (double)c.nnz * ((l16 ? 2.0 : 4.0) + R);
+        *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) +
+                 (double)c.nnz * ((l16 ? 2.0 : 4.0) + (half ? 2.0 : R));
         if (l16) *bytes += 4.0 * ((double)c.num_cells + 2.0);
         if (c.prm.ppe_matrix_free == 0)
             *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R) + (double)c.L.nm_nnz * (4.0 + R);
@@ -1721,6 +1759,7 @@ static int ensure_ppe_ws(Ctx<Real> &c) {
         SPH_CUDA_TRY(cudaMallocHost(&c.red_host, 64 * sizeof(double)));
     }
     if (!c.coef_valid) {
+        c.coef_h_valid = false;
         const size_t m = (size_t)std::max(c.nnz_padded, 1LL);
         if (sizeof(Real) == 4) { c.release(c.coef); SPH_TRY(c.alloc(c.coef, m)); }
         else { c.release(c.coef_d); SPH_TRY(c.alloc(c.coef_d, m)); }
@@ -1759,6 +1798,17 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     c.coef_valid = true;
+    if (sizeof(Real) == 4 && c.prm.ppe_coef_half && !c.coef_h_valid && mode != SPH_PPE_REF_SWEEP) {
+        c.release(c.coef_h);
+        c.release(c.coef_rs);
+        SPH_TRY(c.alloc(c.coef_h, (size_t)nnzp));
+        SPH_TRY(c.alloc(c.coef_rs, (size_t)n));
+        k_coef_half<<<grid_for(n, 128), 128, 0, st>>>(c.row_kind, c.slice_off, c.ncnt, (const float *)c.coef, c.coef_h,
+                                                       c.coef_rs, n);
+        ++c.launches;
+        SPH_CUDA_TRY(cudaGetLastError());
+        c.coef_h_valid = true;
+    }
     if (mode != SPH_PPE_REF_SWEEP && (!c.cg_valid || c.cg_block != c.prm.ppe_coarse_block))
         SPH_TRY(coarse_build(c));
 

@@ -124,7 +124,7 @@ class SphParams(ctypes.Structure):
         ("ppe_wide_index", ctypes.c_int32),
         ("recompute_pairs", ctypes.c_int32),
         ("pressure_force_form", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("ppe_coef_half", ctypes.c_int32),
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
         ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
