@@ -404,6 +404,11 @@ static int regather(Ctx<Real> &c, T *arr, void *scratch) {
 // The fill pass also writes the 16-bit codes of the pressure operator
 // (nbr16, row_cell; flag16 set when a row cannot be coded: a search radius
 // beyond two cells, or an offset beyond 8191 in its cell plane).
+// One warp per row: the lanes test 32 consecutive candidates of a cell run
+// at a time (coalesced loads of pf), __ballot_sync collects the kept ones
+// and each kept lane writes its entry at the row's count plus the kept
+// lanes below it (__popc), so the list keeps the visit order.  The count
+// pass (FILL false) sizes the SELL slices, the fill pass writes them.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restrict__ pf,
                                               const int4 *__restrict__ ty, const int *__restrict__ ncell,
@@ -411,10 +416,11 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
                                               const long long *__restrict__ slice_off, int *__restrict__ nbr,
                                               uint16_t *__restrict__ nbr16, int *__restrict__ row_cell,
                                               int *__restrict__ flag16, int n) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;   // uniform over the warp
     int cnt = 0;
-    if (FILL && nbr16) row_cell[i] = 0;
+    if (FILL && nbr16 && lane == 0) row_cell[i] = 0;
     if (ty[i].x != 3) {
         const float4 xi = pf[i];
         const int ic = search_axis(xi.x, P.xmin, P.xmax, P.dcell, P.NI);
@@ -422,13 +428,14 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
         const int kc = search_axis(xi.z, P.zmin, P.zmax, P.dcell, P.NK);
         const int nc = ncell[i];
         const int x0 = max(ic - nc, 0), x1 = min(ic + nc, P.NI - 1);
-        long long base = 0;
-        if (FILL) base = slice_off[i >> 5] + (i & 31);
+        long long sb = 0, base = 0;
+        if (FILL) { sb = slice_off[i >> 5]; base = sb + (i & 31); }
         const int rc = P.NI * jc + P.NI * P.NJ * kc + x0;
-        if (FILL && nbr16) {
+        if (FILL && nbr16 && lane == 0) {
             row_cell[i] = rc;
             if (nc > 2) atomicOr(flag16, 1);
         }
+        const float reach_i = xi.w;
         for (int dz = -nc; dz <= nc; ++dz) {
             const int zz = kc + dz;
             if (zz < 0 || zz > P.NK - 1) continue;
@@ -439,26 +446,31 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
                 const int kb = P.NI * yy + P.NI * P.NJ * zz;
                 const int s = cs[kb + x0], e = cs[kb + x1 + 1];
                 const int s16 = (FILL && nbr16) ? cs[plane_cell(rc, dz, P.NI, P.NI * P.NJ, P.num_cells + 1)] : 0;
-                for (int j = s; j < e; ++j) {
-                    const float4 xj = pf[j];
-                    const float r = dist_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z);
-                    if (r < __fmul_rn(P.skappa, fmaxf(xi.w, xj.w))) {
-                        if (FILL) {
-                            nbr[base + (long long)cnt * 32] = j;
-                            if (nbr16) {
-                                const int off = j - s16;
-                                if (off < 0 || off > (int)kCodeMask) atomicOr(flag16, 2);
-                                nbr16[sell4(slice_off[i >> 5], i & 31, cnt)] =
-                                    (uint16_t)(((unsigned)(dz + 2) << kCodeShift) | ((unsigned)off & kCodeMask));
-                            }
-                        }
-                        ++cnt;
+                for (int b0 = s; b0 < e; b0 += 32) {
+                    const int j = b0 + lane;
+                    bool keep = false;
+                    if (j < e) {
+                        const float4 xj = pf[j];
+                        const float r = dist_rn(xi.x, xi.y, xi.z, xj.x, xj.y, xj.z);
+                        keep = r < __fmul_rn(P.skappa, fmaxf(reach_i, xj.w));
                     }
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (FILL && keep) {
+                        const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+                        nbr[base + (long long)pos * 32] = j;
+                        if (nbr16) {
+                            const int off = j - s16;
+                            if (off < 0 || off > (int)kCodeMask) atomicOr(flag16, 2);
+                            nbr16[sell4(sb, i & 31, pos)] =
+                                (uint16_t)(((unsigned)(dz + 2) << kCodeShift) | ((unsigned)off & kCodeMask));
+                        }
+                    }
+                    cnt += __popc(m);
                 }
             }
         }
     }
-    if (!FILL) ncnt[i] = cnt;
+    if (!FILL && lane == 0) ncnt[i] = cnt;
 }
 
 // slice width (max count of the 32 particles of a slice, rounded up to a
@@ -1114,8 +1126,8 @@ int nnps_build(Ctx<Real> &c) {
     SPH_TRY(regather(c, c.apr_family, scratch)); SPH_TRY(regather(c, c.apr_target, scratch));
 
     // neighbour lists: count, slice widths, offsets, fill
-    k_list<false><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, nullptr, nullptr,
-                                                    nullptr, nullptr, nullptr, n);
+    k_list<false><<<grid_for(32LL * n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, nullptr,
+                                                           nullptr, nullptr, nullptr, nullptr, n);
     const int nslices = (n + 31) / 32;
     long long *w = (long long *)scratch;
     k_slice_width<<<grid_for(nslices, 256), 256, 0, st>>>(c.ncnt, w, n, nslices);
@@ -1138,8 +1150,9 @@ int nnps_build(Ctx<Real> &c) {
         c.row_cell_cap = std::max(n, 1);
     }
     SPH_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
-    k_list<true><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt, c.slice_off, c.nbr,
-                                                   want16 ? c.nbr16 : nullptr, c.row_cell, err, n);
+    k_list<true><<<grid_for(32LL * n, 128), 128, 0, st>>>(c.dp, c.pf, c.ty, c.ncell, c.cell_start, c.ncnt,
+                                                          c.slice_off, c.nbr, want16 ? c.nbr16 : nullptr, c.row_cell,
+                                                          err, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
     {
