@@ -135,6 +135,19 @@ def condition(P, g_str, g_end, p, target, family):
     return cond, flag
 
 
+def merge_cells(flag, cond, g_str, g_end):
+    """The merging cells of a pass: those holding a marked member (apr_cond -1);
+    the reference numbers every cell whose condition asked to merge, whose
+    slots stay unused when the cell holds no marked member."""
+    out = np.where(flag > 0, flag, 0).astype(np.int32)
+    for k in range(len(flag)):
+        if flag[k] > 0 or g_str[k] < 0:
+            continue
+        if (cond[int(g_str[k]):int(g_end[k])] == -1).any():
+            out[k] = -1
+    return out
+
+
 def numbering(flag):
     """Cell_index: +1, +2, ... for splitting cells, -1, -2, ... for merging cells."""
     num = np.zeros(len(flag), np.int32)
@@ -241,7 +254,7 @@ def apr_pass(P, g_idx, g_str, g_end, p, family=None):
         family = np.arange(1, len(P) + 1, dtype=np.int32)
     target = zone_target(P, g_idx, p)
     cond, flag = condition(P, g_str, g_end, p, target, family)
-    num, pos, neg = numbering(flag)
+    num, pos, neg = numbering(merge_cells(flag, cond, g_str, g_end))
     first_free = int(g_str[NC]) if g_str[NC] >= 0 else len(P)
     Q, T, F, ns, nm = execute(P, g_str, g_end, p, target, family, cond, num, first_free)
     return Q, T, F, ns, pos, nm

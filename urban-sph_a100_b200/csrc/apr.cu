@@ -12,7 +12,10 @@
 //     has M == 1, and the family member of largest index is marked
 //     (apr_cond = -1) and the cell asks to merge;
 //   * Cell_index (functions_APR_etc.cuh:5-20): splitting cells are numbered
-//     1, 2, ... and merging cells -1, -2, ... in cell order;
+//     1, 2, ... and merging cells -1, -2, ... in cell order; the merging
+//     cells here are those that hold a marked member (the reference numbers
+//     every cell whose condition asked, and the merge slots of cells without
+//     a marked member stay unused);
 //   * KERNEL_cell_APR_3D (functions_APR.cuh:406-652), split: the marked
 //     particle becomes eight children at k_num_part + num_buffer + 8 * number,
 //     i.e. from 8 records past the first free record: copies of the parent at
@@ -143,6 +146,20 @@ __global__ void k_apr_condition(Ctx<Real> c, const float *target, const int *fam
             }
     apr_cond[merge_index] = -1;   // the family member of largest index
     flag[k] = -1;
+}
+
+// merging cells are the cells that hold a marked member (wherever the
+// condition that marked it ran); a cell that asked to merge without holding
+// one gets no merge number
+template <class Real>
+__global__ void k_apr_merge_cells(Ctx<Real> c, const int *apr_cond, int *flag) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c.num_cells) return;
+    if (flag[k] > 0) return;
+    int f = 0;
+    for (int j = c.cell_start[k]; j < c.cell_start[k + 1]; ++j)
+        if (apr_cond[j] == -1) { f = -1; break; }
+    flag[k] = f;
 }
 
 template <class T>
@@ -311,7 +328,8 @@ int apr_pass(Ctx<Real> &c, int *n_split, int *n_wanted, int *n_merged) {
         k_apr_zone<<<grid_for(n, 256), 256, 0, st>>>(c.ty, c.pf, c.dp, reach, zone, n);
     k_apr_target<<<grid_for(n, 256), 256, 0, st>>>(c.ty, c.g_idx, zone, NC, std::max(max_level, 0), c.apr_target, n);
     k_apr_condition<Real><<<grid_for(NC, 256), 256, 0, st>>>(c, c.apr_target, c.apr_family, cond, flag);
-    c.launches += 3;
+    k_apr_merge_cells<Real><<<grid_for(NC, 256), 256, 0, st>>>(c, cond, flag);
+    c.launches += 4;
     SPH_CUDA_TRY(cudaGetLastError());
     // Cell_index in cell order, and the free records
     std::vector<int> hf(NC), cs(2);
