@@ -336,6 +336,7 @@ def run_ensemble(args, rank, world, local):
         p.ppe_mode = layout.PPE_MIXED_IR
         p.ppe_tol = 1e-6
         p.ppe_coarse_block = 3
+        p.ppe_refinement = 0 if args.host_control else 4   # each solve one graph under device control
         cases.append((P, p))
     b = abi.Batch(cases, precision=layout.PREC_MIXED, device=local)
     workers, probe_ms = b.autotune(probe_steps=1)
@@ -363,7 +364,9 @@ def run_ensemble(args, rank, world, local):
            "config": {"workload": f"batched ensemble: {args.cases} lid-driven cavity / Taylor-Green cases, "
                                   "20k-200k fluid particles each at dx = 0.01 m, Re in [100, 2000], seeded",
                       "particles": n, "cases": args.cases, "workers": workers, "autotune_probe_ms": probe_ms,
-                      "ppe": "mixed_ir + coarse 3", "parallelism": "replicas" if world > 1 else "single GPU"},
+                      "ppe": "mixed_ir + coarse 3, " + ("host-controlled Krylov loop" if args.host_control else
+                                                         "each solve one CUDA graph under device control"),
+                      "parallelism": "replicas" if world > 1 else "single GPU"},
            "ppe": {"iterations_mean": float(np.mean([s.iterations for s in stats])),
                    "rel_residual_max": float(max(s.rel_residual for s in stats)),
                    "not_converged_steps": sum(1 for s in stats if s.status != 0)},
@@ -525,6 +528,8 @@ def main():
     ap.add_argument("--dx", type=float, default=0.0075, help="transfer config: particle spacing of the cube array")
     ap.add_argument("--train-solves", type=int, default=40, help="transfer config: canyon solves sampled for training")
     ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--host-control", action="store_true",
+                    help="ensemble config: the host-controlled Krylov loop instead of the device-controlled one")
     ap.add_argument("--tol", type=float, default=None, help="PPE tolerance (default 1e-6; tgv config 1e-8)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of the timed form (mixed: FP32 fields and Krylov vectors, FP64 refinement)")

@@ -166,7 +166,15 @@ typedef struct sph_params {
     int32_t ppe_gmres_restart;   /* GMRES restart length (0: 40, max 64)       */
     int32_t ppe_refinement;  /* MIXED_IR: 0 reliable updates (default); 1 / 2 / 3
                                 iterative refinement restarting FP32 GMRES /
-                                BiCGSTAB / IDR(4) at every correction          */
+                                BiCGSTAB / IDR(4) at every correction; 4 the
+                                reliable updates under device control: the
+                                whole solve is one CUDA graph whose conditional
+                                nodes take the host loop's decisions, and
+                                sph_step reads the statistics once, after its
+                                last step (same iterates as 0; used when the
+                                context has its own stream and no live
+                                profiling, learned start or sample collection,
+                                else 0 runs)                                   */
     int32_t ppe_coarse_block;    /* BiCGSTAB preconditioner: 0 Jacobi; B > 0
                                 adds a coarse correction on aggregates of
                                 B x B x B NNPS cells (additive two-level)      */

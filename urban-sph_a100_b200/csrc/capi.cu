@@ -356,7 +356,11 @@ int sph_interaction(sph_ctx *ctx) {
 template <class Real>
 static int ppe_impl(Ctx<Real> &c, sph_ppe_stats *st) {
     if (!c.built) { set_error("sph_ppe before sph_interaction"); return SPH_ERR_STATE; }
-    return phase_ppe(c, st);
+    c.defer_stats = false;
+    sph_ppe_stats ps{};
+    SPH_TRY(phase_ppe(c, &ps));
+    if (st) *st = ps;
+    return ps.status < 0 ? ps.status : SPH_OK;
 }
 int sph_ppe(sph_ctx *ctx, sph_ppe_stats *stats) {
     if (!ctx) return SPH_ERR_BAD_ARG;
@@ -376,23 +380,45 @@ int sph_time_update(sph_ctx *ctx) {
 template <class Real>
 static int step_impl(Ctx<Real> &c, int nsteps, sph_ppe_stats *stats) {
     int last = SPH_OK;
+    // device-controlled solves (ppe_refinement = 4) leave their statistics on
+    // the device: the steps then follow one another without host waits, and
+    // the host reads the last solve's statistics and the worst status of all
+    // of them once, after the last step
+    SPH_TRY(dev_reset_worst(c));
+    c.defer_stats = true;
+    bool pending = false;
     for (int s = 0; s < nsteps; ++s) {
-        SPH_TRY(ensure_built(c));
-        SPH_CUDA_TRY(cudaEventRecord(c.ev[1], c.stream));
-        SPH_TRY(phase_interaction(c));
-        SPH_CUDA_TRY(cudaEventRecord(c.ev[2], c.stream));
+        int st = ensure_built(c);
+        if (st == SPH_OK) st = cudaEventRecord(c.ev[1], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+        if (st == SPH_OK) st = phase_interaction(c);
+        if (st == SPH_OK) st = cudaEventRecord(c.ev[2], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
         sph_ppe_stats ps{};
-        const int st = phase_ppe(c, &ps);
-        if (st < 0) return st;
-        SPH_CUDA_TRY(cudaEventRecord(c.ev[3], c.stream));
-        SPH_TRY(phase_time_update(c));
-        SPH_CUDA_TRY(cudaEventRecord(c.ev[6], c.stream));
-        SPH_CUDA_TRY(cudaEventSynchronize(c.ev[6]));
+        if (st == SPH_OK) st = phase_ppe(c, &ps);
+        if (st == SPH_OK) st = cudaEventRecord(c.ev[3], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+        if (st == SPH_OK) st = phase_time_update(c);
+        if (st == SPH_OK) st = cudaEventRecord(c.ev[6], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+        if (st < 0) { c.defer_stats = false; return st; }
+        pending = c.ppe_pending;
+        if (!pending) {
+            SPH_CUDA_TRY(cudaEventSynchronize(c.ev[6]));
+            cudaEventElapsedTime(&c.phase_ms[1], c.ev[1], c.ev[2]);
+            cudaEventElapsedTime(&c.phase_ms[2], c.ev[2], c.ev[3]);
+            cudaEventElapsedTime(&c.phase_ms[3], c.ev[3], c.ev[6]);
+            if (stats) *stats = ps;
+            last = ps.status;
+        }
+    }
+    c.defer_stats = false;
+    if (pending) {
+        sph_ppe_stats ps{};
+        int worst = SPH_OK;
+        SPH_TRY(dev_solve_stats(c, &ps, &worst));
         cudaEventElapsedTime(&c.phase_ms[1], c.ev[1], c.ev[2]);
         cudaEventElapsedTime(&c.phase_ms[2], c.ev[2], c.ev[3]);
         cudaEventElapsedTime(&c.phase_ms[3], c.ev[3], c.ev[6]);
         if (stats) *stats = ps;
-        last = ps.status;
+        if (worst < 0) { set_error("a device-controlled pressure solve broke down"); return worst; }
+        last = worst;
     }
     return last == SPH_NOT_CONVERGED ? SPH_NOT_CONVERGED : SPH_OK;
 }

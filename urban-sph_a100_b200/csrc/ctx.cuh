@@ -181,6 +181,9 @@ struct Ctx {
     void *idr_ws_r = nullptr;     // IDR(s) workspace in the context precision
     void *idr_ws_f = nullptr;     // IDR(s) workspace with FP32 vectors (inner solves of the refinement)
     void *kgraph = nullptr;       // CUDA graph of the mixed BiCGSTAB's iterations between host checks
+    void *devloop = nullptr;      // CUDA graph of a whole device-controlled solve (ppe_refinement = 4)
+    bool ppe_pending = false;     // a device-controlled solve whose statistics the host has not read
+    bool defer_stats = false;     // inside sph_step: leave those statistics until the last step
     bool kgraph_off = false;      // capture failed once: launch the kernels one by one
     double *xd = nullptr, *rd = nullptr, *bd = nullptr;   // FP64 solution / residual / rhs
     float *xf = nullptr, *bf = nullptr;                   // FP32 correction / residual
@@ -305,6 +308,8 @@ template <class Real, class V> void coarse_apply(Ctx<Real> &c, const V *r, V *z,
 // the caller adds Z c.cg_y
 template <class Real, class V> void coarse_restrict_solve(Ctx<Real> &c, const V *r, const V *w);
 template <class Real> int phase_time_update(Ctx<Real> &c);
+template <class Real> int dev_solve_stats(Ctx<Real> &c, sph_ppe_stats *S, int *worst);
+template <class Real> int dev_reset_worst(Ctx<Real> &c);
 template <class Real> int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax);
 template <class Real> int gradient_correction(Ctx<Real> &c);
 template <class Real> int neumann_pass(Ctx<Real> &c, VarSet<Real> &V);

@@ -1185,6 +1185,315 @@ static int bicgstab_reliable(Ctx<Real> &c, double *x, const double *b, double *y
 }
 
 // ---------------------------------------------------------------------------
+// The same mixed BiCGSTAB with FP64 reliable updates, its control on the
+// device (ppe_refinement = 4): one CUDA graph per solve, whose conditional
+// WHILE node runs `check` iterations and then k_dev_decide, the host loop's
+// decision as a kernel; conditional IF nodes run the reliable update
+// (replace) and the restart.  The host launches the graph and reads nothing
+// until the statistics are wanted, so steps follow one another on the stream
+// without host round trips.  The kernels and their order are those of
+// bicgstab_reliable, so the two give the same iterates.
+// Termination: every trip of the loop counts SC_TRIPS, and the loop ends
+// after maxit / check + 64 trips whatever the scalars say.
+// ---------------------------------------------------------------------------
+enum {
+    SC_MAXRR = SC_COUNT, SC_MAXIT, SC_UPDATES, SC_RESTARTS, SC_TRIPS, SC_TRIPCAP, SC_STATUS, SC_RELRES, SC_BN2,
+    SC_INITREL, SC_CONT, SC_DEV_END
+};
+static_assert(SC_DEV_END <= 32, "device scalars of the device-controlled solve overlap the reduction counter");
+
+__global__ void k_dev_tol(double *scal, double tol, int maxit, int check) {
+    double bb = scal[SC_BB];
+    if (!(bb > 0)) bb = 1.0;
+    scal[SC_BN2] = bb;
+    scal[SC_TOL2] = tol * tol * bb;
+    scal[SC_MAXIT] = maxit;
+    scal[SC_ITN] = 0;
+    scal[SC_UPDATES] = 0;
+    scal[SC_RESTARTS] = 0;
+    scal[SC_TRIPS] = 0;
+    scal[SC_TRIPCAP] = maxit / check + 64;
+    scal[SC_STATUS] = SPH_NOT_CONVERGED;
+    scal[SC_CONT] = 0;
+}
+
+// k_set_scal with the rho of the restart's residual, read on the device
+__global__ void k_dev_set_scal(double *scal) {
+    scal[SC_RHO] = scal[SC_RHO_NEW]; scal[SC_ALPHA] = 1; scal[SC_OMEGA] = 1; scal[SC_BETA] = 0;
+    scal[SC_FLAG] = FLAG_RUN;
+}
+
+// after a reliable update or a restart: the host loop's bookkeeping
+__device__ void dev_finalize(double *scal) {
+    const double rr = scal[SC_RR];
+    scal[SC_MAXRR] = rr;
+    scal[SC_RELRES] = sqrt(rr / scal[SC_BN2]);
+    if (rr <= scal[SC_TOL2]) { scal[SC_STATUS] = SPH_OK; scal[SC_CONT] = 0; }
+    else scal[SC_CONT] = scal[SC_ITN] < scal[SC_MAXIT] ? 1 : 0;
+}
+
+// after the first restart: start residual, and whether to iterate at all
+__global__ void k_dev_start(double *scal, cudaGraphConditionalHandle h_loop) {
+    dev_finalize(scal);
+    scal[SC_INITREL] = scal[SC_RELRES];
+    cudaGraphSetConditional(h_loop, scal[SC_CONT] != 0 ? 1u : 0u);
+}
+
+// after `check` iterations: restart on a breakdown, reliable update on
+// convergence of the recurrence, on a 10x drop or at maxit, else go on
+__global__ void k_dev_decide(double *scal, cudaGraphConditionalHandle h_rep, cudaGraphConditionalHandle h_res) {
+    const double trips = scal[SC_TRIPS] + 1;
+    scal[SC_TRIPS] = trips;
+    unsigned rep = 0, res = 0;
+    const double flag = scal[SC_FLAG], rr = scal[SC_RR];
+    if (trips > scal[SC_TRIPCAP]) {
+        scal[SC_CONT] = 0;
+    } else if (flag == FLAG_BREAKDOWN || !isfinite(rr)) {
+        scal[SC_RESTARTS] += 1;
+        if (scal[SC_RESTARTS] > 20) { scal[SC_STATUS] = SPH_ERR_BREAKDOWN; scal[SC_CONT] = 0; }
+        else { res = 1; scal[SC_UPDATES] += 1; }
+    } else if (flag == FLAG_CONVERGED || rr < RELIABLE_DELTA * RELIABLE_DELTA * scal[SC_MAXRR] ||
+               scal[SC_ITN] >= scal[SC_MAXIT]) {
+        rep = 1;
+        scal[SC_UPDATES] += 1;
+    } else {
+        scal[SC_MAXRR] = fmax(scal[SC_MAXRR], rr);
+        scal[SC_CONT] = 1;
+    }
+    cudaGraphSetConditional(h_rep, rep);
+    cudaGraphSetConditional(h_res, res);
+}
+
+// inside the reliable-update branch: a breakdown of the replaced residual
+// asks for a restart, else the bookkeeping
+__global__ void k_dev_after_replace(double *scal, cudaGraphConditionalHandle h_res) {
+    if (scal[SC_FLAG] == FLAG_BREAKDOWN) {
+        scal[SC_RESTARTS] += 1;
+        if (scal[SC_RESTARTS] > 20) {
+            scal[SC_STATUS] = SPH_ERR_BREAKDOWN;
+            scal[SC_CONT] = 0;
+            cudaGraphSetConditional(h_res, 0u);
+        } else {
+            cudaGraphSetConditional(h_res, 1u);
+        }
+        return;
+    }
+    dev_finalize(scal);
+}
+
+__global__ void k_dev_after_restart(double *scal) { dev_finalize(scal); }
+
+__global__ void k_dev_tail(const double *scal, cudaGraphConditionalHandle h_loop) {
+    cudaGraphSetConditional(h_loop, scal[SC_CONT] != 0 ? 1u : 0u);
+}
+
+struct DevLoopGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uintptr_t> key;
+    cudaStream_t s2 = nullptr, s3 = nullptr;   // capture streams of the loop body and its branches
+    ~DevLoopGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (s2) cudaStreamDestroy(s2);
+        if (s3) cudaStreamDestroy(s3);
+    }
+};
+
+// adds a conditional node at the capture position of `st` and returns its body graph
+static int add_conditional(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                           cudaGraph_t *body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    SPH_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) { set_error("device-controlled solve: stream not capturing"); return SPH_ERR_CUDA; }
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    SPH_CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &np));
+    *body = np.conditional.phGraph_out[0];
+    SPH_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return SPH_OK;
+}
+
+// Solves M x = b as bicgstab_reliable does, for the FP64 x (initial guess in
+// x, b_norm2 in scal[SC_BB]) with FP32 Krylov vectors and the cached operator,
+// under device control.  Returns after queueing the solve; the statistics
+// are in the device scalars (dev_solve_stats reads them).
+template <class Real>
+static int bicgstab_device(Ctx<Real> &c, double *x, const double *b, double *yd, double tol, int maxit) {
+    const int n = c.n;
+    cudaStream_t st = c.stream;
+    float *const *ws = (float *const *)c.kv;
+    float *r = ws[0], *rh = ws[1], *p = ws[2], *v = ws[3], *s = ws[4];
+    float *t = ws[5], *ph = ws[6], *sh = ws[7], *dinv = ws[8];
+    float *xlo = c.xf;
+    const int G = red_grid(n);
+    unsigned int *counter = (unsigned int *)(c.scal + 32);
+    const int check = 4;
+    auto *g = (DevLoopGraph *)c.devloop;
+    if (!g) {
+        g = new DevLoopGraph();
+        c.devloop = g;
+        SPH_CUDA_TRY(cudaStreamCreateWithFlags(&g->s2, cudaStreamNonBlocking));
+        SPH_CUDA_TRY(cudaStreamCreateWithFlags(&g->s3, cudaStreamNonBlocking));
+    }
+    std::vector<uintptr_t> key = krylov_graph_key(c, ws, xlo);
+    const uintptr_t extra[] = {(uintptr_t)x, (uintptr_t)b, (uintptr_t)yd, (uintptr_t)maxit, (uintptr_t)c.coef_h,
+                               (uintptr_t)c.coef_rs, (uintptr_t)(c.prm.ppe_coef_half && c.coef_h_valid),
+                               (uintptr_t)c.nm_ow, (uintptr_t)c.coef};
+    for (uintptr_t q : extra) key.push_back(q);
+    uint64_t tb;
+    memcpy(&tb, &tol, sizeof tb);
+    key.push_back((uintptr_t)tb);
+    if (!g->exec || g->key != key) {
+        if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
+        const long long l0 = c.launches;
+        auto replace = [&]() {
+            k_axpy_cast<float, double><<<grid_for(n, 256), 256, 0, c.stream>>>(xlo, x, n);
+            apply_op<Real, double>(c, x, yd, true);
+            k_reliable_replace<float><<<G, 256, 0, c.stream>>>(b, yd, r, xlo, rh, n, c.red, counter, c.scal);
+        };
+        auto restart = [&]() {
+            replace();
+            k_restart_dirs<float><<<G, 256, 0, c.stream>>>(r, rh, p, v, n);
+            k_norm2<float><<<G, 256, 0, c.stream>>>(r, n, c.red, counter, c.scal, SC_RHO_NEW);
+            k_dev_set_scal<<<1, 1, 0, c.stream>>>(c.scal);
+        };
+        auto iteration = [&]() {
+            k_p_update<float><<<G, 256, 0, c.stream>>>(p, ph, r, v, dinv, n, c.scal);
+            bool mr = precond_coarse<Real, float>(c, p, ph, v, true);
+            apply_op<Real, float>(c, ph, v, true, mr);
+            k_alpha<float><<<G, 256, 0, c.stream>>>(rh, v, n, c.red, counter, c.scal);
+            k_s_update<float><<<G, 256, 0, c.stream>>>(r, v, s, sh, dinv, n, c.scal);
+            mr = precond_coarse<Real, float>(c, s, sh, t, true);
+            apply_op<Real, float>(c, sh, t, true, mr);
+            k_omega<float><<<G, 256, 0, c.stream>>>(t, s, n, c.red, counter, c.scal);
+            k_xr_update<float><<<G, 256, 0, c.stream>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
+        };
+        cudaGraph_t graph = nullptr;
+        cudaGraphConditionalHandle h_loop, h_rep, h_res;
+        cudaGraph_t body = nullptr, body_rep = nullptr, body_res = nullptr;
+        int err = SPH_OK;
+        const bool prof = c.prof;
+        c.prof = false;   // event-record nodes are not allowed in conditional bodies
+        do {
+            if (cudaGraphCreate(&graph, 0) != cudaSuccess) { err = SPH_ERR_CUDA; break; }
+            if (cudaGraphConditionalHandleCreate(&h_loop, graph, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+                err = SPH_ERR_CUDA; break;
+            }
+            // the solve's start: the restart of bicgstab_reliable, then the loop
+            if (cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+                cudaSuccess) { err = SPH_ERR_CUDA; break; }
+            k_dev_tol<<<1, 1, 0, st>>>(c.scal, tol, maxit, check);
+            k_dinv<float, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
+            cudaMemsetAsync(xlo, 0, sizeof(float) * n, st);
+            restart();
+            k_dev_start<<<1, 1, 0, st>>>(c.scal, h_loop);
+            err = add_conditional(st, h_loop, cudaGraphCondTypeWhile, &body);
+            cudaGraph_t done = nullptr;
+            const cudaError_t e1 = cudaStreamEndCapture(st, &done);
+            if (err != SPH_OK || e1 != cudaSuccess) { if (err == SPH_OK) err = SPH_ERR_CUDA; break; }
+            // the loop body on s2, its two branches on s3
+            if (cudaGraphConditionalHandleCreate(&h_rep, body, 0, cudaGraphCondAssignDefault) != cudaSuccess ||
+                cudaGraphConditionalHandleCreate(&h_res, body, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+                err = SPH_ERR_CUDA; break;
+            }
+            c.stream = g->s2;
+            if (cudaStreamBeginCaptureToGraph(g->s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+                cudaSuccess) { err = SPH_ERR_CUDA; c.stream = st; break; }
+            for (int q = 0; q < check; ++q) iteration();
+            k_dev_decide<<<1, 1, 0, g->s2>>>(c.scal, h_rep, h_res);
+            err = add_conditional(g->s2, h_rep, cudaGraphCondTypeIf, &body_rep);
+            if (err == SPH_OK) err = add_conditional(g->s2, h_res, cudaGraphCondTypeIf, &body_res);
+            if (err == SPH_OK) k_dev_tail<<<1, 1, 0, g->s2>>>(c.scal, h_loop);
+            cudaGraph_t done2 = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(g->s2, &done2);
+            if (err != SPH_OK || e2 != cudaSuccess) { if (err == SPH_OK) err = SPH_ERR_CUDA; c.stream = st; break; }
+            // the reliable update, then the restart branch
+            c.stream = g->s3;
+            bool ok = cudaStreamBeginCaptureToGraph(g->s3, body_rep, nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                replace();
+                k_dev_after_replace<<<1, 1, 0, g->s3>>>(c.scal, h_res);
+                cudaGraph_t done3 = nullptr;
+                ok = cudaStreamEndCapture(g->s3, &done3) == cudaSuccess;
+            }
+            if (ok) ok = cudaStreamBeginCaptureToGraph(g->s3, body_res, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                restart();
+                k_dev_after_restart<<<1, 1, 0, g->s3>>>(c.scal);
+                cudaGraph_t done4 = nullptr;
+                ok = cudaStreamEndCapture(g->s3, &done4) == cudaSuccess;
+            }
+            c.stream = st;
+            if (!ok) { err = SPH_ERR_CUDA; break; }
+            if (cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) { g->exec = nullptr; err = SPH_ERR_CUDA; break; }
+            g->key = key;
+        } while (0);
+        c.prof = prof;
+        c.stream = st;
+        c.launches = l0;
+        if (graph) cudaGraphDestroy(graph);
+        if (err != SPH_OK || !g->exec) {
+            const cudaError_t e = cudaGetLastError();
+            static thread_local std::string msg;
+            msg = std::string("device-controlled solve: graph construction failed: ") + cudaGetErrorString(e);
+            set_error(msg.c_str());
+            return SPH_ERR_CUDA;
+        }
+    }
+    SPH_CUDA_TRY(cudaGraphLaunch(g->exec, st));
+    ++c.launches;
+    return SPH_OK;
+}
+
+// worst status of the device-controlled solves since the last reset
+// (scal[48]: most negative error, scal[49]: 1 when a solve did not converge)
+__global__ void k_dev_record(double *scal) {
+    const double stt = scal[SC_STATUS];
+    if (stt < 0) scal[48] = fmin(scal[48], stt);
+    else if (stt > 0) scal[49] = 1;
+}
+
+// statistics of the last device-controlled solve (synchronises the stream)
+template <class Real>
+int dev_solve_stats(Ctx<Real> &c, sph_ppe_stats *S, int *worst) {
+    double h[64];
+    SPH_CUDA_TRY(cudaMemcpyAsync(h, c.scal, sizeof(double) * 64, cudaMemcpyDeviceToHost, c.stream));
+    SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    S->status = (int)h[SC_STATUS];
+    S->iterations = (int)h[SC_ITN];
+    S->refinements = (int)h[SC_UPDATES];
+    S->restarts = (int)h[SC_RESTARTS];
+    S->rel_residual = h[SC_RELRES];
+    S->initial_residual = h[SC_INITREL];
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c.ev[4], c.ev[5]);
+    S->solve_ms = ms;
+    c.last_ppe = *S;
+    c.ppe_pending = false;
+    if (worst) *worst = h[48] < 0 ? (int)h[48] : (h[49] > 0 ? SPH_NOT_CONVERGED : SPH_OK);
+    return SPH_OK;
+}
+
+__global__ void k_dev_reset_worst(double *scal) { scal[48] = 0; scal[49] = 0; }
+
+template <class Real>
+int dev_reset_worst(Ctx<Real> &c) {
+    if (!c.scal) return SPH_OK;
+    k_dev_reset_worst<<<1, 1, 0, c.stream>>>(c.scal);
+    ++c.launches;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+// ---------------------------------------------------------------------------
 // IDR(s), the biorthogonal variant of van Gijzen & Sonneveld ("Algorithm
 // 913: an elegant IDR(s) variant that efficiently exploits
 // bi-orthogonality properties", ACM TOMS 38, 2011), right preconditioned
@@ -1831,6 +2140,32 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         unsigned int *counter = (unsigned int *)(c.scal + 32);
         k_norm2<double><<<G, 256, 0, st>>>(bd, n, c.red, counter, c.scal, SC_BB);
         c.launches += 2;
+        // ppe_refinement = 4: the mixed form's solve under device control, the
+        // host reading nothing until the statistics are wanted (only without
+        // live timing, learned / extrapolated / scaled start vectors and
+        // sample collection, which need the host; else the host-controlled loop)
+        const bool devloop = sizeof(Real) == 4 && mode == SPH_PPE_MIXED_IR && c.prm.ppe_refinement == 4 && cached &&
+                             st != nullptr && !c.prof && c.ml_every == 0 && c.prm.ppe_warm_start == 0;
+        if (devloop) {
+            const double tol = c.prm.ppe_tol > 0 ? c.prm.ppe_tol : 1e-6;
+            const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
+            SPH_TRY(bicgstab_device(c, xd, bd, rd, tol, maxit));
+            k_dev_record<<<1, 1, 0, st>>>(c.scal);
+            k_cast<double, Real><<<grid_for(n, 256), 256, 0, st>>>(xd, c.S.p, n);
+            c.launches += 2;
+            SPH_CUDA_TRY(cudaEventRecord(c.ev[5], st));
+            SPH_TRY(neumann_pass(c, c.S));
+            SPH_TRY(outlet_pass(c, c.S));
+            SPH_CUDA_TRY(cudaGetLastError());
+            c.ppe_pending = true;
+            if (!c.defer_stats) {
+                sph_ppe_stats S2{};
+                SPH_TRY(dev_solve_stats(c, &S2, nullptr));
+                if (stats) *stats = S2;
+                return S2.status < 0 ? S2.status : SPH_OK;
+            }
+            return SPH_OK;
+        }
         SPH_CUDA_TRY(cudaMemcpyAsync(c.red_host, c.scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, st));
         SPH_CUDA_TRY(cudaStreamSynchronize(st));
         double bb = c.red_host[SC_BB];
@@ -1922,7 +2257,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             if (trace) fprintf(stderr, "FP32 solve st %d it %d rel %.3e\n", status, iters, relres);
             k_cast<float, double><<<grid_for(n, 256), 256, 0, st>>>(c.xf, xd, n);
             ++c.launches;
-        } else if (c.prm.ppe_refinement == 0) {
+        } else if (c.prm.ppe_refinement == 0 || c.prm.ppe_refinement == 4) {
             // FP32 BiCGSTAB with FP64 reliable updates; FP64 BiCGSTAB from
             // its last iterate if the FP32 recurrence breaks down
             status = bicgstab_reliable(c, xd, bd, rd, bb, tol, maxit, cached, &iters, &relres, &refinements, &restarts);
@@ -2022,6 +2357,8 @@ void release_solver_ws(Ctx<Real> &c) {
         delete g;
         c.kgraph = nullptr;
     }
+    delete (DevLoopGraph *)c.devloop;
+    c.devloop = nullptr;
     c.gm_ws_r = nullptr;
     c.gm_ws_d = nullptr;
     c.idr_ws_r = nullptr;
@@ -2030,6 +2367,8 @@ void release_solver_ws(Ctx<Real> &c) {
 
 #define INST(R) template int phase_ppe<R>(Ctx<R> &, sph_ppe_stats *); \
     template void release_solver_ws<R>(Ctx<R> &); \
+    template int dev_solve_stats<R>(Ctx<R> &, sph_ppe_stats *, int *); \
+    template int dev_reset_worst<R>(Ctx<R> &); \
     template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int); \
     template int operator_bytes<R>(Ctx<R> &, double *, double *); \
     template void ppe_apply_fp64<R>(Ctx<R> &, const double *, double *);
