@@ -339,7 +339,7 @@ def run_ensemble(args, rank, world, local):
         p.ppe_refinement = 0 if args.host_control else 4   # each solve one graph under device control
         cases.append((P, p))
     b = abi.Batch(cases, precision=layout.PREC_MIXED, device=local)
-    workers, probe_ms = b.autotune(probe_steps=1)
+    workers, pair_block, probe_ms = b.autotune_shapes(probe_steps=1)
     b.step(max(args.warmup - 1, 1))
     clocks = Clocks(local)
     torch.cuda.synchronize()
@@ -363,7 +363,8 @@ def run_ensemble(args, rank, world, local):
            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
            "config": {"workload": f"batched ensemble: {args.cases} lid-driven cavity / Taylor-Green cases, "
                                   "20k-200k fluid particles each at dx = 0.01 m, Re in [100, 2000], seeded",
-                      "particles": n, "cases": args.cases, "workers": workers, "autotune_probe_ms": probe_ms,
+                      "particles": n, "cases": args.cases, "workers": workers, "pair_pass_threads": pair_block,
+                      "autotune_probe_ms": probe_ms,
                       "ppe": "mixed_ir + coarse 3, " + ("host-controlled Krylov loop" if args.host_control else
                                                          "each solve one CUDA graph under device control"),
                       "parallelism": "replicas" if world > 1 else "single GPU"},

@@ -359,6 +359,11 @@ int64_t sph_launch_count(sph_ctx *ctx);
  * neighbour: index and coefficient; the gathered x_j are not counted).
  * `reset` clears the counters after reading. */
 int sph_profile(sph_ctx *ctx, int enable);
+/* Threads per block of the per-step pair passes (prep, no-slip walls,
+ * advection, pressure force): 32, 64 or 128 (default).  No counterpart in
+ * the reference (128 threads per block everywhere, ISPH_Calc.cuh:12).  The
+ * results do not depend on it. */
+int sph_set_pair_block(sph_ctx *ctx, int threads);
 int sph_operator_stats(sph_ctx *ctx, int64_t *launches, double *total_ms, double *bytes_per_launch, int reset);
 /* Algorithmic bytes of one operator launch in two accountings: `stored` is
  * the figure of sph_operator_stats (what the launch's layout streams,
@@ -487,6 +492,10 @@ int sph_batch_step(sph_batch *b, int nsteps, sph_ppe_stats *stats);
  * reports it (the probe steps advance the cases). */
 int sph_batch_set_workers(sph_batch *b, int workers);
 int sph_batch_autotune(sph_batch *b, int probe_steps, int *workers, double *ms_per_step);
+/* sph_batch_autotune, then the thread-block size of the per-step pair passes
+ * (128, 64 or 32 threads, the same for every case) from probe steps at the
+ * chosen worker count; keeps and reports the fastest of both. */
+int sph_batch_autotune_shapes(sph_batch *b, int probe_steps, int *workers, int *pair_block, double *ms_per_step);
 /* The context of case k (owned by the batch), e.g. for sph_download. */
 int sph_batch_case(sph_batch *b, int k, sph_ctx **ctx);
 int64_t sph_batch_particles(sph_batch *b);

@@ -5,12 +5,17 @@
 // each one; the GPU runs the kernels of all streams side by side, so cases
 // of 20k-200k particles, each too small to fill 148 SMs, fill the device
 // together.  The number of workers, i.e. how many cases are in flight at
-// once, is chosen by sph_batch_autotune from timed probe steps.
+// once, is chosen by sph_batch_autotune from timed probe steps;
+// sph_batch_autotune_shapes then also picks the thread-block size of the
+// per-step pair passes (128, 64 or 32 threads: small cases fill the 148 SMs
+// with more, smaller blocks).
 //
-// A case's step is not one CUDA graph: the Krylov solver tests convergence
-// on the host every few iterations.  The iterations between two tests are
-// one graph (captured once per context and replayed, ppe.cu), since every
-// case runs on its own stream.
+// With ppe_refinement = 4 each case's pressure solve is one CUDA graph whose
+// conditional nodes take the convergence decisions on the device (ppe.cu),
+// and sph_step reads a case's statistics once, after its last step: a
+// worker queues all the steps of its case without waiting on the GPU.
+// Without it the Krylov solver tests convergence on the host every few
+// iterations, the iterations between two tests being one graph.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -30,6 +35,8 @@ struct sph_batch {
     std::vector<int64_t> n;
     std::vector<int> order;   // case indices, largest first
 };
+
+#define SPH_TRY_BATCH(x) do { const int s_ = (x); if (s_ < 0) return s_; } while (0)
 
 namespace {
 
@@ -133,6 +140,29 @@ int sph_batch_autotune(sph_batch *b, int probe_steps, int *workers, double *ms_p
     }
     b->workers = best;
     if (workers) *workers = best;
+    if (ms_per_step) *ms_per_step = best_ms / probe_steps;
+    return SPH_OK;
+}
+
+int sph_batch_autotune_shapes(sph_batch *b, int probe_steps, int *workers, int *pair_block, double *ms_per_step) {
+    if (!b || probe_steps <= 0) return SPH_ERR_BAD_ARG;
+    int w = 0;
+    double best_ms = 0;
+    SPH_TRY_BATCH(sph_batch_autotune(b, probe_steps, &w, &best_ms));
+    int best = 128;
+    for (int threads : {64, 32}) {
+        for (sph_ctx *c : b->ctx) SPH_TRY_BATCH(sph_set_pair_block(c, threads));
+        for (cudaStream_t s : b->streams) cudaStreamSynchronize(s);
+        const auto t0 = std::chrono::steady_clock::now();
+        const int st = run(b, probe_steps, b->workers, nullptr);
+        for (cudaStream_t s : b->streams) cudaStreamSynchronize(s);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (st < 0) return st;
+        if (ms < best_ms) { best_ms = ms; best = threads; }
+    }
+    for (sph_ctx *c : b->ctx) SPH_TRY_BATCH(sph_set_pair_block(c, best));
+    if (workers) *workers = w;
+    if (pair_block) *pair_block = best;
     if (ms_per_step) *ms_per_step = best_ms / probe_steps;
     return SPH_OK;
 }

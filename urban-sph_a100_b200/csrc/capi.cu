@@ -444,6 +444,15 @@ int64_t sph_launch_count(sph_ctx *ctx) {
     return DISPATCH(ctx, ctx->f->launches, ctx->d->launches);
 }
 
+int sph_set_pair_block(sph_ctx *ctx, int threads) {
+    if (!ctx || (threads != 32 && threads != 64 && threads != 128)) {
+        set_error("sph_set_pair_block: threads must be 32, 64 or 128");
+        return SPH_ERR_BAD_ARG;
+    }
+    auto go = [&](auto *c) { c->pair_block = threads; return SPH_OK; };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
+}
+
 int sph_profile(sph_ctx *ctx, int enable) {
     if (!ctx) return SPH_ERR_BAD_ARG;
     auto go = [&](auto *c) { c->prof = enable != 0; return SPH_OK; };

@@ -87,6 +87,7 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     int n = 0;
     int num_cells = 0;
+    int pair_block = 128;         // threads per block of the per-step pair passes (32, 64 or 128)
     int count = 0;
     float time = 0.f;
     bool uploaded = false;

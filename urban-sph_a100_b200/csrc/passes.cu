@@ -1292,11 +1292,11 @@ int phase_interaction(Ctx<Real> &c) {
         }
     }
     if (c.prep_valid)
-        k_prep_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, LIST(c), c.prep_row, c.prep_w, c.nnz_padded,
+        k_prep_cached<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, c.ty, LIST(c), c.prep_row, c.prep_w, c.nnz_padded,
                                                               c.S.u, c.mr, c.pr, c.S.flt, vis_stage, c.S.kt, c.S.et, c.SR,
                                                               c.rho_ref_S, tc, tdt, n);
     else
-        k_prep<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
+        k_prep<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
                                                        c.S.et, c.SR, c.rho_ref_S, tc, tdt, n);
     ++c.launches;
     if (c.dp.fv_solve != 0 && (c.dp.turb == 4 || c.dp.turb == 5)) {
@@ -1304,7 +1304,7 @@ int phase_interaction(Ctx<Real> &c) {
         ++c.launches;
     }
     if (c.dp.noslip == 1) {
-        k_boundary<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, n);
+        k_boundary<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, n);
         ++c.launches;
     }
     if (c.L.n_most > 0) {
@@ -1315,15 +1315,15 @@ int phase_interaction(Ctx<Real> &c) {
     if (tc == 0) SPH_TRY(neumann_pass(c, c.S));
     const Scalars sc{c.S.temp, c.S.concn, c.dtemp, c.dconcn};
     const bool th = c.dp.con_solve != 0 || c.dp.concn_solve != 0 || c.dp.boussinesq != 0;
-    const dim3 ga = grid_for(n, 128);
+    const dim3 ga = grid_for(n, c.pair_block);
     if (th) {
-        if (c.dp.fv_solve == 2) k_advection<Real, 2, 1><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
-        else if (c.dp.fv_solve == 1) k_advection<Real, 1, 1><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
-        else k_advection<Real, 0, 1><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        if (c.dp.fv_solve == 2) k_advection<Real, 2, 1><<<ga, c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else if (c.dp.fv_solve == 1) k_advection<Real, 1, 1><<<ga, c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else k_advection<Real, 0, 1><<<ga, c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
     } else {
-        if (c.dp.fv_solve == 2) k_advection<Real, 2, 0><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
-        else if (c.dp.fv_solve == 1) k_advection<Real, 1, 0><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
-        else k_advection<Real, 0, 0><<<ga, 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        if (c.dp.fv_solve == 2) k_advection<Real, 2, 0><<<ga, c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else if (c.dp.fv_solve == 1) k_advection<Real, 1, 0><<<ga, c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
+        else k_advection<Real, 0, 0><<<ga, c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.u, c.eli, c.ft, sc, n);
     }
     ++c.launches;
     if (c.dp.time_type == 1) {
@@ -1360,10 +1360,10 @@ int phase_time_update(Ctx<Real> &c) {
         }
     }
     if (c.pforce_valid)
-        k_pressure_force_cached<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, c.ty, c.mr, LIST(c), c.pforce_w, c.S.p,
+        k_pressure_force_cached<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, c.ty, c.mr, LIST(c), c.pforce_w, c.S.p,
                                                                         c.pres0, c.fp, n);
     else
-        k_pressure_force<Real><<<grid_for(n, 128), 128, 0, st>>>(c.dp, soa(c), LIST(c), c.S.p, c.pres0, c.fp, n);
+        k_pressure_force<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.S.p, c.pres0, c.fp, n);
     ++c.launches;
     if (c.L.n_mk > 0) {
         k_ibm_force<Real><<<grid_for(c.L.n_mk, 128), 128, 0, st>>>(c.dp, soa(c), c.L.mk_rows, c.L.mk_off, c.L.mk_nbr,

@@ -25,10 +25,11 @@ SYMBOLS = (
     "sph_upload", "sph_upload_state", "sph_download", "sph_nnps", "sph_nnps_export",
     "sph_neighbors_export", "sph_interaction", "sph_ppe", "sph_time_update", "sph_step",
     "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_status_string",
-    "sph_last_error", "sph_profile", "sph_operator_stats", "sph_operator_bytes", "sph_nnps_sort_noalloc",
+    "sph_last_error", "sph_profile", "sph_set_pair_block", "sph_operator_stats", "sph_operator_bytes", "sph_nnps_sort_noalloc",
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
+    "sph_batch_autotune_shapes",
     "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_apr_state", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
     "sph_read_solv", "sph_initial_records",
 )
@@ -77,6 +78,7 @@ def lib():
         L.sph_status_string.restype = ctypes.c_char_p
         L.sph_last_error.restype = ctypes.c_char_p
         L.sph_profile.argtypes = [vp, i32]
+        L.sph_set_pair_block.argtypes = [vp, i32]
         L.sph_operator_stats.argtypes = [vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double), i32]
         L.sph_operator_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
@@ -95,6 +97,8 @@ def lib():
         L.sph_batch_step.argtypes = [vp, i32, vp]
         L.sph_batch_set_workers.argtypes = [vp, i32]
         L.sph_batch_autotune.argtypes = [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]
+        L.sph_batch_autotune_shapes.argtypes = [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32),
+                                                ctypes.POINTER(ctypes.c_double)]
         L.sph_batch_case.argtypes = [vp, i32, ctypes.POINTER(vp)]
         L.sph_batch_particles.argtypes = [vp]
         L.sph_batch_particles.restype = i64
@@ -227,6 +231,9 @@ class Simulation:
     def launches(self):
         return int(lib().sph_launch_count(self.h))
 
+    def set_pair_block(self, threads):
+        _check("sph_set_pair_block", lib().sph_set_pair_block(self.h, int(threads)))
+
     def profile(self, enable=True):
         _check("sph_profile", lib().sph_profile(self.h, 1 if enable else 0))
 
@@ -341,6 +348,13 @@ class Batch:
         w, ms = ctypes.c_int32(0), ctypes.c_double(0)
         _check("sph_batch_autotune", lib().sph_batch_autotune(self.h, int(probe_steps), ctypes.byref(w), ctypes.byref(ms)))
         return w.value, ms.value
+
+    def autotune_shapes(self, probe_steps=1):
+        """(workers, pair-pass threads per block, ms per step) of the fastest probe."""
+        w, t, ms = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_double(0)
+        _check("sph_batch_autotune_shapes", lib().sph_batch_autotune_shapes(self.h, int(probe_steps), ctypes.byref(w),
+                                                                            ctypes.byref(t), ctypes.byref(ms)))
+        return w.value, t.value, ms.value
 
     def download(self, k):
         c = ctypes.c_void_p()
