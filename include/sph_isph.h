@@ -171,10 +171,14 @@ typedef struct sph_params {
                                 whole solve is one CUDA graph whose conditional
                                 nodes take the host loop's decisions, and
                                 sph_step reads the statistics once, after its
-                                last step (same iterates as 0; used when the
-                                context has its own stream and no live
-                                profiling, learned start or sample collection,
-                                else 0 runs)                                   */
+                                last step; from the third step of a context
+                                on (count >= 2, buffers and parameters
+                                unchanged since the step before), sph_step
+                                captures a whole step around the solve as one
+                                graph and replays it (same iterates as 0; used
+                                when the context has its own stream and no
+                                live profiling, learned start or sample
+                                collection, else 0 runs)                       */
     int32_t ppe_coarse_block;    /* BiCGSTAB preconditioner: 0 Jacobi; B > 0
                                 adds a coarse correction on aggregates of
                                 B x B x B NNPS cells (additive two-level)      */
@@ -347,8 +351,13 @@ int sph_diagnostics(sph_ctx *ctx, float *max_umag, float *max_drho_pct, float *m
  * phase: [0] nnps, [1] interaction, [2] ppe, [3] time update. */
 int sph_last_phase_ms(sph_ctx *ctx, float *ms4);
 
-/* Kernel launches issued by this context since creation. */
+/* Kernel launches issued by this context since creation (a replay of the
+ * whole-step graph counts the launches it stands for, its solve as one). */
 int64_t sph_launch_count(sph_ctx *ctx);
+
+/* Steps this context ran as a replay of its whole-step graph
+ * (ppe_refinement = 4). */
+int64_t sph_step_graph_count(sph_ctx *ctx);
 
 /* Live timing of the PPE operator kernel (the dominant kernel of a step):
  * with `enable` set, every operator launch is bracketed by CUDA events on the

@@ -52,14 +52,14 @@ def test_batch_equals_cases_stepped_alone(refinement):
     cases = _cases(refinement)
     b = abi.Batch(cases, precision=layout.PREC_MIXED)
     b.set_workers(0)
-    stats = b.step(3)
+    stats = b.step(4)     # under device control steps 2 and 3 replay a whole-step graph
     assert all(s.status == 0 and s.rel_residual <= 1e-6 for s in stats)
     for k, (P, p) in enumerate(cases):
         q = p.copy()
         q.ppe_refinement = 0
         sim = abi.Simulation(q, precision=layout.PREC_MIXED)
         sim.upload(P)
-        for _ in range(3):
+        for _ in range(4):
             sim.step(1)
         A, _, _ = sim.download()
         sim.close()

@@ -6,7 +6,7 @@ loop's decisions (reliable updates, restarts, convergence), so it must give
 the host-controlled solve's iterates exactly: the same pressure and velocity
 bit for bit and the same iteration and update counts, over several steps
 stepped in one sph_step call (whose statistics the host reads once, at the
-end).  A budget too small to converge must come back as SPH_NOT_CONVERGED,
+end), also when later steps replay the whole step as one captured graph.  A budget too small to converge must come back as SPH_NOT_CONVERGED,
 and an ensemble of cases under device control must equal its cases stepped
 alone.
 """
@@ -20,7 +20,7 @@ from sph_b200 import abi, decks, layout
 pytestmark = pytest.mark.gpu
 
 
-def _run(P, p, refinement, steps, per_call=1, max_iter=2000, coarse=2):
+def _run(P, p, refinement, steps, per_call=1, max_iter=2000, coarse=2, calls=None):
     import torch
     q = p.copy()
     q.ppe_mode = layout.PPE_MIXED_IR
@@ -33,14 +33,15 @@ def _run(P, p, refinement, steps, per_call=1, max_iter=2000, coarse=2):
     sim.upload(P)
     stats = []
     status = []
-    for _ in range(steps // per_call):
+    for k in (calls or [per_call] * (steps // per_call)):
         try:
-            stats.append(sim.step(per_call))
+            stats.append(sim.step(k))
             status.append(0)
         except abi.SphError as e:
             status.append(e.status)
             break
     A, _, _ = sim.download()
+    _run.graph_steps = sim.graph_steps()
     sim.close()
     return A, stats, status
 
@@ -61,7 +62,11 @@ def test_device_controlled_solve_equals_host_loop(coarse):
 def test_device_controlled_steps_in_one_call():
     P, p = decks.canyon(scale=0.12)
     A, sa, _ = _run(P, p, 0, 4, per_call=1)
+    assert _run.graph_steps == 0
     B, sb, _ = _run(P, p, 4, 4, per_call=4)     # four steps, statistics read once
+    # steps 0 and 1 launch by launch, step 2 captured as one graph, 2 and 3
+    # replays of it
+    assert _run.graph_steps == 2
     for f in ("pres", "ux", "uy", "uz"):
         assert np.array_equal(A[f], B[f]), f
     last = sb[-1]
@@ -75,3 +80,20 @@ def test_device_controlled_budget_reports_not_converged():
     _, sb, _ = _run(P, p, 4, 1, max_iter=8)
     assert sa[0].status == 1 and sb[0].status == 1     # SPH_NOT_CONVERGED
     assert sa[0].iterations == sb[0].iterations
+
+
+def test_whole_step_graph_follows_the_step_counter():
+    # a filter period of 2 and a wall-temperature ramp over the first steps:
+    # the replayed graph reads the step counter and time from the device, so
+    # it must give the launch-by-launch results at every step, also across
+    # sph_step calls
+    P, p = decks.thermal_mini(nx=16, ny=8, nz=6)
+    p.seti("freq_filt", 2)
+    dt = p.getf("dt")
+    p.t_ini, p.t_con, p.t_start, p.t_con_t = 300.0, 304.0, dt, 6.0 * dt
+    A, sa, _ = _run(P, p, 0, 7, per_call=1, coarse=0)
+    B, sb, _ = _run(P, p, 4, 7, coarse=0, calls=[5, 2])
+    assert _run.graph_steps == 5       # steps 2-6
+    for f in ("pres", "ux", "uy", "uz", "temp", "concn"):
+        assert np.array_equal(A[f], B[f]), f
+    assert (sa[-1].iterations, sa[-1].refinements) == (sb[-1].iterations, sb[-1].refinements)

@@ -43,7 +43,6 @@ DevParams make_dev_params(const sph_params &p) {
     for (int a = 0; a < 6; ++a) d.periodic_box[a] = p.periodic_box[a];
     d.turb = p.vii[SPH_VII_TURBULENCE];
     d.noslip = p.vii[SPH_VII_NOSLIP_BC];
-    d.count = p.vii[SPH_VII_COUNT];
     d.kappa = p.vif[SPH_VIF_KAPPA];
     d.skappa = p.vif[SPH_VIF_SEARCH_KAPPA];
     d.dcell = p.vif[SPH_VIF_DCELL];
@@ -52,7 +51,6 @@ DevParams make_dev_params(const sph_params &p) {
     d.zmin = p.vif[SPH_VIF_Z_MIN]; d.zmax = p.vif[SPH_VIF_Z_MAX];
     d.dt = p.vif[SPH_VIF_DT];
     d.u_limit = p.vif[SPH_VIF_U_LIMIT];
-    d.time = p.vif[SPH_VIF_TIME];
     d.dt_structure = p.vif[SPH_VIF_DT_STRUCTURE];
     d.cs_sgs = p.cs_sgs; d.l2 = p.l2; d.l3 = p.l3; d.l_left = p.l_left; d.l_right = p.l_right;
     d.outlet_probe_dx = p.outlet_probe_dx; d.partner_tol = p.partner_tol; d.ghost_tol = p.ghost_tol;
@@ -240,6 +238,8 @@ int sph_create(const sph_params *p, int precision, int device, void *stream, sph
     return SPH_OK;
 }
 
+static void delete_step_graph(void *g);
+
 void sph_destroy(sph_ctx *ctx) {
     if (!ctx) return;
     auto go = [](auto *c) {
@@ -253,6 +253,7 @@ void sph_destroy(sph_ctx *ctx) {
         }
         if (c->red_host) cudaFreeHost(c->red_host);
         release_solver_ws(*c);
+        delete_step_graph(c->stepgraph);
         c->free_all();
         delete c->allocs;
         delete c;
@@ -287,6 +288,7 @@ int sph_set_params(sph_ctx *ctx, const sph_params *p) {
         }
         c->prm = *p;
         c->dp = make_dev_params(*p);
+        ++c->param_gen;
         if (recompute && c->built) return build_side_lists(*c);
         return SPH_OK;
     };
@@ -377,6 +379,104 @@ int sph_time_update(sph_ctx *ctx) {
     return DISPATCH(ctx, tu_impl(*ctx->f), tu_impl(*ctx->d));
 }
 
+// ---------------------------------------------------------------------------
+// A whole step as one CUDA graph, for contexts whose solve runs under device
+// control (ppe_refinement = 4).  Once a step at count >= 1 has run launch by
+// launch, the next one with the same buffers and parameters is captured:
+// the interaction passes, the solve with its conditional nodes, the time
+// update and the device clock's advance, with the phase events as
+// event-record nodes; later steps replay it.  The kernels read the step
+// counter and time from the device clock, so a replay computes exactly what
+// the launches would.  Steps at count 0 (the markers' normals and the step-0
+// Neumann pass run only there), the first step after any allocation, release
+// or change of parameters, and host-controlled solves run launch by launch.
+// ---------------------------------------------------------------------------
+struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned long long> key;      // state the graph was captured in
+    std::vector<unsigned long long> warm;     // state after the last step run launch by launch at count >= 1
+    std::vector<unsigned long long> failed;   // state in which a capture failed
+    long long launches = 0;                   // launches one replay stands for (the solve counted as one)
+    ~StepGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
+static void delete_step_graph(void *g) { delete (StepGraph *)g; }
+
+template <class Real>
+static std::vector<unsigned long long> step_key(const Ctx<Real> &c) {
+    return {c.mem_gen, c.param_gen, (unsigned long long)c.n, (unsigned long long)c.nnz_padded,
+            (unsigned long long)(uintptr_t)c.stream, (unsigned long long)c.pair_block, (unsigned long long)c.cg_block,
+            (unsigned long long)((c.built ? 1 : 0) | (c.gc_valid ? 2 : 0) | (c.prep_valid ? 4 : 0) |
+                                 (c.pforce_valid ? 8 : 0) | (c.coef_valid ? 16 : 0) | (c.coef_h_valid ? 32 : 0) |
+                                 (c.cg_valid ? 64 : 0) | (c.clk_synced ? 128 : 0))};
+}
+
+// captures one step into sg->exec; on failure nothing has run on the device
+template <class Real>
+static int capture_step(Ctx<Real> &c, StepGraph *sg) {
+    if (sg->exec) { cudaGraphExecDestroy(sg->exec); sg->exec = nullptr; }
+    cudaGraph_t graph = nullptr;
+    SPH_CUDA_TRY(cudaGraphCreate(&graph, 0));
+    if (cudaStreamBeginCaptureToGraph(c.stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess) {
+        cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return SPH_ERR_CUDA;
+    }
+    const long long l0 = c.launches;
+    c.capturing = true;
+    sph_ppe_stats ps{};
+    int st = record_event(c, c.ev[1]) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+    if (st == SPH_OK) st = phase_interaction(c);
+    if (st == SPH_OK) st = record_event(c, c.ev[2]) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+    if (st == SPH_OK) st = phase_ppe(c, &ps);
+    if (st == SPH_OK) st = record_event(c, c.ev[3]) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+    if (st == SPH_OK) st = phase_time_update(c);
+    if (st == SPH_OK) st = record_event(c, c.ev[6]) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
+    c.capturing = false;
+    cudaGraph_t done = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &done);
+    if (st == SPH_OK && e == cudaSuccess && cudaGraphInstantiate(&sg->exec, graph, 0) != cudaSuccess) sg->exec = nullptr;
+    cudaGraphDestroy(graph);
+    sg->launches = c.launches - l0;
+    c.launches = l0;
+    if (!sg->exec) {
+        cudaGetLastError();
+        return st < 0 ? st : SPH_ERR_CUDA;
+    }
+    return SPH_OK;
+}
+
+// runs the step as the step graph when it can; *ran tells whether it did
+template <class Real>
+static int step_graph(Ctx<Real> &c, bool *ran) {
+    *ran = false;
+    if (c.count < 1 || !solve_under_device_control(c)) return SPH_OK;
+    auto *sg = (StepGraph *)c.stepgraph;
+    if (!sg) {
+        sg = new (std::nothrow) StepGraph();
+        if (!sg) return SPH_ERR_OUT_OF_MEMORY;
+        c.stepgraph = sg;
+    }
+    const std::vector<unsigned long long> key = step_key(c);
+    if (!sg->exec || sg->key != key) {
+        if (sg->warm != key || sg->failed == key) return SPH_OK;
+        if (capture_step(c, sg) < 0) {
+            sg->failed = key;
+            return SPH_OK;   // this state steps launch by launch
+        }
+        sg->key = key;
+    }
+    SPH_CUDA_TRY(cudaGraphLaunch(sg->exec, c.stream));
+    c.launches += sg->launches;
+    ++c.graph_steps;
+    c.ppe_pending = true;
+    *ran = true;
+    return finish_step(c);
+}
+
 template <class Real>
 static int step_impl(Ctx<Real> &c, int nsteps, sph_ppe_stats *stats) {
     int last = SPH_OK;
@@ -389,6 +489,15 @@ static int step_impl(Ctx<Real> &c, int nsteps, sph_ppe_stats *stats) {
     bool pending = false;
     for (int s = 0; s < nsteps; ++s) {
         int st = ensure_built(c);
+        bool replayed = false;
+        if (st == SPH_OK) st = step_graph(c, &replayed);
+        if (st < 0) { c.defer_stats = false; return st; }
+        if (replayed) {
+            pending = true;
+            continue;
+        }
+        const int count0 = c.count;
+        const unsigned long long gen0 = c.mem_gen;
         if (st == SPH_OK) st = cudaEventRecord(c.ev[1], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
         if (st == SPH_OK) st = phase_interaction(c);
         if (st == SPH_OK) st = cudaEventRecord(c.ev[2], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
@@ -398,6 +507,14 @@ static int step_impl(Ctx<Real> &c, int nsteps, sph_ppe_stats *stats) {
         if (st == SPH_OK) st = phase_time_update(c);
         if (st == SPH_OK) st = cudaEventRecord(c.ev[6], c.stream) == cudaSuccess ? SPH_OK : SPH_ERR_CUDA;
         if (st < 0) { c.defer_stats = false; return st; }
+        // a step that allocated nothing leaves a state the next step can be
+        // captured in (a context that allocates every step, e.g. with
+        // recompute_gc, stays launch by launch)
+        if (c.stepgraph) {
+            auto *sg = (StepGraph *)c.stepgraph;
+            if (count0 >= 1 && c.mem_gen == gen0) sg->warm = step_key(c);
+            else sg->warm.clear();
+        }
         pending = c.ppe_pending;
         if (!pending) {
             SPH_CUDA_TRY(cudaEventSynchronize(c.ev[6]));
@@ -444,12 +561,17 @@ int64_t sph_launch_count(sph_ctx *ctx) {
     return DISPATCH(ctx, ctx->f->launches, ctx->d->launches);
 }
 
+int64_t sph_step_graph_count(sph_ctx *ctx) {
+    if (!ctx) return -1;
+    return DISPATCH(ctx, ctx->f->graph_steps, ctx->d->graph_steps);
+}
+
 int sph_set_pair_block(sph_ctx *ctx, int threads) {
     if (!ctx || (threads != 32 && threads != 64 && threads != 128)) {
         set_error("sph_set_pair_block: threads must be 32, 64 or 128");
         return SPH_ERR_BAD_ARG;
     }
-    auto go = [&](auto *c) { c->pair_block = threads; return SPH_OK; };
+    auto go = [&](auto *c) { c->pair_block = threads; ++c->param_gen; return SPH_OK; };
     return DISPATCH(ctx, go(ctx->f), go(ctx->d));
 }
 

@@ -39,8 +39,7 @@ struct DevParams {
     int pforce_form;       // pressure-force pair term: 0 the reference's active form, 1 difference form
     double rp_x, rp_y;     // recycling probe
     double periodic_box[6];   // x0,x1,y0,y1,z0,z1 of the periodic box (ghost partners)
-    int count;
-    float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, time, dt_structure;
+    float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, dt_structure;
     double cs_sgs, l2, l3, l_left, l_right, outlet_probe_dx, partner_tol, ghost_tol;
     double ib_box[6], ib_face_tol, most_z0, most_z0h, most_ghost_dz, rho_air, ibm_target_coeff;
     double visc_fluid, visc_wall, visc_marker, av_alpha, av_beta, av_c0;
@@ -51,6 +50,16 @@ struct DevParams {
 };
 
 DevParams make_dev_params(const sph_params &p);
+
+// ---- step counter and time, read on the device ----------------------------
+// The kernels that depend on the step (the filter period, rho_ref at step 0,
+// the thermal ramp) read them here instead of taking them as launch
+// arguments, so that a captured step replays correctly at any later step;
+// the last kernel of each step advances them.
+struct StepClock {
+    int count;      // vii[SPH_VII_COUNT] of the step being computed
+    float time;     // vif[SPH_VIF_TIME] of that step
+};
 
 // ---- neighbour-class bits of a particle (read on the j side of pair loops) --
 enum : int {

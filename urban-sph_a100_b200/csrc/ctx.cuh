@@ -183,6 +183,13 @@ struct Ctx {
     void *idr_ws_f = nullptr;     // IDR(s) workspace with FP32 vectors (inner solves of the refinement)
     void *kgraph = nullptr;       // CUDA graph of the mixed BiCGSTAB's iterations between host checks
     void *devloop = nullptr;      // CUDA graph of a whole device-controlled solve (ppe_refinement = 4)
+    void *stepgraph = nullptr;    // CUDA graph of a whole step around that solve (capi.cu)
+    bool capturing = false;       // the phases are being captured into the step graph
+    long long graph_steps = 0;    // steps run as a replay of it
+    StepClock *clk = nullptr;     // step counter and time on the device
+    bool clk_synced = false;      // clk holds count / time
+    unsigned long long mem_gen = 0;     // bumped by every allocation and release
+    unsigned long long param_gen = 0;   // bumped by every change of the parameters
     bool ppe_pending = false;     // a device-controlled solve whose statistics the host has not read
     bool defer_stats = false;     // inside sph_step: leave those statistics until the last step
     bool kgraph_off = false;      // capture failed once: launch the kernels one by one
@@ -247,6 +254,10 @@ struct Ctx {
 
     template <class T>
     int alloc(T *&ptr, size_t count) {
+        if (capturing) {   // no allocation inside a captured step: the capture fails and the step runs launch by launch
+            set_error("allocation while a step is captured");
+            return SPH_ERR_STATE;
+        }
         void *p = nullptr;
         size_t bytes = sizeof(T) * (count ? count : 1);
         cudaError_t e = cudaMalloc(&p, bytes);
@@ -256,11 +267,13 @@ struct Ctx {
         }
         allocs->push_back(p);
         ptr = (T *)p;
+        ++mem_gen;
         return SPH_OK;
     }
     template <class T>
     void release(T *&ptr) {
-        if (!ptr) return;
+        if (!ptr || capturing) return;   // (see alloc)
+        ++mem_gen;
         for (size_t k = 0; k < allocs->size(); ++k)
             if ((*allocs)[k] == (void *)ptr) {
                 cudaFree(ptr);
@@ -309,8 +322,17 @@ template <class Real, class V> void coarse_apply(Ctx<Real> &c, const V *r, V *z,
 // the caller adds Z c.cg_y
 template <class Real, class V> void coarse_restrict_solve(Ctx<Real> &c, const V *r, const V *w);
 template <class Real> int phase_time_update(Ctx<Real> &c);
+
+// an event record on the context's stream; while a whole step is captured it
+// is an event-record node of the step's graph, so the phase times stay live
+template <class Real>
+inline cudaError_t record_event(const Ctx<Real> &c, cudaEvent_t e) {
+    return c.capturing ? cudaEventRecordWithFlags(e, c.stream, cudaEventRecordExternal) : cudaEventRecord(e, c.stream);
+}
+template <class Real> int finish_step(Ctx<Real> &c);
 template <class Real> int dev_solve_stats(Ctx<Real> &c, sph_ppe_stats *S, int *worst);
 template <class Real> int dev_reset_worst(Ctx<Real> &c);
+template <class Real> bool solve_under_device_control(const Ctx<Real> &c);
 template <class Real> int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax);
 template <class Real> int gradient_correction(Ctx<Real> &c);
 template <class Real> int neumann_pass(Ctx<Real> &c, VarSet<Real> &V);

@@ -232,6 +232,8 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     SPH_CUDA_TRY(cudaGetLastError());
     c.count = c.prm.vii[SPH_VII_COUNT];
     c.time = c.prm.vif[SPH_VIF_TIME];
+    c.clk_synced = false;
+    ++c.param_gen;
     c.release(c.apr_family);   // new records: APR families start again
     c.release(c.apr_target);
     c.uploaded = true;

@@ -38,6 +38,18 @@ __device__ __forceinline__ bool within_hi(const DevParams &P, float4 a, float4 b
     return dist_rn(a.x, a.y, a.z, b.x, b.y, b.z) < __fmul_rn(P.skappa, a.w);
 }
 
+// the device clock: set from the host's copy, and advanced by one step
+// (the same float addition as the host's, so the two stay equal)
+__global__ void k_set_clock(StepClock *clk, int count, float time) {
+    clk->count = count;
+    clk->time = time;
+}
+
+__global__ void k_advance_clock(StepClock *clk, float dt) {
+    clk->count += 1;
+    clk->time = __fadd_rn(clk->time, dt);
+}
+
 // ---------------------------------------------------------------------------
 // step start: SP1 <- P1, SP2 <- P2, memset(P3) (ISPH_Calc.cuh:42-61)
 // ---------------------------------------------------------------------------
@@ -202,10 +214,12 @@ __global__ void __launch_bounds__(128) k_prep_cached(DevParams P, const int4 *__
                                                      const typename V4<Real>::type *__restrict__ pr,
                                                      Real *__restrict__ flt, Real *__restrict__ vis_out,
                                                      Real *__restrict__ kt, Real *__restrict__ et, Real *__restrict__ SR,
-                                                     Real *__restrict__ rho_ref, int tcount, Real tdt, int n) {
+                                                     Real *__restrict__ rho_ref, const StepClock *__restrict__ clk,
+                                                     Real tdt, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 ti = ty[i];
+    const int tcount = clk->count;
     if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
     const size_t N = (size_t)n;
     const bool filt = (tcount % P.freq_filt) == 0;
@@ -256,10 +270,12 @@ template <class Real>
 __global__ void __launch_bounds__(128) k_prep(DevParams P, SoA<Real> s, LIST_ARGS, const Real *__restrict__ g6,
                                               const typename V4<Real>::type *__restrict__ u, Real *__restrict__ flt,
                                               Real *__restrict__ vis_out, Real *__restrict__ kt, Real *__restrict__ et,
-                                              Real *__restrict__ SR, Real *__restrict__ rho_ref, int tcount, Real tdt, int n) {
+                                              Real *__restrict__ SR, Real *__restrict__ rho_ref,
+                                              const StepClock *__restrict__ clk, Real tdt, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int4 ti = s.ty[i];
+    const int tcount = clk->count;
     if (ti.x > 2 || ti.w >= 1000 || ti.w <= 0) return;
     const size_t N = (size_t)n;
     const float4 fi = s.pf[i];
@@ -390,9 +406,10 @@ __device__ __forceinline__ double most_Phi_h(float L, float z, float z0h) { retu
 template <class Real>
 __global__ void k_most(DevParams P, SoA<Real> s, const int *rows, const int *off, const int *tgt, int nrows,
                        const typename V4<Real>::type *u, const Real *temp, typename V4<Real>::type *fm,
-                       typename V4<Real>::type *fl, Real *dtemp, float *us_update, int tcount, float tdt) {
+                       typename V4<Real>::type *fl, Real *dtemp, float *us_update, const StepClock *clk, float tdt) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nrows) return;
+    const int tcount = clk->count;
     const int i = rows[k];
     const auto xi = s.pr[i];
     const auto ui = u[i];
@@ -638,9 +655,10 @@ __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::typ
                              typename V4<Real>::type *u0, const typename V4<Real>::type *ft,
                              const typename V4<Real>::type *fm, Real *rho_ref, const typename V2<Real>::type *mr,
                              const Real *temp, Real *temp0, Real *concn, Real *concn0, const Real *dconcn,
-                             Real tdt, float ttime, int n) {
+                             Real tdt, const StepClock *clk, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const float ttime = clk->time;
     const int4 t = ty[i];
     if (t.x >= 3 || t.w >= 1000) return;
     auto ui = u[i];
@@ -1039,9 +1057,10 @@ __global__ void k_zero_rows4(const int *rows, int nrows, typename V4<Real>::type
 // IBM_corrector (functions_IBM.cuh:615-725): SP1 -> P1
 // ---------------------------------------------------------------------------
 template <class Real>
-__global__ void k_time_update(Ctx<Real> c, Real tdt, int tcount) {
+__global__ void k_time_update(Ctx<Real> c, Real tdt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
+    const int tcount = c.clk->count;
     const int4 t = c.ty[i];
     const VarSet<Real> &S = c.S;
     const VarSet<Real> &A = c.A;
@@ -1259,8 +1278,12 @@ int phase_interaction(Ctx<Real> &c) {
     const int n = c.n;
     const int tc = c.count;
     const Real tdt = (Real)c.dp.dt;
-    c.dp.count = tc;
-    c.dp.time = c.time;
+    if (!c.clk) SPH_TRY(c.alloc(c.clk, 1));
+    if (!c.clk_synced) {
+        k_set_clock<<<1, 1, 0, st>>>(c.clk, c.count, c.time);
+        ++c.launches;
+        c.clk_synced = true;
+    }
     k_begin_step<Real><<<grid_for(n, 256), 256, 0, st>>>(c);
     ++c.launches;
     if (tc == 0) {
@@ -1294,10 +1317,10 @@ int phase_interaction(Ctx<Real> &c) {
     if (c.prep_valid)
         k_prep_cached<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, c.ty, LIST(c), c.prep_row, c.prep_w, c.nnz_padded,
                                                               c.S.u, c.mr, c.pr, c.S.flt, vis_stage, c.S.kt, c.S.et, c.SR,
-                                                              c.rho_ref_S, tc, tdt, n);
+                                                              c.rho_ref_S, c.clk, tdt, n);
     else
         k_prep<Real><<<grid_for(n, c.pair_block), c.pair_block, 0, st>>>(c.dp, soa(c), LIST(c), c.g6, c.S.u, c.S.flt, vis_stage, c.S.kt,
-                                                       c.S.et, c.SR, c.rho_ref_S, tc, tdt, n);
+                                                       c.S.et, c.SR, c.rho_ref_S, c.clk, tdt, n);
     ++c.launches;
     if (c.dp.fv_solve != 0 && (c.dp.turb == 4 || c.dp.turb == 5)) {
         k_merge_vis<Real><<<grid_for(n, 256), 256, 0, st>>>(c.S.u, vis_stage, c.ty, n);
@@ -1309,7 +1332,7 @@ int phase_interaction(Ctx<Real> &c) {
     }
     if (c.L.n_most > 0) {
         k_most<Real><<<grid_for(c.L.n_most, 128), 128, 0, st>>>(c.dp, soa(c), c.L.most_rows, c.L.most_off, c.L.most_tgt,
-                                                               c.L.n_most, c.S.u, c.S.temp, c.S.fm, c.S.fl, c.dtemp, c.us_update, tc, (float)tdt);
+                                                               c.L.n_most, c.S.u, c.S.temp, c.S.fm, c.S.fl, c.dtemp, c.us_update, c.clk, (float)tdt);
         ++c.launches;
     }
     if (tc == 0) SPH_TRY(neumann_pass(c, c.S));
@@ -1329,7 +1352,7 @@ int phase_interaction(Ctx<Real> &c) {
     if (c.dp.time_type == 1) {
         k_projection<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.ty, c.S.u, c.u0, c.ft, c.S.fm, c.rho_ref_S, c.mr,
                                                              c.S.temp, c.temp0, c.S.concn, c.concn0, c.dconcn,
-                                                             tdt, c.time, n);
+                                                             tdt, c.clk, n);
         ++c.launches;
     }
     SPH_TRY(periodic_pass(c, c.S));
@@ -1379,7 +1402,7 @@ int phase_time_update(Ctx<Real> &c) {
         k_zero_rows4<Real><<<grid_for(c.L.n_sp_zero, 256), 256, 0, st>>>(c.L.sp_zero, c.L.n_sp_zero, c.S.fb);
         ++c.launches;
     }
-    k_time_update<Real><<<grid_for(n, 256), 256, 0, st>>>(c, tdt, c.count);
+    k_time_update<Real><<<grid_for(n, 256), 256, 0, st>>>(c, tdt);
     ++c.launches;
     SPH_TRY(neumann_pass(c, c.A));
     SPH_TRY(outlet_pass(c, c.A));
@@ -1389,10 +1412,19 @@ int phase_time_update(Ctx<Real> &c) {
         k_recycle<Real><<<grid_for(c.L.n_rc, 128), 128, 0, st>>>(c.dp, soa(c), c.L.rc_rows, c.L.n_rc, c.us_update, c.A.u);
         ++c.launches;
     }
+    k_advance_clock<<<1, 1, 0, st>>>(c.clk, c.dp.dt);
+    ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
+    if (c.capturing) return SPH_OK;   // a replayed step graph calls finish_step itself
+    return finish_step(c);
+}
+
+// the host's side of the end of a step: its copy of the counter and time,
+// then APR every freq_apr steps (vii[35] = 1: cell-based)
+template <class Real>
+int finish_step(Ctx<Real> &c) {
     c.time = c.time + c.dp.dt;
     c.count += 1;
-    // APR every freq_apr steps (vii[35] = 1: cell-based)
     const int freq_apr = c.prm.vii[SPH_VII_FREQ_APR];
     if (c.prm.vii[SPH_VII_APR_SOLV] == 1 && freq_apr > 0 && c.count % freq_apr == 0)
         SPH_TRY(apr_pass(c, nullptr, nullptr, nullptr));
@@ -1424,6 +1456,7 @@ int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax) {
     template int gradient_correction<R>(Ctx<R> &);                       \
     template int neumann_pass<R>(Ctx<R> &, VarSet<R> &);                 \
     template int outlet_pass<R>(Ctx<R> &, VarSet<R> &);                  \
+    template int finish_step<R>(Ctx<R> &);                               \
     template int periodic_pass<R>(Ctx<R> &, VarSet<R> &);                \
     template int freeslip_pass<R>(Ctx<R> &, VarSet<R> &);                \
     template int phase_interaction<R>(Ctx<R> &);                         \

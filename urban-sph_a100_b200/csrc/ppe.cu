@@ -1319,14 +1319,16 @@ static int add_conditional(cudaStream_t st, cudaGraphConditionalHandle h, cudaGr
     return SPH_OK;
 }
 
-// Solves M x = b as bicgstab_reliable does, for the FP64 x (initial guess in
-// x, b_norm2 in scal[SC_BB]) with FP32 Krylov vectors and the cached operator,
-// under device control.  Returns after queueing the solve; the statistics
-// are in the device scalars (dev_solve_stats reads them).
+// Appends the solve of M x = b, as bicgstab_reliable does it, for the FP64 x
+// (initial guess in x, b_norm2 in scal[SC_BB]) with FP32 Krylov vectors and
+// the cached operator, under device control, to the graph that `st` is
+// capturing: its start, then the WHILE node, whose body and branches are
+// captured on the loop graph's own streams.  The statistics stay in the
+// device scalars (dev_solve_stats reads them).
 template <class Real>
-static int bicgstab_device(Ctx<Real> &c, double *x, const double *b, double *yd, double tol, int maxit) {
+static int append_solve(Ctx<Real> &c, DevLoopGraph *g, cudaStream_t st, double *x, const double *b, double *yd,
+                        double tol, int maxit) {
     const int n = c.n;
-    cudaStream_t st = c.stream;
     float *const *ws = (float *const *)c.kv;
     float *r = ws[0], *rh = ws[1], *p = ws[2], *v = ws[3], *s = ws[4];
     float *t = ws[5], *ph = ws[6], *sh = ws[7], *dinv = ws[8];
@@ -1334,14 +1336,116 @@ static int bicgstab_device(Ctx<Real> &c, double *x, const double *b, double *yd,
     const int G = red_grid(n);
     unsigned int *counter = (unsigned int *)(c.scal + 32);
     const int check = 4;
+    auto replace = [&]() {
+        k_axpy_cast<float, double><<<grid_for(n, 256), 256, 0, c.stream>>>(xlo, x, n);
+        apply_op<Real, double>(c, x, yd, true);
+        k_reliable_replace<float><<<G, 256, 0, c.stream>>>(b, yd, r, xlo, rh, n, c.red, counter, c.scal);
+    };
+    auto restart = [&]() {
+        replace();
+        k_restart_dirs<float><<<G, 256, 0, c.stream>>>(r, rh, p, v, n);
+        k_norm2<float><<<G, 256, 0, c.stream>>>(r, n, c.red, counter, c.scal, SC_RHO_NEW);
+        k_dev_set_scal<<<1, 1, 0, c.stream>>>(c.scal);
+    };
+    auto iteration = [&]() {
+        k_p_update<float><<<G, 256, 0, c.stream>>>(p, ph, r, v, dinv, n, c.scal);
+        bool mr = precond_coarse<Real, float>(c, p, ph, v, true);
+        apply_op<Real, float>(c, ph, v, true, mr);
+        k_alpha<float><<<G, 256, 0, c.stream>>>(rh, v, n, c.red, counter, c.scal);
+        k_s_update<float><<<G, 256, 0, c.stream>>>(r, v, s, sh, dinv, n, c.scal);
+        mr = precond_coarse<Real, float>(c, s, sh, t, true);
+        apply_op<Real, float>(c, sh, t, true, mr);
+        k_omega<float><<<G, 256, 0, c.stream>>>(t, s, n, c.red, counter, c.scal);
+        k_xr_update<float><<<G, 256, 0, c.stream>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
+    };
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    SPH_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, nullptr, nullptr));
+    if (cs != cudaStreamCaptureStatusActive || !graph) { set_error("device-controlled solve: stream not capturing"); return SPH_ERR_CUDA; }
+    cudaGraphConditionalHandle h_loop, h_rep, h_res;
+    cudaGraph_t body = nullptr, body_rep = nullptr, body_res = nullptr;
+    SPH_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_loop, graph, 0, cudaGraphCondAssignDefault));
+    const cudaStream_t outer = c.stream;
+    c.stream = st;
+    // the solve's start: the restart of bicgstab_reliable, then the loop
+    k_dev_tol<<<1, 1, 0, st>>>(c.scal, tol, maxit, check);
+    k_dinv<float, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
+    cudaMemsetAsync(xlo, 0, sizeof(float) * n, st);
+    restart();
+    k_dev_start<<<1, 1, 0, st>>>(c.scal, h_loop);
+    int err = add_conditional(st, h_loop, cudaGraphCondTypeWhile, &body);
+    // the loop body on s2, its two branches on s3
+    if (err == SPH_OK && (cudaGraphConditionalHandleCreate(&h_rep, body, 0, cudaGraphCondAssignDefault) != cudaSuccess ||
+                          cudaGraphConditionalHandleCreate(&h_res, body, 0, cudaGraphCondAssignDefault) != cudaSuccess))
+        err = SPH_ERR_CUDA;
+    if (err == SPH_OK) {
+        c.stream = g->s2;
+        if (cudaStreamBeginCaptureToGraph(g->s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            for (int q = 0; q < check; ++q) iteration();
+            k_dev_decide<<<1, 1, 0, g->s2>>>(c.scal, h_rep, h_res);
+            err = add_conditional(g->s2, h_rep, cudaGraphCondTypeIf, &body_rep);
+            if (err == SPH_OK) err = add_conditional(g->s2, h_res, cudaGraphCondTypeIf, &body_res);
+            if (err == SPH_OK) k_dev_tail<<<1, 1, 0, g->s2>>>(c.scal, h_loop);
+            cudaGraph_t done = nullptr;
+            if (cudaStreamEndCapture(g->s2, &done) != cudaSuccess && err == SPH_OK) err = SPH_ERR_CUDA;
+        } else {
+            err = SPH_ERR_CUDA;
+        }
+    }
+    // the reliable update, then the restart branch
+    if (err == SPH_OK) {
+        c.stream = g->s3;
+        bool ok = cudaStreamBeginCaptureToGraph(g->s3, body_rep, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            replace();
+            k_dev_after_replace<<<1, 1, 0, g->s3>>>(c.scal, h_res);
+            cudaGraph_t done = nullptr;
+            ok = cudaStreamEndCapture(g->s3, &done) == cudaSuccess;
+        }
+        if (ok) ok = cudaStreamBeginCaptureToGraph(g->s3, body_res, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            restart();
+            k_dev_after_restart<<<1, 1, 0, g->s3>>>(c.scal);
+            cudaGraph_t done = nullptr;
+            ok = cudaStreamEndCapture(g->s3, &done) == cudaSuccess;
+        }
+        if (!ok) err = SPH_ERR_CUDA;
+    }
+    c.stream = outer;
+    return err;
+}
+
+template <class Real>
+static DevLoopGraph *devloop_graph(Ctx<Real> &c) {
     auto *g = (DevLoopGraph *)c.devloop;
     if (!g) {
         g = new DevLoopGraph();
         c.devloop = g;
-        SPH_CUDA_TRY(cudaStreamCreateWithFlags(&g->s2, cudaStreamNonBlocking));
-        SPH_CUDA_TRY(cudaStreamCreateWithFlags(&g->s3, cudaStreamNonBlocking));
+        if (cudaStreamCreateWithFlags(&g->s2, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&g->s3, cudaStreamNonBlocking) != cudaSuccess) {
+            set_error("device-controlled solve: stream creation failed");
+            return nullptr;
+        }
     }
-    std::vector<uintptr_t> key = krylov_graph_key(c, ws, xlo);
+    return g;
+}
+
+// The solve as its own graph (launched on the context's stream), or, while a
+// whole step is captured, appended to the step's graph.
+template <class Real>
+static int bicgstab_device(Ctx<Real> &c, double *x, const double *b, double *yd, double tol, int maxit) {
+    cudaStream_t st = c.stream;
+    DevLoopGraph *g = devloop_graph(c);
+    if (!g) return SPH_ERR_CUDA;
+    if (c.capturing) {
+        const long long l0 = c.launches;
+        SPH_TRY(append_solve(c, g, st, x, b, yd, tol, maxit));
+        c.launches = l0 + 1;   // counted as one launch, as the solve's own graph is
+        return SPH_OK;
+    }
+    std::vector<uintptr_t> key = krylov_graph_key(c, (float *const *)c.kv, c.xf);
     const uintptr_t extra[] = {(uintptr_t)x, (uintptr_t)b, (uintptr_t)yd, (uintptr_t)maxit, (uintptr_t)c.coef_h,
                                (uintptr_t)c.coef_rs, (uintptr_t)(c.prm.ppe_coef_half && c.coef_h_valid),
                                (uintptr_t)c.nm_ow, (uintptr_t)c.coef};
@@ -1352,87 +1456,18 @@ static int bicgstab_device(Ctx<Real> &c, double *x, const double *b, double *yd,
     if (!g->exec || g->key != key) {
         if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
         const long long l0 = c.launches;
-        auto replace = [&]() {
-            k_axpy_cast<float, double><<<grid_for(n, 256), 256, 0, c.stream>>>(xlo, x, n);
-            apply_op<Real, double>(c, x, yd, true);
-            k_reliable_replace<float><<<G, 256, 0, c.stream>>>(b, yd, r, xlo, rh, n, c.red, counter, c.scal);
-        };
-        auto restart = [&]() {
-            replace();
-            k_restart_dirs<float><<<G, 256, 0, c.stream>>>(r, rh, p, v, n);
-            k_norm2<float><<<G, 256, 0, c.stream>>>(r, n, c.red, counter, c.scal, SC_RHO_NEW);
-            k_dev_set_scal<<<1, 1, 0, c.stream>>>(c.scal);
-        };
-        auto iteration = [&]() {
-            k_p_update<float><<<G, 256, 0, c.stream>>>(p, ph, r, v, dinv, n, c.scal);
-            bool mr = precond_coarse<Real, float>(c, p, ph, v, true);
-            apply_op<Real, float>(c, ph, v, true, mr);
-            k_alpha<float><<<G, 256, 0, c.stream>>>(rh, v, n, c.red, counter, c.scal);
-            k_s_update<float><<<G, 256, 0, c.stream>>>(r, v, s, sh, dinv, n, c.scal);
-            mr = precond_coarse<Real, float>(c, s, sh, t, true);
-            apply_op<Real, float>(c, sh, t, true, mr);
-            k_omega<float><<<G, 256, 0, c.stream>>>(t, s, n, c.red, counter, c.scal);
-            k_xr_update<float><<<G, 256, 0, c.stream>>>(xlo, r, ph, sh, s, t, rh, n, c.red, counter, c.scal);
-        };
         cudaGraph_t graph = nullptr;
-        cudaGraphConditionalHandle h_loop, h_rep, h_res;
-        cudaGraph_t body = nullptr, body_rep = nullptr, body_res = nullptr;
         int err = SPH_OK;
         const bool prof = c.prof;
         c.prof = false;   // event-record nodes are not allowed in conditional bodies
         do {
             if (cudaGraphCreate(&graph, 0) != cudaSuccess) { err = SPH_ERR_CUDA; break; }
-            if (cudaGraphConditionalHandleCreate(&h_loop, graph, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
-                err = SPH_ERR_CUDA; break;
-            }
-            // the solve's start: the restart of bicgstab_reliable, then the loop
             if (cudaStreamBeginCaptureToGraph(st, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
                 cudaSuccess) { err = SPH_ERR_CUDA; break; }
-            k_dev_tol<<<1, 1, 0, st>>>(c.scal, tol, maxit, check);
-            k_dinv<float, Real><<<grid_for(n, 256), 256, 0, st>>>(c.row_kind, c.diag, dinv, n);
-            cudaMemsetAsync(xlo, 0, sizeof(float) * n, st);
-            restart();
-            k_dev_start<<<1, 1, 0, st>>>(c.scal, h_loop);
-            err = add_conditional(st, h_loop, cudaGraphCondTypeWhile, &body);
+            err = append_solve(c, g, st, x, b, yd, tol, maxit);
             cudaGraph_t done = nullptr;
             const cudaError_t e1 = cudaStreamEndCapture(st, &done);
             if (err != SPH_OK || e1 != cudaSuccess) { if (err == SPH_OK) err = SPH_ERR_CUDA; break; }
-            // the loop body on s2, its two branches on s3
-            if (cudaGraphConditionalHandleCreate(&h_rep, body, 0, cudaGraphCondAssignDefault) != cudaSuccess ||
-                cudaGraphConditionalHandleCreate(&h_res, body, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
-                err = SPH_ERR_CUDA; break;
-            }
-            c.stream = g->s2;
-            if (cudaStreamBeginCaptureToGraph(g->s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
-                cudaSuccess) { err = SPH_ERR_CUDA; c.stream = st; break; }
-            for (int q = 0; q < check; ++q) iteration();
-            k_dev_decide<<<1, 1, 0, g->s2>>>(c.scal, h_rep, h_res);
-            err = add_conditional(g->s2, h_rep, cudaGraphCondTypeIf, &body_rep);
-            if (err == SPH_OK) err = add_conditional(g->s2, h_res, cudaGraphCondTypeIf, &body_res);
-            if (err == SPH_OK) k_dev_tail<<<1, 1, 0, g->s2>>>(c.scal, h_loop);
-            cudaGraph_t done2 = nullptr;
-            const cudaError_t e2 = cudaStreamEndCapture(g->s2, &done2);
-            if (err != SPH_OK || e2 != cudaSuccess) { if (err == SPH_OK) err = SPH_ERR_CUDA; c.stream = st; break; }
-            // the reliable update, then the restart branch
-            c.stream = g->s3;
-            bool ok = cudaStreamBeginCaptureToGraph(g->s3, body_rep, nullptr, nullptr, 0,
-                                                    cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-            if (ok) {
-                replace();
-                k_dev_after_replace<<<1, 1, 0, g->s3>>>(c.scal, h_res);
-                cudaGraph_t done3 = nullptr;
-                ok = cudaStreamEndCapture(g->s3, &done3) == cudaSuccess;
-            }
-            if (ok) ok = cudaStreamBeginCaptureToGraph(g->s3, body_res, nullptr, nullptr, 0,
-                                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-            if (ok) {
-                restart();
-                k_dev_after_restart<<<1, 1, 0, g->s3>>>(c.scal);
-                cudaGraph_t done4 = nullptr;
-                ok = cudaStreamEndCapture(g->s3, &done4) == cudaSuccess;
-            }
-            c.stream = st;
-            if (!ok) { err = SPH_ERR_CUDA; break; }
             if (cudaGraphInstantiate(&g->exec, graph, 0) != cudaSuccess) { g->exec = nullptr; err = SPH_ERR_CUDA; break; }
             g->key = key;
         } while (0);
@@ -2078,6 +2113,15 @@ static int ensure_ppe_ws(Ctx<Real> &c) {
     return SPH_OK;
 }
 
+// ppe_refinement = 4 and what the device-controlled solve needs: the mixed
+// form with the cached operator, a stream of its own, no live timing, no
+// learned / extrapolated / scaled start and no sample collection
+template <class Real>
+bool solve_under_device_control(const Ctx<Real> &c) {
+    return sizeof(Real) == 4 && c.prm.ppe_mode == SPH_PPE_MIXED_IR && c.prm.ppe_refinement == 4 &&
+           c.prm.ppe_matrix_free == 0 && c.stream != nullptr && !c.prof && c.ml_every == 0 && c.prm.ppe_warm_start == 0;
+}
+
 template <class Real>
 int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     cudaStream_t st = c.stream;
@@ -2088,7 +2132,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
     sph_ppe_stats S{};
     SPH_TRY(ensure_ppe_ws(c));
     Real *b = c.kv[9];
-    SPH_CUDA_TRY(cudaEventRecord(c.ev[4], st));
+    SPH_CUDA_TRY(record_event(c, c.ev[4]));
     // b_i, A_i every step; c_ij once per neighbour-list build (time-invariant
     // while the particles do not move)
     const long long nnzp = std::max(c.nnz_padded, 1LL);
@@ -2144,8 +2188,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         // host reading nothing until the statistics are wanted (only without
         // live timing, learned / extrapolated / scaled start vectors and
         // sample collection, which need the host; else the host-controlled loop)
-        const bool devloop = sizeof(Real) == 4 && mode == SPH_PPE_MIXED_IR && c.prm.ppe_refinement == 4 && cached &&
-                             st != nullptr && !c.prof && c.ml_every == 0 && c.prm.ppe_warm_start == 0;
+        const bool devloop = solve_under_device_control(c);
         if (devloop) {
             const double tol = c.prm.ppe_tol > 0 ? c.prm.ppe_tol : 1e-6;
             const int maxit = c.prm.ppe_max_iter > 0 ? c.prm.ppe_max_iter : 2000;
@@ -2153,7 +2196,7 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
             k_dev_record<<<1, 1, 0, st>>>(c.scal);
             k_cast<double, Real><<<grid_for(n, 256), 256, 0, st>>>(xd, c.S.p, n);
             c.launches += 2;
-            SPH_CUDA_TRY(cudaEventRecord(c.ev[5], st));
+            SPH_CUDA_TRY(record_event(c, c.ev[5]));
             SPH_TRY(neumann_pass(c, c.S));
             SPH_TRY(outlet_pass(c, c.S));
             SPH_CUDA_TRY(cudaGetLastError());
@@ -2359,6 +2402,7 @@ void release_solver_ws(Ctx<Real> &c) {
     }
     delete (DevLoopGraph *)c.devloop;
     c.devloop = nullptr;
+    ++c.mem_gen;   // a step graph captured over these workspaces is stale
     c.gm_ws_r = nullptr;
     c.gm_ws_d = nullptr;
     c.idr_ws_r = nullptr;
@@ -2369,6 +2413,7 @@ void release_solver_ws(Ctx<Real> &c) {
     template void release_solver_ws<R>(Ctx<R> &); \
     template int dev_solve_stats<R>(Ctx<R> &, sph_ppe_stats *, int *); \
     template int dev_reset_worst<R>(Ctx<R> &); \
+    template bool solve_under_device_control<R>(const Ctx<R> &); \
     template int operator_stats<R>(Ctx<R> &, int64_t *, double *, double *, int); \
     template int operator_bytes<R>(Ctx<R> &, double *, double *); \
     template void ppe_apply_fp64<R>(Ctx<R> &, const double *, double *);
