@@ -548,8 +548,9 @@ def main():
     ap.add_argument("--wide-index", action="store_true",
                     help="pressure operator on 32-bit neighbour indices instead of the 16-bit codes")
     ap.add_argument("--coarse", type=int, default=None,
-                    help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; "
-                         "default 5 for the canyon, 9 for the cube array)")
+                    help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; -B: "
+                         "aggregates balanced by row count from blocks of B^3 cells; default 5 for the canyon, 9 "
+                         "for the cube array)")
     ap.add_argument("--coarse-mode", default="additive", choices=["additive", "multiplicative"],
                     help="two-level form: D^-1 r + Z E^-1 Z^T r, or the coarse correction of the residual the "
                          "Jacobi step leaves (one more operator application per preconditioner call)")
@@ -567,8 +568,9 @@ def main():
     ap.add_argument("--pforce-form", default=None, choices=["active", "difference"],
                     help="pressure-force pair term: the reference's active form, or its commented-out difference "
                          "form (no force from a constant pressure); default difference with APR, else active")
-    ap.add_argument("--coef-half", action="store_true",
-                    help="FP32 operator applications read row-scaled FP16 coefficients (ppe_coef_half)")
+    ap.add_argument("--coef-half", action=argparse.BooleanOptionalAction, default=True,
+                    help="FP32 operator applications of the mixed form read row-scaled FP16 coefficients "
+                         "(ppe_coef_half; default on)")
     ap.add_argument("--start-proj", default="none", choices=["none", "galerkin", "ls"],
                     help="start vector projected on [previous pressure change, coarse correction of the start "
                          "residual, network prediction with --warm learned]: Galerkin or least squares")
@@ -800,7 +802,7 @@ def main():
             fp64 = timed_form(layout.PREC_FP64, fp64_mode, 0, kd, keep=True)
             fp64.update({"solver": args.fp64_mode + " + jacobi", "ppe_tol": args.tol})
             err64 = error_vs(fp64.pop("_state"), kd + 2)
-            if args.coarse > 0:
+            if args.coarse != 0:
                 # FP64 with this run's preconditioner: isolates the precision change
                 fp64_same = timed_form(layout.PREC_FP64, layout.PPE_BICGSTAB, args.coarse, kd)
                 fp64_same.update({"solver": f"bicgstab + coarse {args.coarse}", "ppe_tol": args.tol})
@@ -834,7 +836,8 @@ def main():
     # (rows, stored entries and Neumann entries grow together)
     nc = ncu_traffic(f"ppe_operator_{args.config}.json")
     traffic = None
-    if nc and "measured_at" in nc and nc.get("apr", False) == bool(args.apr):
+    if (nc and "measured_at" in nc and nc.get("apr", False) == bool(args.apr)
+            and nc.get("coef_half", False) == bool(p.ppe_coef_half)):
         m = nc["measured_at"]
         traffic = m["traffic_over_algorithmic"] * op_bytes
     ph = np.mean(np.array(phases), axis=0) if phases else np.zeros(4)
@@ -861,8 +864,11 @@ def main():
                    "ppe_start_vector": {"prev": "previous pressure", "extrap": "linear extrapolation in time",
                                         "scaled": "previous pressure times its residual-minimising factor",
                                         "learned": "learned per-particle MLP on the previous pressure"}[args.warm],
-                   "ppe_preconditioner": f"jacobi + coarse aggregates of {args.coarse}^3 cells ({args.coarse_mode})"
-                   if args.coarse > 0 else "jacobi",
+                   "ppe_preconditioner": (f"jacobi + coarse aggregates of {args.coarse}^3 cells ({args.coarse_mode})"
+                                          if args.coarse > 0 else
+                                          f"jacobi + coarse aggregates balanced by row count, octree boxes from "
+                                          f"{-args.coarse}^3 cells, at most 4096 ({args.coarse_mode})"
+                                          if args.coarse < 0 else "jacobi"),
                    "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": len(P) * layout.PART1.itemsize,

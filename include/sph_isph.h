@@ -181,7 +181,11 @@ typedef struct sph_params {
                                 collection, else 0 runs)                       */
     int32_t ppe_coarse_block;    /* BiCGSTAB preconditioner: 0 Jacobi; B > 0
                                 adds a coarse correction on aggregates of
-                                B x B x B NNPS cells (additive two-level)      */
+                                B x B x B NNPS cells (additive two-level); -B
+                                aggregates balanced by row count: blocks of
+                                B x B x B cells, the block with the most rows
+                                split into octants again and again while at
+                                most 4096 aggregates result                   */
     int32_t ppe_warm_start;  /* start vector of the converged solves: 0 previous
                                 pressure; 1 linear extrapolation in time,
                                 2 p_n - p_(n-1), once two solutions exist;

@@ -135,15 +135,45 @@ def condition(P, g_str, g_end, p, target, family):
     return cond, flag
 
 
-def merge_cells(flag, cond, g_str, g_end):
-    """The merging cells of a pass: those holding a marked member (apr_cond -1);
-    the reference numbers every cell whose condition asked to merge, whose
-    slots stay unused when the cell holds no marked member."""
+def family_members(P, p, g_str, g_end, family, j, blood):
+    """Active (i_type 1) members of family `blood` in the cells around record j."""
+    out = []
+    for kk in _cells_around(P, j, p):
+        if g_str[kk] < 0:
+            continue
+        out += [i for i in range(int(g_str[kk]), int(g_end[kk])) if P["i_type"][i] == 1 and family[i] == blood]
+    return out
+
+
+def merge_record(P, p, g_str, g_end, family, cond, k):
+    """The record cell k merges: its first marked member, when that member's
+    family is complete (eight active members around it) and it is the
+    family's member of largest index; else -1."""
+    s, e = int(g_str[k]), int(g_end[k])
+    js = [j for j in range(s, e) if cond[j] == -1]
+    if not js:
+        return -1
+    j = js[0]
+    blood = int(family[j])
+    if blood == 0:
+        return -1
+    members = family_members(P, p, g_str, g_end, family, j, blood)
+    return j if len(members) == 8 and max(members) == j else -1
+
+
+def merge_cells(flag, cond, g_str, g_end, P, p, family):
+    """The merging cells of a pass: those holding a marked member (apr_cond -1)
+    whose family merges in this pass, so that the free records at the tail
+    go to merges that happen.  The reference numbers every cell whose
+    condition asked to merge (Cell_index on its flags), whose slots stay
+    unused when the cell holds no marked member or the family is incomplete;
+    its 3-D merge is commented out, and with few free records left that
+    numbering would hand every slot to cells that do not merge."""
     out = np.where(flag > 0, flag, 0).astype(np.int32)
     for k in range(len(flag)):
         if flag[k] > 0 or g_str[k] < 0:
             continue
-        if (cond[int(g_str[k]):int(g_end[k])] == -1).any():
+        if merge_record(P, p, g_str, g_end, family, cond, k) >= 0:
             out[k] = -1
     return out
 
@@ -210,21 +240,10 @@ def execute(P, g_str, g_end, p, target, family, cond, num, first_free):
             continue
         if n + q < min_slot:
             continue
-        js = [j for j in range(s, e) if cond[j] == -1]
-        if not js:
+        j = merge_record(P, p, g_str, g_end, family, cond, k)
+        if j < 0:
             continue
-        j = js[0]
-        blood = int(family[j])
-        if blood == 0:
-            continue
-        members = []
-        for kk in _cells_around(P, j, p):
-            if g_str[kk] < 0:
-                continue
-            members += [i for i in range(int(g_str[kk]), int(g_end[kk]))
-                        if P["i_type"][i] == 1 and family[i] == blood]
-        if len(members) != 8 or max(members) != j:
-            continue
+        members = family_members(P, p, g_str, g_end, family, j, int(family[j]))
         acc = {f: f32(0) for f in ("m", "vol", "x", "y", "z", "ux", "uy", "uz", "pres")}
         for i in members:
             acc["m"] = f32(acc["m"] + P["m"][i])
@@ -254,7 +273,7 @@ def apr_pass(P, g_idx, g_str, g_end, p, family=None):
         family = np.arange(1, len(P) + 1, dtype=np.int32)
     target = zone_target(P, g_idx, p)
     cond, flag = condition(P, g_str, g_end, p, target, family)
-    num, pos, neg = numbering(merge_cells(flag, cond, g_str, g_end))
+    num, pos, neg = numbering(merge_cells(flag, cond, g_str, g_end, P, p, family))
     first_free = int(g_str[NC]) if g_str[NC] >= 0 else len(P)
     Q, T, F, ns, nm = execute(P, g_str, g_end, p, target, family, cond, num, first_free)
     return Q, T, F, ns, pos, nm

@@ -148,18 +148,52 @@ __global__ void k_apr_condition(Ctx<Real> c, const float *target, const int *fam
     flag[k] = -1;
 }
 
-// merging cells are the cells that hold a marked member (wherever the
-// condition that marked it ran); a cell that asked to merge without holding
-// one gets no merge number
+// calls f(i) for every active (i_type 1) member of family `blood` in the
+// cells around record j (the reach of the condition's family search)
+template <class Real, class F>
+__device__ __forceinline__ void for_family(const Ctx<Real> &c, const int *family, int j, int blood, F &&f) {
+    const DevParams &P = c.dp;
+    const float4 xa = c.pf[j];
+    const int ic = bin_axis(xa.x, P.xmin, P.xmax, P.NI), jc = bin_axis(xa.y, P.ymin, P.ymax, P.NJ),
+              kc = bin_axis(xa.z, P.zmin, P.zmax, P.NK);
+    const int range = (int)ceilf(__fdiv_rn(__fmul_rn((float)kNcellInit, xa.w), (float)c.h_ref[j]));
+    for (int dz = -range; dz <= range; ++dz)
+        for (int dy = -range; dy <= range; ++dy)
+            for (int dx = -range; dx <= range; ++dx) {
+                const int a = ic + dx, b = jc + dy, cc = kc + dz;
+                if (a < 0 || a > P.NI - 1 || b < 0 || b > P.NJ - 1 || cc < 0 || cc > P.NK - 1) continue;
+                const int kk = a + P.NI * b + P.NI * P.NJ * cc;
+                for (int i = c.cell_start[kk]; i < c.cell_start[kk + 1]; ++i)
+                    if (c.ty[i].x == 1 && family[i] == blood) f(i);
+            }
+}
+
+// the record a merging cell merges: its first marked member, when that
+// member's family is complete (eight active members around it) and it is the
+// family's member of largest index; else -1
 template <class Real>
-__global__ void k_apr_merge_cells(Ctx<Real> c, const int *apr_cond, int *flag) {
+__device__ int merge_record(const Ctx<Real> &c, const int *apr_cond, const int *family, int k) {
+    int j = -1;
+    for (int a = c.cell_start[k]; a < c.cell_start[k + 1]; ++a)
+        if (apr_cond[a] == -1) { j = a; break; }
+    if (j < 0) return -1;
+    const int blood = family[j];
+    if (blood == 0) return -1;
+    int count = 0, last = -1;
+    for_family(c, family, j, blood, [&](int i) { ++count; last = max(last, i); });
+    return (count == 8 && last == j) ? j : -1;
+}
+
+// merging cells are the cells that hold a marked member (wherever the
+// condition that marked it ran) whose family merges in this pass; only they
+// get merge numbers, so the free records at the tail go to merges that
+// happen
+template <class Real>
+__global__ void k_apr_merge_cells(Ctx<Real> c, const int *apr_cond, const int *family, int *flag) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= c.num_cells) return;
     if (flag[k] > 0) return;
-    int f = 0;
-    for (int j = c.cell_start[k]; j < c.cell_start[k + 1]; ++j)
-        if (apr_cond[j] == -1) { f = -1; break; }
-    flag[k] = f;
+    flag[k] = merge_record(c, apr_cond, family, k) >= 0 ? -1 : 0;
 }
 
 template <class T>
@@ -229,34 +263,10 @@ __global__ void k_apr_execute(Ctx<Real> c, const int *number, const int *apr_con
         return;
     }
     if (c.n + q < min_slot) return;
-    int j = -1;
-    for (int a = s; a < e; ++a)
-        if (apr_cond[a] == -1) { j = a; break; }
+    const int j = merge_record(c, apr_cond, family, k);
     if (j < 0) return;
     const int blood = family[j];
-    if (blood == 0) return;
-    const DevParams &P = c.dp;
-    const float4 xa = c.pf[j];
-    const int ic = bin_axis(xa.x, P.xmin, P.xmax, P.NI), jc = bin_axis(xa.y, P.ymin, P.ymax, P.NJ),
-              kc = bin_axis(xa.z, P.zmin, P.zmax, P.NK);
-    const int range = (int)ceilf(__fdiv_rn(__fmul_rn((float)kNcellInit, xa.w), (float)c.h_ref[j]));
-    // members: the family's active records in the cells around the marked one
-    auto for_members = [&](auto &&f) {
-        for (int dz = -range; dz <= range; ++dz)
-            for (int dy = -range; dy <= range; ++dy)
-                for (int dx = -range; dx <= range; ++dx) {
-                    const int a = ic + dx, b = jc + dy, cc = kc + dz;
-                    if (a < 0 || a > P.NI - 1 || b < 0 || b > P.NJ - 1 || cc < 0 || cc > P.NK - 1) continue;
-                    const int kk = a + P.NI * b + P.NI * P.NJ * cc;
-                    for (int i = c.cell_start[kk]; i < c.cell_start[kk + 1]; ++i)
-                        if (c.ty[i].x == 1 && family[i] == blood) f(i);
-                }
-    };
-    // a complete family of eight, merged once: by the thread of its member
-    // of largest index
-    int count = 0, last = -1;
-    for_members([&](int i) { ++count; last = max(last, i); });
-    if (count != 8 || last != j) return;
+    auto for_members = [&](auto &&f) { for_family(c, family, j, blood, f); };
     Real m_sum = 0, vol_sum = 0, x_avg = 0, y_avg = 0, z_avg = 0, ux_avg = 0, uy_avg = 0, uz_avg = 0, p_avg = 0;
     for_members([&](int i) {
         const R4 xi = c.pr[i];
@@ -328,7 +338,7 @@ int apr_pass(Ctx<Real> &c, int *n_split, int *n_wanted, int *n_merged) {
         k_apr_zone<<<grid_for(n, 256), 256, 0, st>>>(c.ty, c.pf, c.dp, reach, zone, n);
     k_apr_target<<<grid_for(n, 256), 256, 0, st>>>(c.ty, c.g_idx, zone, NC, std::max(max_level, 0), c.apr_target, n);
     k_apr_condition<Real><<<grid_for(NC, 256), 256, 0, st>>>(c, c.apr_target, c.apr_family, cond, flag);
-    k_apr_merge_cells<Real><<<grid_for(NC, 256), 256, 0, st>>>(c, cond, flag);
+    k_apr_merge_cells<Real><<<grid_for(NC, 256), 256, 0, st>>>(c, cond, c.apr_family, flag);
     c.launches += 4;
     SPH_CUDA_TRY(cudaGetLastError());
     // Cell_index in cell order, and the free records

@@ -1,5 +1,6 @@
 // Two-level preconditioner of the converged pressure solve: Jacobi plus an
-// additive coarse correction on aggregates of B x B x B NNPS cells,
+// additive coarse correction on aggregates of B x B x B NNPS cells (or
+// balanced octree boxes, ppe_coarse_block = -B),
 //     M^-1 r = D^-1 r + Z E^-1 Z^T r,   E = Z^T M Z,
 // with Z the indicator vectors of the aggregates (every row of the operator
 // except identity / pinned rows belongs to exactly one) and M the converged
@@ -19,6 +20,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 #include "ctx.cuh"
@@ -26,6 +28,7 @@
 namespace sph {
 
 constexpr int kCoarseMaxAgg = 4096;
+constexpr int kCoarsePiece = 1024;   // rows per block of the restriction
 
 // deterministic block sum (fixed shuffle pattern, warps summed in order)
 template <int NT>
@@ -204,19 +207,36 @@ __global__ void k_eye(double *A, int m) {
 
 // ---- application ----------------------------------------------------------
 
-// s_I = sum over the rows of aggregate I of r (minus w when given)
+// s_I = sum over the rows of aggregate I of r (minus w when given).  The
+// rows of every aggregate are cut into pieces of at most kCoarsePiece
+// entries, one block per piece, so the launch has enough blocks to hide the
+// gathers however few the aggregates; the last block of an aggregate to
+// finish sums its pieces' partials in piece order, so the result does not
+// depend on the order the blocks run in.
 template <class V>
-__global__ void __launch_bounds__(256) k_coarse_restrict(const int *off, const int *rows, const V *r, const V *w,
-                                                         double *s) {
+__global__ void __launch_bounds__(256) k_coarse_restrict(const int *__restrict__ piece, const int *__restrict__ pfirst,
+                                                         const int *__restrict__ rows, const V *r, const V *w,
+                                                         double *part, unsigned int *cnt, double *s) {
     __shared__ double sh[8];
-    const int I = blockIdx.x;
+    const int p = blockIdx.x;
+    const int I = piece[3 * p], q0 = piece[3 * p + 1], q1 = piece[3 * p + 2];
     double v = 0;
     if (w)
-        for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) { const int i = rows[q]; v += (double)(r[i] - w[i]); }
+        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) { const int i = rows[q]; v += (double)(r[i] - w[i]); }
     else
-        for (int q = off[I] + threadIdx.x; q < off[I + 1]; q += blockDim.x) v += (double)r[rows[q]];
+        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) v += (double)r[rows[q]];
     v = block_sum<256>(v, sh);
-    if (threadIdx.x == 0) s[I] = v;
+    if (threadIdx.x != 0) return;
+    const int p0 = pfirst[I], np = pfirst[I + 1] - p0;
+    if (np == 1) { s[I] = v; return; }
+    part[p] = v;
+    __threadfence();
+    if (atomicAdd(&cnt[I], 1u) != (unsigned)(np - 1)) return;
+    __threadfence();
+    double t = 0;
+    for (int k = 0; k < np; ++k) t += __ldcg(part + p0 + k);
+    s[I] = t;
+    cnt[I] = 0;
 }
 
 // y = E^-1 s, one warp per row; E^-1 is stored in FP32 (a preconditioner
@@ -245,7 +265,8 @@ __global__ void k_coarse_add(const int *agg, const double *y, V *z, int n) {
 template <class Real, class V>
 void coarse_restrict_solve(Ctx<Real> &c, const V *r, const V *w) {
     const int m = c.cg_m;
-    k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, w, c.cg_s);
+    k_coarse_restrict<V><<<c.cg_np, 256, 0, c.stream>>>(c.cg_piece, c.cg_pfirst, c.cg_rows, r, w, c.cg_part, c.cg_cnt,
+                                                        c.cg_s);
     k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_invf, c.cg_s, c.cg_y, m);
     c.launches += 2;
 }
@@ -254,10 +275,87 @@ template <class Real, class V>
 void coarse_apply(Ctx<Real> &c, const V *r, V *z, const V *w) {
     if (c.cg_m <= 0) return;
     const int m = c.cg_m;
-    k_coarse_restrict<V><<<m, 256, 0, c.stream>>>(c.cg_off, c.cg_rows, r, w, c.cg_s);
+    k_coarse_restrict<V><<<c.cg_np, 256, 0, c.stream>>>(c.cg_piece, c.cg_pfirst, c.cg_rows, r, w, c.cg_part, c.cg_cnt,
+                                                        c.cg_s);
     k_coarse_solve<<<div_up((long long)m * 32, 256), 256, 0, c.stream>>>(c.cg_invf, c.cg_s, c.cg_y, m);
     k_coarse_add<V><<<grid_for(c.n, 256), 256, 0, c.stream>>>(c.cg_agg, c.cg_y, z, c.n);
     c.launches += 3;
+}
+
+// Balanced aggregates (ppe_coarse_block = -B): start from blocks of B^3
+// cells and split the block holding the most rows into its (up to eight)
+// non-empty octants, again and again, while the aggregate count stays within
+// kCoarseMaxAgg and the block is wider than one cell.  On an APR-refined deck
+// a block of the refined zone holds eight times the rows of a block outside
+// it; splitting by row count gives every aggregate about the same number of
+// rows, i.e. aggregates about twice finer (in cells) where the particles are.
+// cell[3 * k ..] are the cell coordinates of member k, rows[k] its row;
+// returns the aggregate of every member, numbered 0.. in any order.
+static std::vector<int> octree_aggregates(const std::vector<int> &cell, int nmem, int B, int NI, int NJ, int NK,
+                                          int maxagg) {
+    struct Box {
+        int x0, x1, y0, y1, z0, z1;
+        std::vector<int> mem;
+    };
+    std::vector<Box> boxes;
+    {
+        const int NBx = (NI + B - 1) / B, NBy = (NJ + B - 1) / B;
+        std::vector<int> id((size_t)NBx * NBy * ((NK + B - 1) / B), -1);
+        for (int k = 0; k < nmem; ++k) {
+            const int bx = cell[3 * k] / B, by = cell[3 * k + 1] / B, bz = cell[3 * k + 2] / B;
+            int &b = id[((size_t)bz * NBy + by) * NBx + bx];
+            if (b < 0) {
+                b = (int)boxes.size();
+                boxes.push_back(Box{bx * B, std::min(NI, bx * B + B), by * B, std::min(NJ, by * B + B), bz * B,
+                                    std::min(NK, bz * B + B), {}});
+            }
+            boxes[b].mem.push_back(k);
+        }
+    }
+    if ((int)boxes.size() <= maxagg) {
+        // largest first (ties: lower box index), each split replaces one box by its non-empty octants
+        auto larger = [&](int a, int b) {
+            return boxes[a].mem.size() != boxes[b].mem.size() ? boxes[a].mem.size() < boxes[b].mem.size() : a > b;
+        };
+        std::vector<int> heap;
+        for (int b = 0; b < (int)boxes.size(); ++b) heap.push_back(b);
+        std::make_heap(heap.begin(), heap.end(), larger);
+        while (!heap.empty()) {
+            std::pop_heap(heap.begin(), heap.end(), larger);
+            const int b = heap.back();
+            heap.pop_back();
+            Box &bx = boxes[b];
+            if (bx.mem.size() < 2) break;   // every remaining box holds at most one row
+            const int mx = bx.x1 - bx.x0 > 1 ? bx.x0 + (bx.x1 - bx.x0 + 1) / 2 : bx.x1;
+            const int my = bx.y1 - bx.y0 > 1 ? bx.y0 + (bx.y1 - bx.y0 + 1) / 2 : bx.y1;
+            const int mz = bx.z1 - bx.z0 > 1 ? bx.z0 + (bx.z1 - bx.z0 + 1) / 2 : bx.z1;
+            if (mx == bx.x1 && my == bx.y1 && mz == bx.z1) continue;   // one cell wide: cannot split
+            std::vector<int> part[8];
+            for (int k : bx.mem)
+                part[(cell[3 * k] >= mx ? 1 : 0) | (cell[3 * k + 1] >= my ? 2 : 0) | (cell[3 * k + 2] >= mz ? 4 : 0)]
+                    .push_back(k);
+            int nonempty = 0;
+            for (int q = 0; q < 8; ++q) nonempty += part[q].empty() ? 0 : 1;
+            if ((int)boxes.size() + nonempty - 1 > maxagg) break;   // the largest box cannot split any more
+            const Box parent = Box{bx.x0, bx.x1, bx.y0, bx.y1, bx.z0, bx.z1, {}};
+            bool first = true;
+            for (int q = 0; q < 8; ++q) {
+                if (part[q].empty()) continue;
+                Box child{(q & 1) ? mx : parent.x0, (q & 1) ? parent.x1 : mx, (q & 2) ? my : parent.y0,
+                          (q & 2) ? parent.y1 : my, (q & 4) ? mz : parent.z0, (q & 4) ? parent.z1 : mz,
+                          std::move(part[q])};
+                int id;
+                if (first) { boxes[b] = std::move(child); id = b; first = false; }
+                else { boxes.push_back(std::move(child)); id = (int)boxes.size() - 1; }
+                heap.push_back(id);
+                std::push_heap(heap.begin(), heap.end(), larger);
+            }
+        }
+    }
+    std::vector<int> agg(nmem, -1);
+    for (int b = 0; b < (int)boxes.size(); ++b)
+        for (int k : boxes[b].mem) agg[k] = b;
+    return agg;
 }
 
 template <class Real>
@@ -266,7 +364,7 @@ int coarse_build(Ctx<Real> &c) {
     c.cg_valid = true;
     c.cg_block = B;
     c.cg_m = 0;
-    if (B <= 0) return SPH_OK;
+    if (B == 0) return SPH_OK;
     const int n = c.n;
     cudaStream_t st = c.stream;
     // host copies of what the aggregation needs
@@ -288,20 +386,38 @@ int coarse_build(Ctx<Real> &c) {
     // so that every coarse vector satisfies the copy rows exactly: a ghost
     // and the interior record it mirrors across the box share an aggregate.
     const DevParams &P = c.dp;
-    const int NBx = (P.NI + B - 1) / B, NBy = (P.NJ + B - 1) / B, NBz = (P.NK + B - 1) / B;
-    std::vector<int> block_agg((size_t)NBx * NBy * NBz, -1), agg(n, -1), size;
+    const int Bb = B > 0 ? B : -B;
     auto member = [&](int k) { return kind[k] == 1 || kind[k] == 2 || kind[k] == 3; };
-    int m = 0;
+    std::vector<int> cell, mrow;   // cell coordinates and row of each member
+    cell.reserve(3 * (size_t)n);
     for (int i = 0; i < n; ++i) {
         if (!member(i)) continue;
         int src = i;
         if (kind[i] == 3 && aux[i] >= 0 && aux[i] < n && member(aux[i])) src = aux[i];
-        const int bx = bin_axis(pos[src].x, P.xmin, P.xmax, P.NI) / B;
-        const int by = bin_axis(pos[src].y, P.ymin, P.ymax, P.NJ) / B;
-        const int bz = bin_axis(pos[src].z, P.zmin, P.zmax, P.NK) / B;
-        int &a = block_agg[((size_t)bz * NBy + by) * NBx + bx];
-        if (a < 0) { a = m++; size.push_back(0); }
-        agg[i] = a;
+        cell.push_back(bin_axis(pos[src].x, P.xmin, P.xmax, P.NI));
+        cell.push_back(bin_axis(pos[src].y, P.ymin, P.ymax, P.NJ));
+        cell.push_back(bin_axis(pos[src].z, P.zmin, P.zmax, P.NK));
+        mrow.push_back(i);
+    }
+    const int nmem = (int)mrow.size();
+    std::vector<int> box(nmem);   // block (B > 0) or balanced box (B < 0) of each member
+    if (B > 0) {
+        const int NBx = (P.NI + Bb - 1) / Bb, NBy = (P.NJ + Bb - 1) / Bb;
+        for (int k = 0; k < nmem; ++k)
+            box[k] = ((cell[3 * k + 2] / Bb) * NBy + cell[3 * k + 1] / Bb) * NBx + cell[3 * k] / Bb;
+    } else {
+        box = octree_aggregates(cell, nmem, Bb, P.NI, P.NJ, P.NK, kCoarseMaxAgg);
+    }
+    // aggregates numbered in order of their first row (rows ascending)
+    std::vector<int> agg(n, -1), size;
+    std::unordered_map<int, int> number;
+    int m = 0;
+    for (int k = 0; k < nmem; ++k) {
+        auto it = number.find(box[k]);
+        int a;
+        if (it == number.end()) { a = m++; number.emplace(box[k], a); size.push_back(0); }
+        else a = it->second;
+        agg[mrow[k]] = a;
         ++size[a];
     }
     if (m > kCoarseMaxAgg) {
@@ -336,6 +452,27 @@ int coarse_build(Ctx<Real> &c) {
     SPH_TRY(up(c.cg_agg, agg));
     SPH_TRY(up(c.cg_off, off));
     SPH_TRY(up(c.cg_rows, rows));
+    // pieces of the restriction: every aggregate in ceil(rows / kCoarsePiece)
+    // pieces of about equal length
+    std::vector<int> piece, pfirst(m + 1, 0);
+    for (int a = 0; a < m; ++a) {
+        const int len = off[a + 1] - off[a];
+        const int np = std::max(1, (len + kCoarsePiece - 1) / kCoarsePiece);
+        for (int k = 0; k < np; ++k) {
+            piece.push_back(a);
+            piece.push_back(off[a] + (int)((long long)len * k / np));
+            piece.push_back(off[a] + (int)((long long)len * (k + 1) / np));
+        }
+        pfirst[a + 1] = pfirst[a] + np;
+    }
+    c.cg_np = pfirst[m];
+    SPH_TRY(up(c.cg_piece, piece));
+    SPH_TRY(up(c.cg_pfirst, pfirst));
+    c.release(c.cg_part);
+    c.release(c.cg_cnt);
+    SPH_TRY(c.alloc(c.cg_part, (size_t)c.cg_np));
+    SPH_TRY(c.alloc(c.cg_cnt, (size_t)m));
+    SPH_CUDA_TRY(cudaMemsetAsync(c.cg_cnt, 0, sizeof(unsigned int) * (size_t)m, st));
     int *d_nm_idx = nullptr, *d_cnt_comp = nullptr, *d_piv = nullptr, *d_err = nullptr;
     SPH_TRY(up(d_nm_idx, nm_idx));
     SPH_TRY(up(d_cnt_comp, cnt_comp));

@@ -205,6 +205,11 @@ struct Ctx {
     double *cg_inv = nullptr;     // E^-1 while it is built (FP64 Gauss-Jordan)
     float *cg_invf = nullptr;     // E^-1, m x m, FP32 copy the solve reads
     double *cg_s = nullptr, *cg_y = nullptr;     // restricted residual, coarse correction
+    int cg_np = 0;                // pieces of the restriction (at most kCoarsePiece rows each)
+    int *cg_piece = nullptr;      // per piece: aggregate, first and end entry of cg_rows
+    int *cg_pfirst = nullptr;     // first piece of each aggregate (m + 1)
+    double *cg_part = nullptr;    // partial sum of each piece
+    unsigned int *cg_cnt = nullptr;   // pieces summed per aggregate (back to 0 after each restriction)
     // live operator timing (sph_profile)
     bool prof = false;
     cudaEvent_t *prof_ev = nullptr;   // 512 events, created on first use

@@ -244,6 +244,30 @@ template <class V, class C>
 __device__ __forceinline__ V coef_to(C a) { return (V)a; }
 template <>
 __device__ __forceinline__ float coef_to<float, __half>(__half a) { return __half2float(a); }
+// Gathers of the operand x_j with an L2 evict-last policy: the launch
+// streams its codes and coefficients once (loaded evict-first with __ldcs),
+// while x is gathered once per stored entry, so x should stay in L2 while
+// the stream passes through it
+__device__ __forceinline__ unsigned long long l2_keep_policy() {
+    unsigned long long pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+template <class V>
+__device__ __forceinline__ V ld_keep(const V *p, unsigned long long pol);
+template <>
+__device__ __forceinline__ float ld_keep<float>(const float *p, unsigned long long pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+template <>
+__device__ __forceinline__ double ld_keep<double>(const double *p, unsigned long long pol) {
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 struct List16 {
     const uint16_t *code;
     const int *row_cell, *cs;
@@ -257,7 +281,8 @@ struct List16 {
 template <bool L16, bool GUARD, class V, class C>
 __device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane, const C *__restrict__ coef,
                                           const uint16_t *__restrict__ code, const int *__restrict__ nbr,
-                                          const int *plane_start, const V *__restrict__ x, V xi, V &s) {
+                                          const int *plane_start, const V *__restrict__ x, V xi, V &s,
+                                          unsigned long long pol) {
     const long long e4 = sell4(sb, lane, k);
     C a[4];
     load_coef4<C>(coef + e4, a);
@@ -276,7 +301,7 @@ __device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane
     }
     V xj[4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) xj[t] = (!GUARD || k + t < cnt) ? x[j[t]] : xi;
+    for (int t = 0; t < 4; ++t) xj[t] = (!GUARD || k + t < cnt) ? ld_keep<V>(x + j[t], pol) : xi;
 #pragma unroll
     for (int t = 0; t < 4; ++t)   // difference form, entries in list order
         if (!GUARD || k + t < cnt) s += coef_to<V, C>(a[t]) * (xi - xj[t]);
@@ -334,9 +359,10 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
                 ps[128 * q] = __ldg(&l16.cs[plane_cell(rc, q - 2, l16.NI, l16.NINJ, l16.cs_max)]);
         }
         const int full = cnt & ~3;
+        const unsigned long long pol = l2_keep_policy();
         int k = 0;
-        for (; k < full; k += 4) quad_step<L16, false, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s);
-        if (k < cnt) quad_step<L16, true, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s);
+        for (; k < full; k += 4) quad_step<L16, false, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s, pol);
+        if (k < cnt) quad_step<L16, true, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s, pol);
         yi = rowscale ? s * (V)rowscale[i] : s;
         if (comp_id) {
             const int cc = comp_id[i];
@@ -978,10 +1004,11 @@ static std::vector<uintptr_t> krylov_graph_key(Ctx<Real> &c, float *const *ws, c
     for (int q = 0; q < 9; ++q) k.push_back((uintptr_t)ws[q]);
     const void *ptrs[] = {xlo, c.scal, c.red, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, c.diag,
                           c.comp_id, c.comp_inv, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.cg_off, c.cg_rows,
-                          c.cg_s, c.cg_y, c.cg_invf, c.cg_agg, c.nbr16, c.row_cell, c.cell_start};
+                          c.cg_s, c.cg_y, c.cg_invf, c.cg_agg, c.nbr16, c.row_cell, c.cell_start, c.cg_piece,
+                          c.cg_pfirst, c.cg_part, c.cg_cnt};
     for (const void *q : ptrs) k.push_back((uintptr_t)q);
     const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode, c.prof ? 1 : 0, c.list16 ? 1 : 0,
-                               c.num_cells};
+                               c.num_cells, c.cg_np};
     for (long long q : sizes) k.push_back((uintptr_t)q);
     return k;
 }
