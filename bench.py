@@ -551,6 +551,8 @@ def main():
                     help="two-level BiCGSTAB preconditioner: aggregate edge in NNPS cells (0: Jacobi; -B: "
                          "aggregates balanced by row count from blocks of B^3 cells; default 5 for the canyon, 9 "
                          "for the cube array)")
+    ap.add_argument("--coarse-max", type=int, default=0,
+                    help="balanced coarse space (--coarse < 0): most aggregates (0: 4096, at most 16384)")
     ap.add_argument("--coarse-mode", default="additive", choices=["additive", "multiplicative"],
                     help="two-level form: D^-1 r + Z E^-1 Z^T r, or the coarse correction of the residual the "
                          "Jacobi step leaves (one more operator application per preconditioner call)")
@@ -625,6 +627,7 @@ def main():
     p.ppe_coef_half = 1 if args.coef_half else 0
     p.ppe_refinement = {"reliable": 0, "restart-gmres": 1, "restart-bicgstab": 2, "restart-idrs": 3}[args.refinement]
     p.ppe_coarse_block = args.coarse
+    p.ppe_coarse_max = args.coarse_max
     p.ppe_coarse_mode = 1 if args.coarse_mode == "multiplicative" else 0
     if args.pair_h is None:
         args.pair_h = "avg" if args.apr else "ref"
@@ -725,13 +728,22 @@ def main():
     f0 = torch.cuda.Event(enable_timing=True)
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
-    for _ in range(ke):
+    seg = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(ke)]
+    for k in range(ke):
         sim.upload_state(host)
+        seg[k][0].record(stream)
         sim.step(1)
+        seg[k][1].record(stream)
         sim.download_into(host)
+        seg[k][2].record(stream)
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
+    # where the end-to-end time goes: upload (H2D + unpack), step, download (pack + D2H)
+    e2e_split = {"upload_ms": (f0.elapsed_time(seg[0][0])
+                               + sum(seg[k - 1][2].elapsed_time(seg[k][0]) for k in range(1, ke))) / ke,
+                 "step_ms": sum(seg[k][0].elapsed_time(seg[k][1]) for k in range(ke)) / ke,
+                 "download_ms": sum(seg[k][1].elapsed_time(seg[k][2]) for k in range(ke)) / ke}
     e2e, e2e_ms = replicas.throughput(n, ke, e2e_ms, device="cuda")
 
     # ---- other forms on the same deck, rank 0 only ----
@@ -867,11 +879,12 @@ def main():
                    "ppe_preconditioner": (f"jacobi + coarse aggregates of {args.coarse}^3 cells ({args.coarse_mode})"
                                           if args.coarse > 0 else
                                           f"jacobi + coarse aggregates balanced by row count, octree boxes from "
-                                          f"{-args.coarse}^3 cells, at most 4096 ({args.coarse_mode})"
+                                          f"{-args.coarse}^3 cells, at most {args.coarse_max or 4096} "
+                                          f"({args.coarse_mode})"
                                           if args.coarse < 0 else "jacobi"),
                    "l2": "inputs larger than L2 (particle state and neighbour lists exceed 126 MB)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": len(P) * layout.PART1.itemsize,
+        "e2e": {"value": e2e, "unit": METRIC, "split": e2e_split, "h2d_bytes_per_step": len(P) * layout.PART1.itemsize,
                 "d2h_bytes_per_step": len(P) * layout.PART1.itemsize, "steps": ke},
         "gpu_launches": int(launches),
         "ppe": {"iterations_mean": statistics.mean(s[0] for s in stats),

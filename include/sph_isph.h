@@ -247,6 +247,11 @@ typedef struct sph_params {
                                 applications (true residuals, the solution
                                 the tolerance is checked on) keep the FP32
                                 coefficients                                  */
+    int32_t ppe_coarse_max;  /* most aggregates of the balanced coarse space
+                                (ppe_coarse_block < 0): 0 means 4096; at most
+                                16384 (the dense coarse inverse holds m^2
+                                entries)                                      */
+    int32_t reserved0;       /* 0                                             */
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

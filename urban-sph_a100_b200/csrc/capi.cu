@@ -78,6 +78,9 @@ static int check_params(const sph_params &p) {
     if (p.n_profile < 2 || p.n_profile > SPH_MAX_PROFILE) { set_error("n_profile must be in [2, 32]"); return SPH_ERR_BAD_ARG; }
     if (!(p.vif[SPH_VIF_DT] > 0)) { set_error("dt must be positive"); return SPH_ERR_BAD_ARG; }
     if (p.outlet_bc < 0 || p.outlet_bc > 2) { set_error("outlet_bc must be 0, 1 or 2"); return SPH_ERR_BAD_ARG; }
+    if (p.ppe_coarse_max < 0 || p.ppe_coarse_max > 16384 || p.reserved0 != 0) {
+        set_error("ppe_coarse_max must be in [0, 16384] and reserved0 0"); return SPH_ERR_BAD_ARG;
+    }
     if (p.pressure_force_form < 0 || p.pressure_force_form > 1) {
         set_error("pressure_force_form must be 0 or 1"); return SPH_ERR_BAD_ARG;
     }
@@ -461,14 +464,24 @@ static int step_graph(Ctx<Real> &c, bool *ran) {
         c.stepgraph = sg;
     }
     const std::vector<unsigned long long> key = step_key(c);
+    static const bool trace = getenv("SPH_TRACE_STEP") != nullptr;
     if (!sg->exec || sg->key != key) {
-        if (sg->warm != key || sg->failed == key) return SPH_OK;
+        if (sg->warm != key || sg->failed == key) {
+            if (trace)
+                fprintf(stderr, "step %d: launch by launch (%s; mem_gen %llu param_gen %llu flags %llu)\n", c.count,
+                        sg->failed == key ? "capture failed in this state" : "state not yet steady", c.mem_gen,
+                        c.param_gen, key.back());
+            return SPH_OK;
+        }
         if (capture_step(c, sg) < 0) {
+            if (trace) fprintf(stderr, "step %d: capture failed: %s\n", c.count, sph_last_error());
             sg->failed = key;
             return SPH_OK;   // this state steps launch by launch
         }
+        if (trace) fprintf(stderr, "step %d: captured (%lld launches)\n", c.count, sg->launches);
         sg->key = key;
     }
+    if (trace) fprintf(stderr, "step %d: replay\n", c.count);
     SPH_CUDA_TRY(cudaGraphLaunch(sg->exec, c.stream));
     c.launches += sg->launches;
     ++c.graph_steps;
@@ -514,6 +527,8 @@ static int step_impl(Ctx<Real> &c, int nsteps, sph_ppe_stats *stats) {
             auto *sg = (StepGraph *)c.stepgraph;
             if (count0 >= 1 && c.mem_gen == gen0) sg->warm = step_key(c);
             else sg->warm.clear();
+            if (getenv("SPH_TRACE_STEP"))
+                fprintf(stderr, "step %d ran launch by launch: mem_gen %llu -> %llu\n", count0, gen0, c.mem_gen);
         }
         pending = c.ppe_pending;
         if (!pending) {

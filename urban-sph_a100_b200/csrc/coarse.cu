@@ -27,7 +27,8 @@
 
 namespace sph {
 
-constexpr int kCoarseMaxAgg = 4096;
+constexpr int kCoarseMaxAgg = 16384;      // the dense inverse holds m^2 entries
+constexpr int kCoarseDefaultAgg = 4096;   // balanced aggregates without ppe_coarse_max
 constexpr int kCoarsePiece = 1024;   // rows per block of the restriction
 
 // deterministic block sum (fixed shuffle pattern, warps summed in order)
@@ -285,7 +286,7 @@ void coarse_apply(Ctx<Real> &c, const V *r, V *z, const V *w) {
 // Balanced aggregates (ppe_coarse_block = -B): start from blocks of B^3
 // cells and split the block holding the most rows into its (up to eight)
 // non-empty octants, again and again, while the aggregate count stays within
-// kCoarseMaxAgg and the block is wider than one cell.  On an APR-refined deck
+// ppe_coarse_max (default 4096) and the block is wider than one cell.  On an APR-refined deck
 // a block of the refined zone holds eight times the rows of a block outside
 // it; splitting by row count gives every aggregate about the same number of
 // rows, i.e. aggregates about twice finer (in cells) where the particles are.
@@ -363,6 +364,7 @@ int coarse_build(Ctx<Real> &c) {
     const int B = c.prm.ppe_coarse_block;
     c.cg_valid = true;
     c.cg_block = B;
+    c.cg_max = c.prm.ppe_coarse_max;
     c.cg_m = 0;
     if (B == 0) return SPH_OK;
     const int n = c.n;
@@ -406,7 +408,8 @@ int coarse_build(Ctx<Real> &c) {
         for (int k = 0; k < nmem; ++k)
             box[k] = ((cell[3 * k + 2] / Bb) * NBy + cell[3 * k + 1] / Bb) * NBx + cell[3 * k] / Bb;
     } else {
-        box = octree_aggregates(cell, nmem, Bb, P.NI, P.NJ, P.NK, kCoarseMaxAgg);
+        const int cap = c.prm.ppe_coarse_max > 0 ? std::min(c.prm.ppe_coarse_max, kCoarseMaxAgg) : kCoarseDefaultAgg;
+        box = octree_aggregates(cell, nmem, Bb, P.NI, P.NJ, P.NK, cap);
     }
     // aggregates numbered in order of their first row (rows ascending)
     std::vector<int> agg(n, -1), size;

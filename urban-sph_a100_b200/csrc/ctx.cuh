@@ -200,6 +200,7 @@ struct Ctx {
     // two-level preconditioner (coarse.cu), rebuilt with the lists
     bool cg_valid = false;
     int cg_block = 0, cg_m = 0;   // aggregate edge in cells, aggregates in use
+    int cg_max = 0;               // ppe_coarse_max the coarse space was built with
     int *cg_agg = nullptr;        // aggregate of each row, -1 for identity / pinned rows
     int *cg_off = nullptr, *cg_rows = nullptr;   // rows of each aggregate, ascending
     double *cg_inv = nullptr;     // E^-1 while it is built (FP64 Gauss-Jordan)

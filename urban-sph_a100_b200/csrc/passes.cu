@@ -473,30 +473,51 @@ __global__ void k_most(DevParams P, SoA<Real> s, const int *rows, const int *off
 // the Shepard weights; rows without fluid in range get p = 0.
 // ---------------------------------------------------------------------------
 template <class Real>
-__global__ void k_neumann_gather(const int *rows, const int *off, const int *nb, const int *mirror,
-                                 const double *w, const double *gw, int nrows, const Real *p,
-                                 const typename V4<Real>::type *u, const int4 *ty, Real *out_p,
-                                 typename V4<Real>::type *out_u) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nrows) return;
+__global__ void __launch_bounds__(128) k_neumann_gather(const int *rows, const int *off, const int *nb, const int *mirror,
+                                                        const double *w, const double *gw, int nrows, const Real *p,
+                                                        const typename V4<Real>::type *u, const int4 *ty, Real *out_p,
+                                                        typename V4<Real>::type *out_u) {
+    // one warp per row: the lanes load 32 consecutive entries at a time
+    // (coalesced) and form their terms, and every lane adds the terms in
+    // entry order from the shuffles, so the sums are those of a sequential
+    // loop over the row
+    const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= nrows) return;   // uniform over the warp
     const int i = rows[k];
     const int s = off[k], e = off[k + 1];
     auto ui = u[i];
     Real pv = 0;
     if (e > s && !(mirror[k] & 2)) {
         const bool mir = (mirror[k] & 1) != 0;
+        const bool vel = ty[i].w == -1;
         Real sp = 0, sx = 0, sy = 0, sz = 0;
-        for (int q = s; q < e; ++q) {
-            const int j = nb[q];
-            const Real wj = (Real)w[q];
-            sp += (mir ? (Real)gw[q] : wj) * p[j];
-            if (ty[i].w == -1) { const auto uj = u[j]; sx += wj * uj.x; sy += wj * uj.y; sz += wj * uj.z; }
+        for (int q0 = s; q0 < e; q0 += 32) {
+            const int q = q0 + lane;
+            Real tp = 0, tx = 0, ty_ = 0, tz = 0;
+            if (q < e) {
+                const int j = nb[q];
+                const Real wj = (Real)w[q];
+                tp = (mir ? (Real)gw[q] : wj) * p[j];
+                if (vel) { const auto uj = u[j]; tx = wj * uj.x; ty_ = wj * uj.y; tz = wj * uj.z; }
+            }
+            const int cnt = min(32, e - q0);
+            for (int l = 0; l < cnt; ++l) {
+                sp += __shfl_sync(0xffffffffu, tp, l);
+                if (vel) {
+                    sx += __shfl_sync(0xffffffffu, tx, l);
+                    sy += __shfl_sync(0xffffffffu, ty_, l);
+                    sz += __shfl_sync(0xffffffffu, tz, l);
+                }
+            }
         }
         pv = sp;
-        if (ty[i].w == -1) { ui.x = sx; ui.y = sy; ui.z = sz; }
+        if (vel) { ui.x = sx; ui.y = sy; ui.z = sz; }
     }
-    out_p[k] = pv;
-    out_u[k] = ui;
+    if (lane == 0) {
+        out_p[k] = pv;
+        out_u[k] = ui;
+    }
 }
 
 template <class Real>
@@ -1209,7 +1230,7 @@ int neumann_pass(Ctx<Real> &c, VarSet<Real> &V) {
     if (L.n_nm == 0) return SPH_OK;
     typename V4<Real>::type *ou; Real *op, *ot;
     SPH_TRY(scratch_rows(c, ou, op, ot));
-    k_neumann_gather<Real><<<grid_for(L.n_nm, 128), 128, 0, c.stream>>>(L.nm_rows, L.nm_off, L.nm_nbr, L.nm_ghost,
+    k_neumann_gather<Real><<<grid_for(32LL * L.n_nm, 128), 128, 0, c.stream>>>(L.nm_rows, L.nm_off, L.nm_nbr, L.nm_ghost,
                                                                         c.nm_w, c.nm_gw, L.n_nm, V.p, V.u, c.ty, op, ou);
     k_neumann_scatter<Real><<<grid_for(L.n_nm, 128), 128, 0, c.stream>>>(L.nm_rows, L.n_nm, op, ou, V.p, V.u);
     c.launches += 2;

@@ -2189,7 +2189,8 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         SPH_CUDA_TRY(cudaGetLastError());
         c.coef_h_valid = true;
     }
-    if (mode != SPH_PPE_REF_SWEEP && (!c.cg_valid || c.cg_block != c.prm.ppe_coarse_block))
+    if (mode != SPH_PPE_REF_SWEEP &&
+        (!c.cg_valid || c.cg_block != c.prm.ppe_coarse_block || c.cg_max != c.prm.ppe_coarse_max))
         SPH_TRY(coarse_build(c));
 
     if (mode == SPH_PPE_REF_SWEEP) {

@@ -125,6 +125,8 @@ class SphParams(ctypes.Structure):
         ("recompute_pairs", ctypes.c_int32),
         ("pressure_force_form", ctypes.c_int32),
         ("ppe_coef_half", ctypes.c_int32),
+        ("ppe_coarse_max", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
         ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
@@ -159,7 +161,7 @@ class PpeStats(ctypes.Structure):
     ]
 
 
-assert ctypes.sizeof(SphParams) == 1336, ctypes.sizeof(SphParams)
+assert ctypes.sizeof(SphParams) == 1344, ctypes.sizeof(SphParams)
 
 BUFFER_PERIODIC_GHOST = 7   # buffer_type of a periodic ghost (sph_params.periodic_box)
 
