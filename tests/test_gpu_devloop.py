@@ -91,8 +91,9 @@ def test_whole_step_graph_follows_the_step_counter():
     p.seti("freq_filt", 2)
     dt = p.getf("dt")
     p.t_ini, p.t_con, p.t_start, p.t_con_t = 300.0, 304.0, dt, 6.0 * dt
-    A, sa, _ = _run(P, p, 0, 7, per_call=1, coarse=0)
-    B, sb, _ = _run(P, p, 4, 7, coarse=0, calls=[5, 2])
+    A, sa, ra = _run(P, p, 0, 7, per_call=1)
+    B, sb, rb = _run(P, p, 4, 7, calls=[5, 2])
+    assert ra == [0] * 7 and rb == [0, 0]   # every solve converged
     assert _run.graph_steps == 5       # steps 2-6
     for f in ("pres", "ux", "uy", "uz", "temp", "concn"):
         assert np.array_equal(A[f], B[f]), f

@@ -162,8 +162,8 @@ def test_fp16_coefficients_reach_tolerance_and_match_fp64(deck, coarse):
 
 def test_coarse_block_too_small_is_rejected(deck):
     # one aggregate per cell exceeds the aggregate limit on a deck with more
-    # than 4096 occupied cells: the solve reports SPH_ERR_UNSUPPORTED
-    P, p = decks.canyon(scale=0.3)
+    # than 16384 occupied cells: the solve reports SPH_ERR_UNSUPPORTED
+    P, p = decks.canyon(scale=1.0)
     q = p.copy()
     q.ppe_mode = layout.PPE_BICGSTAB
     q.ppe_coarse_block = 1
@@ -173,6 +173,28 @@ def test_coarse_block_too_small_is_rejected(deck):
         sim.step(1)
     assert e.value.status == -7
     sim.close()
+
+
+def test_balanced_coarse_space_converges_in_fewer_iterations():
+    # aggregates balanced by row count (ppe_coarse_block = -B) up to
+    # ppe_coarse_max: with the blocked Gauss-Jordan inverse (checked on four
+    # of its columns inside the build) the FP64 solve reaches the pressure of
+    # the Jacobi-only solve (both to 1e-8) in fewer iterations, and more
+    # aggregates need fewer iterations
+    P, p = decks.canyon(scale=0.3)
+    A0, s0 = _gpu_step(P, p, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8)
+    assert s0[-1].status == 0
+    iters = {}
+    for cmax in (4096, 12000):
+        q = p.copy()
+        q.ppe_coarse_max = cmax
+        A1, s1 = _gpu_step(P, q, layout.PREC_FP64, layout.PPE_BICGSTAB, 1e-8, coarse=-4)
+        assert s1[-1].status == 0 and s1[-1].rel_residual <= 1e-8
+        assert rel_err(A1["pres"], A0["pres"]) <= PRES_TOL_FP64
+        for f in ("ux", "uy", "uz"):
+            assert rel_err(A1[f], A0[f]) <= PRES_TOL_FP64, f
+        iters[cmax] = s1[-1].iterations
+    assert iters[12000] < iters[4096] < s0[-1].iterations, (iters, s0[-1].iterations)
 
 
 def _two_level_deck():

@@ -15,7 +15,9 @@
 //
 // Determinism: E is accumulated in 64-bit fixed point (integer atomics are
 // order-independent), every reduction has a fixed order, and the inverse is
-// Gauss-Jordan with partial pivoting in a fixed sequence of launches.
+// a blocked Gauss-Jordan with partial pivoting in a fixed sequence of
+// launches (panel sweeps, then FP64 rank-64 updates with a fixed summation
+// order), checked on four of its columns.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -162,48 +164,156 @@ __global__ void k_gj_pivot(const double *W, int m, int k, int *piv, double *pval
     }
 }
 
-// swap rows k and piv, scale row k by 1/pivot (one thread per column of [W | Inv])
-__global__ void k_gj_swap_scale(double *W, double *Inv, int m, int k, const int *piv, const double *pval,
-                                const int *err) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= 2 * m || *err) return;
-    const int p = *piv;
+// ---- blocked in-place Gauss-Jordan inverse ------------------------------------
+// W (m x m, row-major, FP64) is inverted in place with partial pivoting, in
+// panels of kGjPanel columns.  Within a panel each pivot column k is swept as
+// the classical in-place Gauss-Jordan step restricted to the panel's columns
+// (rows swapped and the pivot row scaled in the panel, every other row
+// eliminated in the panel).  After the panel, with K its pivot rows, R the
+// other rows and J the columns outside it, the block sweep
+//     A_KJ <- A_KK^-1 A_KJ,   A_RJ <- A_RJ - A_RK A_KK^-1 A_KJ
+// is W[:, J] <- (rows K zeroed) W[:, J] + N Bk, with N the panel's swept
+// columns (A_KK^-1 in rows K, -A_RK A_KK^-1 in rows R) and Bk the pivot
+// rows of the other columns before the sweep: one rank-kGjPanel update in
+// FP64 (tiled, fixed summation order), after the panel's row swaps have
+// been applied to the other columns.  The row interchanges leave the
+// inverse's columns permuted; the FP32 copy gathers them back.
+constexpr int kGjPanel = 64;
+
+// panel step k: row k takes the pivot row's panel values (the pivot row
+// takes row k's), scaled by 1 / pivot, with 1 / pivot in column k
+__global__ void k_gj_pivot_row(double *W, int m, int k, int k0, int kb, const int *piv, const double *pval,
+                               const int *err) {
+    const int t = threadIdx.x;
+    if (t >= kb || *err) return;
+    const int p = *piv, c = k0 + t;
+    const double a = W[(size_t)k * m + c], b = W[(size_t)p * m + c];
+    if (p != k) W[(size_t)p * m + c] = a;
     const double inv = 1.0 / *pval;
-    double *A = col < m ? W : Inv;
-    const int cc = col < m ? col : col - m;
-    const double b = A[(size_t)p * m + cc];
-    if (p != k) A[(size_t)p * m + cc] = A[(size_t)k * m + cc];
-    A[(size_t)k * m + cc] = b * inv;
+    W[(size_t)k * m + c] = (c == k) ? inv : b * inv;
 }
 
-__global__ void k_gj_col(const double *W, double *colk, int m, int k) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < m) colk[r] = W[(size_t)r * m + k];
-}
-
-// eliminate column k from every row r != k (columns of W left of k are done)
-__global__ void k_gj_elim(double *W, double *Inv, const double *colk, int m, int k, const int *err) {
-    const int r = blockIdx.y;
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r == k || *err) return;
-    const double f = colk[r];
+// panel step k, every row i != k (one warp per row): f = W[i,k];
+// W[i,c] -= f W[k,c] in the panel, W[i,k] = -f / pivot
+__global__ void k_gj_panel_elim(double *W, int m, int k, int k0, int kb, const int *err) {
+    const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= m || i == k || *err) return;   // uniform over the warp
+    double *row = W + (size_t)i * m + k0;
+    const double *rk = W + (size_t)k * m + k0;
+    const double f = row[k - k0];
+    __syncwarp();
     if (f == 0.0) return;
-    if (col < m) {
-        if (col >= k) W[(size_t)r * m + col] -= f * W[(size_t)k * m + col];
-    } else if (col < 2 * m) {
-        const int cc = col - m;
-        Inv[(size_t)r * m + cc] -= f * Inv[(size_t)k * m + cc];
+    for (int c = lane; c < kb; c += 32) {
+        if (k0 + c == k) row[c] = -f * rk[c];
+        else row[c] -= f * rk[c];
     }
 }
 
-__global__ void k_to_float(const double *a, float *b, long long n) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) b[t] = (float)a[t];
+// the panel's row interchanges, in order, in every column outside it
+__global__ void k_gj_swap_rows(double *W, int m, int k0, int kb, const int *piv, const int *err) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m || (j >= k0 && j < k0 + kb) || *err) return;
+    for (int t = 0; t < kb; ++t) {
+        const int k = k0 + t, p = piv[k];
+        if (p == k) continue;
+        const double a = W[(size_t)k * m + j];
+        W[(size_t)k * m + j] = W[(size_t)p * m + j];
+        W[(size_t)p * m + j] = a;
+    }
 }
 
-__global__ void k_eye(double *A, int m) {
+// Bk = the panel's pivot rows (kb x m)
+__global__ void k_gj_copy_rows(const double *W, double *Bk, int m, int k0, int kb) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < (long long)m * m) A[t] = (t / m == t % m) ? 1.0 : 0.0;
+    if (t >= (long long)kb * m) return;
+    const int r = (int)(t / m), j = (int)(t % m);
+    Bk[t] = W[(size_t)(k0 + r) * m + j];
+}
+
+// W[i,j] = (i a pivot row of the panel ? 0 : W[i,j]) + sum_t W[i,k0+t] Bk[t,j]
+// for every column j outside the panel: 64 x 64 tiles, 4 x 4 per thread,
+// t ascending in chunks of 32
+__global__ void __launch_bounds__(256) k_gj_update(double *W, const double *__restrict__ Bk, int m, int k0, int kb,
+                                                   const int *err) {
+    __shared__ double Ns[64][33];
+    __shared__ double Bs[32][64];
+    const int j0 = blockIdx.x * 64, i0 = blockIdx.y * 64;
+    if (j0 == k0 || *err) return;   // panels start at multiples of 64: this tile is the panel
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+    for (int t0 = 0; t0 < kb; t0 += 32) {
+        for (int e = threadIdx.x; e < 64 * 32; e += 256) {
+            const int r = e >> 5, t = e & 31;
+            const int i = i0 + r;
+            Ns[r][t] = (i < m && t0 + t < kb) ? W[(size_t)i * m + k0 + t0 + t] : 0.0;
+        }
+        for (int e = threadIdx.x; e < 32 * 64; e += 256) {
+            const int t = e >> 6, q = e & 63;
+            const int j = j0 + q;
+            Bs[t][q] = (j < m && t0 + t < kb) ? Bk[(size_t)(t0 + t) * m + j] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int t = 0; t < 32; ++t) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = Ns[ty * 4 + r][t];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = Bs[t][tx + 16 * q];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int i = i0 + ty * 4 + r;
+        if (i >= m) continue;
+        const bool pivot_row = i >= k0 && i < k0 + kb;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int j = j0 + tx + 16 * q;
+            if (j >= m) continue;
+            double *w = W + (size_t)i * m + j;
+            *w = (pivot_row ? 0.0 : *w) + acc[r][q];
+        }
+    }
+}
+
+// FP32 copy of the inverse with its columns put back: column c of the
+// inverse is column col[c] of W
+__global__ void k_gj_to_float(const double *W, const int *col, float *out, int m) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)m * m) return;
+    const int i = (int)(t / m), c = (int)(t % m);
+    out[t] = (float)W[(size_t)i * m + col[c]];
+}
+
+// check of the inverse on a few of its columns: dev[q] = max_i |(E X)_ic - delta_ic|
+// for c = cols[q] (one warp per row i, X[:, c] = W[:, col[c]])
+__global__ void k_gj_check(const double *E, const double *W, const int *col, const int *cols, int ncheck, int m,
+                           unsigned long long *dev) {
+    const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= m) return;
+    for (int q = 0; q < ncheck; ++q) {
+        const int c = cols[q], wc = col[c];
+        double v = 0;
+        for (int j = lane; j < m; j += 32) v += E[(size_t)i * m + j] * W[(size_t)j * m + wc];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) {
+            const double d = fabs(v - (i == c ? 1.0 : 0.0));
+            atomicMax(dev, (unsigned long long)__double_as_longlong(d == d ? d : 1e300));
+        }
+    }
 }
 
 // ---- application ----------------------------------------------------------
@@ -479,18 +589,22 @@ int coarse_build(Ctx<Real> &c) {
     int *d_nm_idx = nullptr, *d_cnt_comp = nullptr, *d_piv = nullptr, *d_err = nullptr;
     SPH_TRY(up(d_nm_idx, nm_idx));
     SPH_TRY(up(d_cnt_comp, cnt_comp));
-    double *E = nullptr, *a_comp = nullptr, *colk = nullptr, *pval = nullptr;
-    unsigned long long *amax = nullptr;
-    c.release(c.cg_inv); c.release(c.cg_s); c.release(c.cg_y);
-    SPH_TRY(c.alloc(c.cg_inv, (size_t)m * m));
+    double *E = nullptr, *E0 = nullptr, *Bk = nullptr, *a_comp = nullptr, *pval = nullptr;
+    unsigned long long *amax = nullptr, *d_dev = nullptr;
+    int *d_col = nullptr, *d_cols = nullptr;
+    c.release(c.cg_s); c.release(c.cg_y);
     SPH_TRY(c.alloc(c.cg_s, m));
     SPH_TRY(c.alloc(c.cg_y, m));
     SPH_TRY(c.alloc(E, (size_t)m * m));
+    SPH_TRY(c.alloc(E0, (size_t)m * m));
+    SPH_TRY(c.alloc(Bk, (size_t)kGjPanel * m));
     SPH_TRY(c.alloc(a_comp, (size_t)m * std::max(ncomp, 1)));
-    SPH_TRY(c.alloc(colk, m));
     SPH_TRY(c.alloc(pval, 1));
     SPH_TRY(c.alloc(amax, 1));
-    SPH_TRY(c.alloc(d_piv, 1));
+    SPH_TRY(c.alloc(d_dev, 1));
+    SPH_TRY(c.alloc(d_piv, m));
+    SPH_TRY(c.alloc(d_col, m));
+    SPH_TRY(c.alloc(d_cols, 4));
     SPH_TRY(c.alloc(d_err, 1));
 
     // fixed-point scale: every term below 2^61 / (terms per entry)
@@ -528,30 +642,67 @@ int coarse_build(Ctx<Real> &c) {
         k_coarse_rank_one<<<div_up(mm, 256), 256, 0, st>>>(E, a_comp, d_cnt_comp, c.comp_inv, m, ncomp);
         SPH_CUDA_TRY(cudaGetLastError());
     }
-    // E^-1
-    k_eye<<<div_up(mm, 256), 256, 0, st>>>(c.cg_inv, m);
+    // E^-1: blocked in-place Gauss-Jordan on E, E0 keeping E for the check
+    SPH_CUDA_TRY(cudaMemcpyAsync(E0, E, sizeof(double) * (size_t)mm, cudaMemcpyDeviceToDevice, st));
     SPH_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-    for (int k = 0; k < m; ++k) {
-        k_gj_pivot<<<1, 1024, 0, st>>>(E, m, k, d_piv, pval, d_err);
-        k_gj_swap_scale<<<div_up(2LL * m, 256), 256, 0, st>>>(E, c.cg_inv, m, k, d_piv, pval, d_err);
-        k_gj_col<<<div_up(m, 256), 256, 0, st>>>(E, colk, m, k);
-        k_gj_elim<<<dim3(div_up(2LL * m, 256), m), 256, 0, st>>>(E, c.cg_inv, colk, m, k, d_err);
+    const dim3 tiles((unsigned)div_up(m, 64), (unsigned)div_up(m, 64));
+    for (int k0 = 0; k0 < m; k0 += kGjPanel) {
+        const int kb = std::min(kGjPanel, m - k0);
+        for (int k = k0; k < k0 + kb; ++k) {
+            k_gj_pivot<<<1, 1024, 0, st>>>(E, m, k, d_piv + k, pval, d_err);
+            k_gj_pivot_row<<<1, kGjPanel, 0, st>>>(E, m, k, k0, kb, d_piv + k, pval, d_err);
+            k_gj_panel_elim<<<div_up(32LL * m, 256), 256, 0, st>>>(E, m, k, k0, kb, d_err);
+        }
+        c.launches += 3LL * kb;
+        if (kb < m) {
+            k_gj_swap_rows<<<div_up(m, 256), 256, 0, st>>>(E, m, k0, kb, d_piv, d_err);
+            k_gj_copy_rows<<<div_up((long long)kb * m, 256), 256, 0, st>>>(E, Bk, m, k0, kb);
+            k_gj_update<<<tiles, 256, 0, st>>>(E, Bk, m, k0, kb, d_err);
+            c.launches += 3;
+        }
     }
-    c.launches += 4LL * m + 6;
     SPH_CUDA_TRY(cudaGetLastError());
     int herr = 0;
+    std::vector<int> piv(m), col(m);
     SPH_CUDA_TRY(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SPH_CUDA_TRY(cudaMemcpyAsync(piv.data(), d_piv, sizeof(int) * m, cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
+    // the row interchanges permuted the inverse's columns: undo them in
+    // reverse order (column c of the inverse is column col[c] of E)
+    for (int k = 0; k < m; ++k) col[k] = k;
+    for (int k = m - 1; k >= 0; --k) {
+        const int p = (piv[k] >= 0 && piv[k] < m) ? piv[k] : k;
+        std::swap(col[k], col[p]);
+    }
+    const int cols[4] = {0, m / 3, (2 * m) / 3, m - 1};
+    SPH_CUDA_TRY(cudaMemcpyAsync(d_col, col.data(), sizeof(int) * m, cudaMemcpyHostToDevice, st));
+    SPH_CUDA_TRY(cudaMemcpyAsync(d_cols, cols, sizeof cols, cudaMemcpyHostToDevice, st));
+    SPH_CUDA_TRY(cudaMemsetAsync(d_dev, 0, sizeof(unsigned long long), st));
+    if (!herr) {
+        k_gj_check<<<div_up(32LL * m, 256), 256, 0, st>>>(E0, E, d_col, d_cols, 4, m, d_dev);
+        ++c.launches;
+    }
     c.release(c.cg_invf);
     SPH_TRY(c.alloc(c.cg_invf, (size_t)m * m));
-    k_to_float<<<div_up(mm, 256), 256, 0, st>>>(c.cg_inv, c.cg_invf, mm);
+    k_gj_to_float<<<div_up(mm, 256), 256, 0, st>>>(E, d_col, c.cg_invf, m);
+    ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
+    unsigned long long dbits = 0;
+    SPH_CUDA_TRY(cudaMemcpyAsync(&dbits, d_dev, sizeof dbits, cudaMemcpyDeviceToHost, st));
     SPH_CUDA_TRY(cudaStreamSynchronize(st));
-    c.release(c.cg_inv);
-    c.release(E); c.release(a_comp); c.release(colk); c.release(pval); c.release(amax);
-    c.release(d_piv); c.release(d_err); c.release(d_nm_idx); c.release(d_cnt_comp);
+    double dev = 0;
+    memcpy(&dev, &dbits, sizeof dev);
+    c.release(E); c.release(E0); c.release(Bk); c.release(a_comp); c.release(pval); c.release(amax);
+    c.release(d_dev); c.release(d_piv); c.release(d_col); c.release(d_cols); c.release(d_err);
+    c.release(d_nm_idx); c.release(d_cnt_comp);
     if (herr) {
         set_error("coarse operator is singular");
+        return SPH_ERR_BREAKDOWN;
+    }
+    if (!(dev <= 1e-6)) {   // E X - I on four columns of the inverse
+        static thread_local char msg[128];
+        snprintf(msg, sizeof msg, "coarse inverse check failed: max |E X - I| = %.3e on sampled columns", dev);
+        set_error(msg);
         return SPH_ERR_BREAKDOWN;
     }
     c.cg_m = m;

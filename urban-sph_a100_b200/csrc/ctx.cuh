@@ -203,7 +203,6 @@ struct Ctx {
     int cg_max = 0;               // ppe_coarse_max the coarse space was built with
     int *cg_agg = nullptr;        // aggregate of each row, -1 for identity / pinned rows
     int *cg_off = nullptr, *cg_rows = nullptr;   // rows of each aggregate, ascending
-    double *cg_inv = nullptr;     // E^-1 while it is built (FP64 Gauss-Jordan)
     float *cg_invf = nullptr;     // E^-1, m x m, FP32 copy the solve reads
     double *cg_s = nullptr, *cg_y = nullptr;     // restricted residual, coarse correction
     int cg_np = 0;                // pieces of the restriction (at most kCoarsePiece rows each)
