@@ -552,7 +552,7 @@ def main():
                          "aggregates balanced by row count from blocks of B^3 cells; default 5 for the canyon, -16 "
                          "for the cube array)")
     ap.add_argument("--coarse-max", type=int, default=None,
-                    help="balanced coarse space (--coarse < 0): most aggregates (0: 4096, at most 16384; default "
+                    help="balanced coarse space (--coarse < 0): most aggregates (0: 4096, at most 32768; default "
                          "16384)")
     ap.add_argument("--coarse-mode", default="additive", choices=["additive", "multiplicative"],
                     help="two-level form: D^-1 r + Z E^-1 Z^T r, or the coarse correction of the residual the "

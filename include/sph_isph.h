@@ -185,7 +185,7 @@ typedef struct sph_params {
                                 aggregates balanced by row count: blocks of
                                 B x B x B cells, the block with the most rows
                                 split into octants again and again while at
-                                most 4096 aggregates result                   */
+                                most ppe_coarse_max aggregates result         */
     int32_t ppe_warm_start;  /* start vector of the converged solves: 0 previous
                                 pressure; 1 linear extrapolation in time,
                                 2 p_n - p_(n-1), once two solutions exist;
@@ -249,8 +249,8 @@ typedef struct sph_params {
                                 coefficients                                  */
     int32_t ppe_coarse_max;  /* most aggregates of the balanced coarse space
                                 (ppe_coarse_block < 0): 0 means 4096; at most
-                                16384 (the dense coarse inverse holds m^2
-                                entries)                                      */
+                                32768 (the dense coarse inverse holds m^2
+                                entries: 4.3 GB in FP32 at 32768)             */
     int32_t reserved0;       /* 0                                             */
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */

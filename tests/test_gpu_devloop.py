@@ -83,11 +83,12 @@ def test_device_controlled_budget_reports_not_converged():
 
 
 def test_whole_step_graph_follows_the_step_counter():
-    # a filter period of 2 and a wall-temperature ramp over the first steps:
-    # the replayed graph reads the step counter and time from the device, so
-    # it must give the launch-by-launch results at every step, also across
+    # a filter period of 2 and a wall-temperature ramp over the first steps
+    # (the time update sets the walls' temperature from the step's time): the
+    # replayed graph reads the step counter and time from the device, so it
+    # must give the launch-by-launch results at every step, also across
     # sph_step calls
-    P, p = decks.thermal_mini(nx=16, ny=8, nz=6)
+    P, p = decks.canyon(scale=0.12)
     p.seti("freq_filt", 2)
     dt = p.getf("dt")
     p.t_ini, p.t_con, p.t_start, p.t_con_t = 300.0, 304.0, dt, 6.0 * dt
@@ -95,6 +96,6 @@ def test_whole_step_graph_follows_the_step_counter():
     B, sb, rb = _run(P, p, 4, 7, calls=[5, 2])
     assert ra == [0] * 7 and rb == [0, 0]   # every solve converged
     assert _run.graph_steps == 5       # steps 2-6
-    for f in ("pres", "ux", "uy", "uz", "temp", "concn"):
+    for f in ("pres", "ux", "uy", "uz", "temp"):
         assert np.array_equal(A[f], B[f]), f
     assert (sa[-1].iterations, sa[-1].refinements) == (sb[-1].iterations, sb[-1].refinements)

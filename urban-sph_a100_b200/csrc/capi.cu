@@ -78,8 +78,8 @@ static int check_params(const sph_params &p) {
     if (p.n_profile < 2 || p.n_profile > SPH_MAX_PROFILE) { set_error("n_profile must be in [2, 32]"); return SPH_ERR_BAD_ARG; }
     if (!(p.vif[SPH_VIF_DT] > 0)) { set_error("dt must be positive"); return SPH_ERR_BAD_ARG; }
     if (p.outlet_bc < 0 || p.outlet_bc > 2) { set_error("outlet_bc must be 0, 1 or 2"); return SPH_ERR_BAD_ARG; }
-    if (p.ppe_coarse_max < 0 || p.ppe_coarse_max > 16384 || p.reserved0 != 0) {
-        set_error("ppe_coarse_max must be in [0, 16384] and reserved0 0"); return SPH_ERR_BAD_ARG;
+    if (p.ppe_coarse_max < 0 || p.ppe_coarse_max > 32768 || p.reserved0 != 0) {
+        set_error("ppe_coarse_max must be in [0, 32768] and reserved0 0"); return SPH_ERR_BAD_ARG;
     }
     if (p.pressure_force_form < 0 || p.pressure_force_form > 1) {
         set_error("pressure_force_form must be 0 or 1"); return SPH_ERR_BAD_ARG;

@@ -29,7 +29,7 @@
 
 namespace sph {
 
-constexpr int kCoarseMaxAgg = 16384;      // the dense inverse holds m^2 entries
+constexpr int kCoarseMaxAgg = 32768;      // the dense inverse holds m^2 entries
 constexpr int kCoarseDefaultAgg = 4096;   // balanced aggregates without ppe_coarse_max
 constexpr int kCoarsePiece = 1024;   // rows per block of the restriction
 
@@ -71,10 +71,13 @@ __global__ void __launch_bounds__(256) k_coarse_assemble(
     int m, const int *agg, const int *off, const int *rows, const int *kind, const int *aux,
     const long long *slice_off, const int *ncnt, const int *nbr, const C *coef, const int *nm_idx, const int *nm_off,
     const int *nm_nbr, const double *nm_ow, const int *comp_id, const Real *diag, int ncomp, double scale, double *E,
-    double *a_comp) {
-    extern __shared__ unsigned long long acc[];
+    double *a_comp, bool in_smem) {
+    // row I of E accumulates in shared memory, or (m too large for it) in
+    // its own row of E, read as 64-bit integers; only block I touches row I
+    extern __shared__ unsigned long long acc_sh[];
     __shared__ double sh[8];
     const int I = blockIdx.x;
+    unsigned long long *acc = in_smem ? acc_sh : reinterpret_cast<unsigned long long *>(E + (size_t)I * m);
     for (int J = threadIdx.x; J < m; J += blockDim.x) acc[J] = 0ull;
     __syncthreads();
     double asum[SPH_MAX_COMP];
@@ -116,7 +119,10 @@ __global__ void __launch_bounds__(256) k_coarse_assemble(
         }
     }
     __syncthreads();
-    for (int J = threadIdx.x; J < m; J += blockDim.x) E[(size_t)I * m + J] = (double)(long long)acc[J] / scale;
+    for (int J = threadIdx.x; J < m; J += blockDim.x) {
+        const unsigned long long a = in_smem ? acc[J] : __ldcg(acc + J);
+        E[(size_t)I * m + J] = (double)(long long)a / scale;
+    }
     for (int t = 0; t < ncomp; ++t) {
         const double s = block_sum<256>(asum[t], sh);
         if (threadIdx.x == 0) a_comp[(size_t)I * ncomp + t] = s;
@@ -134,7 +140,8 @@ __global__ void k_coarse_rank_one(double *E, const double *a_comp, const int *cn
     E[t] += v;
 }
 
-// Gauss-Jordan with partial pivoting on W (m x m), Inv starts as identity
+// pivot of column k: the row r >= k of largest |W[r,k]| (ties: the lowest
+// row), its value, and the error flag when the column is zero from row k down
 __global__ void k_gj_pivot(const double *W, int m, int k, int *piv, double *pval, int *err) {
     __shared__ double bv[32];
     __shared__ int bi[32];
@@ -622,19 +629,22 @@ int coarse_build(Ctx<Real> &c) {
     const double terms = (double)max_rows * (double)std::max(max_cnt, 64) + 1.0;
     const double scale = std::ldexp(1.0, (int)std::floor(61.0 - std::log2(cmax) - std::log2(terms)));
 
-    const size_t shmem = sizeof(unsigned long long) * (size_t)m;
+    const bool in_smem = m <= 24576;   // 192 KB of the 227 KB a block may use
+    const size_t shmem = in_smem ? sizeof(unsigned long long) * (size_t)m : 0;
     if (sizeof(Real) == 4) {
         SPH_CUDA_TRY(cudaFuncSetAttribute(k_coarse_assemble<float, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)shmem));
         k_coarse_assemble<float, Real><<<m, 256, shmem, st>>>(
             m, c.cg_agg, c.cg_off, c.cg_rows, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, d_nm_idx,
-            c.L.nm_off, c.L.nm_nbr, c.nm_ow, ncomp > 0 ? c.comp_id : nullptr, c.diag, ncomp, scale, E, a_comp);
+            c.L.nm_off, c.L.nm_nbr, c.nm_ow, ncomp > 0 ? c.comp_id : nullptr, c.diag, ncomp, scale, E, a_comp,
+            in_smem);
     } else {
         SPH_CUDA_TRY(cudaFuncSetAttribute(k_coarse_assemble<double, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)shmem));
         k_coarse_assemble<double, Real><<<m, 256, shmem, st>>>(
             m, c.cg_agg, c.cg_off, c.cg_rows, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef_d, d_nm_idx,
-            c.L.nm_off, c.L.nm_nbr, c.nm_ow, ncomp > 0 ? c.comp_id : nullptr, c.diag, ncomp, scale, E, a_comp);
+            c.L.nm_off, c.L.nm_nbr, c.nm_ow, ncomp > 0 ? c.comp_id : nullptr, c.diag, ncomp, scale, E, a_comp,
+            in_smem);
     }
     SPH_CUDA_TRY(cudaGetLastError());
     const long long mm = (long long)m * m;
