@@ -138,6 +138,7 @@ struct Ctx {
     // its own and every offset fits in 13 bits
     uint16_t *nbr16 = nullptr;
     int *row_cell = nullptr;      // cell index of the row's first x-run cell (dy = dz = 0)
+    int *op_blk = nullptr;        // order of the pressure operator's row blocks (ppe.cu), rebuilt with the lists
     int row_cell_cap = 0;
     bool list16 = false;
     SideLists L;
