@@ -725,6 +725,7 @@ def main():
     ms = e0.elapsed_time(e1)
     launches = sim.launches() - l0
     op_n, op_ms, op_bytes = sim.operator_stats(reset=True)
+    op_counts = sim.operator_counts()
     _, op_index_bytes = sim.operator_bytes()
     sim.profile(False)
     value, ms = replicas.throughput(n, args.steps, ms, device="cuda")
@@ -915,7 +916,7 @@ def main():
                                        "frac": achieved_stored / hbm,
                                        "rule": "what the launch streams: 16-bit codes or 32-bit indices plus the "
                                                "cached coefficient per entry, Neumann weights, code tables"},
-                     "launch_ms": per_launch_ms, "launches": op_n},
+                     "launch_ms": per_launch_ms, "launches": op_n, "operator_counts": op_counts},
         "plain_fp64": fp64,
         "error_vs_plain_fp64": err64,
         "fp64_same_preconditioner": fp64_same,

@@ -240,13 +240,14 @@ typedef struct sph_params {
                                 stabilisation term zero), which exerts no force
                                 for a constant pressure                       */
     int32_t ppe_coef_half;   /* 1: the FP32 operator applications of the mixed
-                                form read the cached coefficients as FP16,
-                                each row's c_ij divided by the row's largest
-                                |c_ij| (one FP32 scale per row): 2 bytes per
-                                stored entry instead of 4.  The FP64
-                                applications (true residuals, the solution
-                                the tolerance is checked on) keep the FP32
-                                coefficients                                  */
+                                form read the cached coefficients and the
+                                Neumann rows' weights as FP16, each row
+                                divided by its largest |c_ij| or weight (one
+                                FP32 scale per row): 2 bytes per stored entry
+                                instead of 4.  The FP64 applications (true
+                                residuals, the solution the tolerance is
+                                checked on) keep the FP32 coefficients and the
+                                FP64 weights                                  */
     int32_t ppe_coarse_max;  /* most aggregates of the balanced coarse space
                                 (ppe_coarse_block < 0): 0 means 4096; at most
                                 32768 (the dense coarse inverse holds m^2
@@ -363,6 +364,11 @@ int sph_last_phase_ms(sph_ctx *ctx, float *ms4);
 /* Kernel launches issued by this context since creation (a replay of the
  * whole-step graph counts the launches it stands for, its solve as one). */
 int64_t sph_launch_count(sph_ctx *ctx);
+
+/* Sizes of the pressure operator of the current neighbour lists:
+ * counts[0] rows (records), [1] stored entries of the fluid rows, [2]
+ * Neumann rows, [3] their weight entries, [4] NNPS cells. */
+int sph_operator_counts(sph_ctx *ctx, int64_t counts[5]);
 
 /* Steps this context ran as a replay of its whole-step graph
  * (ppe_refinement = 4). */

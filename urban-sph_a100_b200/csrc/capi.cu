@@ -576,6 +576,19 @@ int64_t sph_launch_count(sph_ctx *ctx) {
     return DISPATCH(ctx, ctx->f->launches, ctx->d->launches);
 }
 
+int sph_operator_counts(sph_ctx *ctx, int64_t counts[5]) {
+    if (!ctx || !counts) return SPH_ERR_BAD_ARG;
+    auto go = [&](auto *c) {
+        counts[0] = c->n;
+        counts[1] = c->nnz;
+        counts[2] = c->L.n_nm;
+        counts[3] = c->L.nm_nnz;
+        counts[4] = c->num_cells;
+        return SPH_OK;
+    };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
+}
+
 int64_t sph_step_graph_count(sph_ctx *ctx) {
     if (!ctx) return -1;
     return DISPATCH(ctx, ctx->f->graph_steps, ctx->d->graph_steps);

@@ -138,7 +138,6 @@ struct Ctx {
     // its own and every offset fits in 13 bits
     uint16_t *nbr16 = nullptr;
     int *row_cell = nullptr;      // cell index of the row's first x-run cell (dy = dz = 0)
-    int *op_blk = nullptr;        // order of the pressure operator's row blocks (ppe.cu), rebuilt with the lists
     int row_cell_cap = 0;
     bool list16 = false;
     SideLists L;
@@ -154,6 +153,8 @@ struct Ctx {
     double *nm_gw = nullptr;      // mirror-row gradient weights
     double *nm_ow = nullptr;      // weights of the Neumann rows in the converged operator
     float *nm_owf = nullptr;      // the same in FP32 (mixed form)
+    __half *nm_owh = nullptr;     // the same divided by the row's largest weight, FP16 (ppe_coef_half)
+    float *nm_rsh = nullptr;      // that largest weight per Neumann row
     float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
     double *coef_d = nullptr;     // cached c_ij, FP64 form
     bool coef_valid = false;

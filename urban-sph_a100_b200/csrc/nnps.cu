@@ -1079,7 +1079,6 @@ template <class Real>
 int nnps_build(Ctx<Real> &c) {
     const int n = c.n, NC = c.num_cells;
     cudaStream_t st = c.stream;
-    c.release(c.op_blk);   // the operator's block order follows the new lists
     // scratch: h_ref as float, dummy flags / ranks
     float *href = nullptr;
     int *dflag = nullptr, *drank = nullptr, *big = nullptr, *nbig = nullptr, *err = nullptr;

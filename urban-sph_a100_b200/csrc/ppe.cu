@@ -219,48 +219,27 @@ __global__ void __launch_bounds__(128) k_ppe_sweep(const int4 *__restrict__ ty, 
 // come from the cell-start array (cache resident) once per row, and a
 // select chain picks one per entry.  Both forms visit the entries of the
 // 32-bit list in its order, so their sums are identical.
-// The streamed entries (codes, coefficients) are read once per launch: loaded
-// with an L2 evict-first policy and no L1 allocation, so that they pass
-// through the caches without displacing the gathered operand
-__device__ __forceinline__ unsigned long long l2_stream_policy() {
-    unsigned long long pol;
-    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-__device__ __forceinline__ uint2 ld_stream_u2(const void *p, unsigned long long pol) {
-    uint2 v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(pol));
-    return v;
-}
-__device__ __forceinline__ uint4 ld_stream_u4(const void *p, unsigned long long pol) {
-    uint4 v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
-    return v;
-}
-
 template <class C>
-__device__ __forceinline__ void load_coef4s(const C *p, C (&a)[4], unsigned long long pol);
+__device__ __forceinline__ void load_coef4(const C *p, C (&a)[4]);
 template <>
-__device__ __forceinline__ void load_coef4s<float>(const float *p, float (&a)[4], unsigned long long pol) {
-    const uint4 v = ld_stream_u4(p, pol);
-    a[0] = __uint_as_float(v.x); a[1] = __uint_as_float(v.y); a[2] = __uint_as_float(v.z); a[3] = __uint_as_float(v.w);
+__device__ __forceinline__ void load_coef4<float>(const float *p, float (&a)[4]) {
+    const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+    a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
 }
 template <>
-__device__ __forceinline__ void load_coef4s<double>(const double *p, double (&a)[4], unsigned long long pol) {
-    const uint4 v = ld_stream_u4(p, pol), w = ld_stream_u4(p + 2, pol);
-    a[0] = __hiloint2double((int)v.y, (int)v.x); a[1] = __hiloint2double((int)v.w, (int)v.z);
-    a[2] = __hiloint2double((int)w.y, (int)w.x); a[3] = __hiloint2double((int)w.w, (int)w.z);
+__device__ __forceinline__ void load_coef4<double>(const double *p, double (&a)[4]) {
+    const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 w = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    a[0] = v.x; a[1] = v.y; a[2] = w.x; a[3] = w.y;
 }
 template <>
-__device__ __forceinline__ void load_coef4s<__half>(const __half *p, __half (&a)[4], unsigned long long pol) {
-    const uint2 v = ld_stream_u2(p, pol);
+__device__ __forceinline__ void load_coef4<__half>(const __half *p, __half (&a)[4]) {
+    const uint2 v = __ldcs(reinterpret_cast<const uint2 *>(p));
     a[0] = __ushort_as_half((unsigned short)(v.x & 0xffffu));
     a[1] = __ushort_as_half((unsigned short)(v.x >> 16));
     a[2] = __ushort_as_half((unsigned short)(v.y & 0xffffu));
     a[3] = __ushort_as_half((unsigned short)(v.y >> 16));
 }
-
 template <class V, class C>
 __device__ __forceinline__ V coef_to(C a) { return (V)a; }
 template <>
@@ -289,6 +268,13 @@ __device__ __forceinline__ double ld_keep<double>(const double *p, unsigned long
     return v;
 }
 
+// a Neumann weight of the operator (streamed once per launch)
+__device__ __forceinline__ double nm_weight(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ double nm_weight(const float *p) { return (double)__ldcs(p); }
+__device__ __forceinline__ double nm_weight(const __half *p) {
+    return (double)__half2float(__ushort_as_half(__ldcs(reinterpret_cast<const unsigned short *>(p))));
+}
+
 struct List16 {
     const uint16_t *code;
     const int *row_cell, *cs;
@@ -303,13 +289,13 @@ template <bool L16, bool GUARD, class V, class C>
 __device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane, const C *__restrict__ coef,
                                           const uint16_t *__restrict__ code, const int *__restrict__ nbr,
                                           const int *plane_start, const V *__restrict__ x, V xi, V &s,
-                                          unsigned long long pol, unsigned long long spol) {
+                                          unsigned long long pol) {
     const long long e4 = sell4(sb, lane, k);
     C a[4];
-    load_coef4s<C>(coef + e4, a, spol);
+    load_coef4<C>(coef + e4, a);
     int j[4];
     if (L16) {
-        const uint2 q = ld_stream_u2(code + e4, spol);
+        const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(code + e4));
         const unsigned cc[4] = {q.x & 0xffffu, q.x >> 16, q.y & 0xffffu, q.y >> 16};
         // the padding entries of a last group hold no code: not decoded
 #pragma unroll
@@ -335,8 +321,8 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
                                                     const D *__restrict__ diag, const int *__restrict__ comp_id,
                                                     const double *__restrict__ cmean, const int *__restrict__ nm_rows,
                                                     const int *__restrict__ nm_off, const int *__restrict__ nm_nb,
-                                                    const W *__restrict__ nm_w, int n_nm, const V *__restrict__ x,
-                                                    V *__restrict__ y, int n, const int *__restrict__ blk_order) {
+                                                    const W *__restrict__ nm_w, const float *__restrict__ nm_rs,
+                                                    int n_nm, const V *__restrict__ x, V *__restrict__ y, int n) {
     const int b = blockIdx.x;
     const int m = min(nb_nm, nb_sell);
     bool neu;
@@ -352,13 +338,14 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         const V xi = x[i];
         const int q0 = nm_off[k], q1 = nm_off[k + 1];
         double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
-        for (int q = q0 + lane; q < q1; q += 32) s += (double)__ldcs(&nm_w[q]) * (double)(xi - x[__ldcs(&nm_nb[q])]);
+        for (int q = q0 + lane; q < q1; q += 32) s += nm_weight(nm_w + q) * (double)(xi - x[__ldcs(&nm_nb[q])]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (nm_rs) s *= (double)nm_rs[k];   // FP16 weights are stored divided by the row's largest
         if (lane == 0) y[i] = (q1 > q0) ? (V)s : xi;
         return;
     }
-    const int i = (blk_order ? blk_order[idx] : idx) * 128 + threadIdx.x;
+    const int i = idx * 128 + threadIdx.x;
     if (i >= n) return;
     const int kd = kind[i];
     if (kd == 2) return;   // written by the Neumann blocks
@@ -380,11 +367,10 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
                 ps[128 * q] = __ldg(&l16.cs[plane_cell(rc, q - 2, l16.NI, l16.NINJ, l16.cs_max)]);
         }
         const int full = cnt & ~3;
-        const unsigned long long pol = l2_keep_policy(), spol = l2_stream_policy();
+        const unsigned long long pol = l2_keep_policy();
         int k = 0;
-        for (; k < full; k += 4)
-            quad_step<L16, false, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s, pol, spol);
-        if (k < cnt) quad_step<L16, true, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s, pol, spol);
+        for (; k < full; k += 4) quad_step<L16, false, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s, pol);
+        if (k < cnt) quad_step<L16, true, V, C>(k, cnt, sb, lane, coef, l16.code, nbr, ps, x, xi, s, pol);
         yi = rowscale ? s * (V)rowscale[i] : s;
         if (comp_id) {
             const int cc = comp_id[i];
@@ -395,6 +381,25 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         if (j >= 0) yi = xi - x[j];
     }
     y[i] = yi;
+}
+
+// FP16 copy of the Neumann rows' operator weights, each row divided by its
+// largest weight (kept as an FP32 row scale; 1 for rows without weights);
+// one warp per row
+__global__ void __launch_bounds__(128) k_nm_half(const int *__restrict__ nm_off, const double *__restrict__ w,
+                                                 __half *__restrict__ wh, float *__restrict__ rs, int n_nm) {
+    const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k >= n_nm) return;   // uniform over the warp
+    const int q0 = nm_off[k], q1 = nm_off[k + 1];
+    float mx = 0.f;
+    for (int q = q0 + lane; q < q1; q += 32) mx = fmaxf(mx, fabsf((float)w[q]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float scale = mx > 0.f ? mx : 1.f;
+    const float inv = 1.f / scale;
+    for (int q = q0 + lane; q < q1; q += 32) wh[q] = __float2half_rn((float)w[q] * inv);
+    if (lane == 0) rs[k] = scale;
 }
 
 // FP16 copy of the cached FP32 coefficients of the fluid rows, each row
@@ -749,25 +754,25 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
         // FP64 applications (true residuals) keep the FP64 weights
         const int nb_nm = div_up((long long)c.L.n_nm, 4), nb_sell = div_up((long long)n, 128);
         const List16 l16{c.nbr16, c.row_cell, c.cell_start, c.dp.NI, c.dp.NI * c.dp.NJ, c.num_cells + 1};
-#define SPMV_FUSED(C_, W_, COEF, RS, NMW)                                                                          \
+#define SPMV_FUSED(C_, W_, COEF, RS, NMW, NMRS)                                                                    \
     do {                                                                                                       \
         if (c.list16)                                                                                          \
             k_spmv_fused<V, C_, Real, W_, true><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                        \
                 nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, RS, c.diag, cid,   \
-                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n, c.op_blk);                  \
+                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, NMRS, c.L.n_nm, x, y, n);                      \
         else                                                                                                   \
             k_spmv_fused<V, C_, Real, W_, false><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                       \
                 nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, RS, c.diag, cid,   \
-                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n, c.op_blk);                  \
+                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, NMRS, c.L.n_nm, x, y, n);                      \
     } while (0)
         if (sizeof(Real) == 4 && sizeof(V) == 4 && c.prm.ppe_coef_half && c.coef_h_valid)
-            SPMV_FUSED(__half, float, c.coef_h, c.coef_rs, c.nm_owf);
+            SPMV_FUSED(__half, __half, c.coef_h, c.coef_rs, c.nm_owh, c.nm_rsh);
         else if (sizeof(Real) == 4 && sizeof(V) == 4)
-            SPMV_FUSED(float, float, (const float *)c.coef, nullptr, c.nm_owf);
+            SPMV_FUSED(float, float, (const float *)c.coef, nullptr, c.nm_owf, nullptr);
         else if (sizeof(Real) == 4)
-            SPMV_FUSED(float, double, (const float *)c.coef, nullptr, c.nm_ow);
+            SPMV_FUSED(float, double, (const float *)c.coef, nullptr, c.nm_ow, nullptr);
         else
-            SPMV_FUSED(double, double, c.coef_d, nullptr, c.nm_ow);
+            SPMV_FUSED(double, double, c.coef_d, nullptr, c.nm_ow, nullptr);
 #undef SPMV_FUSED
     } else {
         k_spmv_mf<Real, V><<<grid_for(n, 128), 128, 0, c.stream>>>(c.dp, c.row_kind, c.row_aux, c.pr, c.mr, c.jc, c.slice_off,
@@ -842,7 +847,7 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
                  (double)c.nnz * ((l16 ? 2.0 : 4.0) + (half ? 2.0 : R));
         if (l16) *bytes += 4.0 * ((double)c.num_cells + 2.0);
         if (c.prm.ppe_matrix_free == 0)
-            *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R) + (double)c.L.nm_nnz * (4.0 + R);
+            *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R + (half ? 4.0 : 0.0)) + (double)c.L.nm_nnz * (4.0 + (half ? 2.0 : R));
     }
     if (reset) { c.prof_launches = 0; c.prof_ms = 0; }
     return SPH_OK;
@@ -1027,7 +1032,7 @@ static std::vector<uintptr_t> krylov_graph_key(Ctx<Real> &c, float *const *ws, c
     const void *ptrs[] = {xlo, c.scal, c.red, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, c.diag,
                           c.comp_id, c.comp_inv, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.cg_off, c.cg_rows,
                           c.cg_s, c.cg_y, c.cg_invf, c.cg_agg, c.nbr16, c.row_cell, c.cell_start, c.cg_piece,
-                          c.cg_pfirst, c.cg_part, c.cg_cnt, c.op_blk, c.coef_h, c.coef_rs};
+                          c.cg_pfirst, c.cg_part, c.cg_cnt, c.coef_h, c.coef_rs, c.nm_owh, c.nm_rsh};
     for (const void *q : ptrs) k.push_back((uintptr_t)q);
     const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode, c.prof ? 1 : 0, c.list16 ? 1 : 0,
                                c.num_cells, c.cg_np};
@@ -2138,36 +2143,6 @@ static int gmres(Ctx<Real> &c, GmresWs<Real, V> &ws, V *x, const V *b, double bn
     return status;
 }
 
-// Order in which the operator launch visits its row blocks (128 rows each):
-// by tiles of 8 x 8 cells in y and z (all x), then in storage order.  The
-// rows are stored in cell order (x fastest), so in storage order the blocks
-// in flight span about one z-plane of cells and a gathered x_j is reused by
-// rows up to two planes later, after several times the L2's size of
-// streamed coefficients has passed; within a tile of planes its reuses are
-// close together.  Each row's sums are unchanged: only the order in which
-// blocks are issued differs.
-template <class Real>
-static int operator_block_order(Ctx<Real> &c) {
-    const int n = c.n, nb = div_up((long long)n, 128);
-    std::vector<int> key(n);
-    SPH_CUDA_TRY(cudaMemcpyAsync(key.data(), c.g_idx, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
-    SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    const int NI = std::max(c.dp.NI, 1), NJ = std::max(c.dp.NJ, 1), T = 8, NTy = (NJ + T - 1) / T;
-    std::vector<long long> order(nb);
-    for (int b = 0; b < nb; ++b) {
-        const int k = std::min(std::max(key[(size_t)b * 128], 0), std::max(c.num_cells - 1, 0));   // dummies: last cell
-        const int cy = (k / NI) % NJ, cz = k / (NI * NJ);
-        order[b] = ((long long)(cz / T) * NTy + cy / T) * nb + b;
-    }
-    std::sort(order.begin(), order.end());
-    std::vector<int> blk(nb);
-    for (int q = 0; q < nb; ++q) blk[q] = (int)(order[q] % nb);
-    SPH_TRY(c.alloc(c.op_blk, (size_t)nb));
-    SPH_CUDA_TRY(cudaMemcpyAsync(c.op_blk, blk.data(), sizeof(int) * (size_t)nb, cudaMemcpyHostToDevice, c.stream));
-    SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    return SPH_OK;
-}
-
 template <class Real>
 static int ensure_ppe_ws(Ctx<Real> &c) {
     const int n = c.n;
@@ -2181,7 +2156,6 @@ static int ensure_ppe_ws(Ctx<Real> &c) {
         SPH_CUDA_TRY(cudaMemsetAsync(c.scal, 0, 64 * sizeof(double), c.stream));
         SPH_CUDA_TRY(cudaMallocHost(&c.red_host, 64 * sizeof(double)));
     }
-    if (!c.op_blk && n > 0) SPH_TRY(operator_block_order(c));
     if (!c.coef_valid) {
         c.coef_h_valid = false;
         const size_t m = (size_t)std::max(c.nnz_padded, 1LL);
@@ -2239,6 +2213,14 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         k_coef_half<<<grid_for(n, 128), 128, 0, st>>>(c.row_kind, c.slice_off, c.ncnt, (const float *)c.coef, c.coef_h,
                                                        c.coef_rs, n);
         ++c.launches;
+        c.release(c.nm_owh);
+        c.release(c.nm_rsh);
+        if (c.L.n_nm > 0) {
+            SPH_TRY(c.alloc(c.nm_owh, (size_t)std::max(c.L.nm_nnz, 1LL)));
+            SPH_TRY(c.alloc(c.nm_rsh, (size_t)c.L.n_nm));
+            k_nm_half<<<grid_for(32LL * c.L.n_nm, 128), 128, 0, st>>>(c.L.nm_off, c.nm_ow, c.nm_owh, c.nm_rsh, c.L.n_nm);
+            ++c.launches;
+        }
         SPH_CUDA_TRY(cudaGetLastError());
         c.coef_h_valid = true;
     }

@@ -24,7 +24,7 @@ SYMBOLS = (
     "sph_params_init", "sph_domain_setup", "sph_create", "sph_destroy", "sph_set_params",
     "sph_upload", "sph_upload_state", "sph_download", "sph_nnps", "sph_nnps_export",
     "sph_neighbors_export", "sph_interaction", "sph_ppe", "sph_time_update", "sph_step",
-    "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_step_graph_count", "sph_status_string",
+    "sph_diagnostics", "sph_last_phase_ms", "sph_launch_count", "sph_step_graph_count", "sph_operator_counts", "sph_status_string",
     "sph_last_error", "sph_profile", "sph_set_pair_block", "sph_operator_stats", "sph_operator_bytes", "sph_nnps_sort_noalloc",
     "sph_ml_collect", "sph_ml_samples", "sph_ml_train", "sph_ml_set_weights", "sph_ml_get_weights",
     "sph_ml_grad", "sph_ml_predict_samples",
@@ -76,6 +76,8 @@ def lib():
         L.sph_launch_count.restype = i64
         L.sph_step_graph_count.argtypes = [vp]
         L.sph_step_graph_count.restype = i64
+        L.sph_operator_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+        L.sph_operator_counts.restype = ctypes.c_int
         L.sph_status_string.argtypes = [i32]
         L.sph_status_string.restype = ctypes.c_char_p
         L.sph_last_error.restype = ctypes.c_char_p
@@ -232,6 +234,12 @@ class Simulation:
 
     def launches(self):
         return int(lib().sph_launch_count(self.h))
+
+    def operator_counts(self):
+        """Rows, fluid-row entries, Neumann rows, Neumann entries and cells of the pressure operator."""
+        a = (ctypes.c_int64 * 5)()
+        _check("sph_operator_counts", lib().sph_operator_counts(self.h, a))
+        return {"rows": a[0], "entries": a[1], "neumann_rows": a[2], "neumann_entries": a[3], "cells": a[4]}
 
     def graph_steps(self):
         """Steps run as a replay of the whole-step graph."""
