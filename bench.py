@@ -860,7 +860,8 @@ def main():
     nc = ncu_traffic(f"ppe_operator_{args.config}.json")
     traffic = None
     if (nc and "measured_at" in nc and nc.get("apr", False) == bool(args.apr)
-            and nc.get("coef_half", False) == bool(p.ppe_coef_half)):
+            and nc.get("coef_half", False) == bool(p.ppe_coef_half)
+            and nc.get("entries_counted") == "fluid rows"):
         m = nc["measured_at"]
         traffic = m["traffic_over_algorithmic"] * op_bytes
     ph = np.mean(np.array(phases), axis=0) if phases else np.zeros(4)

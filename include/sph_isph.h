@@ -240,14 +240,13 @@ typedef struct sph_params {
                                 stabilisation term zero), which exerts no force
                                 for a constant pressure                       */
     int32_t ppe_coef_half;   /* 1: the FP32 operator applications of the mixed
-                                form read the cached coefficients and the
-                                Neumann rows' weights as FP16, each row
-                                divided by its largest |c_ij| or weight (one
-                                FP32 scale per row): 2 bytes per stored entry
-                                instead of 4.  The FP64 applications (true
-                                residuals, the solution the tolerance is
-                                checked on) keep the FP32 coefficients and the
-                                FP64 weights                                  */
+                                form read the cached coefficients as FP16,
+                                each row's c_ij divided by the row's largest
+                                |c_ij| (one FP32 scale per row): 2 bytes per
+                                stored entry instead of 4.  The FP64
+                                applications (true residuals, the solution
+                                the tolerance is checked on) keep the FP32
+                                coefficients                                  */
     int32_t ppe_coarse_max;  /* most aggregates of the balanced coarse space
                                 (ppe_coarse_block < 0): 0 means 4096; at most
                                 32768 (the dense coarse inverse holds m^2

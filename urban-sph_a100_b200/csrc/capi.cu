@@ -580,7 +580,7 @@ int sph_operator_counts(sph_ctx *ctx, int64_t counts[5]) {
     if (!ctx || !counts) return SPH_ERR_BAD_ARG;
     auto go = [&](auto *c) {
         counts[0] = c->n;
-        counts[1] = c->nnz;
+        counts[1] = c->nnz_op;
         counts[2] = c->L.n_nm;
         counts[3] = c->L.nm_nnz;
         counts[4] = c->num_cells;

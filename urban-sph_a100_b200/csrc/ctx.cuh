@@ -132,6 +132,7 @@ struct Ctx {
     long long *slice_off = nullptr;
     int *nbr = nullptr;
     long long nnz = 0, nnz_padded = 0;
+    long long nnz_op = 0;         // entries of the fluid rows, the ones the pressure operator reads
     long long nbr_cap = 0;
     // the same list as 16-bit codes for the pressure operator (plane_cell in
     // common.cuh): valid when every row searches at most two cells around
@@ -153,8 +154,6 @@ struct Ctx {
     double *nm_gw = nullptr;      // mirror-row gradient weights
     double *nm_ow = nullptr;      // weights of the Neumann rows in the converged operator
     float *nm_owf = nullptr;      // the same in FP32 (mixed form)
-    __half *nm_owh = nullptr;     // the same divided by the row's largest weight, FP16 (ppe_coef_half)
-    float *nm_rsh = nullptr;      // that largest weight per Neumann row
     float *coef = nullptr;        // cached c_ij (SELL layout), mixed form
     double *coef_d = nullptr;     // cached c_ij, FP64 form
     bool coef_valid = false;

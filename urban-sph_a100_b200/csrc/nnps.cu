@@ -1068,6 +1068,16 @@ int build_side_lists(Ctx<Real> &c) {
         SPH_CUDA_TRY(cudaMemcpyAsync(c.row_kind, kind.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.stream));
         SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
     }
+    {   // stored entries of the rows the pressure operator visits (fluid rows)
+        std::vector<int> cnt(n), kd(n);
+        SPH_CUDA_TRY(cudaMemcpyAsync(cnt.data(), c.ncnt, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+        SPH_CUDA_TRY(cudaMemcpyAsync(kd.data(), c.row_kind, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+        SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        long long s = 0;
+        for (int i = 0; i < n; ++i)
+            if (kd[i] == 1) s += cnt[i];
+        c.nnz_op = s;
+    }
     c.cg_valid = false;   // the coarse preconditioner follows the row kinds
     return SPH_OK;
 }

@@ -268,13 +268,6 @@ __device__ __forceinline__ double ld_keep<double>(const double *p, unsigned long
     return v;
 }
 
-// a Neumann weight of the operator (streamed once per launch)
-__device__ __forceinline__ double nm_weight(const double *p) { return __ldcs(p); }
-__device__ __forceinline__ double nm_weight(const float *p) { return (double)__ldcs(p); }
-__device__ __forceinline__ double nm_weight(const __half *p) {
-    return (double)__half2float(__ushort_as_half(__ldcs(reinterpret_cast<const unsigned short *>(p))));
-}
-
 struct List16 {
     const uint16_t *code;
     const int *row_cell, *cs;
@@ -321,8 +314,8 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
                                                     const D *__restrict__ diag, const int *__restrict__ comp_id,
                                                     const double *__restrict__ cmean, const int *__restrict__ nm_rows,
                                                     const int *__restrict__ nm_off, const int *__restrict__ nm_nb,
-                                                    const W *__restrict__ nm_w, const float *__restrict__ nm_rs,
-                                                    int n_nm, const V *__restrict__ x, V *__restrict__ y, int n) {
+                                                    const W *__restrict__ nm_w, int n_nm, const V *__restrict__ x,
+                                                    V *__restrict__ y, int n) {
     const int b = blockIdx.x;
     const int m = min(nb_nm, nb_sell);
     bool neu;
@@ -338,10 +331,9 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         const V xi = x[i];
         const int q0 = nm_off[k], q1 = nm_off[k + 1];
         double s = 0;   // the weights sum to one: x_w - sum w x_k = sum w (x_w - x_k)
-        for (int q = q0 + lane; q < q1; q += 32) s += nm_weight(nm_w + q) * (double)(xi - x[__ldcs(&nm_nb[q])]);
+        for (int q = q0 + lane; q < q1; q += 32) s += (double)__ldcs(&nm_w[q]) * (double)(xi - x[__ldcs(&nm_nb[q])]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (nm_rs) s *= (double)nm_rs[k];   // FP16 weights are stored divided by the row's largest
         if (lane == 0) y[i] = (q1 > q0) ? (V)s : xi;
         return;
     }
@@ -381,25 +373,6 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         if (j >= 0) yi = xi - x[j];
     }
     y[i] = yi;
-}
-
-// FP16 copy of the Neumann rows' operator weights, each row divided by its
-// largest weight (kept as an FP32 row scale; 1 for rows without weights);
-// one warp per row
-__global__ void __launch_bounds__(128) k_nm_half(const int *__restrict__ nm_off, const double *__restrict__ w,
-                                                 __half *__restrict__ wh, float *__restrict__ rs, int n_nm) {
-    const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (k >= n_nm) return;   // uniform over the warp
-    const int q0 = nm_off[k], q1 = nm_off[k + 1];
-    float mx = 0.f;
-    for (int q = q0 + lane; q < q1; q += 32) mx = fmaxf(mx, fabsf((float)w[q]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    const float scale = mx > 0.f ? mx : 1.f;
-    const float inv = 1.f / scale;
-    for (int q = q0 + lane; q < q1; q += 32) wh[q] = __float2half_rn((float)w[q] * inv);
-    if (lane == 0) rs[k] = scale;
 }
 
 // FP16 copy of the cached FP32 coefficients of the fluid rows, each row
@@ -754,25 +727,25 @@ static void apply_op(Ctx<Real> &c, const V *x, V *y, bool cached, bool mean_read
         // FP64 applications (true residuals) keep the FP64 weights
         const int nb_nm = div_up((long long)c.L.n_nm, 4), nb_sell = div_up((long long)n, 128);
         const List16 l16{c.nbr16, c.row_cell, c.cell_start, c.dp.NI, c.dp.NI * c.dp.NJ, c.num_cells + 1};
-#define SPMV_FUSED(C_, W_, COEF, RS, NMW, NMRS)                                                                    \
+#define SPMV_FUSED(C_, W_, COEF, RS, NMW)                                                                          \
     do {                                                                                                       \
         if (c.list16)                                                                                          \
             k_spmv_fused<V, C_, Real, W_, true><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                        \
                 nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, RS, c.diag, cid,   \
-                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, NMRS, c.L.n_nm, x, y, n);                      \
+                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                            \
         else                                                                                                   \
             k_spmv_fused<V, C_, Real, W_, false><<<nb_nm + nb_sell, 128, 0, c.stream>>>(                       \
                 nb_nm, nb_sell, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, l16, COEF, RS, c.diag, cid,   \
-                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, NMRS, c.L.n_nm, x, y, n);                      \
+                cmean, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, NMW, c.L.n_nm, x, y, n);                            \
     } while (0)
         if (sizeof(Real) == 4 && sizeof(V) == 4 && c.prm.ppe_coef_half && c.coef_h_valid)
-            SPMV_FUSED(__half, __half, c.coef_h, c.coef_rs, c.nm_owh, c.nm_rsh);
+            SPMV_FUSED(__half, float, c.coef_h, c.coef_rs, c.nm_owf);
         else if (sizeof(Real) == 4 && sizeof(V) == 4)
-            SPMV_FUSED(float, float, (const float *)c.coef, nullptr, c.nm_owf, nullptr);
+            SPMV_FUSED(float, float, (const float *)c.coef, nullptr, c.nm_owf);
         else if (sizeof(Real) == 4)
-            SPMV_FUSED(float, double, (const float *)c.coef, nullptr, c.nm_ow, nullptr);
+            SPMV_FUSED(float, double, (const float *)c.coef, nullptr, c.nm_ow);
         else
-            SPMV_FUSED(double, double, c.coef_d, nullptr, c.nm_ow, nullptr);
+            SPMV_FUSED(double, double, c.coef_d, nullptr, c.nm_ow);
 #undef SPMV_FUSED
     } else {
         k_spmv_mf<Real, V><<<grid_for(n, 128), 128, 0, c.stream>>>(c.dp, c.row_kind, c.row_aux, c.pr, c.mr, c.jc, c.slice_off,
@@ -831,10 +804,12 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
     if (bytes) {
         // per row: kind and list length (4 + 4) + x_i + y_i (Real), with the
         // rank-one term also component id (4) + A_i (Real); per slice of 32
-        // rows its offset (8); per stored entry: index (4, or 2 for the
+        // rows its offset (8); per stored entry of a fluid row (the only
+        // rows whose entries the launch reads): index (4, or 2 for the
         // 16-bit codes, which add the row's cell (4) per row and the cell
-        // starts once) + coefficient (float in the mixed form, double in
-        // the FP64 form).  The Neumann rows of the same launch: row index
+        // starts once) + coefficient (float, or half with ppe_coef_half, in
+        // the mixed form; double in the FP64 form; the FP16 coefficients add
+        // a row scale (4) per row).  The Neumann rows of the same launch: row index
         // and offset (4 + 4) + x_i + y_i, per entry index (4) + weight
         // (Real).  The gathers x_j are not counted: an ideal kernel serves
         // them from L2.
@@ -844,10 +819,10 @@ int operator_stats(Ctx<Real> &c, int64_t *launches, double *total_ms, double *by
         double row = 8.0 + 2.0 * R + (l16 ? 4.0 : 0.0) + (half ? 4.0 : 0.0);
         if (c.n_comp > 0) row += 4.0 + R;
         *bytes = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) +
-                 (double)c.nnz * ((l16 ? 2.0 : 4.0) + (half ? 2.0 : R));
+                 (double)c.nnz_op * ((l16 ? 2.0 : 4.0) + (half ? 2.0 : R));
         if (l16) *bytes += 4.0 * ((double)c.num_cells + 2.0);
         if (c.prm.ppe_matrix_free == 0)
-            *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R + (half ? 4.0 : 0.0)) + (double)c.L.nm_nnz * (4.0 + (half ? 2.0 : R));
+            *bytes += (double)c.L.n_nm * (8.0 + 2.0 * R) + (double)c.L.nm_nnz * (4.0 + R);
     }
     if (reset) { c.prof_launches = 0; c.prof_ms = 0; }
     return SPH_OK;
@@ -868,7 +843,7 @@ int operator_bytes(Ctx<Real> &c, double *stored, double *index_rule) {
         const double R = (double)sizeof(Real);
         double row = 8.0 + 2.0 * R;
         if (c.n_comp > 0) row += 4.0 + R;
-        *index_rule = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + 4.0 * (double)c.nnz +
+        *index_rule = (double)c.n * row + 8.0 * (double)((c.n + 31) / 32) + 4.0 * (double)c.nnz_op +
                       (double)c.L.n_nm * (8.0 + 2.0 * R) + 4.0 * (double)c.L.nm_nnz;
     }
     return SPH_OK;
@@ -1032,7 +1007,7 @@ static std::vector<uintptr_t> krylov_graph_key(Ctx<Real> &c, float *const *ws, c
     const void *ptrs[] = {xlo, c.scal, c.red, c.row_kind, c.row_aux, c.slice_off, c.ncnt, c.nbr, c.coef, c.diag,
                           c.comp_id, c.comp_inv, c.L.nm_rows, c.L.nm_off, c.L.nm_nbr, c.nm_owf, c.cg_off, c.cg_rows,
                           c.cg_s, c.cg_y, c.cg_invf, c.cg_agg, c.nbr16, c.row_cell, c.cell_start, c.cg_piece,
-                          c.cg_pfirst, c.cg_part, c.cg_cnt, c.coef_h, c.coef_rs, c.nm_owh, c.nm_rsh};
+                          c.cg_pfirst, c.cg_part, c.cg_cnt, c.coef_h, c.coef_rs};
     for (const void *q : ptrs) k.push_back((uintptr_t)q);
     const long long sizes[] = {c.n, c.n_comp, c.L.n_nm, c.cg_m, c.prm.ppe_coarse_mode, c.prof ? 1 : 0, c.list16 ? 1 : 0,
                                c.num_cells, c.cg_np};
@@ -2213,14 +2188,6 @@ int phase_ppe(Ctx<Real> &c, sph_ppe_stats *stats) {
         k_coef_half<<<grid_for(n, 128), 128, 0, st>>>(c.row_kind, c.slice_off, c.ncnt, (const float *)c.coef, c.coef_h,
                                                        c.coef_rs, n);
         ++c.launches;
-        c.release(c.nm_owh);
-        c.release(c.nm_rsh);
-        if (c.L.n_nm > 0) {
-            SPH_TRY(c.alloc(c.nm_owh, (size_t)std::max(c.L.nm_nnz, 1LL)));
-            SPH_TRY(c.alloc(c.nm_rsh, (size_t)c.L.n_nm));
-            k_nm_half<<<grid_for(32LL * c.L.n_nm, 128), 128, 0, st>>>(c.L.nm_off, c.nm_ow, c.nm_owh, c.nm_rsh, c.L.n_nm);
-            ++c.launches;
-        }
         SPH_CUDA_TRY(cudaGetLastError());
         c.coef_h_valid = true;
     }
