@@ -877,7 +877,9 @@ def main():
                    "precision": "mixed FP32/FP64" if args.precision == "mixed" else "FP64",
                    "ppe": args.mode, "ppe_tol": args.tol,
                    "ppe_operator": "matrix-free" if args.matrix_free else
-                   ("cached c_ij, 32-bit neighbour indices" if args.wide_index else "cached c_ij, 16-bit neighbour codes")
+                   ("cached c_ij, 16-bit neighbour codes" if op_counts["codes16"] else
+                    "cached c_ij, 32-bit neighbour indices" + ("" if args.wide_index else
+                                                               " (16-bit codes asked for, not representable)"))
                    + (", FP16 row-scaled c_ij in the FP32 applications" if args.coef_half else ""),
                    "ppe_refinement": args.refinement,
                    "ppe_pair_h": {"ref": "h_i", "avg": "(h_i + h_j) / 2"}[args.pair_h],

@@ -217,12 +217,12 @@ typedef struct sph_params {
                                 KERNEL_pressureforce3D uses (:598-602)         */
     int32_t ppe_wide_index;  /* 1: the pressure operator reads the 32-bit
                                 neighbour indices; 0 (default): 16-bit codes
-                                (cell plane of the entry, offset from the
-                                plane's first reachable record) wherever every
-                                row searches at most two cells around its own
-                                and every offset is below 8192 -- same
-                                entries, same order, same results, fewer
-                                bytes                                         */
+                                (the entry's x-run of cells (dy, dz) around
+                                the row's cell, offset from the run's first
+                                record) wherever every row searches at most
+                                two cells around its own and every offset is
+                                below 2048 -- same entries, same order, same
+                                results, fewer bytes                          */
     int32_t recompute_pairs; /* 1: the prep pass and the pressure force evaluate
                                 their pair terms every step, as the reference
                                 does; 0 (default): their time-invariant pair
@@ -366,8 +366,9 @@ int64_t sph_launch_count(sph_ctx *ctx);
 
 /* Sizes of the pressure operator of the current neighbour lists:
  * counts[0] rows (records), [1] stored entries of the fluid rows, [2]
- * Neumann rows, [3] their weight entries, [4] NNPS cells. */
-int sph_operator_counts(sph_ctx *ctx, int64_t counts[5]);
+ * Neumann rows, [3] their weight entries, [4] NNPS cells, [5] 1 when the
+ * operator reads 16-bit neighbour codes, 0 when 32-bit indices. */
+int sph_operator_counts(sph_ctx *ctx, int64_t counts[6]);
 
 /* Steps this context ran as a replay of its whole-step graph
  * (ppe_refinement = 4). */

@@ -576,7 +576,7 @@ int64_t sph_launch_count(sph_ctx *ctx) {
     return DISPATCH(ctx, ctx->f->launches, ctx->d->launches);
 }
 
-int sph_operator_counts(sph_ctx *ctx, int64_t counts[5]) {
+int sph_operator_counts(sph_ctx *ctx, int64_t counts[6]) {
     if (!ctx || !counts) return SPH_ERR_BAD_ARG;
     auto go = [&](auto *c) {
         counts[0] = c->n;
@@ -584,6 +584,7 @@ int sph_operator_counts(sph_ctx *ctx, int64_t counts[5]) {
         counts[2] = c->L.n_nm;
         counts[3] = c->L.nm_nnz;
         counts[4] = c->num_cells;
+        counts[5] = (c->list16 && c->prm.ppe_matrix_free == 0) ? 1 : 0;
         return SPH_OK;
     };
     return DISPATCH(ctx, go(ctx->f), go(ctx->d));

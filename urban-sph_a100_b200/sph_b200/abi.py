@@ -236,10 +236,12 @@ class Simulation:
         return int(lib().sph_launch_count(self.h))
 
     def operator_counts(self):
-        """Rows, fluid-row entries, Neumann rows, Neumann entries and cells of the pressure operator."""
-        a = (ctypes.c_int64 * 5)()
+        """Rows, fluid-row entries, Neumann rows, Neumann entries, cells of the pressure operator, and
+        whether it reads 16-bit neighbour codes."""
+        a = (ctypes.c_int64 * 6)()
         _check("sph_operator_counts", lib().sph_operator_counts(self.h, a))
-        return {"rows": a[0], "entries": a[1], "neumann_rows": a[2], "neumann_entries": a[3], "cells": a[4]}
+        return {"rows": a[0], "entries": a[1], "neumann_rows": a[2], "neumann_entries": a[3], "cells": a[4],
+                "codes16": bool(a[5])}
 
     def graph_steps(self):
         """Steps run as a replay of the whole-step graph."""
