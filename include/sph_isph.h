@@ -217,12 +217,13 @@ typedef struct sph_params {
                                 KERNEL_pressureforce3D uses (:598-602)         */
     int32_t ppe_wide_index;  /* 1: the pressure operator reads the 32-bit
                                 neighbour indices; 0 (default): 16-bit codes
-                                (the entry's x-run of cells (dy, dz) around
-                                the row's cell, offset from the run's first
-                                record) wherever every row searches at most
-                                two cells around its own and every offset is
-                                below 2048 -- same entries, same order, same
-                                results, fewer bytes                          */
+                                (cell plane of the entry, offset from the
+                                plane's first reachable record) wherever every
+                                row searches at most two cells around its own
+                                and every offset is below 8192 -- same
+                                entries, same order, same results, fewer
+                                bytes; otherwise the 32-bit indices
+                                (sph_operator_counts tells which)             */
     int32_t recompute_pairs; /* 1: the prep pass and the pressure force evaluate
                                 their pair terms every step, as the reference
                                 does; 0 (default): their time-invariant pair

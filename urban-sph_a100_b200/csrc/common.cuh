@@ -236,13 +236,11 @@ __device__ __forceinline__ Real visc2(const DevParams &P, int jc) {
 
 __host__ __device__ inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// 16-bit neighbour codes of the pressure operator.  A row searches the x-runs
-// of cells (dy, dz) in [-2, 2]^2 around its own; the records of run (dy, dz)
-// start at cell_start[run_cell(rc, dy, dz)], with rc the row's first x-run
-// cell in its own y-row and plane (dy = dz = 0).  An entry j is
-// ((dz + 2) * 5 + dy + 2) << 11 | (j - that start): a run spans at most five
-// cells, so the offsets stay below 2048 even where APR children pack eight
-// times the records into a cell.
+// 16-bit neighbour codes of the pressure operator.  A row searches cell
+// planes dz in [-2, 2] around its own; the records of plane dz that it can
+// reach lie in cell_start[plane_cell(rc, dz)] ... onwards, with rc the
+// row's first x-run cell in its own y-row and plane (dy = dz = 0).  An entry
+// j is (dz + 2) << 13 | (j - that start), offsets up to 8191.
 //
 // The pressure coefficients and these codes are stored four entries of a row
 // together (a slice of 32 rows holds a multiple of four entries per row):
@@ -251,11 +249,10 @@ __host__ __device__ inline int div_up(long long a, long long b) { return (int)((
 __host__ __device__ inline long long sell4(long long slice_base, int lane, int k) {
     return slice_base + 128LL * (k >> 2) + 4 * lane + (k & 3);
 }
-constexpr int kCodeShift = 11;
+constexpr int kCodeShift = 13;
 constexpr unsigned kCodeMask = (1u << kCodeShift) - 1u;
-constexpr int kCodeRuns = 25;   // (dy, dz) in [-2, 2]^2
-__host__ __device__ inline int run_cell(int rc, int dy, int dz, int NI, int NINJ, int cs_max) {
-    const int k = rc + dy * NI + dz * NINJ;
+__host__ __device__ inline int plane_cell(int rc, int dz, int NI, int NINJ, int cs_max) {
+    const int k = rc - 2 * NI + dz * NINJ;
     return k < 0 ? 0 : (k > cs_max ? cs_max : k);
 }
 

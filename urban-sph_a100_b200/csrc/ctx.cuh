@@ -134,9 +134,9 @@ struct Ctx {
     long long nnz = 0, nnz_padded = 0;
     long long nnz_op = 0;         // entries of the fluid rows, the ones the pressure operator reads
     long long nbr_cap = 0;
-    // the same list as 16-bit codes for the pressure operator (run_cell in
+    // the same list as 16-bit codes for the pressure operator (plane_cell in
     // common.cuh): valid when every row searches at most two cells around
-    // its own and every offset fits in 11 bits
+    // its own and every offset fits in 13 bits
     uint16_t *nbr16 = nullptr;
     int *row_cell = nullptr;      // cell index of the row's first x-run cell (dy = dz = 0)
     int row_cell_cap = 0;

@@ -405,7 +405,7 @@ static int regather(Ctx<Real> &c, T *arr, void *scratch) {
 // change an FP32 comparison with a positive radius).
 // The fill pass also writes the 16-bit codes of the pressure operator
 // (nbr16, row_cell; flag16 set when a row cannot be coded: a search radius
-// beyond two cells, or an offset beyond 2047 in its cell run).
+// beyond two cells, or an offset beyond 8191 in its cell plane).
 // One warp per row: the lanes test 32 consecutive candidates of a cell run
 // at a time (coalesced loads of pf), __ballot_sync collects the kept ones
 // and each kept lane writes its entry at the row's count plus the kept
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
                 if (x0 > x1) continue;
                 const int kb = P.NI * yy + P.NI * P.NJ * zz;
                 const int s = cs[kb + x0], e = cs[kb + x1 + 1];
-                const unsigned run = (unsigned)((dz + 2) * 5 + dy + 2);   // codes count from the run's start s
+                const int s16 = (FILL && nbr16) ? cs[plane_cell(rc, dz, P.NI, P.NI * P.NJ, P.num_cells + 1)] : 0;
                 for (int b0 = s; b0 < e; b0 += 32) {
                     const int j = b0 + lane;
                     bool keep = false;
@@ -461,9 +461,10 @@ __global__ void __launch_bounds__(128) k_list(DevParams P, const float4 *__restr
                         const int pos = cnt + __popc(m & ((1u << lane) - 1u));
                         nbr[base + (long long)pos * 32] = j;
                         if (nbr16) {
-                            const int off = j - s;
+                            const int off = j - s16;
                             if (off < 0 || off > (int)kCodeMask) atomicOr(flag16, 2);
-                            nbr16[sell4(sb, i & 31, pos)] = (uint16_t)((run << kCodeShift) | ((unsigned)off & kCodeMask));
+                            nbr16[sell4(sb, i & 31, pos)] =
+                                (uint16_t)(((unsigned)(dz + 2) << kCodeShift) | ((unsigned)off & kCodeMask));
                         }
                     }
                     cnt += __popc(m);

@@ -213,12 +213,12 @@ __global__ void __launch_bounds__(128) k_ppe_sweep(const int4 *__restrict__ ty, 
 // The coefficients are read four entries at a time (sell4 layout): one
 // 16-byte load per four FP32 coefficients, then the four gathers, which
 // halves the load requests of the stream against one entry per load.
-// L16: the neighbours are 16-bit codes (cell run (dy, dz) of the entry,
-// offset from that run's first record; run_cell in common.cuh), four per
-// 8-byte load, instead of 32-bit indices.  A row's 25 run starts come from
-// the cell-start array (cache resident) once per row into the thread's
-// column of a shared table.  Both forms visit the entries of the 32-bit list
-// in its order, so their sums are identical.
+// L16: the neighbours are 16-bit codes (cell plane dz of the entry, offset
+// from that plane's first reachable record; plane_cell in common.cuh), four
+// per 8-byte load, instead of 32-bit indices.  A row's five plane starts
+// come from the cell-start array (cache resident) once per row, and a
+// select chain picks one per entry.  Both forms visit the entries of the
+// 32-bit list in its order, so their sums are identical.
 template <class C>
 __device__ __forceinline__ void load_coef4(const C *p, C (&a)[4]);
 template <>
@@ -275,13 +275,13 @@ struct List16 {
 };
 
 // one group of four entries of a row: the coefficients in one load, the
-// neighbours from four 16-bit codes (run starts in the thread's column of
+// neighbours from four 16-bit codes (plane starts in the thread's column of
 // the shared table) or from the 32-bit list; GUARD only for the row's last,
 // partly filled group
 template <bool L16, bool GUARD, class V, class C>
 __device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane, const C *__restrict__ coef,
                                           const uint16_t *__restrict__ code, const int *__restrict__ nbr,
-                                          const int *run_start, const V *__restrict__ x, V xi, V &s,
+                                          const int *plane_start, const V *__restrict__ x, V xi, V &s,
                                           unsigned long long pol) {
     const long long e4 = sell4(sb, lane, k);
     C a[4];
@@ -293,7 +293,7 @@ __device__ __forceinline__ void quad_step(int k, int cnt, long long sb, int lane
         // the padding entries of a last group hold no code: not decoded
 #pragma unroll
         for (int t = 0; t < 4; ++t)
-            j[t] = (!GUARD || k + t < cnt) ? run_start[128 * (cc[t] >> kCodeShift)] + (int)(cc[t] & kCodeMask) : 0;
+            j[t] = (!GUARD || k + t < cnt) ? plane_start[128 * (cc[t] >> kCodeShift)] + (int)(cc[t] & kCodeMask) : 0;
     } else {
         const long long e = sb + lane + 32LL * k;
 #pragma unroll
@@ -348,15 +348,15 @@ __global__ void __launch_bounds__(128) k_spmv_fused(int nb_nm, int nb_sell, cons
         const int lane = i & 31;
         const int cnt = ncnt[i];
         V s = 0;
-        // the row's 25 run starts, in this thread's column (no other thread
-        // reads it, so no barrier)
-        __shared__ int plane_tab[kCodeRuns * 128];
+        // the row's five plane starts, in this thread's column (no other
+        // thread reads it, so no barrier)
+        __shared__ int plane_tab[5 * 128];
         int *ps = plane_tab + threadIdx.x;
         if (L16) {
             const int rc = l16.row_cell[i];
 #pragma unroll
-            for (int q = 0; q < kCodeRuns; ++q)
-                ps[128 * q] = __ldg(&l16.cs[run_cell(rc, q % 5 - 2, q / 5 - 2, l16.NI, l16.NINJ, l16.cs_max)]);
+            for (int q = 0; q < 5; ++q)
+                ps[128 * q] = __ldg(&l16.cs[plane_cell(rc, q - 2, l16.NI, l16.NINJ, l16.cs_max)]);
         }
         const int full = cnt & ~3;
         const unsigned long long pol = l2_keep_policy();
