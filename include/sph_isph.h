@@ -252,7 +252,15 @@ typedef struct sph_params {
                                 (ppe_coarse_block < 0): 0 means 4096; at most
                                 32768 (the dense coarse inverse holds m^2
                                 entries: 4.3 GB in FP32 at 32768)             */
-    int32_t reserved0;       /* 0                                             */
+    int32_t enthalpy_eqn;    /* with vii con_solve = 1: 1 the energy equation
+                                in enthalpy (the reference's enthalpy_eqn,
+                                Parameters.cuh:96, compiled out there): the
+                                conduction sum is the enthalpy rate, the
+                                projection sets enthalpy0 and the temperature
+                                htoT(enthalpy) from the built-in corium table
+                                (functions_PROP.cuh:43-67), the time update
+                                advances the enthalpy; 0 (default) the
+                                temperature form                              */
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
                                 refinement forms of SPH_PPE_MIXED_IR (0: 1e-3) */
     double  apr_zone;        /* APR: distance from an IBM marker's cell within

@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(HERE, "_ref", "libsophia_ref.so")
 
 # host builds of the reference: as shipped (None), and with the pressure
 # force's commented-out difference form in place of its active line ("dp")
-VARIANTS = {None: LIB_PATH, "dp": os.path.join(HERE, "_ref", "libsophia_ref_dp.so")}
+VARIANTS = {None: LIB_PATH, "dp": os.path.join(HERE, "_ref", "libsophia_ref_dp.so"),
+            "enth": os.path.join(HERE, "_ref", "libsophia_ref_enth.so")}
 _libs = {}
 
 
@@ -27,7 +28,7 @@ def available(variant=None):
 def lib(variant=None):
     if variant not in _libs:
         if not available(variant):
-            raise FileNotFoundError(f"{VARIANTS[variant]} not built (make -C oracle ref ref_dp)")
+            raise FileNotFoundError(f"{VARIANTS[variant]} not built (make -C oracle ref ref_dp ref_enth)")
         L = ctypes.CDLL(VARIANTS[variant])
         vp = ctypes.c_void_p
         L.ref_set_params.argtypes = [vp, vp]

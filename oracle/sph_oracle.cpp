@@ -43,6 +43,7 @@ struct P {
     int fv_solve() const { return p.vii[13]; }
     int fg_solve() const { return p.vii[14]; }
     int con_solve() const { return p.vii[15]; }
+    int enthalpy_eqn() const { return p.enthalpy_eqn; }
     int boussinesq() const { return p.vii[16]; }
     int kgc_solve() const { return p.vii[17]; }
     int turb() const { return p.vii[18]; }
@@ -185,18 +186,42 @@ struct State {
 
 template <class Real>
 struct P2State {
-    std::vector<Real> rho_ref, SR, x0, y0, z0, ux0, uy0, uz0, temp0, concn0;
+    std::vector<Real> rho_ref, SR, x0, y0, z0, ux0, uy0, uz0, temp0, concn0, enthalpy0;
     void resize(int n) {
-        for (auto *v : {&rho_ref, &SR, &x0, &y0, &z0, &ux0, &uy0, &uz0, &temp0, &concn0}) v->assign(n, Real(0));
+        for (auto *v : {&rho_ref, &SR, &x0, &y0, &z0, &ux0, &uy0, &uz0, &temp0, &concn0, &enthalpy0})
+            v->assign(n, Real(0));
     }
 };
 
+// htoT with the built-in corium table (functions_PROP.cuh:43-67, the
+// prop_table = 0 branch) and its interp2 (functions_PROP.cuh:8-41), in the
+// reference's Real arithmetic: linear inside the table, the end segments
+// extended outside it
+template <class Real>
+static Real htoT(Real h) {
+    static const Real xd[5] = {Real(-554932), Real(215789), Real(757894), Real(905263), Real(1268421)};
+    static const Real yd[5] = {Real(280), Real(1537), Real(2300), Real(2450), Real(2650)};
+    auto seg = [&](int a) {
+        Real y = yd[a + 1] - yd[a];
+        y /= (xd[a + 1] - xd[a]);
+        y *= (h - xd[a]);
+        y += yd[a];
+        return y;
+    };
+    if (xd[4] < h) return seg(3);
+    if (h <= xd[0]) return seg(0);
+    for (int a = 0; a < 4; ++a)
+        if (xd[a] < h && h <= xd[a + 1]) return seg(a);
+    return yd[4];
+}
+
 template <class Real>
 struct P3State {
-    std::vector<Real> ftx, fty, ftz, ft, fpx, fpy, fpz, dtemp, dconcn, nx, ny, nz, gxx, gyy, gzz, gxy, gyz, gzx;
+    std::vector<Real> ftx, fty, ftz, ft, fpx, fpy, fpz, dtemp, dconcn, denthalpy, nx, ny, nz, gxx, gyy, gzz, gxy,
+        gyz, gzx;
     void reset(int n) {
-        for (auto *v : {&ftx, &fty, &ftz, &ft, &fpx, &fpy, &fpz, &dtemp, &dconcn, &nx, &ny, &nz, &gxx, &gyy,
-                        &gzz, &gxy, &gyz, &gzx})
+        for (auto *v : {&ftx, &fty, &ftz, &ft, &fpx, &fpy, &fpz, &dtemp, &dconcn, &denthalpy, &nx, &ny, &nz, &gxx,
+                        &gyy, &gzz, &gxy, &gyz, &gzx})
             v->assign(n, Real(0));
     }
 };
@@ -771,7 +796,10 @@ struct Oracle {
             if (bsq && ptypei > 0 && ptypei < 1000) tz = betai * GRAV * (tmp_temp / tmp_flt - TEMPB);
             S3.ftx[i] = tx - ex; S3.fty[i] = ty - ey; S3.ftz[i] = tz - ez;
             S3.ft[i] = std::sqrt(tx * tx + ty * ty + tz * tz);
-            if (con) S3.dtemp[i] += tmp_Rc / cpi - eulert;
+            if (con) {   // functions_PPE.cuh:460-468
+                if (Q.enthalpy_eqn()) S3.denthalpy[i] = tmp_Rc * (ptypei != -1);
+                else S3.dtemp[i] += tmp_Rc / cpi - eulert;
+            }
             if (cnc) S3.dconcn[i] = tmp_Rd;
         }
     }
@@ -800,7 +828,15 @@ struct Oracle {
                 S2.ux0[i] = tux0; S2.uy0[i] = tuy0; S2.uz0[i] = tuz0;
             }
             if (ttime == 0) S2.rho_ref[i] = A.rho[i];
-            if (q().con_solve() == 1) S2.temp0[i] = A.temp[i];
+            if (q().con_solve() == 1) {   // functions_TIME_ISPH.cuh:89-101
+                if (q().enthalpy_eqn()) {
+                    const Real th = A.enthalpy[i];
+                    S2.enthalpy0[i] = th;
+                    A.temp[i] = htoT<Real>(th);
+                } else {
+                    S2.temp0[i] = A.temp[i];
+                }
+            }
             if (q().concn_solve() == 1) {
                 Real tconcn = A.concn[i];
                 S2.concn0[i] = tconcn;
@@ -1517,8 +1553,13 @@ struct Oracle {
                 if ((uxc * uxc + uyc * uyc + uzc * uzc) >= ul * ul) { uxc = tux0; uyc = tuy0; uzc = tuz0; }
                 T.ux[i] = uxc; T.uy[i] = uyc; T.uz[i] = uzc;
             }
-            if (q().con_solve() == 1) {
-                T.temp[i] = S2.temp0[i] + S3.dtemp[i] * tdt * (bt == 0);
+            if (q().con_solve() == 1) {   // functions_TIME_ISPH.cuh:203-215
+                if (q().enthalpy_eqn()) {
+                    T.enthalpy[i] = S2.enthalpy0[i] + S3.denthalpy[i] * tdt;
+                    T.temp[i] = S.temp[i];
+                } else {
+                    T.temp[i] = S2.temp0[i] + S3.dtemp[i] * tdt * (bt == 0);
+                }
             } else {
                 T.enthalpy[i] = S.enthalpy[i];
                 T.temp[i] = S.temp[i];
@@ -1673,14 +1714,14 @@ struct Oracle {
                 r.SR = S2.SR.empty() ? 0 : S2.SR[i];
                 r.x0 = S2.x0[i]; r.y0 = S2.y0[i]; r.z0 = S2.z0[i];
                 r.ux0 = S2.ux0[i]; r.uy0 = S2.uy0[i]; r.uz0 = S2.uz0[i];
-                r.temp0 = S2.temp0[i]; r.concn0 = S2.concn0[i];
+                r.temp0 = S2.temp0[i]; r.concn0 = S2.concn0[i]; r.enthalpy0 = S2.enthalpy0[i];
             }
             if (C) {
                 sph_part3 &r = C[i];
                 std::memset(&r, 0, sizeof(r));
                 r.ftotalx = S3.ftx[i]; r.ftotaly = S3.fty[i]; r.ftotalz = S3.ftz[i]; r.ftotal = S3.ft[i];
                 r.fpx = S3.fpx[i]; r.fpy = S3.fpy[i]; r.fpz = S3.fpz[i]; r.dtemp = S3.dtemp[i];
-                r.dconcn = S3.dconcn[i];
+                r.dconcn = S3.dconcn[i]; r.denthalpy = S3.denthalpy[i];
                 r.nx = S3.nx[i]; r.ny = S3.ny[i]; r.nz = S3.nz[i];
                 r.inv_cm_xx = S3.gxx[i]; r.inv_cm_yy = S3.gyy[i]; r.inv_cm_zz = S3.gzz[i];
                 r.inv_cm_xy = S3.gxy[i]; r.inv_cm_yz = S3.gyz[i]; r.inv_cm_zx = S3.gzx[i];

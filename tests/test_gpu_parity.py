@@ -160,6 +160,24 @@ def test_thermal_step_matches_oracle(name, precision, tol):
         assert np.abs(B3["dconcn"][fluid]).max() > 0
 
 
+@pytest.mark.parametrize("precision,tol", [(layout.PREC_MIXED, FP32_TOL), (layout.PREC_FP64, FP64_TOL)],
+                         ids=["fp32", "fp64"])
+def test_enthalpy_form_step_matches_oracle(precision, tol):
+    """enthalpy_eqn = 1 (the reference's compiled-out enthalpy form; the
+    oracle is bit-exact against the reference built with it,
+    tests/test_oracle.py): the enthalpy rate, enthalpy0, the htoT
+    temperature and the enthalpy update within the step bar."""
+    P, p = decks.enthalpy_mini()
+    A, A2, A3, B, B2, B3 = _run_pair(P, p, precision, nsteps=3)
+    lim = FP64_MOST_TOL if precision == layout.PREC_FP64 else tol
+    errs = {f: rel_err(A[f], B[f]) for f in FIELDS + ["concn", "enthalpy"]}
+    bad = {f: e for f, e in errs.items() if e > lim}
+    assert not bad, bad
+    assert rel_err(A3["denthalpy"], B3["denthalpy"]) <= stored_tol(B3["denthalpy"], lim * 10)
+    assert rel_err(A2["enthalpy0"], B2["enthalpy0"]) <= stored_tol(B2["enthalpy0"], lim)
+    assert np.abs(B3["denthalpy"][B["p_type"] == 1]).max() > 0
+
+
 BOUNDARY = {"extrapolation": (layout.OUTLET_EXTRAPOLATION, 0), "inout": (layout.OUTLET_INOUT, 0),
             "recycling_probe": (layout.OUTLET_DONOTHING, 1), "inout_recycling_probe": (layout.OUTLET_INOUT, 1)}
 

@@ -183,6 +183,34 @@ def test_thermal_step_bit_exact_vs_reference(name):
         assert np.abs(B3["dconcn"][fluid]).max() > 0
 
 
+@pytest.mark.skipif(not refhost.available("enth"), reason="reference host build (enthalpy form) absent")
+def test_enthalpy_form_bit_exact_vs_reference():
+    """enthalpy_eqn = 1 against the reference compiled with its own
+    `#define enthalpy_eqn 1`: the enthalpy rate of the conduction sum, the
+    projection's enthalpy0 and htoT temperature, the time update of the
+    enthalpy."""
+    P, p = decks.enthalpy_mini()
+    R = refhost.RefHost(P, p, parallel=False, variant="enth")
+    O = restated.Restated(P, p, 0)
+    for _ in range(3):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, B2, B3 = O.download()
+    for f in FIELDS + ["concn", "enthalpy"]:
+        assert np.array_equal(R.P1[f], B[f]), f
+    for f in ("ftotalx", "ftotaly", "ftotalz", "ftotal", "denthalpy", "dconcn"):
+        assert np.array_equal(R.P3[f], B3[f]), f
+    for f in ("enthalpy0", "concn0"):
+        assert np.array_equal(R.SP2[f], B2[f]), f
+    fluid = B["p_type"] == 1
+    assert np.abs(B3["denthalpy"][fluid]).max() > 0
+    # inside the domain (no outlet or side copy) the temperature is the
+    # table's at the projection's enthalpy
+    inner = fluid & (B["buffer_type"] == 0)
+    t = np.interp(B2["enthalpy0"][inner].astype(np.float64), decks.CORIUM_H, decks.CORIUM_T)
+    assert np.allclose(B["temp"][inner], t, rtol=1e-5)
+
+
 BOUNDARY = {"extrapolation": (layout.OUTLET_EXTRAPOLATION, 0), "inout": (layout.OUTLET_INOUT, 0),
             "recycling": (layout.OUTLET_DONOTHING, 1), "inout_recycling": (layout.OUTLET_INOUT, 1)}
 

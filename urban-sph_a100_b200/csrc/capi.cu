@@ -38,6 +38,7 @@ DevParams make_dev_params(const sph_params &p) {
     d.outlet_bc = p.outlet_bc;
     d.ppe_pair_h = p.ppe_pair_h;
     d.pforce_form = p.pressure_force_form;
+    d.enthalpy_eqn = p.enthalpy_eqn;
     d.inlet_recycling = p.inlet_recycling;
     d.rp_x = p.recycle_probe_x; d.rp_y = p.recycle_probe_y;
     for (int a = 0; a < 6; ++a) d.periodic_box[a] = p.periodic_box[a];
@@ -78,9 +79,10 @@ static int check_params(const sph_params &p) {
     if (p.n_profile < 2 || p.n_profile > SPH_MAX_PROFILE) { set_error("n_profile must be in [2, 32]"); return SPH_ERR_BAD_ARG; }
     if (!(p.vif[SPH_VIF_DT] > 0)) { set_error("dt must be positive"); return SPH_ERR_BAD_ARG; }
     if (p.outlet_bc < 0 || p.outlet_bc > 2) { set_error("outlet_bc must be 0, 1 or 2"); return SPH_ERR_BAD_ARG; }
-    if (p.ppe_coarse_max < 0 || p.ppe_coarse_max > 32768 || p.reserved0 != 0) {
-        set_error("ppe_coarse_max must be in [0, 32768] and reserved0 0"); return SPH_ERR_BAD_ARG;
+    if (p.ppe_coarse_max < 0 || p.ppe_coarse_max > 32768) {
+        set_error("ppe_coarse_max must be in [0, 32768]"); return SPH_ERR_BAD_ARG;
     }
+    if (p.enthalpy_eqn < 0 || p.enthalpy_eqn > 1) { set_error("enthalpy_eqn must be 0 or 1"); return SPH_ERR_BAD_ARG; }
     if (p.pressure_force_form < 0 || p.pressure_force_form > 1) {
         set_error("pressure_force_form must be 0 or 1"); return SPH_ERR_BAD_ARG;
     }

@@ -37,6 +37,7 @@ struct DevParams {
     int outlet_bc, inlet_recycling;
     int ppe_pair_h;        // 1: pair-averaged h in the pressure system
     int pforce_form;       // pressure-force pair term: 0 the reference's active form, 1 difference form
+    int enthalpy_eqn;      // 1: the energy equation in enthalpy (with con_solve)
     double rp_x, rp_y;     // recycling probe
     double periodic_box[6];   // x0,x1,y0,y1,z0,z1 of the periodic box (ghost partners)
     float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, dt_structure;

@@ -120,6 +120,8 @@ struct Ctx {
     Real *dconcn = nullptr; // P3: dconcn (concn_solve)
     Real *temp0 = nullptr;  // SP2: temp0 (con_solve), concn0 (concn_solve)
     Real *concn0 = nullptr;
+    Real *enth0 = nullptr;  // SP2: enthalpy0 (con_solve with enthalpy_eqn)
+    Real *denth = nullptr;  // P3: denthalpy
     R4 *nrm = nullptr;      // P3: nx, ny, nz
     float *us_update = nullptr;   // u* of the recycling probe, kept across steps
     Real *g6 = nullptr;     // inv_cm: 6 arrays of n (xx, yy, zz, xy, yz, zx)

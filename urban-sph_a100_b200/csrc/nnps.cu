@@ -160,7 +160,7 @@ __global__ void k_pack(Ctx<Real> c, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3,
             r.x0 = (float)x.x; r.y0 = (float)x.y; r.z0 = (float)x.z;
         }
         r.ux0 = (float)u0.x; r.uy0 = (float)u0.y; r.uz0 = (float)u0.z;
-        r.temp0 = (float)c.temp0[i]; r.concn0 = (float)c.concn0[i];
+        r.temp0 = (float)c.temp0[i]; r.concn0 = (float)c.concn0[i]; r.enthalpy0 = (float)c.enth0[i];
         P2[i] = r;
     }
     if (P3) {
@@ -171,6 +171,7 @@ __global__ void k_pack(Ctx<Real> c, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3,
         r.fpx = (float)fp.x; r.fpy = (float)fp.y; r.fpz = (float)fp.z;
         r.dtemp = (float)c.dtemp[i];
         r.dconcn = (float)c.dconcn[i];
+        r.denthalpy = (float)c.denth[i];
         r.nx = (float)nr.x; r.ny = (float)nr.y; r.nz = (float)nr.z;
         const size_t N = (size_t)c.n;
         r.inv_cm_xx = (float)c.g6[i]; r.inv_cm_yy = (float)c.g6[N + i]; r.inv_cm_zz = (float)c.g6[2 * N + i];
@@ -201,6 +202,7 @@ int ctx_allocate(Ctx<Real> &c) {
     SPH_TRY(c.alloc(c.u0, n)); SPH_TRY(c.alloc(c.ft, n)); SPH_TRY(c.alloc(c.fp, n));
     SPH_TRY(c.alloc(c.dtemp, n)); SPH_TRY(c.alloc(c.nrm, n)); SPH_TRY(c.alloc(c.g6, 6 * (size_t)n));
     SPH_TRY(c.alloc(c.dconcn, n)); SPH_TRY(c.alloc(c.temp0, n)); SPH_TRY(c.alloc(c.concn0, n));
+    SPH_TRY(c.alloc(c.enth0, n)); SPH_TRY(c.alloc(c.denth, n));
     SPH_TRY(c.alloc(c.us_update, 1));
     SPH_CUDA_TRY(cudaMemsetAsync(c.us_update, 0, sizeof(float), c.stream));
     SPH_TRY(c.alloc(c.key, n)); SPH_TRY(c.alloc(c.perm, n)); SPH_TRY(c.alloc(c.g_idx, n));

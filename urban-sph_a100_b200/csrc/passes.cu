@@ -69,6 +69,7 @@ __global__ void k_begin_step(Ctx<Real> c) {
     c.u0[i] = z; c.ft[i] = z; c.fp[i] = z; c.nrm[i] = z;
     c.dtemp[i] = 0;
     c.dconcn[i] = 0; c.temp0[i] = 0; c.concn0[i] = 0;
+    c.enth0[i] = 0; c.denth[i] = 0;
 }
 
 // KERNEL_clc_IB_normal_vector3D, functions_PREP.cuh:923-1015 (step 0 only)
@@ -542,7 +543,7 @@ __global__ void k_neumann_scatter(const int *rows, int nrows, const Real *in_p, 
 // ---------------------------------------------------------------------------
 struct Scalars {
     const void *temp, *concn;
-    void *dtemp, *dconcn;
+    void *dtemp, *dconcn, *denth;
 };
 
 __device__ __forceinline__ float th_k(int pt) {      // Solid_k / Air_k
@@ -661,11 +662,38 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
     if (P.fg_solve) tz += (Real)-9.810;
     if (bsq && ti.w < 1000) tz = (Real)(1.0 / P.t_ini) * (Real)9.810 * (btemp / bflt - (Real)300);   // tempb 300 K
     ft[i] = mk4<Real>(tx - ex, ty_ - ey, tz - ez, sqrt(tx * tx + ty_ * ty_ + tz * tz));
-    if (con) {
-        Real *dtemp = (Real *)sc.dtemp;
-        dtemp[i] += Rc / (Real)th_cp(ti.w) - eulert;
+    if (con) {   // functions_PPE.cuh:460-468
+        if (P.enthalpy_eqn) ((Real *)sc.denth)[i] = Rc * (Real)(ti.w != -1);
+        else ((Real *)sc.dtemp)[i] += Rc / (Real)th_cp(ti.w) - eulert;
     }
     if (cnc) ((Real *)sc.dconcn)[i] = Rd;
+}
+
+// htoT of the enthalpy form with the reference's built-in corium table
+// (functions_PROP.cuh:43-67, prop_table = 0) and its interp2 (:8-41): linear
+// inside the table, the end segments extended outside it, each step of the
+// segment formula rounded as the reference's Real arithmetic rounds it
+template <class Real>
+__device__ __forceinline__ Real seg_rn(Real y0, Real y1, Real x0, Real x1, Real x);
+template <>
+__device__ __forceinline__ float seg_rn<float>(float y0, float y1, float x0, float x1, float x) {
+    return __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(y1, y0), __fsub_rn(x1, x0)), __fsub_rn(x, x0)), y0);
+}
+template <>
+__device__ __forceinline__ double seg_rn<double>(double y0, double y1, double x0, double x1, double x) {
+    return __dadd_rn(__dmul_rn(__ddiv_rn(__dsub_rn(y1, y0), __dsub_rn(x1, x0)), __dsub_rn(x, x0)), y0);
+}
+template <class Real>
+__device__ Real corium_htoT(Real h) {
+    const Real xd[5] = {(Real)-554932, (Real)215789, (Real)757894, (Real)905263, (Real)1268421};
+    const Real yd[5] = {(Real)280, (Real)1537, (Real)2300, (Real)2450, (Real)2650};
+    int a = 0;
+    if (xd[4] < h) a = 3;
+    else if (h <= xd[0]) a = 0;
+    else
+        for (int q = 0; q < 4; ++q)
+            if (xd[q] < h && h <= xd[q + 1]) { a = q; break; }
+    return seg_rn<Real>(yd[a], yd[a + 1], xd[a], xd[a + 1], h);
 }
 
 // ---------------------------------------------------------------------------
@@ -675,8 +703,8 @@ template <class Real>
 __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::type *u,
                              typename V4<Real>::type *u0, const typename V4<Real>::type *ft,
                              const typename V4<Real>::type *fm, Real *rho_ref, const typename V2<Real>::type *mr,
-                             const Real *temp, Real *temp0, Real *concn, Real *concn0, const Real *dconcn,
-                             Real tdt, const StepClock *clk, int n) {
+                             Real *temp, Real *temp0, Real *concn, Real *concn0, const Real *dconcn,
+                             const Real *enth, Real *enth0, Real tdt, const StepClock *clk, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float ttime = clk->time;
@@ -700,7 +728,15 @@ __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::typ
     }
     u[i] = ui;
     if (ttime == 0) rho_ref[i] = mr[i].y;
-    if (P.con_solve == 1) temp0[i] = temp[i];
+    if (P.con_solve == 1) {   // functions_TIME_ISPH.cuh:89-101
+        if (P.enthalpy_eqn) {
+            const Real h = enth[i];
+            enth0[i] = h;
+            temp[i] = corium_htoT<Real>(h);
+        } else {
+            temp0[i] = temp[i];
+        }
+    }
     if (P.concn_solve == 1) {
         const Real cc = concn[i];
         concn0[i] = cc;
@@ -1121,7 +1157,10 @@ __global__ void k_time_update(Ctx<Real> c, Real tdt) {
     ua.w = us.w;   // vis_t
     A.u[i] = ua;
     Real temp = S.temp[i];
-    if (P.con_solve == 1) temp = c.temp0[i] + c.dtemp[i] * tdt * (Real)(t.y == 0);
+    if (P.con_solve == 1) {   // functions_TIME_ISPH.cuh:203-215
+        if (P.enthalpy_eqn) A.enth[i] = c.enth0[i] + c.denth[i] * tdt;   // the temperature stays the projection's
+        else temp = c.temp0[i] + c.dtemp[i] * tdt * (Real)(t.y == 0);
+    }
     if (t.w == 0) {
         const double tt = (double)(tdt * (Real)tcount);
         if (tt >= P.t_start && tt < P.t_con_t) temp = (Real)(P.t_ini + tt * (P.t_con - P.t_ini) / (P.t_con_t - P.t_start));
@@ -1357,7 +1396,7 @@ int phase_interaction(Ctx<Real> &c) {
         ++c.launches;
     }
     if (tc == 0) SPH_TRY(neumann_pass(c, c.S));
-    const Scalars sc{c.S.temp, c.S.concn, c.dtemp, c.dconcn};
+    const Scalars sc{c.S.temp, c.S.concn, c.dtemp, c.dconcn, c.denth};
     const bool th = c.dp.con_solve != 0 || c.dp.concn_solve != 0 || c.dp.boussinesq != 0;
     const dim3 ga = grid_for(n, c.pair_block);
     if (th) {
@@ -1373,7 +1412,7 @@ int phase_interaction(Ctx<Real> &c) {
     if (c.dp.time_type == 1) {
         k_projection<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.ty, c.S.u, c.u0, c.ft, c.S.fm, c.rho_ref_S, c.mr,
                                                              c.S.temp, c.temp0, c.S.concn, c.concn0, c.dconcn,
-                                                             tdt, c.clk, n);
+                                                             c.S.enth, c.enth0, tdt, c.clk, n);
         ++c.launches;
     }
     SPH_TRY(periodic_pass(c, c.S));

@@ -163,6 +163,23 @@ def thermal_mini(con=1, bouss=1, concn=1, seed=11, nx=12, ny=6, nz=5):
     return P, p
 
 
+# the reference's built-in corium table (functions_PROP.cuh:67-70): enthalpy
+# [J/kg] against temperature [K], the one htoT reads with prop_table = 0
+CORIUM_H = np.array([-554932, 215789, 757894, 905263, 1268421], np.float32)
+CORIUM_T = np.array([280, 1537, 2300, 2450, 2650], np.float32)
+
+
+def enthalpy_mini(seed=11):
+    """thermal_mini with the energy equation in enthalpy (enthalpy_eqn = 1)
+    and every record's enthalpy on the corium table at its temperature: the
+    reference reads no enthalpy from its decks and keeps its
+    temperature-to-enthalpy kernel commented out, so the caller sets it."""
+    P, p = thermal_mini(1, 1, 1, seed=seed)
+    P["enthalpy"] = np.interp(P["temp"].astype(np.float64), CORIUM_T, CORIUM_H).astype(np.float32)
+    p.enthalpy_eqn = 1
+    return P, p
+
+
 def with_headroom(P, p, frac):
     """Appends int(frac * len(P)) free dummy records (i_type 3), the room the
     reference reserves for buffer and APR particles (ISPH.cuh:116)."""

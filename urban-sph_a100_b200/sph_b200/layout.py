@@ -126,7 +126,7 @@ class SphParams(ctypes.Structure):
         ("pressure_force_form", ctypes.c_int32),
         ("ppe_coef_half", ctypes.c_int32),
         ("ppe_coarse_max", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("enthalpy_eqn", ctypes.c_int32),
         ("ppe_inner_tol", ctypes.c_double),
         ("apr_zone", ctypes.c_double),
         ("recycle_probe_x", ctypes.c_double), ("recycle_probe_y", ctypes.c_double),
