@@ -258,7 +258,9 @@ typedef struct sph_params {
                                 conduction sum is the enthalpy rate, the
                                 projection sets enthalpy0 and the temperature
                                 htoT(enthalpy) from the built-in corium table
-                                (functions_PROP.cuh:43-67), the time update
+                                (functions_PROP.cuh:43-67), or with
+                                vii[prop_table] = 1 from the tables of
+                                sph_set_prop_tables, the time update
                                 advances the enthalpy; 0 (default) the
                                 temperature form                              */
     double  ppe_inner_tol;   /* inner FP32 tolerance of the restarted
@@ -423,6 +425,50 @@ int sph_read_deck(const char *path, sph_part1 *out, int capacity, int *n);
  * ISPH_Calc.cuh:366), change nothing.  plot-variables labels go to
  * plot_labels (20 x 20 chars, may be NULL), their count to *n_labels. */
 int sph_read_solv(const char *path, sph_params *p, char *plot_labels, int *n_labels);
+
+/* ---- property tables: host_Tab_* / host_table_index / host_table_size ----
+ * (SOPHIA_gpu.cu:51-78, table_size 50 of Parameters.cuh:66).  Table t holds
+ * entries index[t] .. index[t] + size[t] - 1 of each column and belongs to
+ * the records with |p_type| = t. */
+#define SPH_TABLE_SIZE  50
+#define SPH_TABLE_SLOTS 10
+typedef struct sph_prop_tables {
+    int32_t n_tables;                 /* number_of_tables                     */
+    int32_t n_data;                   /* data_numbers: entries in use          */
+    int32_t index[SPH_TABLE_SLOTS];   /* host_table_index (0 past n_tables)    */
+    int32_t size[SPH_TABLE_SLOTS];    /* host_table_size (0 past n_tables)     */
+    double T[SPH_TABLE_SIZE], h[SPH_TABLE_SIZE], k[SPH_TABLE_SIZE];
+    double cp[SPH_TABLE_SIZE], mu[SPH_TABLE_SIZE];   /* unset entries 0      */
+} sph_prop_tables;                    /* 2088 bytes */
+
+/* read_table (function_init.cuh:724-905), the file the reference reads as
+ * input/data.txt (SOPHIA_gpu.cu:127-132): lines of at most 999 characters;
+ * a line whose first space-separated token begins with `#p_type` opens table
+ * number atoi(next token); inside it, a line whose first token begins with
+ * `//T`, `//h`, `//k`, `//c` or `//m` (the reference compares three
+ * characters of //T, //h, //k, //cp, //mu) is followed by one line of
+ * comma-separated values (atof of every token, so a trailing comma adds a
+ * 0), and a line beginning `#end` closes the table; other lines are skipped.
+ * Every table's size is the value count of its last column line and the
+ * tables are laid end to end in file order.  Where the reference's arrays or
+ * arithmetic would be undefined the call returns SPH_ERR_BAD_ARG: a table
+ * number other than 0, 1, 2, ... in file order (index and size come from the
+ * cumulative counts of tables 0 .. n-1), more than SPH_TABLE_SLOTS tables, a
+ * table with no column line or with column lines of different lengths, more
+ * than SPH_TABLE_SIZE entries in all, a table left open at the end of the
+ * file, or `#p_type` with no number. */
+int sph_read_table(const char *path, sph_prop_tables *out);
+
+/* The upload of the tables (ISPH_Calc.cuh:370-377) to the context, rounded
+ * to its precision.  With vii[prop_table] = 1 (and con_solve = 1,
+ * enthalpy_eqn = 1) the projection's htoT interpolates table |p_type| (h to
+ * T, functions_PROP.cuh:43-67 with interp2 of :8-41) instead of the built-in
+ * corium table; a step then needs tables set, and every record the
+ * projection reaches (i_type < 3, p_type < 1000) needs |p_type| below
+ * SPH_TABLE_SLOTS with a table of at least two entries (SPH_ERR_BAD_ARG
+ * otherwise).  Rejected: sizes outside 0..SPH_TABLE_SIZE, an index + size
+ * past SPH_TABLE_SIZE. */
+int sph_set_prop_tables(sph_ctx *ctx, const sph_prop_tables *t);
 /* The host pass the reference runs on deck records before upload
  * (c_initial_inner_outer_particle_single, functions_NNPS.cuh:196-373), in
  * place: i_type 1, buffer_type 0, m_ref = m, uy = uz = 0, temp 300,

@@ -383,4 +383,26 @@ void ref_save_vtk(part1 *P1, part2 *P2, part3 *P3, int n, int step, const char *
     save_vtk_bin_single_flag(P1, P2, P3);
 }
 
+// read_table (function_init.cuh:724-905) on the given file, then the upload
+// of ISPH_Calc.cuh:370-377 into the k_Tab_* arrays the device code reads.
+// cols receives T, h, k, cp, mu (table_size entries each, as stored in Real).
+// The arrays are cleared first, so entries past the file's stay 0.
+void ref_read_table(const char *path, double *cols, int *index, int *size) {
+    Real *tabs[5] = {host_Tab_T, host_Tab_h, host_Tab_k, host_Tab_cp, host_Tab_vis};
+    for (Real *t : tabs) std::fill(t, t + table_size, Real(0));
+    std::fill(host_table_index, host_table_index + 10, 0);
+    std::fill(host_table_size, host_table_size + 10, 0);
+    read_table(path);
+    for (int c = 0; c < 5; ++c)
+        for (int k = 0; k < table_size; ++k) cols[c * table_size + k] = (double)tabs[c][k];
+    for (int k = 0; k < 10; ++k) { index[k] = host_table_index[k]; size[k] = host_table_size[k]; }
+    std::copy(host_Tab_T, host_Tab_T + table_size, k_Tab_T);
+    std::copy(host_Tab_h, host_Tab_h + table_size, k_Tab_h);
+    std::copy(host_Tab_k, host_Tab_k + table_size, k_Tab_k);
+    std::copy(host_Tab_cp, host_Tab_cp + table_size, k_Tab_cp);
+    std::copy(host_Tab_vis, host_Tab_vis + table_size, k_Tab_vis);
+    std::copy(host_table_index, host_table_index + 10, k_table_index);
+    std::copy(host_table_size, host_table_size + 10, k_table_size);
+}
+
 }  // extern "C"

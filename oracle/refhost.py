@@ -47,6 +47,22 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def read_table(path, variant=None):
+    """The reference's read_table on `path` (and its upload to the arrays
+    the device code reads): {"T", "h", "k", "cp", "mu"} as stored in Real
+    (table_size entries each), index and size per slot."""
+    L = lib(variant)
+    L.ref_read_table.argtypes = [ctypes.c_char_p] + [ctypes.c_void_p] * 3
+    L.ref_read_table.restype = None
+    cols = np.zeros((5, 50), np.float64)
+    index = np.zeros(10, np.int32)
+    size = np.zeros(10, np.int32)
+    L.ref_read_table(str(path).encode(), _p(cols), _p(index), _p(size))
+    out = dict(zip(("T", "h", "k", "cp", "mu"), cols))
+    out["index"], out["size"] = index, size
+    return out
+
+
 class RefHost:
     """Reference step on the host, one instance per deck."""
 

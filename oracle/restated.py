@@ -30,6 +30,7 @@ def lib():
         L.orc_step.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp, vp]
         L.orc_pin_row.argtypes = [vp]
         L.orc_download.argtypes = [vp] * 4
+        L.orc_set_tables.argtypes = [vp, vp]
         _lib = L
     return _lib
 
@@ -83,6 +84,10 @@ class Restated:
         for _ in range(nsteps):
             st = lib().orc_step(self.h, mode, tol, maxit, ctypes.byref(rr), ctypes.byref(it))
         return st, rr.value, it.value
+
+    def set_tables(self, tables):
+        """Property tables (a PropTables) for htoT with vii[prop_table] = 1."""
+        lib().orc_set_tables(self.h, ctypes.byref(tables))
 
     def pin_row(self):
         return lib().orc_pin_row(self.h)

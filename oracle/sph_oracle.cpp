@@ -27,6 +27,7 @@
 #include <cstring>
 #include <functional>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "sph_isph.h"
@@ -44,6 +45,7 @@ struct P {
     int fg_solve() const { return p.vii[14]; }
     int con_solve() const { return p.vii[15]; }
     int enthalpy_eqn() const { return p.enthalpy_eqn; }
+    int prop_table() const { return p.vii[2]; }
     int boussinesq() const { return p.vii[16]; }
     int kgc_solve() const { return p.vii[17]; }
     int turb() const { return p.vii[18]; }
@@ -193,26 +195,48 @@ struct P2State {
     }
 };
 
-// htoT with the built-in corium table (functions_PROP.cuh:43-67, the
-// prop_table = 0 branch) and its interp2 (functions_PROP.cuh:8-41), in the
-// reference's Real arithmetic: linear inside the table, the end segments
-// extended outside it
+// interp2 (functions_PROP.cuh:8-41) over n >= 2 points, in the reference's
+// Real arithmetic: linear inside the table, the end segments extended
+// outside it.  The reference's search loop also tests the pair (n-1, n),
+// one entry past the table, but only for an x it cannot bracket, which a
+// table with increasing x_data does not leave (NaN x leaves its result
+// unset; here it is the last value).
 template <class Real>
-static Real htoT(Real h) {
-    static const Real xd[5] = {Real(-554932), Real(215789), Real(757894), Real(905263), Real(1268421)};
-    static const Real yd[5] = {Real(280), Real(1537), Real(2300), Real(2450), Real(2650)};
+static Real interp2(const Real *xd, const Real *yd, int n, Real x) {
     auto seg = [&](int a) {
         Real y = yd[a + 1] - yd[a];
         y /= (xd[a + 1] - xd[a]);
-        y *= (h - xd[a]);
+        y *= (x - xd[a]);
         y += yd[a];
         return y;
     };
-    if (xd[4] < h) return seg(3);
-    if (h <= xd[0]) return seg(0);
-    for (int a = 0; a < 4; ++a)
-        if (xd[a] < h && h <= xd[a + 1]) return seg(a);
-    return yd[4];
+    const int e = n - 1;
+    if (xd[e] < x) return seg(e - 1);
+    if (x <= xd[0]) return seg(0);
+    for (int a = 0; a < e; ++a)
+        if (xd[a] < x && x <= xd[a + 1]) return seg(a);
+    return yd[e];
+}
+
+// htoT (functions_PROP.cuh:43-67): with prop_table = 0 the built-in corium
+// table, with prop_table = 1 table |p_type| of the property tables (the
+// device copies k_Tab_h / k_Tab_T at k_table_index, k_table_size).  A slot
+// without a table of two entries leaves the temperature as it was (the
+// library refuses such a step before it runs).
+template <class Real>
+struct PropTables {
+    bool set = false;
+    Real h[SPH_TABLE_SIZE] = {}, T[SPH_TABLE_SIZE] = {};
+    int index[SPH_TABLE_SLOTS] = {}, size[SPH_TABLE_SLOTS] = {};
+};
+template <class Real>
+static Real htoT(Real h, int p_type, bool prop_table, const PropTables<Real> &tab, Real keep) {
+    static const Real xd[5] = {Real(-554932), Real(215789), Real(757894), Real(905263), Real(1268421)};
+    static const Real yd[5] = {Real(280), Real(1537), Real(2300), Real(2450), Real(2650)};
+    if (!prop_table) return interp2<Real>(xd, yd, 5, h);
+    const int t = p_type < 0 ? -p_type : p_type;
+    if (t >= SPH_TABLE_SLOTS || tab.size[t] < 2) return keep;
+    return interp2<Real>(tab.h + tab.index[t], tab.T + tab.index[t], tab.size[t], h);
 }
 
 template <class Real>
@@ -253,6 +277,7 @@ struct Oracle {
     P2State<Real> S2;       // dev_SP2 (P2 keeps only rho_ref between steps)
     std::vector<Real> p2_rho_ref;
     P3State<Real> S3;
+    PropTables<Real> tab;               // k_Tab_h / k_Tab_T, k_table_index / k_table_size
     std::vector<float> xf, yf, zf, hf;   // FP32 positions / h, sorted (NNPS precision)
     std::vector<int> g_idx, p_idx, g_str, g_end;
     std::vector<int64_t> nb_off;
@@ -832,7 +857,7 @@ struct Oracle {
                 if (q().enthalpy_eqn()) {
                     const Real th = A.enthalpy[i];
                     S2.enthalpy0[i] = th;
-                    A.temp[i] = htoT<Real>(th);
+                    A.temp[i] = htoT<Real>(th, A.p_type[i], q().prop_table() == 1, tab, A.temp[i]);
                 } else {
                     S2.temp0[i] = A.temp[i];
                 }
@@ -1746,6 +1771,22 @@ void *orc_create(const sph_params *p, int precision) {
     if (precision == SPH_PREC_FP64) { h->d = new Oracle<double>(); h->d->prm = *p; h->d->prec = 1; }
     else { h->f = new Oracle<float>(); h->f->prm = *p; h->f->prec = 0; }
     return h;
+}
+
+// the property tables of the enthalpy form's htoT (the upload of
+// ISPH_Calc.cuh:370-377): h and T columns, index and size per slot
+int orc_set_tables(void *hh, const sph_prop_tables *t) {
+    OracleHandle *h = (OracleHandle *)hh;
+    auto go = [&](auto *o) {
+        if (!o) return;
+        typedef typename std::remove_reference<decltype(o->tab.h[0])>::type R;
+        for (int k = 0; k < SPH_TABLE_SIZE; ++k) { o->tab.h[k] = (R)t->h[k]; o->tab.T[k] = (R)t->T[k]; }
+        for (int k = 0; k < SPH_TABLE_SLOTS; ++k) { o->tab.index[k] = t->index[k]; o->tab.size[k] = t->size[k]; }
+        o->tab.set = true;
+    };
+    go(h->f);
+    go(h->d);
+    return SPH_OK;
 }
 
 void orc_destroy(void *hh) {

@@ -135,3 +135,71 @@ def test_initial_records_rejects_short_tables():
     P = S["init_in"].view(layout.PART1)[:4]
     with pytest.raises(abi.SphError):
         abi.initial_records(p, P, k_table=([0.0], [1.0]))
+
+
+T = np.load(os.path.join(HERE, "golden", "table_ref.npz"))
+
+
+def test_read_table_matches_reference_reader(tmp_path):
+    """Columns, table indices and sizes equal what the reference's read_table
+    stored (in Real = float) for the same file; tests/golden/table_ref.npz is
+    made by tests/golden/make_table_golden.py."""
+    for name in T["names"]:
+        name = str(name)
+        path = tmp_path / (name + ".txt")
+        path.write_bytes(T["text_" + name].tobytes())
+        t = abi.read_table(path)
+        assert np.array_equal(np.array(t.index[:]), T["index_" + name]), name
+        assert np.array_equal(np.array(t.size[:]), T["size_" + name]), name
+        for c in ("T", "h", "k", "cp", "mu"):
+            col = np.ctypeslib.as_array(getattr(t, c)).astype(np.float32)
+            assert col.tobytes() == T[c + "_" + name].tobytes(), (name, c)
+        used = np.array(t.size[:]) > 0
+        assert t.n_tables == int(used.sum()) and t.n_data == int(T["size_" + name].sum()), name
+
+
+def test_read_table_columns_by_slot(tmp_path):
+    path = tmp_path / "t.txt"
+    path.write_bytes(T["text_two_materials"].tobytes())
+    t = abi.read_table(path)
+    assert t.n_tables == 2
+    from sph_b200 import decks
+    for k, ref in enumerate((decks.TABLE_WALL, decks.TABLE_FLUID)):
+        for c in ("T", "h", "k", "cp", "mu"):
+            assert np.array_equal(t.column(c, k), ref[c]), (k, c)
+    u = layout.PropTables.from_columns([{c: t.column(c, k) for c in ("T", "h", "k", "cp", "mu")} for k in range(2)])
+    assert bytes(u) == bytes(t)
+
+
+BAD_TABLES = {
+    "out_of_order": "#p_type 1\n//T\n1,2\n//h\n1,2\n#end\n",
+    "skipped_slot": "#p_type 0\n//T\n1,2\n//h\n1,2\n#end\n#p_type 2\n//T\n1,2\n//h\n1,2\n#end\n",
+    "no_number": "#p_type\n//T\n1,2\n#end\n",
+    "unclosed": "#p_type 0\n//T\n1,2\n//h\n1,2\n",
+    "no_columns": "#p_type 0\n# nothing\n#end\n",
+    "ragged": "#p_type 0\n//T\n1,2,3\n//h\n1,2\n#end\n",
+    "too_many_entries": "#p_type 0\n//T\n" + ",".join(["1"] * 51) + "\n#end\n",
+    "eleven_tables": "".join("#p_type {}\n//T\n1,2\n#end\n".format(k) for k in range(11)),
+    "column_at_end": "#p_type 0\n//T\n",
+    "no_value_token": "#p_type 0\n//T\n,,,",
+}
+
+
+@pytest.mark.parametrize("name", list(BAD_TABLES))
+def test_read_table_rejects_what_the_reference_leaves_undefined(tmp_path, name):
+    path = tmp_path / "bad.txt"
+    path.write_text(BAD_TABLES[name])
+    with pytest.raises(abi.SphError):
+        abi.read_table(path)
+
+
+def test_read_table_missing_file_is_an_error(tmp_path):
+    with pytest.raises(abi.SphError):
+        abi.read_table(tmp_path / "absent.txt")
+
+
+def test_read_table_without_tables_is_empty(tmp_path):
+    path = tmp_path / "none.txt"
+    path.write_text("// no tables here\n#end\n")
+    t = abi.read_table(path)
+    assert t.n_tables == 0 and t.n_data == 0 and not any(t.size)

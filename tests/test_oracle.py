@@ -211,6 +211,43 @@ def test_enthalpy_form_bit_exact_vs_reference():
     assert np.allclose(B["temp"][inner], t, rtol=1e-5)
 
 
+@pytest.mark.skipif(not refhost.available("enth"), reason="reference host build (enthalpy form) absent")
+def test_property_tables_bit_exact_vs_reference(tmp_path):
+    """prop_table = 1 with the enthalpy form: the reference (built with
+    enthalpy_eqn 1) reads the two-material table file with its own
+    read_table and interpolates table |p_type| in htoT; the oracle gets the
+    same tables and must agree bit for bit."""
+    P, p, tables = decks.enthalpy_tables_mini()
+    G = np.load(os.path.join(HERE, "golden", "table_ref.npz"))
+    path = tmp_path / "data.txt"
+    path.write_bytes(G["text_two_materials"].tobytes())
+    ref = refhost.read_table(path, "enth")
+    # the deck's tables are the file's (as the reference stored them)
+    assert np.array_equal(ref["index"], np.array(tables.index[:])) and np.array_equal(ref["size"], np.array(tables.size[:]))
+    for c in ("T", "h"):
+        assert np.array_equal(ref[c].astype(np.float32), np.ctypeslib.as_array(getattr(tables, c)).astype(np.float32))
+    R = refhost.RefHost(P, p, parallel=False, variant="enth")
+    O = restated.Restated(P, p, 0)
+    O.set_tables(tables)
+    for _ in range(3):
+        R.step(1)
+        O.step(1, mode=layout.PPE_REF_SWEEP)
+    B, B2, B3 = O.download()
+    for f in FIELDS + ["concn", "enthalpy"]:
+        assert np.array_equal(R.P1[f], B[f]), f
+    assert np.array_equal(R.SP2["enthalpy0"], B2["enthalpy0"])
+    # inside the domain the temperature is table |p_type|'s at enthalpy0,
+    # not the corium table's
+    inner = (B["p_type"] == 1) & (B["buffer_type"] == 0)
+    h0 = B2["enthalpy0"][inner].astype(np.float64)
+    t = np.interp(h0, decks.TABLE_FLUID["h"], decks.TABLE_FLUID["T"])
+    assert np.allclose(B["temp"][inner], t, rtol=1e-5)
+    assert not np.allclose(B["temp"][inner], np.interp(h0, decks.CORIUM_H, decks.CORIUM_T), rtol=1e-5)
+    walls = (B["p_type"] == 0) & (B["i_type"] < 3)
+    hw = B2["enthalpy0"][walls].astype(np.float64)
+    assert (hw < decks.TABLE_WALL["h"][0]).any() and (hw > decks.TABLE_WALL["h"][0]).any()   # both segments met
+
+
 BOUNDARY = {"extrapolation": (layout.OUTLET_EXTRAPOLATION, 0), "inout": (layout.OUTLET_INOUT, 0),
             "recycling": (layout.OUTLET_DONOTHING, 1), "inout_recycling": (layout.OUTLET_INOUT, 1)}
 

@@ -5,6 +5,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 
 #include "ctx.cuh"
 
@@ -39,6 +40,7 @@ DevParams make_dev_params(const sph_params &p) {
     d.ppe_pair_h = p.ppe_pair_h;
     d.pforce_form = p.pressure_force_form;
     d.enthalpy_eqn = p.enthalpy_eqn;
+    d.prop_table = p.vii[SPH_VII_PROP_TABLE] == 1;   // the table slots come from the context
     d.inlet_recycling = p.inlet_recycling;
     d.rp_x = p.recycle_probe_x; d.rp_y = p.recycle_probe_y;
     for (int a = 0; a < 6; ++a) d.periodic_box[a] = p.periodic_box[a];
@@ -83,6 +85,10 @@ static int check_params(const sph_params &p) {
         set_error("ppe_coarse_max must be in [0, 32768]"); return SPH_ERR_BAD_ARG;
     }
     if (p.enthalpy_eqn < 0 || p.enthalpy_eqn > 1) { set_error("enthalpy_eqn must be 0 or 1"); return SPH_ERR_BAD_ARG; }
+    if (p.vii[SPH_VII_PROP_TABLE] < 0 || p.vii[SPH_VII_PROP_TABLE] > 1) {
+        set_error("vii[prop_table] must be 0 (NO) or 1 (YES)");
+        return SPH_ERR_BAD_ARG;
+    }
     if (p.pressure_force_form < 0 || p.pressure_force_form > 1) {
         set_error("pressure_force_form must be 0 or 1"); return SPH_ERR_BAD_ARG;
     }
@@ -205,6 +211,12 @@ int sph_domain_setup(sph_params *p, const sph_part1 *P1, int num_part) {
     return SPH_OK;
 }
 
+// the property-table slots of the context into its device parameters
+template <class Real>
+static void apply_tables(Ctx<Real> &c) {
+    for (int t = 0; t < SPH_TABLE_SLOTS; ++t) { c.dp.tab_index[t] = c.tab_index[t]; c.dp.tab_size[t] = c.tab_size[t]; }
+}
+
 template <class Real>
 static int create_impl(const sph_params *p, int device, void *stream, Ctx<Real> **out) {
     Ctx<Real> *c = new (std::nothrow) Ctx<Real>();
@@ -212,6 +224,7 @@ static int create_impl(const sph_params *p, int device, void *stream, Ctx<Real> 
     c->allocs = new std::vector<void *>();
     c->prm = *p;
     c->dp = make_dev_params(*p);
+    apply_tables(*c);
     c->device = device;
     c->stream = (cudaStream_t)stream;
     c->n = p->vii[SPH_VII_NUM_PART2];
@@ -293,6 +306,7 @@ int sph_set_params(sph_ctx *ctx, const sph_params *p) {
         }
         c->prm = *p;
         c->dp = make_dev_params(*p);
+        apply_tables(*c);
         ++c->param_gen;
         if (recompute && c->built) return build_side_lists(*c);
         return SPH_OK;
@@ -587,6 +601,30 @@ int sph_operator_counts(sph_ctx *ctx, int64_t counts[6]) {
         counts[3] = c->L.nm_nnz;
         counts[4] = c->num_cells;
         counts[5] = (c->list16 && c->prm.ppe_matrix_free == 0) ? 1 : 0;
+        return SPH_OK;
+    };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
+}
+
+int sph_set_prop_tables(sph_ctx *ctx, const sph_prop_tables *t) {
+    if (!ctx || !t) return SPH_ERR_BAD_ARG;
+    for (int k = 0; k < SPH_TABLE_SLOTS; ++k)
+        if (t->size[k] < 0 || t->size[k] > SPH_TABLE_SIZE || t->index[k] < 0 ||
+            t->index[k] + t->size[k] > SPH_TABLE_SIZE) {
+            set_error("sph_set_prop_tables: a table lies outside the SPH_TABLE_SIZE entries");
+            return SPH_ERR_BAD_ARG;
+        }
+    auto go = [&](auto *c) -> int {
+        typedef typename std::remove_pointer<decltype(c->tab)>::type R;
+        R host[2 * SPH_TABLE_SIZE];
+        for (int k = 0; k < SPH_TABLE_SIZE; ++k) { host[k] = (R)t->h[k]; host[SPH_TABLE_SIZE + k] = (R)t->T[k]; }
+        SPH_CUDA_TRY(cudaSetDevice(c->device));
+        // from pageable memory: the copy has taken the values when it returns
+        SPH_CUDA_TRY(cudaMemcpyAsync(c->tab, host, sizeof(host), cudaMemcpyHostToDevice, c->stream));
+        for (int k = 0; k < SPH_TABLE_SLOTS; ++k) { c->tab_index[k] = t->index[k]; c->tab_size[k] = t->size[k]; }
+        c->tab_set = true;
+        apply_tables(*c);
+        ++c->param_gen;
         return SPH_OK;
     };
     return DISPATCH(ctx, go(ctx->f), go(ctx->d));

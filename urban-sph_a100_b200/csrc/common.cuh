@@ -38,6 +38,8 @@ struct DevParams {
     int ppe_pair_h;        // 1: pair-averaged h in the pressure system
     int pforce_form;       // pressure-force pair term: 0 the reference's active form, 1 difference form
     int enthalpy_eqn;      // 1: the energy equation in enthalpy (with con_solve)
+    int prop_table;        // vii[2] = 1: htoT reads the property tables (k_table_index / k_table_size)
+    int tab_index[SPH_TABLE_SLOTS], tab_size[SPH_TABLE_SLOTS];
     double rp_x, rp_y;     // recycling probe
     double periodic_box[6];   // x0,x1,y0,y1,z0,z1 of the periodic box (ghost partners)
     float kappa, skappa, dcell, xmin, xmax, ymin, ymax, zmin, zmax, dt, u_limit, dt_structure;

@@ -123,6 +123,13 @@ struct Ctx {
     Real *enth0 = nullptr;  // SP2: enthalpy0 (con_solve with enthalpy_eqn)
     Real *denth = nullptr;  // P3: denthalpy
     R4 *nrm = nullptr;      // P3: nx, ny, nz
+    // property tables of htoT (k_Tab_h then k_Tab_T, SPH_TABLE_SIZE each),
+    // allocated with the context so that captured steps keep the pointer
+    Real *tab = nullptr;
+    bool tab_set = false;
+    int tab_index[SPH_TABLE_SLOTS] = {}, tab_size[SPH_TABLE_SLOTS] = {};
+    unsigned ptype_slots = 0;     // bit t: a record the projection reaches has |p_type| = t
+    bool ptype_wide = false;      // such a record has |p_type| >= SPH_TABLE_SLOTS
     float *us_update = nullptr;   // u* of the recycling probe, kept across steps
     Real *g6 = nullptr;     // inv_cm: 6 arrays of n (xx, yy, zz, xy, yz, zx)
     // ---- NNPS ----

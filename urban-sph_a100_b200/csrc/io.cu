@@ -326,6 +326,77 @@ extern "C" int sph_read_solv(const char *path, sph_params *p, char *plot_labels,
     return SPH_OK;
 }
 
+// ---- property tables ------------------------------------------------------------
+// read_table (function_init.cuh:724-905): fgets lines of at most 999
+// characters, space-separated first tokens compared by prefix, values split
+// at commas and read by atof, each table as long as its last column line, the
+// tables laid end to end.  The cases the reference leaves undefined (an
+// unnumbered table slot, an uninitialised count, a read past the arrays or
+// past the end of the file) are errors here.
+extern "C" int sph_read_table(const char *path, sph_prop_tables *out) {
+    using namespace sph;
+    if (!path || !out) return SPH_ERR_BAD_ARG;
+    FILE *f = fopen(path, "r");
+    if (!f) { set_error("sph_read_table: cannot open the property table file"); return SPH_ERR_BAD_ARG; }
+    sph_prop_tables t;
+    memset(&t, 0, sizeof(t));
+    double *cols[5] = {t.T, t.h, t.k, t.cp, t.mu};
+    const char *keys[5] = {"//T", "//h", "//k", "//c", "//m"};
+    char line[1000];
+    int data_numbers = 0, ntab = 0;
+    int cum[SPH_TABLE_SLOTS] = {0};
+    const char *err = nullptr;
+    while (!err && fgets(line, sizeof(line), f)) {
+        char *save = nullptr;
+        char *tok = strtok_r(line, " ", &save);
+        if (!tok || strncmp(tok, "#p_type", 7) != 0) continue;
+        tok = strtok_r(nullptr, " ", &save);
+        if (!tok) { err = "#p_type without a table number"; break; }
+        const int number = atoi(tok);
+        if (number != ntab) { err = "tables must be numbered 0, 1, 2, ... in file order"; break; }
+        if (++ntab > SPH_TABLE_SLOTS) { err = "more than SPH_TABLE_SLOTS tables"; break; }
+        int len = -1;   // values per column line of this table
+        for (;;) {
+            if (!fgets(line, sizeof(line), f)) { err = "table left open (no #end)"; break; }
+            if (strncmp(line, "#end", 4) == 0) break;
+            tok = strtok_r(line, " ", &save);
+            if (!tok) continue;
+            int col = -1;
+            for (int c = 0; c < 5; ++c)
+                if (strncmp(tok, keys[c], 3) == 0) { col = c; break; }
+            if (col < 0) continue;
+            if (!fgets(line, sizeof(line), f)) { err = "column line without a value line"; break; }
+            int count = 0;
+            for (tok = strtok_r(line, ",", &save); tok; tok = strtok_r(nullptr, ",", &save)) {
+                if (data_numbers + count >= SPH_TABLE_SIZE) { err = "more than SPH_TABLE_SIZE entries"; break; }
+                cols[col][data_numbers + count] = atof(tok);
+                ++count;
+            }
+            if (err) break;
+            if (count == 0) { err = "empty value line"; break; }
+            if (len >= 0 && count != len) { err = "column lines of one table differ in length"; break; }
+            len = count;
+        }
+        if (err) break;
+        if (len < 0) { err = "table without a column line"; break; }
+        data_numbers += len;
+        cum[number] = data_numbers;
+    }
+    fclose(f);
+    if (err) {
+        set_error((std::string("sph_read_table: ") + err).c_str());
+        return SPH_ERR_BAD_ARG;
+    }
+    t.n_tables = ntab;
+    t.n_data = data_numbers;
+    for (int i = 0; i < ntab; ++i) {
+        t.index[i] = i == 0 ? 0 : cum[i - 1];
+        t.size[i] = cum[i] - t.index[i];
+    }
+    *out = t;
+    return SPH_OK;
+}
+
 // ---- record initialisation -------------------------------------------------------
 // c_initial_inner_outer_particle_single (functions_NNPS.cuh:196-373): the
 // host pass that turns deck records into the records the step starts from.

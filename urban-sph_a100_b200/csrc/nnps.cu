@@ -203,6 +203,8 @@ int ctx_allocate(Ctx<Real> &c) {
     SPH_TRY(c.alloc(c.dtemp, n)); SPH_TRY(c.alloc(c.nrm, n)); SPH_TRY(c.alloc(c.g6, 6 * (size_t)n));
     SPH_TRY(c.alloc(c.dconcn, n)); SPH_TRY(c.alloc(c.temp0, n)); SPH_TRY(c.alloc(c.concn0, n));
     SPH_TRY(c.alloc(c.enth0, n)); SPH_TRY(c.alloc(c.denth, n));
+    SPH_TRY(c.alloc(c.tab, 2 * SPH_TABLE_SIZE));
+    SPH_CUDA_TRY(cudaMemsetAsync(c.tab, 0, sizeof(Real) * 2 * SPH_TABLE_SIZE, c.stream));
     SPH_TRY(c.alloc(c.us_update, 1));
     SPH_CUDA_TRY(cudaMemsetAsync(c.us_update, 0, sizeof(float), c.stream));
     SPH_TRY(c.alloc(c.key, n)); SPH_TRY(c.alloc(c.perm, n)); SPH_TRY(c.alloc(c.g_idx, n));
@@ -232,6 +234,16 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     k_unpack<Real><<<grid_for(n, 256), 256, 0, c.stream>>>(c, d1, P2 ? d2 : nullptr, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
+    // the |p_type| slots htoT can read (records are only ever copied from
+    // these: APR children and merged records keep their p_type)
+    c.ptype_slots = 0;
+    c.ptype_wide = false;
+    for (int i = 0; i < n; ++i) {
+        if (P1[i].i_type >= 3 || P1[i].p_type >= 1000) continue;
+        const int t = P1[i].p_type < 0 ? -P1[i].p_type : P1[i].p_type;
+        if (t < SPH_TABLE_SLOTS) c.ptype_slots |= 1u << t;
+        else c.ptype_wide = true;
+    }
     c.count = c.prm.vii[SPH_VII_COUNT];
     c.time = c.prm.vif[SPH_VIF_TIME];
     c.clk_synced = false;

@@ -696,6 +696,31 @@ __device__ Real corium_htoT(Real h) {
     return seg_rn<Real>(yd[a], yd[a + 1], xd[a], xd[a + 1], h);
 }
 
+// htoT with the property tables (functions_PROP.cuh:43-67, prop_table = 1):
+// interp2 over table |p_type|, whose h and T entries start at
+// tab[index] and tab[SPH_TABLE_SIZE + index].  The host refuses a step in
+// which a record the projection reaches has no table of two entries; a slot
+// without one leaves the temperature as it was.  The reference's search
+// also tests the pair one past the table, but only for an h it cannot
+// bracket, which a table with increasing h does not leave.
+template <class Real>
+__device__ Real table_htoT(const DevParams &P, const Real *tab, int p_type, Real h, Real keep) {
+    const int t = p_type < 0 ? -p_type : p_type;
+    if (t >= SPH_TABLE_SLOTS) return keep;
+    const int n = P.tab_size[t];
+    if (n < 2) return keep;
+    const Real *xd = tab + P.tab_index[t];
+    const Real *yd = tab + SPH_TABLE_SIZE + P.tab_index[t];
+    const int e = n - 1;
+    int a = 0;
+    if (xd[e] < h) a = e - 1;
+    else if (h <= xd[0]) a = 0;
+    else
+        for (int q = 0; q < e; ++q)
+            if (xd[q] < h && h <= xd[q + 1]) { a = q; break; }
+    return seg_rn<Real>(yd[a], yd[a + 1], xd[a], xd[a + 1], h);
+}
+
 // ---------------------------------------------------------------------------
 // KERNEL_clc_projection, functions_TIME_ISPH.cuh:2-112 (predictor)
 // ---------------------------------------------------------------------------
@@ -704,7 +729,8 @@ __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::typ
                              typename V4<Real>::type *u0, const typename V4<Real>::type *ft,
                              const typename V4<Real>::type *fm, Real *rho_ref, const typename V2<Real>::type *mr,
                              Real *temp, Real *temp0, Real *concn, Real *concn0, const Real *dconcn,
-                             const Real *enth, Real *enth0, Real tdt, const StepClock *clk, int n) {
+                             const Real *enth, Real *enth0, const Real *tab, Real tdt, const StepClock *clk,
+                             int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float ttime = clk->time;
@@ -732,7 +758,7 @@ __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::typ
         if (P.enthalpy_eqn) {
             const Real h = enth[i];
             enth0[i] = h;
-            temp[i] = corium_htoT<Real>(h);
+            temp[i] = P.prop_table ? table_htoT<Real>(P, tab, t.w, h, temp[i]) : corium_htoT<Real>(h);
         } else {
             temp0[i] = temp[i];
         }
@@ -1332,8 +1358,31 @@ int freeslip_pass(Ctx<Real> &c, VarSet<Real> &V) {
     return SPH_OK;
 }
 
+// a step whose projection reads the property tables (prop_table = 1 with
+// the enthalpy form, time_type 1) needs a table of two entries for every
+// |p_type| among the records it reaches
+template <class Real>
+static int check_tables(const Ctx<Real> &c) {
+    if (!(c.dp.prop_table && c.dp.con_solve == 1 && c.dp.enthalpy_eqn && c.dp.time_type == 1)) return SPH_OK;
+    if (!c.tab_set) {
+        set_error("prop_table = 1 with the enthalpy form needs sph_set_prop_tables");
+        return SPH_ERR_STATE;
+    }
+    if (c.ptype_wide) {
+        set_error("prop_table = 1: a record has |p_type| >= SPH_TABLE_SLOTS, which no table serves");
+        return SPH_ERR_BAD_ARG;
+    }
+    for (int t = 0; t < SPH_TABLE_SLOTS; ++t)
+        if (((c.ptype_slots >> t) & 1u) && c.tab_size[t] < 2) {
+            set_error("prop_table = 1: a record's |p_type| has no property table of at least two entries");
+            return SPH_ERR_BAD_ARG;
+        }
+    return SPH_OK;
+}
+
 template <class Real>
 int phase_interaction(Ctx<Real> &c) {
+    SPH_TRY(check_tables(c));
     cudaStream_t st = c.stream;
     const int n = c.n;
     const int tc = c.count;
@@ -1412,7 +1461,7 @@ int phase_interaction(Ctx<Real> &c) {
     if (c.dp.time_type == 1) {
         k_projection<Real><<<grid_for(n, 256), 256, 0, st>>>(c.dp, c.ty, c.S.u, c.u0, c.ft, c.S.fm, c.rho_ref_S, c.mr,
                                                              c.S.temp, c.temp0, c.S.concn, c.concn0, c.dconcn,
-                                                             c.S.enth, c.enth0, tdt, c.clk, n);
+                                                             c.S.enth, c.enth0, c.tab, tdt, c.clk, n);
         ++c.launches;
     }
     SPH_TRY(periodic_pass(c, c.S));

@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from .layout import PART1, PART2, PART3, PpeStats, SphParams
+from .layout import PART1, PART2, PART3, PpeStats, PropTables, SphParams
 
 ML_NPARAM = 5569   # SPH_ML_NPARAM
 
@@ -31,7 +31,7 @@ SYMBOLS = (
     "sph_batch_create", "sph_batch_destroy", "sph_batch_step", "sph_batch_set_workers", "sph_batch_autotune",
     "sph_batch_autotune_shapes",
     "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_apr_state", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
-    "sph_read_solv", "sph_initial_records",
+    "sph_read_solv", "sph_initial_records", "sph_read_table", "sph_set_prop_tables",
 )
 
 _lib = None
@@ -112,6 +112,8 @@ def lib():
         L.sph_read_deck.argtypes = [ctypes.c_char_p, vp, i32, ctypes.POINTER(i32)]
         L.sph_read_solv.argtypes = [ctypes.c_char_p, vp, vp, ctypes.POINTER(i32)]
         L.sph_initial_records.argtypes = [vp, vp, i32, vp, i32, ctypes.c_double, ctypes.c_double]
+        L.sph_read_table.argtypes = [ctypes.c_char_p, vp]
+        L.sph_set_prop_tables.argtypes = [vp, vp]
         L.sph_write_vtk.argtypes = [ctypes.c_char_p, vp, vp, vp, i32, ctypes.POINTER(ctypes.c_char_p), i32]
         _lib = L
     return _lib
@@ -242,6 +244,11 @@ class Simulation:
         _check("sph_operator_counts", lib().sph_operator_counts(self.h, a))
         return {"rows": a[0], "entries": a[1], "neumann_rows": a[2], "neumann_entries": a[3], "cells": a[4],
                 "codes16": bool(a[5])}
+
+    def set_prop_tables(self, tables):
+        """Uploads property tables (a PropTables, e.g. from read_table) for the
+        enthalpy form's htoT with vii[prop_table] = 1."""
+        _check("sph_set_prop_tables", lib().sph_set_prop_tables(self.h, ctypes.byref(tables)))
 
     def graph_steps(self):
         """Steps run as a replay of the whole-step graph."""
@@ -408,6 +415,13 @@ def read_solv(path, params=None):
     _check("sph_read_solv", lib().sph_read_solv(str(path).encode(), ctypes.byref(p), labels, ctypes.byref(n)))
     raw = labels.raw
     return p, [raw[20 * k:20 * k + 20].split(b"\0")[0].decode() for k in range(min(n.value, 20))]
+
+
+def read_table(path):
+    """Property tables from a file in the reference's data.txt format."""
+    t = PropTables()
+    _check("sph_read_table", lib().sph_read_table(str(path).encode(), ctypes.byref(t)))
+    return t
 
 
 CASEH_L4 = 2210.0          # functions_NNPS.cuh:7

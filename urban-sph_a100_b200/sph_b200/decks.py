@@ -180,6 +180,27 @@ def enthalpy_mini(seed=11):
     return P, p
 
 
+# two-material property tables for prop_table = 1 (slot 0: walls, |p_type|
+# 0; slot 1: fluid and the p_type -1 wall layer), h ascending, with
+# breakpoints inside the enthalpy range of enthalpy_mini so that htoT meets
+# inner segments and both extrapolated ends
+TABLE_WALL = dict(T=[297.0, 300.0, 305.0, 2400.0], h=[-542600.0, -541800.0, -541000.0, 900000.0],
+                  k=[1.5, 1.6, 1.7, 2.5], cp=[480.0, 490.0, 500.0, 600.0], mu=[0.0, 0.0, 0.0, 0.0])
+TABLE_FLUID = dict(T=[250.0, 290.0, 299.0, 301.5, 304.0, 2650.0],
+                   h=[-560000.0, -546000.0, -543500.0, -542000.0, -540500.0, 1268421.0],
+                   k=[2.0, 2.1, 2.2, 2.3, 2.4, 3.0], cp=[500.0, 510.0, 515.0, 520.0, 530.0, 560.0],
+                   mu=[4e-3, 3.9e-3, 3.8e-3, 3.7e-3, 3.6e-3, 1e-3])
+
+
+def enthalpy_tables_mini(seed=11):
+    """enthalpy_mini with vii[prop_table] = 1 and the two-material tables
+    (a PropTables for sph_set_prop_tables): htoT reads table |p_type|."""
+    from .layout import PropTables
+    P, p = enthalpy_mini(seed=seed)
+    p.seti("prop_table", 1)
+    return P, p, PropTables.from_columns([TABLE_WALL, TABLE_FLUID])
+
+
 def with_headroom(P, p, frac):
     """Appends int(frac * len(P)) free dummy records (i_type 3), the room the
     reference reserves for buffer and APR particles (ISPH.cuh:116)."""

@@ -163,6 +163,47 @@ class PpeStats(ctypes.Structure):
 
 assert ctypes.sizeof(SphParams) == 1344, ctypes.sizeof(SphParams)
 
+TABLE_SIZE = 50     # table_size, Parameters.cuh:66
+TABLE_SLOTS = 10    # k_table_index / k_table_size, SOPHIA_gpu.cu:56-57
+
+
+class PropTables(ctypes.Structure):
+    """ctypes mirror of ``sph_prop_tables``: the property tables of read_table
+    (function_init.cuh:724-905); table t spans entries index[t] ..
+    index[t] + size[t] - 1 of each column and serves |p_type| = t."""
+    _fields_ = [
+        ("n_tables", ctypes.c_int32), ("n_data", ctypes.c_int32),
+        ("index", ctypes.c_int32 * TABLE_SLOTS), ("size", ctypes.c_int32 * TABLE_SLOTS),
+        ("T", ctypes.c_double * TABLE_SIZE), ("h", ctypes.c_double * TABLE_SIZE),
+        ("k", ctypes.c_double * TABLE_SIZE), ("cp", ctypes.c_double * TABLE_SIZE),
+        ("mu", ctypes.c_double * TABLE_SIZE),
+    ]
+
+    def column(self, name, t):
+        """Entries of column `name` in table t."""
+        a = np.ctypeslib.as_array(getattr(self, name))
+        return a[self.index[t]:self.index[t] + self.size[t]].copy()
+
+    @classmethod
+    def from_columns(cls, tables):
+        """Tables from a list (slot 0, 1, ...) of dicts of equal-length columns
+        (T, h, k, cp, mu; missing ones 0), laid end to end as read_table
+        lays them."""
+        out = cls()
+        at = 0
+        for t, cols in enumerate(tables):
+            n = len(next(iter(cols.values())))
+            for name, v in cols.items():
+                assert len(v) == n, name
+                getattr(out, name)[at:at + n] = [float(x) for x in v]
+            out.index[t], out.size[t] = at, n
+            at += n
+        out.n_tables, out.n_data = len(tables), at
+        return out
+
+
+assert ctypes.sizeof(PropTables) == 2088, ctypes.sizeof(PropTables)
+
 BUFFER_PERIODIC_GHOST = 7   # buffer_type of a periodic ghost (sph_params.periodic_box)
 
 OUTLET_DONOTHING = 0      # KERNEL_donothing_buffer3D (the shipped step)
