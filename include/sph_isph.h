@@ -469,6 +469,19 @@ int sph_read_table(const char *path, sph_prop_tables *out);
  * otherwise).  Rejected: sizes outside 0..SPH_TABLE_SIZE, an index + size
  * past SPH_TABLE_SIZE. */
 int sph_set_prop_tables(sph_ctx *ctx, const sph_prop_tables *t);
+
+/* The energy conversions of functions_ENERGY.cuh on the context's current
+ * records, every record but i_type 3: to_enthalpy = 1 is
+ * KERNEL_clc_TemptoEnthalpy (:3-12), enthalpy = enthalpy0 = Ttoh(temp,
+ * p_type), the start-up pass the reference keeps commented out before its
+ * time loop (ISPH_Calc.cuh:480-482); to_enthalpy = 0 is
+ * KERNEL_clc_EnthalpytoTemp (:15-25), temp = htoT(enthalpy, p_type).  Ttoh
+ * and htoT (functions_PROP.cuh:43-93) read the built-in corium table, or
+ * with vii[prop_table] = 1 table |p_type| of sph_set_prop_tables (needed
+ * then); a record whose |p_type| has no table of two entries keeps its value
+ * (the reference reads past its arrays there).  Call after sph_upload;
+ * asynchronous on the context's stream. */
+int sph_energy_convert(sph_ctx *ctx, int to_enthalpy);
 /* The host pass the reference runs on deck records before upload
  * (c_initial_inner_outer_particle_single, functions_NNPS.cuh:196-373), in
  * place: i_type 1, buffer_type 0, m_ref = m, uy = uz = 0, temp 300,

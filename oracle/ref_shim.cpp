@@ -98,6 +98,7 @@ thread_local int sharedHash[129];
 #include "functions_MOST.cuh"
 #include "functions_TIME_ISPH.cuh"
 #include "functions_OUTPUT.cuh"
+#include "functions_ENERGY.cuh"
 
 // ---- launcher ---------------------------------------------------------------
 // Runs `body` for every thread of a <<<ceil(n/128),128>>> launch.  Blocks run in
@@ -403,6 +404,16 @@ void ref_read_table(const char *path, double *cols, int *index, int *size) {
     std::copy(host_Tab_vis, host_Tab_vis + table_size, k_Tab_vis);
     std::copy(host_table_index, host_table_index + 10, k_table_index);
     std::copy(host_table_size, host_table_size + 10, k_table_size);
+}
+
+// KERNEL_clc_TemptoEnthalpy (functions_ENERGY.cuh:3-12), the launch that
+// ISPH_Calc.cuh:480-482 keeps commented out before the time loop, and
+// KERNEL_clc_EnthalpytoTemp (:15-25), over the first k_num_part2 records
+void ref_temp_to_enthalpy(part1 *P1, part2 *P2, int n) {
+    launch(n, false, [&] { KERNEL_clc_TemptoEnthalpy(P1, P2); });
+}
+void ref_enthalpy_to_temp(part1 *P1, int n) {
+    launch(n, false, [&] { KERNEL_clc_EnthalpytoTemp(P1); });
 }
 
 }  // extern "C"

@@ -89,6 +89,16 @@ class RefHost:
         self.count = self.params.geti("count")
         self.time = np.float32(self.params.getf("time"))
 
+    def temp_to_enthalpy(self):
+        """The reference's KERNEL_clc_TemptoEnthalpy on the records (P1, P2)."""
+        self.L.ref_temp_to_enthalpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        self.L.ref_temp_to_enthalpy(_p(self.P1), _p(self.P2), self.n)
+
+    def enthalpy_to_temp(self):
+        """The reference's KERNEL_clc_EnthalpytoTemp on the records (P1)."""
+        self.L.ref_enthalpy_to_temp.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self.L.ref_enthalpy_to_temp(_p(self.P1), self.n)
+
     def _load_params(self):
         vii = np.ctypeslib.as_array(self.params.vii).copy()
         vif = np.ctypeslib.as_array(self.params.vif).copy()

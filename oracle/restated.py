@@ -31,6 +31,7 @@ def lib():
         L.orc_pin_row.argtypes = [vp]
         L.orc_download.argtypes = [vp] * 4
         L.orc_set_tables.argtypes = [vp, vp]
+        L.orc_temp_to_enthalpy.argtypes = [vp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -88,6 +89,14 @@ class Restated:
     def set_tables(self, tables):
         """Property tables (a PropTables) for htoT with vii[prop_table] = 1."""
         lib().orc_set_tables(self.h, ctypes.byref(tables))
+
+    def temp_to_enthalpy(self):
+        """enthalpy = enthalpy0 = Ttoh(temp, p_type) for every record but i_type 3."""
+        lib().orc_temp_to_enthalpy(self.h, 0)
+
+    def enthalpy_to_temp(self):
+        """temp = htoT(enthalpy, p_type) for every record but i_type 3."""
+        lib().orc_temp_to_enthalpy(self.h, 1)
 
     def pin_row(self):
         return lib().orc_pin_row(self.h)

@@ -197,24 +197,27 @@ struct P2State {
 
 // interp2 (functions_PROP.cuh:8-41) over n >= 2 points, in the reference's
 // Real arithmetic: linear inside the table, the end segments extended
-// outside it.  The reference's search loop also tests the pair (n-1, n),
-// one entry past the table, but only for an x it cannot bracket, which a
-// table with increasing x_data does not leave (NaN x leaves its result
-// unset; here it is the last value).
+// outside it.  Each segment's slope multiplies the distance from its left
+// point, except past the last point, where the reference measures from the
+// last point and adds its value (:16-21; equal in exact arithmetic, not in
+// rounding).  The reference's search loop also tests the pair (n-1, n), one
+// entry past the table, but only for an x it cannot bracket, which a table
+// with increasing x_data does not leave (NaN x leaves its result unset;
+// here it is the last value).
 template <class Real>
 static Real interp2(const Real *xd, const Real *yd, int n, Real x) {
-    auto seg = [&](int a) {
+    auto seg = [&](int a, int at) {
         Real y = yd[a + 1] - yd[a];
         y /= (xd[a + 1] - xd[a]);
-        y *= (x - xd[a]);
-        y += yd[a];
+        y *= (x - xd[at]);
+        y += yd[at];
         return y;
     };
     const int e = n - 1;
-    if (xd[e] < x) return seg(e - 1);
-    if (x <= xd[0]) return seg(0);
+    if (xd[e] < x) return seg(e - 1, e);
+    if (x <= xd[0]) return seg(0, 0);
     for (int a = 0; a < e; ++a)
-        if (xd[a] < x && x <= xd[a + 1]) return seg(a);
+        if (xd[a] < x && x <= xd[a + 1]) return seg(a, a);
     return yd[e];
 }
 
@@ -237,6 +240,19 @@ static Real htoT(Real h, int p_type, bool prop_table, const PropTables<Real> &ta
     const int t = p_type < 0 ? -p_type : p_type;
     if (t >= SPH_TABLE_SLOTS || tab.size[t] < 2) return keep;
     return interp2<Real>(tab.h + tab.index[t], tab.T + tab.index[t], tab.size[t], h);
+}
+
+// Ttoh (functions_PROP.cuh:69-93): the inverse lookup, T to h, on the same
+// tables (the built-in corium pairs with the columns swapped, or table
+// |p_type| with k_Tab_T as x and k_Tab_h as y)
+template <class Real>
+static Real Ttoh(Real T, int p_type, bool prop_table, const PropTables<Real> &tab, Real keep) {
+    static const Real xd[5] = {Real(280), Real(1537), Real(2300), Real(2450), Real(2650)};
+    static const Real yd[5] = {Real(-554932), Real(215789), Real(757894), Real(905263), Real(1268421)};
+    if (!prop_table) return interp2<Real>(xd, yd, 5, T);
+    const int t = p_type < 0 ? -p_type : p_type;
+    if (t >= SPH_TABLE_SLOTS || tab.size[t] < 2) return keep;
+    return interp2<Real>(tab.T + tab.index[t], tab.h + tab.index[t], tab.size[t], T);
 }
 
 template <class Real>
@@ -1716,6 +1732,26 @@ struct Oracle {
         return st;
     }
 
+    // KERNEL_clc_TemptoEnthalpy (functions_ENERGY.cuh:3-12): every record
+    // but i_type 3 gets enthalpy = enthalpy0 = Ttoh(temp, p_type)
+    void temp_to_enthalpy() {
+        const bool pt = P{prm}.prop_table() == 1;
+        for (int i = 0; i < n(); ++i) {
+            if (S1.i_type[i] == 3) continue;
+            const Real v = Ttoh<Real>(S1.temp[i], S1.p_type[i], pt, tab, S1.enthalpy[i]);
+            S1.enthalpy[i] = v;
+            S2.enthalpy0[i] = v;
+        }
+    }
+    // KERNEL_clc_EnthalpytoTemp (functions_ENERGY.cuh:15-25): temp = htoT(enthalpy, p_type)
+    void enthalpy_to_temp() {
+        const bool pt = P{prm}.prop_table() == 1;
+        for (int i = 0; i < n(); ++i) {
+            if (S1.i_type[i] == 3) continue;
+            S1.temp[i] = htoT<Real>(S1.enthalpy[i], S1.p_type[i], pt, tab, S1.temp[i]);
+        }
+    }
+
     void download(sph_part1 *A, sph_part2 *B, sph_part3 *C) const {
         for (int i = 0; i < n(); ++i) {
             if (A) {
@@ -1783,6 +1819,18 @@ int orc_set_tables(void *hh, const sph_prop_tables *t) {
         for (int k = 0; k < SPH_TABLE_SIZE; ++k) { o->tab.h[k] = (R)t->h[k]; o->tab.T[k] = (R)t->T[k]; }
         for (int k = 0; k < SPH_TABLE_SLOTS; ++k) { o->tab.index[k] = t->index[k]; o->tab.size[k] = t->size[k]; }
         o->tab.set = true;
+    };
+    go(h->f);
+    go(h->d);
+    return SPH_OK;
+}
+
+int orc_temp_to_enthalpy(void *hh, int inverse) {
+    OracleHandle *h = (OracleHandle *)hh;
+    auto go = [&](auto *o) {
+        if (!o) return;
+        if (inverse) o->enthalpy_to_temp();
+        else o->temp_to_enthalpy();
     };
     go(h->f);
     go(h->d);

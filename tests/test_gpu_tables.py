@@ -111,3 +111,57 @@ def test_tables_outside_the_entries_are_refused():
     with pytest.raises(abi.SphError):
         sim.set_prop_tables(bad)
     sim.close()
+
+
+@pytest.mark.parametrize("precision", [layout.PREC_MIXED, layout.PREC_FP64], ids=["fp32", "fp64"])
+@pytest.mark.parametrize("tables", [False, True], ids=["corium", "tables"])
+def test_energy_conversions_match_oracle_bit_for_bit(precision, tables):
+    """sph_energy_convert (KERNEL_clc_TemptoEnthalpy / KERNEL_clc_EnthalpytoTemp)
+    against the oracle, which is bit-exact against the reference's kernels
+    (tests/test_oracle.py): one interpolation per record, each step rounded
+    as the reference's arithmetic rounds it, so the results are equal.
+    Temperatures and enthalpies span every branch of the lookup; with the
+    tables the deck's IBM markers (|p_type| 1000, no table) keep their
+    values."""
+    if tables:
+        P, p, t = decks.enthalpy_tables_mini()
+    else:
+        (P, p), t = decks.enthalpy_mini(), None
+    P = P.copy()
+    rng = np.random.default_rng(9)
+    P["temp"] = rng.uniform(200.0, 3000.0, len(P)).astype(np.float32)
+    sim = abi.Simulation(p, precision=precision)
+    O = restated.Restated(P, p, precision)
+    if t is not None:
+        sim.set_prop_tables(t)
+        O.set_tables(t)
+    sim.upload(P)
+    sim.enthalpy_from_temperature()
+    A, A2, _ = sim.download()
+    O.temp_to_enthalpy()
+    B, B2, _ = O.download()
+    assert np.array_equal(A["enthalpy"], B["enthalpy"])
+    assert np.array_equal(A2["enthalpy0"], B2["enthalpy0"])
+    if t is not None:
+        markers = P["p_type"] == 1000
+        assert np.array_equal(A["enthalpy"][markers], P["enthalpy"][markers])
+    Q = np.array(A, copy=True)
+    Q["enthalpy"] = rng.uniform(-7.0e5, 1.5e6, len(Q)).astype(np.float32)
+    sim.upload(Q)
+    sim.temperature_from_enthalpy()
+    C, _, _ = sim.download()
+    O2 = restated.Restated(Q, p, precision)
+    if t is not None:
+        O2.set_tables(t)
+    O2.enthalpy_to_temp()
+    D, _, _ = O2.download()
+    sim.close()
+    assert np.array_equal(C["temp"], D["temp"])
+
+
+def test_energy_conversion_needs_tables_when_asked_for():
+    P, p, _ = decks.enthalpy_tables_mini()
+    sim = _sim(P, p)
+    with pytest.raises(abi.SphError):
+        sim.enthalpy_from_temperature()
+    sim.close()

@@ -248,6 +248,52 @@ def test_property_tables_bit_exact_vs_reference(tmp_path):
     assert (hw < decks.TABLE_WALL["h"][0]).any() and (hw > decks.TABLE_WALL["h"][0]).any()   # both segments met
 
 
+@pytest.mark.skipif(not refhost.available("enth"), reason="reference host build (enthalpy form) absent")
+@pytest.mark.parametrize("tables", [False, True], ids=["corium", "tables"])
+def test_energy_conversions_bit_exact_vs_reference(tmp_path, tables):
+    """KERNEL_clc_TemptoEnthalpy and KERNEL_clc_EnthalpytoTemp
+    (functions_ENERGY.cuh:3-25) against the oracle, with temperatures and
+    enthalpies below, inside and above the tables (every branch of interp2,
+    the end point's own anchoring past the last entry included).  With the
+    property tables the reference reads k_table_index[|p_type|] for every
+    record but i_type 3, past its ten entries for the IBM markers (p_type
+    1000), so that case runs on the deck without its markers."""
+    if tables:
+        P, p, t = decks.enthalpy_tables_mini()
+        P = P[P["p_type"] < 1000].copy()
+        decks.domain_setup(p, P)
+    else:
+        P, p = decks.enthalpy_mini()
+        P = P.copy()
+    rng = np.random.default_rng(5)
+    P["temp"] = rng.uniform(200.0, 3000.0, len(P)).astype(np.float32)
+    R = refhost.RefHost(P, p, parallel=False, variant="enth")
+    O = restated.Restated(P, p, 0)
+    if tables:
+        path = tmp_path / "data.txt"
+        path.write_bytes(np.load(os.path.join(HERE, "golden", "table_ref.npz"))["text_two_materials"].tobytes())
+        refhost.read_table(path, "enth")
+        O.set_tables(t)
+    R.temp_to_enthalpy()
+    O.temp_to_enthalpy()
+    B, B2, _ = O.download()
+    assert np.array_equal(R.P1["enthalpy"], B["enthalpy"])
+    assert np.array_equal(R.P2["enthalpy0"], B2["enthalpy0"])
+    top = 2650.0
+    assert (P["temp"] > top).any() and (P["temp"] < 250.0).any()
+    # and back, from enthalpies over the whole range
+    Q = np.array(R.P1, copy=True)
+    Q["enthalpy"] = rng.uniform(-7.0e5, 1.5e6, len(Q)).astype(np.float32)
+    R.P1[:] = Q
+    O2 = restated.Restated(Q, p, 0)
+    if tables:
+        O2.set_tables(t)
+    R.enthalpy_to_temp()
+    O2.enthalpy_to_temp()
+    C, _, _ = O2.download()
+    assert np.array_equal(R.P1["temp"], C["temp"])
+
+
 BOUNDARY = {"extrapolation": (layout.OUTLET_EXTRAPOLATION, 0), "inout": (layout.OUTLET_INOUT, 0),
             "recycling": (layout.OUTLET_DONOTHING, 1), "inout_recycling": (layout.OUTLET_INOUT, 1)}
 

@@ -630,6 +630,20 @@ int sph_set_prop_tables(sph_ctx *ctx, const sph_prop_tables *t) {
     return DISPATCH(ctx, go(ctx->f), go(ctx->d));
 }
 
+int sph_energy_convert(sph_ctx *ctx, int to_enthalpy) {
+    if (!ctx || (to_enthalpy != 0 && to_enthalpy != 1)) return SPH_ERR_BAD_ARG;
+    auto go = [&](auto *c) -> int {
+        if (!c->uploaded) { set_error("sph_energy_convert: no records uploaded"); return SPH_ERR_STATE; }
+        if (c->dp.prop_table && !c->tab_set) {
+            set_error("sph_energy_convert: prop_table = 1 needs sph_set_prop_tables");
+            return SPH_ERR_STATE;
+        }
+        SPH_CUDA_TRY(cudaSetDevice(c->device));
+        return energy_convert(*c, to_enthalpy);
+    };
+    return DISPATCH(ctx, go(ctx->f), go(ctx->d));
+}
+
 int64_t sph_step_graph_count(sph_ctx *ctx) {
     if (!ctx) return -1;
     return DISPATCH(ctx, ctx->f->graph_steps, ctx->d->graph_steps);

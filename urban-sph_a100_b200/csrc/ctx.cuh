@@ -345,6 +345,9 @@ inline cudaError_t record_event(const Ctx<Real> &c, cudaEvent_t e) {
     return c.capturing ? cudaEventRecordWithFlags(e, c.stream, cudaEventRecordExternal) : cudaEventRecord(e, c.stream);
 }
 template <class Real> int finish_step(Ctx<Real> &c);
+// enthalpy = enthalpy0 = Ttoh(temp) (to_h = 1) or temp = htoT(enthalpy)
+// (to_h = 0) for every record but i_type 3, on the current records
+template <class Real> int energy_convert(Ctx<Real> &c, int to_h);
 template <class Real> int dev_solve_stats(Ctx<Real> &c, sph_ppe_stats *S, int *worst);
 template <class Real> int dev_reset_worst(Ctx<Real> &c);
 template <class Real> bool solve_under_device_control(const Ctx<Real> &c);

@@ -234,6 +234,8 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     k_unpack<Real><<<grid_for(n, 256), 256, 0, c.stream>>>(c, d1, P2 ? d2 : nullptr, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
+    // enthalpy0 of new records is 0 until a projection or sph_energy_convert sets it
+    SPH_CUDA_TRY(cudaMemsetAsync(c.enth0, 0, sizeof(Real) * (size_t)n, c.stream));
     // the |p_type| slots htoT can read (records are only ever copied from
     // these: APR children and merged records keep their p_type)
     c.ptype_slots = 0;

@@ -669,56 +669,85 @@ __global__ void __launch_bounds__(128) k_advection(DevParams P, SoA<Real> s, LIS
     if (cnc) ((Real *)sc.dconcn)[i] = Rd;
 }
 
-// htoT of the enthalpy form with the reference's built-in corium table
-// (functions_PROP.cuh:43-67, prop_table = 0) and its interp2 (:8-41): linear
-// inside the table, the end segments extended outside it, each step of the
-// segment formula rounded as the reference's Real arithmetic rounds it
+// interp2 (functions_PROP.cuh:8-41) over n >= 2 points: linear inside the
+// table, the end segments extended outside it, each step of the segment
+// formula rounded as the reference's Real arithmetic rounds it.  The slope
+// multiplies the distance from the segment's left point, except past the
+// last point, where the reference measures from the last point and adds its
+// value (:16-21; equal in exact arithmetic, not in rounding).  The
+// reference's search also tests the pair one past the table, but only for
+// an x it cannot bracket, which a table with increasing x does not leave.
 template <class Real>
-__device__ __forceinline__ Real seg_rn(Real y0, Real y1, Real x0, Real x1, Real x);
+__device__ __forceinline__ Real seg_rn(Real y0, Real y1, Real x0, Real x1, Real xa, Real ya, Real x);
 template <>
-__device__ __forceinline__ float seg_rn<float>(float y0, float y1, float x0, float x1, float x) {
-    return __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(y1, y0), __fsub_rn(x1, x0)), __fsub_rn(x, x0)), y0);
+__device__ __forceinline__ float seg_rn<float>(float y0, float y1, float x0, float x1, float xa, float ya, float x) {
+    return __fadd_rn(__fmul_rn(__fdiv_rn(__fsub_rn(y1, y0), __fsub_rn(x1, x0)), __fsub_rn(x, xa)), ya);
 }
 template <>
-__device__ __forceinline__ double seg_rn<double>(double y0, double y1, double x0, double x1, double x) {
-    return __dadd_rn(__dmul_rn(__ddiv_rn(__dsub_rn(y1, y0), __dsub_rn(x1, x0)), __dsub_rn(x, x0)), y0);
+__device__ __forceinline__ double seg_rn<double>(double y0, double y1, double x0, double x1, double xa, double ya,
+                                                 double x) {
+    return __dadd_rn(__dmul_rn(__ddiv_rn(__dsub_rn(y1, y0), __dsub_rn(x1, x0)), __dsub_rn(x, xa)), ya);
 }
 template <class Real>
-__device__ Real corium_htoT(Real h) {
-    const Real xd[5] = {(Real)-554932, (Real)215789, (Real)757894, (Real)905263, (Real)1268421};
-    const Real yd[5] = {(Real)280, (Real)1537, (Real)2300, (Real)2450, (Real)2650};
+__device__ Real interp2_rn(const Real *xd, const Real *yd, int n, Real x) {
+    const int e = n - 1;
+    if (xd[e] < x) return seg_rn<Real>(yd[e - 1], yd[e], xd[e - 1], xd[e], xd[e], yd[e], x);
     int a = 0;
-    if (xd[4] < h) a = 3;
-    else if (h <= xd[0]) a = 0;
-    else
-        for (int q = 0; q < 4; ++q)
-            if (xd[q] < h && h <= xd[q + 1]) { a = q; break; }
-    return seg_rn<Real>(yd[a], yd[a + 1], xd[a], xd[a + 1], h);
+    if (!(x <= xd[0]))
+        for (int q = 0; q < e; ++q)
+            if (xd[q] < x && x <= xd[q + 1]) { a = q; break; }
+    return seg_rn<Real>(yd[a], yd[a + 1], xd[a], xd[a + 1], xd[a], yd[a], x);
 }
 
-// htoT with the property tables (functions_PROP.cuh:43-67, prop_table = 1):
-// interp2 over table |p_type|, whose h and T entries start at
-// tab[index] and tab[SPH_TABLE_SIZE + index].  The host refuses a step in
-// which a record the projection reaches has no table of two entries; a slot
-// without one leaves the temperature as it was.  The reference's search
-// also tests the pair one past the table, but only for an h it cannot
-// bracket, which a table with increasing h does not leave.
+// htoT / Ttoh (functions_PROP.cuh:43-93).  prop_table = 0: the built-in
+// corium pairs (:45-46, :72-73).  prop_table = 1: table |p_type| of the
+// property tables, whose h and T entries start at tab[index] and
+// tab[SPH_TABLE_SIZE + index]; a slot without a table of two entries
+// leaves the value as it was (the step refuses to run when a record the
+// projection reaches has none).
 template <class Real>
-__device__ Real table_htoT(const DevParams &P, const Real *tab, int p_type, Real h, Real keep) {
+__device__ Real prop_lookup(const DevParams &P, const Real *tab, int p_type, Real x, Real keep, bool to_h) {
+    if (!P.prop_table) {
+        const Real H[5] = {(Real)-554932, (Real)215789, (Real)757894, (Real)905263, (Real)1268421};
+        const Real T[5] = {(Real)280, (Real)1537, (Real)2300, (Real)2450, (Real)2650};
+        return to_h ? interp2_rn<Real>(T, H, 5, x) : interp2_rn<Real>(H, T, 5, x);
+    }
     const int t = p_type < 0 ? -p_type : p_type;
     if (t >= SPH_TABLE_SLOTS) return keep;
     const int n = P.tab_size[t];
     if (n < 2) return keep;
-    const Real *xd = tab + P.tab_index[t];
-    const Real *yd = tab + SPH_TABLE_SIZE + P.tab_index[t];
-    const int e = n - 1;
-    int a = 0;
-    if (xd[e] < h) a = e - 1;
-    else if (h <= xd[0]) a = 0;
-    else
-        for (int q = 0; q < e; ++q)
-            if (xd[q] < h && h <= xd[q + 1]) { a = q; break; }
-    return seg_rn<Real>(yd[a], yd[a + 1], xd[a], xd[a + 1], h);
+    const Real *h = tab + P.tab_index[t];
+    const Real *T = tab + SPH_TABLE_SIZE + P.tab_index[t];
+    return to_h ? interp2_rn<Real>(T, h, n, x) : interp2_rn<Real>(h, T, n, x);
+}
+
+// KERNEL_clc_TemptoEnthalpy (functions_ENERGY.cuh:3-12; its launch before
+// the time loop, ISPH_Calc.cuh:480-482, is commented out there) and
+// KERNEL_clc_EnthalpytoTemp (:15-25): every record but i_type 3
+template <class Real>
+__global__ void k_energy_convert(DevParams P, const int4 *ty, Real *temp, Real *enth, Real *enth0, const Real *tab,
+                                 int to_h, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 t = ty[i];
+    if (t.x == 3) return;
+    if (to_h) {
+        const Real v = prop_lookup<Real>(P, tab, t.w, temp[i], enth[i], true);
+        enth[i] = v;
+        enth0[i] = v;
+    } else {
+        temp[i] = prop_lookup<Real>(P, tab, t.w, enth[i], temp[i], false);
+    }
+}
+
+template <class Real>
+int energy_convert(Ctx<Real> &c, int to_h) {
+    const int n = c.n;
+    k_energy_convert<Real><<<grid_for(n, 256), 256, 0, c.stream>>>(c.dp, c.ty, c.A.temp, c.A.enth, c.enth0, c.tab,
+                                                                  to_h, n);
+    ++c.launches;
+    SPH_CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -758,7 +787,7 @@ __global__ void k_projection(DevParams P, const int4 *ty, typename V4<Real>::typ
         if (P.enthalpy_eqn) {
             const Real h = enth[i];
             enth0[i] = h;
-            temp[i] = P.prop_table ? table_htoT<Real>(P, tab, t.w, h, temp[i]) : corium_htoT<Real>(h);
+            temp[i] = prop_lookup<Real>(P, tab, t.w, h, temp[i], false);
         } else {
             temp0[i] = temp[i];
         }
@@ -1569,6 +1598,7 @@ int ctx_diagnostics(Ctx<Real> &c, float *umax, float *drho, float *fmax) {
     template int periodic_pass<R>(Ctx<R> &, VarSet<R> &);                \
     template int freeslip_pass<R>(Ctx<R> &, VarSet<R> &);                \
     template int phase_interaction<R>(Ctx<R> &);                         \
+    template int energy_convert<R>(Ctx<R> &, int);                       \
     template int phase_time_update<R>(Ctx<R> &);                         \
     template int ctx_diagnostics<R>(Ctx<R> &, float *, float *, float *);
 INST(float)

@@ -32,6 +32,7 @@ SYMBOLS = (
     "sph_batch_autotune_shapes",
     "sph_batch_case", "sph_batch_particles", "sph_apr", "sph_apr_state", "sph_set_ib_boxes", "sph_read_deck", "sph_write_vtk",
     "sph_read_solv", "sph_initial_records", "sph_read_table", "sph_set_prop_tables",
+    "sph_energy_convert",
 )
 
 _lib = None
@@ -114,6 +115,7 @@ def lib():
         L.sph_initial_records.argtypes = [vp, vp, i32, vp, i32, ctypes.c_double, ctypes.c_double]
         L.sph_read_table.argtypes = [ctypes.c_char_p, vp]
         L.sph_set_prop_tables.argtypes = [vp, vp]
+        L.sph_energy_convert.argtypes = [vp, i32]
         L.sph_write_vtk.argtypes = [ctypes.c_char_p, vp, vp, vp, i32, ctypes.POINTER(ctypes.c_char_p), i32]
         _lib = L
     return _lib
@@ -249,6 +251,16 @@ class Simulation:
         """Uploads property tables (a PropTables, e.g. from read_table) for the
         enthalpy form's htoT with vii[prop_table] = 1."""
         _check("sph_set_prop_tables", lib().sph_set_prop_tables(self.h, ctypes.byref(tables)))
+
+    def enthalpy_from_temperature(self):
+        """enthalpy = enthalpy0 = Ttoh(temp, p_type) on the current records
+        (the reference's KERNEL_clc_TemptoEnthalpy)."""
+        _check("sph_energy_convert", lib().sph_energy_convert(self.h, 1))
+
+    def temperature_from_enthalpy(self):
+        """temp = htoT(enthalpy, p_type) on the current records (the
+        reference's KERNEL_clc_EnthalpytoTemp)."""
+        _check("sph_energy_convert", lib().sph_energy_convert(self.h, 0))
 
     def graph_steps(self):
         """Steps run as a replay of the whole-step graph."""
