@@ -126,3 +126,24 @@ def test_written_deck_and_solver_input_read_back(tmp_path):
             assert int(vii[layout.VII[slot]]) == p.geti(slot), slot
         for slot in ("dt", "time_end", "u_limit"):
             assert vif[layout.VIF[slot]] == np.float32(p.getf(slot)), slot
+
+
+def test_property_tables_are_read_beside_the_solver_input(tmp_path):
+    """property_table YES: the tables come from data.txt beside solv.txt (the
+    reference's ./input layout) or from the path given; without the file the
+    case is refused; with NO nothing is read."""
+    solv, deck, _ = write_case(tmp_path)
+    p, _, _ = driver.setup(solv, deck)
+    assert driver.read_tables(solv, p) is None
+    solv.write_text(solv.read_text() + "property_table(YES/NO): YES\n")
+    p, _, _ = driver.setup(solv, deck)
+    assert p.geti("prop_table") == 1
+    with pytest.raises(FileNotFoundError):
+        driver.read_tables(solv, p)
+    G = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "table_ref.npz"))
+    (tmp_path / "data.txt").write_bytes(G["text_two_materials"].tobytes())
+    t = driver.read_tables(solv, p)
+    assert t.n_tables == 2 and np.array_equal(t.column("T", 1), decks.TABLE_FLUID["T"])
+    other = tmp_path / "elsewhere.txt"
+    other.write_bytes(G["text_ten_tables"].tobytes())
+    assert driver.read_tables(solv, p, other).n_tables == 10

@@ -17,7 +17,17 @@ plot-variables.  Settings the solver input does not carry (the PPE solver
 form, the wall-model and MOST constants, the inflow profile) come from
 ``base`` (default: ``params.default_params()``).
 
-    python -m sph_b200.driver solv.txt deck.txt out_dir [--steps N]
+The reference's main also reads the property tables of ./input/data.txt
+(read_table, SOPHIA_gpu.cu:132), beside its solv.txt.  Here they are read
+when the solver input sets property_table YES (the only case in which the
+step reads them): from ``table_path``, else data.txt beside the solver
+input.  With the enthalpy form (``--enthalpy``, the reference's
+compile-time enthalpy_eqn) the records' enthalpy is set from their
+temperature after the upload (KERNEL_clc_TemptoEnthalpy, the start-up
+pass ISPH_Calc.cuh:480-482 keeps commented out), since decks carry
+temperatures only.
+
+    python -m sph_b200.driver solv.txt deck.txt out_dir [--steps N] [--table data.txt] [--enthalpy]
 """
 import argparse
 import math
@@ -111,9 +121,22 @@ def setup(solv_path, deck_path, base=None):
     return p, labels, P1
 
 
-def run(solv_path, deck_path, out_dir=None, base=None, precision=0, max_steps=None, log=print):
+def read_tables(solv_path, p, table_path=None):
+    """The property tables of a case (a PropTables), or None when its
+    parameters do not ask for them (vii[prop_table] = 0)."""
+    if p.geti("prop_table") != 1:
+        return None
+    path = table_path if table_path is not None else os.path.join(os.path.dirname(os.path.abspath(solv_path)),
+                                                                   "data.txt")
+    if not os.path.exists(path):
+        raise FileNotFoundError("property_table YES needs the table file %s" % path)
+    return abi.read_table(path)
+
+
+def run(solv_path, deck_path, out_dir=None, base=None, precision=0, max_steps=None, log=print, table_path=None):
     """Steps a case from its solver input and deck; returns (steps, final records)."""
     p, labels, P1 = setup(solv_path, deck_path, base)
+    tables = read_tables(solv_path, p, table_path)
     if out_dir is not None:
         os.makedirs(out_dir, exist_ok=True)
     freq = max(p.geti("freq_output"), 1)
@@ -123,7 +146,11 @@ def run(solv_path, deck_path, out_dir=None, base=None, precision=0, max_steps=No
     count = p.geti("count")
     sim = abi.Simulation(p, precision=precision)
     try:
+        if tables is not None:
+            sim.set_prop_tables(tables)
         sim.upload(P1)
+        if p.enthalpy_eqn and p.geti("con_solve") == 1:
+            sim.enthalpy_from_temperature()
         wall0 = _wall.perf_counter()
         steps = 0
         while True:
@@ -154,8 +181,14 @@ def main(argv=None):
     ap.add_argument("out_dir")
     ap.add_argument("--steps", type=int, default=None, help="stop after this many steps")
     ap.add_argument("--fp64", action="store_true", help="FP64 context instead of FP32")
+    ap.add_argument("--table", default=None, help="property tables (default: data.txt beside the solver input)")
+    ap.add_argument("--enthalpy", action="store_true",
+                    help="energy equation in enthalpy (with Conduction YES), enthalpy set from temperature")
     a = ap.parse_args(argv)
-    run(a.solv, a.deck, a.out_dir, precision=1 if a.fp64 else 0, max_steps=a.steps)
+    base = _params.default_params()
+    if a.enthalpy:
+        base.enthalpy_eqn = 1
+    run(a.solv, a.deck, a.out_dir, base=base, precision=1 if a.fp64 else 0, max_steps=a.steps, table_path=a.table)
     return 0
 
 
