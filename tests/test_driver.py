@@ -1,7 +1,9 @@
 """The case runner: solver input + particle deck in the reference's formats
 through set-up, stepping and VTK output (set-up on the CPU, the run on the
 GPU)."""
+import json
 import os
+import subprocess
 
 import numpy as np
 import pytest
@@ -147,3 +149,71 @@ def test_property_tables_are_read_beside_the_solver_input(tmp_path):
     other = tmp_path / "elsewhere.txt"
     other.write_bytes(G["text_ten_tables"].tobytes())
     assert driver.read_tables(solv, p, other).n_tables == 10
+
+
+NATIVE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "urban-sph_a100_b200", "lib", "sophia_b200")
+needs_native = pytest.mark.skipif(not os.path.exists(NATIVE), reason="native runner not built (build.py)")
+
+
+def _native(*args):
+    return subprocess.run([NATIVE] + [str(a) for a in args], capture_output=True, text=True, timeout=120)
+
+
+@needs_native
+@pytest.mark.parametrize("apr,t0", [("NO", "0.0"), ("Cell", "0.0025")])
+def test_native_runner_sets_up_the_case_as_the_python_runner(tmp_path, apr, t0):
+    """sophia_b200 --setup-only (solver input, deck, domain, host record
+    pass, APR headroom, step counter; no device call) against driver.setup."""
+    solv, deck, _ = write_case(tmp_path, apr=apr, t0=t0)
+    r = _native(solv, deck, tmp_path / "out", "--setup-only")
+    assert r.returncode == 0, r.stderr
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    p, labels, Q = driver.setup(solv, deck)
+    assert got["num_part2"] == len(Q) == p.geti("num_part2") and got["num_part"] == p.geti("num_part")
+    assert got["count"] == p.geti("count")
+    for k in ("NI", "NJ", "NK", "num_cells"):
+        assert got[k] == p.geti(k), k
+    assert np.float32(got["dcell"]) == np.float32(p.getf("dcell"))
+    assert got["labels"] == len(labels) and got["prop_table"] == 0 and got["tables"] == 0
+
+
+@needs_native
+def test_native_runner_reads_the_tables_beside_the_solver_input(tmp_path):
+    solv, deck, _ = write_case(tmp_path)
+    solv.write_text(solv.read_text() + "property_table(YES/NO): YES\n")
+    r = _native(solv, deck, tmp_path / "out", "--setup-only")
+    assert r.returncode == 1 and "data.txt" in r.stderr
+    G = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "table_ref.npz"))
+    (tmp_path / "data.txt").write_bytes(G["text_two_materials"].tobytes())
+    r = _native(solv, deck, tmp_path / "out", "--setup-only")
+    assert r.returncode == 0, r.stderr
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    assert got["prop_table"] == 1 and got["tables"] == 2
+    bad = tmp_path / "bad.txt"
+    bad.write_text("#p_type 3\n//T\n1,2\n#end\n")
+    r = _native(solv, deck, tmp_path / "out", "--setup-only", "--table", bad)
+    assert r.returncode == 1 and "property tables" in r.stderr
+
+
+@needs_native
+def test_native_runner_rejects_bad_arguments(tmp_path):
+    assert _native().returncode == 2
+    assert _native("a", "b", "c", "--bogus").returncode == 2
+    r = _native(tmp_path / "absent.txt", tmp_path / "deck.txt", tmp_path / "out", "--setup-only")
+    assert r.returncode == 1 and "solver input" in r.stderr
+
+
+@pytest.mark.gpu
+@needs_native
+def test_native_runner_writes_the_python_runners_files(tmp_path):
+    """Three steps through sophia_b200 and through driver.run: the same VTK
+    series, byte for byte (the same library, called the same way)."""
+    solv, deck, _ = write_case(tmp_path)
+    r = _native(solv, deck, tmp_path / "native", "--steps", 3)
+    assert r.returncode == 0, r.stderr
+    driver.run(solv, deck, tmp_path / "python", max_steps=3, log=None)
+    names = sorted(os.listdir(tmp_path / "python"))
+    assert names == sorted(os.listdir(tmp_path / "native")) == ["fluid_0stp.vtk", "fluid_2stp.vtk"]
+    for f in names:
+        assert (tmp_path / "native" / f).read_bytes() == (tmp_path / "python" / f).read_bytes(), f
+    assert "tu_max" in r.stdout

@@ -1,4 +1,6 @@
-"""Builds lib/libsph_b200.so: every CUDA source of csrc/ for sm_100a.
+"""Builds lib/libsph_b200.so (every CUDA source of csrc/ for sm_100a) and
+lib/sophia_b200, the native case runner (csrc/sophia_b200.cpp, host C++ over
+the library's C ABI).
 
 Usage: python build.py [-j N]    (also called by __graft_entry__.build)
 """
@@ -13,6 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 OBJ_DIR = os.path.join(HERE, "lib", "obj")
 LIB = os.path.join(LIB_DIR, "libsph_b200.so")
+DRIVER_SRC = os.path.join(CSRC, "sophia_b200.cpp")
+DRIVER = os.path.join(LIB_DIR, "sophia_b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -42,7 +46,21 @@ def build(jobs=None, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s" % r.stderr)
+    build_driver()
     return LIB
+
+
+def build_driver():
+    """The native runner, linked to the library beside it (rpath $ORIGIN)."""
+    deps = [DRIVER_SRC, LIB, os.path.join(ROOT, "include", "sph_isph.h")]
+    if os.path.exists(DRIVER) and all(os.path.getmtime(DRIVER) >= os.path.getmtime(d) for d in deps):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I" + os.path.join(ROOT, "include"), DRIVER_SRC,
+           "-L" + LIB_DIR, "-lsph_b200", "-Wl,-rpath,$ORIGIN", "-Wl,--allow-shlib-undefined", "-o", DRIVER]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("driver build failed:\n%s" % r.stderr)
+    return DRIVER
 
 
 if __name__ == "__main__":
