@@ -313,10 +313,13 @@ void sph_destroy(sph_ctx *ctx);
 /* Replaces the parameters (dt, time, flags); grid fields must not change. */
 int sph_set_params(sph_ctx *ctx, const sph_params *p);
 
-/* Uploads host AoS records (the reference's DHP1 after
- * c_initial_inner_outer_particle_single, ISPH_Calc.cuh:386-387).  P2 may be
- * NULL (zeroed as at ISPH_Calc.cuh:357).  Resets the step counter to
- * vii[count]. */
+/* Uploads AoS records (the reference's DHP1 after
+ * c_initial_inner_outer_particle_single, ISPH_Calc.cuh:386-387, or its
+ * dev_P1 / dev_P2 copies): P1 and P2 may point to host memory (pageable or
+ * pinned) or to device memory of the context's device.  P2 may be NULL
+ * (zeroed as at ISPH_Calc.cuh:357).  Resets the step counter to vii[count].
+ * With device records the call waits for its stream once (to learn the
+ * records' p_type classes). */
 int sph_upload(sph_ctx *ctx, const sph_part1 *P1, const sph_part2 *P2, int n);
 
 /* Same as sph_upload for state that is already sorted by an earlier
@@ -325,7 +328,8 @@ int sph_upload(sph_ctx *ctx, const sph_part1 *P1, const sph_part2 *P2, int n);
 int sph_upload_state(sph_ctx *ctx, const sph_part1 *P1, int n);
 
 /* Downloads the state in the reference layout: P1 (= dev_P1 after the step),
- * P2 (= dev_SP2), P3 (= dev_P3).  Any pointer may be NULL.  Synchronises. */
+ * P2 (= dev_SP2), P3 (= dev_P3), to host memory or to device memory of the
+ * context's device.  Any pointer may be NULL.  Synchronises. */
 int sph_download(sph_ctx *ctx, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3);
 
 /* NNPS, ISPH_Calc.cuh:20-45: set_ncell, cell hash, stable sort, cell

@@ -130,6 +130,7 @@ struct Ctx {
     int tab_index[SPH_TABLE_SLOTS] = {}, tab_size[SPH_TABLE_SLOTS] = {};
     unsigned ptype_slots = 0;     // bit t: a record the projection reaches has |p_type| = t
     bool ptype_wide = false;      // such a record has |p_type| >= SPH_TABLE_SLOTS
+    unsigned *ptype_dev = nullptr;   // the same two words, found on the device for device records
     float *us_update = nullptr;   // u* of the recycling probe, kept across steps
     Real *g6 = nullptr;     // inv_cm: 6 arrays of n (xx, yy, zz, xy, yz, zx)
     // ---- NNPS ----

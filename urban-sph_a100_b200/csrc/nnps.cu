@@ -224,13 +224,37 @@ int ctx_allocate(Ctx<Real> &c) {
     return SPH_OK;
 }
 
+// Records may sit in host memory (pageable or pinned) or in device memory:
+// with unified addressing one cudaMemcpyDefault copy serves both.
+static bool in_host_memory(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
+}
+
+// the |p_type| slots of the records the projection reaches (i_type < 3,
+// p_type < 1000): bit t of out[0] for |p_type| = t < SPH_TABLE_SLOTS, out[1]
+// set for any larger one
+__global__ void k_ptype_slots(const sph_part1 *P1, int n, unsigned *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int it = P1[i].i_type, pt = P1[i].p_type;
+    if (it >= 3 || pt >= 1000) return;
+    const int t = pt < 0 ? -pt : pt;
+    if (t < SPH_TABLE_SLOTS) atomicOr(&out[0], 1u << t);
+    else atomicOr(&out[1], 1u);
+}
+
 template <class Real>
 int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     if (n != c.n) { set_error("sph_upload: n differs from num_part2"); return SPH_ERR_BAD_ARG; }
     sph_part1 *d1 = (sph_part1 *)c.aos;
     sph_part2 *d2 = (sph_part2 *)((char *)c.aos + sizeof(sph_part1) * (size_t)n);
-    SPH_CUDA_TRY(cudaMemcpyAsync(d1, P1, sizeof(sph_part1) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
-    if (P2) SPH_CUDA_TRY(cudaMemcpyAsync(d2, P2, sizeof(sph_part2) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(d1, P1, sizeof(sph_part1) * (size_t)n, cudaMemcpyDefault, c.stream));
+    if (P2) SPH_CUDA_TRY(cudaMemcpyAsync(d2, P2, sizeof(sph_part2) * (size_t)n, cudaMemcpyDefault, c.stream));
     k_unpack<Real><<<grid_for(n, 256), 256, 0, c.stream>>>(c, d1, P2 ? d2 : nullptr, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
@@ -240,11 +264,24 @@ int ctx_upload(Ctx<Real> &c, const sph_part1 *P1, const sph_part2 *P2, int n) {
     // these: APR children and merged records keep their p_type)
     c.ptype_slots = 0;
     c.ptype_wide = false;
-    for (int i = 0; i < n; ++i) {
-        if (P1[i].i_type >= 3 || P1[i].p_type >= 1000) continue;
-        const int t = P1[i].p_type < 0 ? -P1[i].p_type : P1[i].p_type;
-        if (t < SPH_TABLE_SLOTS) c.ptype_slots |= 1u << t;
-        else c.ptype_wide = true;
+    if (in_host_memory(P1)) {
+        for (int i = 0; i < n; ++i) {
+            if (P1[i].i_type >= 3 || P1[i].p_type >= 1000) continue;
+            const int t = P1[i].p_type < 0 ? -P1[i].p_type : P1[i].p_type;
+            if (t < SPH_TABLE_SLOTS) c.ptype_slots |= 1u << t;
+            else c.ptype_wide = true;
+        }
+    } else {
+        if (!c.ptype_dev) SPH_TRY(c.alloc(c.ptype_dev, 2));
+        SPH_CUDA_TRY(cudaMemsetAsync(c.ptype_dev, 0, 2 * sizeof(unsigned), c.stream));
+        k_ptype_slots<<<grid_for(n, 256), 256, 0, c.stream>>>(d1, n, c.ptype_dev);
+        ++c.launches;
+        SPH_CUDA_TRY(cudaGetLastError());
+        unsigned h[2] = {0, 0};
+        SPH_CUDA_TRY(cudaMemcpyAsync(h, c.ptype_dev, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        c.ptype_slots = h[0];
+        c.ptype_wide = h[1] != 0;
     }
     c.count = c.prm.vii[SPH_VII_COUNT];
     c.time = c.prm.vif[SPH_VIF_TIME];
@@ -266,7 +303,7 @@ int ctx_upload_state(Ctx<Real> &c, const sph_part1 *P1, int n) {
     if (n != c.n) { set_error("sph_upload_state: n differs from num_part2"); return SPH_ERR_BAD_ARG; }
     if (!c.built) { set_error("sph_upload_state: no sorted state yet (run a step first)"); return SPH_ERR_STATE; }
     sph_part1 *d1 = (sph_part1 *)c.aos;
-    SPH_CUDA_TRY(cudaMemcpyAsync(d1, P1, sizeof(sph_part1) * (size_t)n, cudaMemcpyHostToDevice, c.stream));
+    SPH_CUDA_TRY(cudaMemcpyAsync(d1, P1, sizeof(sph_part1) * (size_t)n, cudaMemcpyDefault, c.stream));
     k_unpack_state<Real><<<grid_for(n, 256), 256, 0, c.stream>>>(c, d1, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
@@ -282,9 +319,9 @@ int ctx_download(Ctx<Real> &c, sph_part1 *P1, sph_part2 *P2, sph_part3 *P3) {
     k_pack<Real><<<grid_for(n, 128), 128, 0, c.stream>>>(c, P1 ? d1 : nullptr, P2 ? d2 : nullptr, P3 ? d3 : nullptr, n);
     ++c.launches;
     SPH_CUDA_TRY(cudaGetLastError());
-    if (P1) SPH_CUDA_TRY(cudaMemcpyAsync(P1, d1, sizeof(sph_part1) * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
-    if (P2) SPH_CUDA_TRY(cudaMemcpyAsync(P2, d2, sizeof(sph_part2) * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
-    if (P3) SPH_CUDA_TRY(cudaMemcpyAsync(P3, d3, sizeof(sph_part3) * (size_t)n, cudaMemcpyDeviceToHost, c.stream));
+    if (P1) SPH_CUDA_TRY(cudaMemcpyAsync(P1, d1, sizeof(sph_part1) * (size_t)n, cudaMemcpyDefault, c.stream));
+    if (P2) SPH_CUDA_TRY(cudaMemcpyAsync(P2, d2, sizeof(sph_part2) * (size_t)n, cudaMemcpyDefault, c.stream));
+    if (P3) SPH_CUDA_TRY(cudaMemcpyAsync(P3, d3, sizeof(sph_part3) * (size_t)n, cudaMemcpyDefault, c.stream));
     SPH_CUDA_TRY(cudaStreamSynchronize(c.stream));
     return SPH_OK;
 }
