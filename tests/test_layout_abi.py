@@ -45,6 +45,21 @@ def test_every_params_field_at_the_header_offset(tmp_path):
     assert out == [getattr(layout.SphParams, f).offset for f in names]
 
 
+def test_prop_tables_fields_at_the_header_offset(tmp_path):
+    # sph_prop_tables (the property tables of read_table) and its ctypes mirror
+    names = [f for f, _ in layout.PropTables._fields_]
+    body = 'printf("%zu\\n", sizeof(sph_prop_tables));' + "".join(
+        'printf("%%zu\\n", offsetof(sph_prop_tables, %s));' % f for f in names)
+    src = tmp_path / "tab.c"
+    src.write_text('#include "sph_isph.h"\n#include <stdio.h>\n#include <stddef.h>\nint main(){' + body + '}')
+    exe = tmp_path / "tab"
+    subprocess.check_call(["gcc", "-I" + os.path.dirname(HEADER), str(src), "-o", str(exe)])
+    out = [int(v) for v in subprocess.check_output([str(exe)]).decode().split()]
+    assert out[0] == ctypes.sizeof(layout.PropTables) == 2088
+    assert out[1:] == [getattr(layout.PropTables, f).offset for f in names]
+    assert layout.TABLE_SIZE == 50 and layout.TABLE_SLOTS == 10
+
+
 def test_library_loads_and_exports_every_symbol():
     L = abi.lib()
     declared = set()
