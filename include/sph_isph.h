@@ -17,8 +17,9 @@
  *     no exception or exit() crosses the boundary;
  *   - a context owns all of its device memory, is bound to one device and one
  *     CUDA stream, and is not thread-safe (one host thread at a time);
- *   - calls are stream-ordered; only the *_download / *_export calls and
- *     sph_ppe's statistics synchronise the stream;
+ *   - calls are stream-ordered; only the *_download / *_export calls,
+ *     sph_ppe's statistics and sph_upload of records in device memory
+ *     synchronise the stream;
  *   - particle indices in exported arrays are in the reference's sorted
  *     order (the order KERNEL_reorder produces, functions_NNPS.cuh:840-843).
  */
