@@ -217,3 +217,30 @@ def test_native_runner_writes_the_python_runners_files(tmp_path):
     for f in names:
         assert (tmp_path / "native" / f).read_bytes() == (tmp_path / "python" / f).read_bytes(), f
     assert "tu_max" in r.stdout
+
+
+@needs_native
+@pytest.mark.parametrize("flags,kw", [
+    ([], {}),
+    (["--ppe", "sweep"], dict(ppe="sweep")),
+    (["--ppe", "gmres", "--tol", "1e-8", "--coarse", "-16", "--coarse-max", "16384", "--coef-half",
+      "--device-control", "--pair-h", "--pforce-difference", "--enthalpy"],
+     dict(ppe="gmres", tol=1e-8, coarse=-16, coarse_max=16384, coef_half=True, device_control=True, pair_h=True,
+          pforce_difference=True, enthalpy=True)),
+])
+def test_native_runner_solver_options_match_the_python_runner(tmp_path, flags, kw):
+    solv, deck, _ = write_case(tmp_path)
+    r = _native(solv, deck, tmp_path / "out", "--setup-only", *flags)
+    assert r.returncode == 0, r.stderr
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    p = driver.solver_params(**kw)
+    for f in ("ppe_mode", "ppe_coarse_block", "ppe_coarse_max", "ppe_coef_half", "ppe_refinement", "ppe_pair_h",
+              "pressure_force_form", "enthalpy_eqn"):
+        assert got[f] == getattr(p, f), f
+    assert got["ppe_tol"] == p.ppe_tol
+
+
+@needs_native
+def test_native_runner_rejects_an_unknown_solver(tmp_path):
+    solv, deck, _ = write_case(tmp_path)
+    assert _native(solv, deck, tmp_path / "out", "--setup-only", "--ppe", "cg").returncode == 2

@@ -2,7 +2,18 @@
 // as a thin native driver of the C ABI in include/sph_isph.h.
 //
 //   sophia_b200 solv.txt deck.txt out_dir [--steps N] [--fp64] [--table data.txt]
-//               [--enthalpy] [--setup-only]
+//               [--enthalpy] [--setup-only] [solver options]
+//
+// Solver options (settings the solver input cannot carry):
+//   --ppe sweep|bicgstab|mixed|gmres|idrs   pressure solve (default mixed)
+//   --tol X                                  its relative residual (default 1e-6)
+//   --coarse B                               two-level preconditioner on B^3-cell
+//                                            blocks; -B balanced by row count
+//   --coarse-max M                           most balanced aggregates
+//   --coef-half                              FP16 row-scaled coefficients
+//   --device-control                         each solve one graph under device control
+//   --pair-h                                 pair-averaged h in the pressure rows
+//   --pforce-difference                      difference form of the pressure force
 //
 // What the reference does, and where:
 //   * main (SOPHIA_gpu.cu:120-141): read_solv_input on the solver input, then
@@ -49,12 +60,26 @@ struct Args {
     std::string solv, deck, out, table;
     long long steps = -1;
     bool fp64 = false, enthalpy = false, setup_only = false;
+    int ppe = -1, coarse = 0, coarse_max = 0;
+    double tol = 0;
+    bool coef_half = false, device_control = false, pair_h = false, pforce_difference = false;
 };
+
+int ppe_mode_of(const std::string &s) {
+    if (s == "sweep") return SPH_PPE_REF_SWEEP;
+    if (s == "bicgstab") return SPH_PPE_BICGSTAB;
+    if (s == "mixed") return SPH_PPE_MIXED_IR;
+    if (s == "gmres") return SPH_PPE_GMRES;
+    if (s == "idrs") return SPH_PPE_IDRS;
+    return -1;
+}
 
 int usage() {
     fprintf(stderr,
             "usage: sophia_b200 solv.txt deck.txt out_dir [--steps N] [--fp64] [--table data.txt] [--enthalpy] "
-            "[--setup-only]\n");
+            "[--setup-only]\n"
+            "       [--ppe sweep|bicgstab|mixed|gmres|idrs] [--tol X] [--coarse B] [--coarse-max M] [--coef-half]\n"
+            "       [--device-control] [--pair-h] [--pforce-difference]\n");
     return 2;
 }
 
@@ -67,6 +92,17 @@ bool parse(int argc, char **argv, Args &a) {
         else if (s == "--fp64") a.fp64 = true;
         else if (s == "--enthalpy") a.enthalpy = true;
         else if (s == "--setup-only") a.setup_only = true;
+        else if (s == "--ppe" && k + 1 < argc) {
+            a.ppe = ppe_mode_of(argv[++k]);
+            if (a.ppe < 0) return false;
+        }
+        else if (s == "--tol" && k + 1 < argc) a.tol = atof(argv[++k]);
+        else if (s == "--coarse" && k + 1 < argc) a.coarse = atoi(argv[++k]);
+        else if (s == "--coarse-max" && k + 1 < argc) a.coarse_max = atoi(argv[++k]);
+        else if (s == "--coef-half") a.coef_half = true;
+        else if (s == "--device-control") a.device_control = true;
+        else if (s == "--pair-h") a.pair_h = true;
+        else if (s == "--pforce-difference") a.pforce_difference = true;
         else if (!s.empty() && s[0] == '-') return false;
         else pos.push_back(s);
     }
@@ -102,6 +138,14 @@ int main(int argc, char **argv) {
     sph_params p;
     sph_params_init(&p);
     if (a.enthalpy) p.enthalpy_eqn = 1;
+    if (a.ppe >= 0) p.ppe_mode = a.ppe;
+    if (a.tol > 0) p.ppe_tol = a.tol;
+    p.ppe_coarse_block = a.coarse;
+    p.ppe_coarse_max = a.coarse_max;
+    if (a.coef_half) p.ppe_coef_half = 1;
+    if (a.device_control) p.ppe_refinement = 4;
+    if (a.pair_h) p.ppe_pair_h = 1;
+    if (a.pforce_difference) p.pressure_force_form = 1;
     char labels_buf[20 * 20] = {0};
     int nlab = 0;
     int st = sph_read_solv(a.solv.c_str(), &p, labels_buf, &nlab);
@@ -154,10 +198,14 @@ int main(int argc, char **argv) {
 
     if (a.setup_only) {
         printf("{\"num_part\": %d, \"num_part2\": %d, \"count\": %lld, \"NI\": %d, \"NJ\": %d, \"NK\": %d, "
-               "\"num_cells\": %d, \"dcell\": %.9g, \"labels\": %d, \"tables\": %d, \"prop_table\": %d}\n",
+               "\"num_cells\": %d, \"dcell\": %.9g, \"labels\": %d, \"tables\": %d, \"prop_table\": %d, "
+               "\"ppe_mode\": %d, \"ppe_tol\": %.17g, \"ppe_coarse_block\": %d, \"ppe_coarse_max\": %d, "
+               "\"ppe_coef_half\": %d, \"ppe_refinement\": %d, \"ppe_pair_h\": %d, \"pressure_force_form\": %d, "
+               "\"enthalpy_eqn\": %d}\n",
                n, p.vii[SPH_VII_NUM_PART2], count, p.vii[SPH_VII_NI], p.vii[SPH_VII_NJ], p.vii[SPH_VII_NK],
                p.vii[SPH_VII_NUM_CELLS], (double)p.vif[SPH_VIF_DCELL], nlab, use_tables ? tables.n_tables : 0,
-               p.vii[SPH_VII_PROP_TABLE]);
+               p.vii[SPH_VII_PROP_TABLE], p.ppe_mode, p.ppe_tol, p.ppe_coarse_block, p.ppe_coarse_max,
+               p.ppe_coef_half, p.ppe_refinement, p.ppe_pair_h, p.pressure_force_form, p.enthalpy_eqn);
         return 0;
     }
 

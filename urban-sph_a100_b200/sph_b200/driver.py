@@ -28,6 +28,11 @@ pass ISPH_Calc.cuh:480-482 keeps commented out), since decks carry
 temperatures only.
 
     python -m sph_b200.driver solv.txt deck.txt out_dir [--steps N] [--table data.txt] [--enthalpy]
+        [--ppe sweep|bicgstab|mixed|gmres|idrs] [--tol X] [--coarse B] [--coarse-max M] [--coef-half]
+        [--device-control] [--pair-h] [--pforce-difference]
+
+The solver options (``solver_params``) set what the solver input cannot
+carry, as the native runner's do (urban-sph_a100_b200/csrc/sophia_b200.cpp).
 """
 import argparse
 import math
@@ -121,6 +126,37 @@ def setup(solv_path, deck_path, base=None):
     return p, labels, P1
 
 
+PPE_MODES = {"sweep": 0, "bicgstab": 1, "mixed": 2, "gmres": 4, "idrs": 5}   # SPH_PPE_*
+
+
+def solver_params(ppe=None, tol=None, coarse=0, coarse_max=0, coef_half=False, device_control=False,
+                  pair_h=False, pforce_difference=False, enthalpy=False):
+    """Default parameters with the solver settings a solver input does not
+    carry: the PPE form and tolerance, the two-level preconditioner (coarse
+    blocks of B^3 cells, -B balanced by row count, at most coarse_max
+    aggregates), FP16 coefficients, device-controlled solves, the
+    pair-averaged h, the difference form of the pressure force, the
+    enthalpy form."""
+    p = _params.default_params()
+    if ppe is not None:
+        p.ppe_mode = PPE_MODES[ppe]
+    if tol is not None and tol > 0:
+        p.ppe_tol = tol
+    p.ppe_coarse_block = int(coarse)
+    p.ppe_coarse_max = int(coarse_max)
+    if coef_half:
+        p.ppe_coef_half = 1
+    if device_control:
+        p.ppe_refinement = 4
+    if pair_h:
+        p.ppe_pair_h = 1
+    if pforce_difference:
+        p.pressure_force_form = 1
+    if enthalpy:
+        p.enthalpy_eqn = 1
+    return p
+
+
 def read_tables(solv_path, p, table_path=None):
     """The property tables of a case (a PropTables), or None when its
     parameters do not ask for them (vii[prop_table] = 0)."""
@@ -184,10 +220,18 @@ def main(argv=None):
     ap.add_argument("--table", default=None, help="property tables (default: data.txt beside the solver input)")
     ap.add_argument("--enthalpy", action="store_true",
                     help="energy equation in enthalpy (with Conduction YES), enthalpy set from temperature")
+    ap.add_argument("--ppe", choices=sorted(PPE_MODES), default=None, help="pressure solve (default mixed)")
+    ap.add_argument("--tol", type=float, default=None, help="relative residual of the solve (default 1e-6)")
+    ap.add_argument("--coarse", type=int, default=0,
+                    help="two-level preconditioner on B^3-cell blocks (-B: balanced by row count)")
+    ap.add_argument("--coarse-max", type=int, default=0, help="most balanced aggregates")
+    ap.add_argument("--coef-half", action="store_true", help="FP16 row-scaled coefficients")
+    ap.add_argument("--device-control", action="store_true", help="each solve one graph under device control")
+    ap.add_argument("--pair-h", action="store_true", help="pair-averaged h in the pressure rows")
+    ap.add_argument("--pforce-difference", action="store_true", help="difference form of the pressure force")
     a = ap.parse_args(argv)
-    base = _params.default_params()
-    if a.enthalpy:
-        base.enthalpy_eqn = 1
+    base = solver_params(a.ppe, a.tol, a.coarse, a.coarse_max, a.coef_half, a.device_control, a.pair_h,
+                         a.pforce_difference, a.enthalpy)
     run(a.solv, a.deck, a.out_dir, base=base, precision=1 if a.fp64 else 0, max_steps=a.steps, table_path=a.table)
     return 0
 
