@@ -203,3 +203,55 @@ def test_read_table_without_tables_is_empty(tmp_path):
     path.write_text("// no tables here\n#end\n")
     t = abi.read_table(path)
     assert t.n_tables == 0 and t.n_data == 0 and not any(t.size)
+
+
+def _random_table_file(rng):
+    """A well-formed table file (tables 0..n-1 in order, closed, at most 50
+    entries, equal-length columns) in a random spelling of the format."""
+    nl = "\r\n" if rng.random() < 0.2 else "\n"
+    ntab = int(rng.integers(1, 11))
+    budget = 50
+    out = []
+    if rng.random() < 0.5:
+        out.append("// generated property tables" + nl)
+    for t in range(ntab):
+        left = ntab - t - 1
+        size = int(rng.integers(1, max(2, min(12, budget - left) + 1)))
+        size = max(1, min(size, budget - left))
+        budget -= size
+        out.append("#p_type%s%d%s%s" % (" " * int(rng.integers(1, 3)), t,
+                                         " material" if rng.random() < 0.5 else "", nl))
+        cols = [c for c in ("//T", "//h", "//k", "//cp", "//mu") if rng.random() < 0.7] or ["//T"]
+        trailing = rng.random() < 0.15 and size >= 2
+        for c in cols:
+            if rng.random() < 0.3:
+                out.append("# note" + nl)
+            out.append(c + (" values" if rng.random() < 0.3 else "") + nl)
+            n = size - 1 if trailing else size
+            vals = []
+            for _ in range(n):
+                form = rng.integers(0, 4)
+                v = rng.normal() * 10.0 ** int(rng.integers(-3, 7))
+                vals.append({0: "%d" % int(v), 1: "%.6f" % v, 2: "%.9e" % v, 3: repr(float(np.float32(v)))}[int(form)])
+            sep = ", " if rng.random() < 0.3 else ","
+            out.append(sep.join(vals) + ("," if trailing else "") + nl)
+        out.append("#end" + nl)
+    return "".join(out)
+
+
+@pytest.mark.skipif(not __import__("refhost").available(), reason="reference host build absent")
+def test_read_table_matches_reference_reader_on_generated_files(tmp_path):
+    """60 seeded files through the reference's own read_table and this
+    reader: the same columns (as stored in Real = float), indices and sizes."""
+    import refhost
+    rng = np.random.default_rng(2024)
+    for k in range(60):
+        path = tmp_path / ("gen%d.txt" % k)
+        path.write_text(_random_table_file(rng), newline="")
+        ref = refhost.read_table(path)
+        t = abi.read_table(path)
+        assert np.array_equal(np.array(t.index[:]), ref["index"]), k
+        assert np.array_equal(np.array(t.size[:]), ref["size"]), k
+        for c in ("T", "h", "k", "cp", "mu"):
+            mine = np.ctypeslib.as_array(getattr(t, c)).astype(np.float32)
+            assert mine.tobytes() == ref[c].astype(np.float32).tobytes(), (k, c)
