@@ -578,3 +578,54 @@ def test_taylor_green_pressure_converges_to_analytic():
         out.append(((pn * pa).sum() / np.sqrt((pn * pn).sum() * (pa * pa).sum()), np.abs(pn - pa).max()))
     assert out[1][0] > 0.999 and out[0][0] > 0.99
     assert out[1][1] < 0.6 * out[0][1]
+
+
+@pytest.mark.skipif(not refhost.available("enth"), reason="reference host build (enthalpy form) absent")
+def test_energy_conversions_bit_exact_vs_reference_on_generated_tables(tmp_path):
+    """Ttoh / htoT through the reference's conversion kernels and the oracle
+    on 12 seeded table sets: 1 to 6 tables of 2 to 8 ascending entries, the
+    records spread over every slot, temperatures and enthalpies beyond both
+    ends of every table."""
+    from sph_b200 import abi
+    base, p, _ = decks.enthalpy_tables_mini()
+    base = base[base["p_type"] < 1000].copy()
+    decks.domain_setup(p, base)
+    rng = np.random.default_rng(77)
+    for k in range(12):
+        ntab = int(rng.integers(1, 7))
+        cols = []
+        for _ in range(ntab):
+            m = int(rng.integers(2, 9))
+            T = np.sort(rng.choice(np.arange(200, 3200, 7), m, replace=False)).astype(np.float64)
+            h = np.sort(rng.choice(np.arange(-800000, 1500000, 997), m, replace=False)).astype(np.float64)
+            cols.append({"T": T, "h": h})
+        text = "".join("#p_type %d\n//T\n%s\n//h\n%s\n#end\n" % (t, ",".join(repr(float(v)) for v in c["T"]),
+                                                                   ",".join(repr(float(v)) for v in c["h"]))
+                       for t, c in enumerate(cols))
+        path = tmp_path / ("tables%d.txt" % k)
+        path.write_text(text)
+        P = base.copy()
+        P["p_type"] = rng.integers(-(ntab - 1), ntab, len(P))
+        P["temp"] = rng.uniform(100.0, 3500.0, len(P)).astype(np.float32)
+        R = refhost.RefHost(P, p, parallel=False, variant="enth")
+        refhost.read_table(path, "enth")
+        tables = abi.read_table(path)
+        assert np.array_equal(tables.column("T", ntab - 1), cols[-1]["T"])
+        O = restated.Restated(P, p, 0)
+        O.set_tables(tables)
+        R.temp_to_enthalpy()
+        O.temp_to_enthalpy()
+        B, B2, _ = O.download()
+        assert np.isfinite(B["enthalpy"]).all(), k
+        assert np.array_equal(R.P1["enthalpy"], B["enthalpy"]), k
+        assert np.array_equal(R.P2["enthalpy0"], B2["enthalpy0"]), k
+        Q = np.array(R.P1, copy=True)
+        Q["enthalpy"] = rng.uniform(-1.0e6, 2.0e6, len(Q)).astype(np.float32)
+        R.P1[:] = Q
+        O2 = restated.Restated(Q, p, 0)
+        O2.set_tables(tables)
+        R.enthalpy_to_temp()
+        O2.enthalpy_to_temp()
+        C, _, _ = O2.download()
+        assert np.isfinite(C["temp"]).all(), k
+        assert np.array_equal(R.P1["temp"], C["temp"]), k
