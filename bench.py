@@ -89,9 +89,10 @@ class Clocks:
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            with open(self.path, "w") as out:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                              "--format=csv,noheader,nounits", "-lms", "200"],
+                                             stdout=out, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
@@ -104,14 +105,15 @@ class Clocks:
         except Exception:
             self.proc.kill()
         rows = []
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
-            except ValueError:
-                continue
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    continue
         os.unlink(self.path)
         if not rows:
             return None

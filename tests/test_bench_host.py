@@ -61,7 +61,8 @@ def test_peak_bandwidth_source():
     v, kind = bench.peaks()
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
-        assert kind == "measured" and v == float(json.load(open(path))["hbm_gbs"])
+        with open(path) as f:
+            assert kind == "measured" and v == float(json.load(f)["hbm_gbs"])
     else:
         assert (v, kind) == (6650.0, "fallback")
 

@@ -64,10 +64,11 @@ def test_library_loads_and_exports_every_symbol():
     L = abi.lib()
     declared = set()
     import re
-    for line in open(HEADER):
-        m = re.match(r"^(?:const char \*|int64_t |int |void )(sph_\w+)\(", line.strip())
-        if m:
-            declared.add(m.group(1))
+    with open(HEADER) as f:
+        for line in f:
+            m = re.match(r"^(?:const char \*|int64_t |int |void )(sph_\w+)\(", line.strip())
+            if m:
+                declared.add(m.group(1))
     assert declared == set(abi.SYMBOLS)
     for name in declared:
         assert hasattr(L, name), name

@@ -29,7 +29,7 @@ def _worker(rank, world, port, out):
 
 def test_two_ranks_sum_units_and_take_the_slowest_time():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
