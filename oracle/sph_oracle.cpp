@@ -15,7 +15,14 @@
 //   * particles with i_type >= 3 (dummies) are not processed by the Neumann
 //     pass (the reference runs it on them with meaningless positions);
 //   * the converged pressure solves (BiCGSTAB, pinned row) are new work with
-//     no reference counterpart.
+//     no reference counterpart;
+//   * with the property tables, a record whose |p_type| has no table of two
+//     entries keeps its value in htoT / Ttoh (the reference reads past its
+//     ten-entry k_table_index there, e.g. for the IBM markers in its
+//     conversion kernels).
+// Beyond the step it restates the energy conversions of functions_ENERGY.cuh
+// (Ttoh / htoT on the records), pinned to the reference's kernels on the
+// built-in corium table and on property tables its read_table loaded.
 // Nothing here is linked into the product library.
 
 #include <algorithm>
