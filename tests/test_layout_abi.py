@@ -105,3 +105,41 @@ def test_create_without_gpu_fails_loudly():
     P, p = decks.caseh_mini(nx=6, ny=4, nz=3)
     with pytest.raises(abi.SphError):
         abi.Simulation(p)
+
+
+class _FakeDeviceArray:
+    """Stands in for a CUDA tensor: only the __cuda_array_interface__ that
+    records_arg reads (the pointer is never dereferenced here)."""
+
+    def __init__(self, nbytes, ptr=0x7f0000000000, strides=None, typestr="|u1"):
+        self.__cuda_array_interface__ = {"shape": (nbytes // np.dtype(typestr).itemsize,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": strides}
+
+
+def test_records_arg_passes_device_pointers_through():
+    n = 7
+    a = _FakeDeviceArray(n * layout.PART1.itemsize)
+    ptr, keep, count = abi.records_arg(a, layout.PART1)
+    assert ptr.value == 0x7f0000000000 and keep is a and count == n
+    assert abi.records_arg(a, layout.PART1, n)[2] == n
+    # 4-byte elements, a whole number of records
+    b = _FakeDeviceArray(3 * layout.PART2.itemsize, typestr="<f4")
+    assert abi.records_arg(b, layout.PART2)[2] == 3
+
+
+@pytest.mark.parametrize("make,n", [
+    (lambda: _FakeDeviceArray(layout.PART1.itemsize * 3 + 4), None),        # not whole records
+    (lambda: _FakeDeviceArray(layout.PART1.itemsize * 3), 4),               # wrong count
+    (lambda: _FakeDeviceArray(layout.PART1.itemsize * 2, strides=(2,)), None),   # not contiguous
+])
+def test_records_arg_rejects_malformed_device_arrays(make, n):
+    with pytest.raises(ValueError):
+        abi.records_arg(make(), layout.PART1, n)
+
+
+def test_records_arg_host_arrays_keep_their_buffer():
+    P = np.zeros(5, layout.PART1)
+    ptr, keep, count = abi.records_arg(P, layout.PART1)
+    assert count == 5 and keep is P and ptr.value == P.ctypes.data      # no copy of contiguous records
+    with pytest.raises(ValueError):
+        abi.records_arg(P, layout.PART1, 6)

@@ -125,6 +125,39 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
+def records_arg(a, dtype, n=None):
+    """(pointer, keep-alive, count) of a record array for the upload and
+    download calls.  Device arrays (anything with __cuda_array_interface__,
+    e.g. a CUDA torch tensor of uint8 or a CuPy array) pass their device
+    pointer as they are, which the C ABI takes as well as host memory; they
+    must be C-contiguous and hold a whole number of records (n of them when
+    n is given).  Host arrays are made contiguous records of `dtype`."""
+    cai = getattr(a, "__cuda_array_interface__", None)
+    if cai is not None:
+        shape = tuple(cai["shape"])
+        item = np.dtype(cai["typestr"]).itemsize
+        strides = cai.get("strides")
+        if strides is not None:
+            want, s_ = [], item
+            for d in reversed(shape):
+                want.append(s_)
+                s_ *= d
+            if tuple(strides) != tuple(reversed(want)):
+                raise ValueError("device records must be C-contiguous")
+        nbytes = int(np.prod(shape, dtype=np.int64)) * item
+        if nbytes % dtype.itemsize:
+            raise ValueError("device array of %d bytes is not a whole number of %d-byte records"
+                             % (nbytes, dtype.itemsize))
+        count = nbytes // dtype.itemsize
+        if n is not None and count != n:
+            raise ValueError("device array holds %d records, %d expected" % (count, n))
+        return ctypes.c_void_p(int(cai["data"][0])), a, count
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    if n is not None and len(arr) != n:
+        raise ValueError("array holds %d records, %d expected" % (len(arr), n))
+    return _p(arr), arr, len(arr)
+
+
 def _check(where, st, ok=(0,)):
     if st not in ok and st < 0:
         raise SphError(where, st)
@@ -173,13 +206,13 @@ class Simulation:
         _check("sph_set_params", lib().sph_set_params(self.h, ctypes.byref(self.params)))
 
     def upload(self, P1, P2=None):
-        P1 = np.ascontiguousarray(P1, dtype=PART1)
-        P2 = None if P2 is None else np.ascontiguousarray(P2, dtype=PART2)
-        _check("sph_upload", lib().sph_upload(self.h, _p(P1), _p(P2), len(P1)))
+        p1, keep1, n = records_arg(P1, PART1)
+        p2, keep2 = (None, None) if P2 is None else records_arg(P2, PART2, n)[:2]
+        _check("sph_upload", lib().sph_upload(self.h, p1, p2, n))
 
     def upload_state(self, P1):
-        P1 = np.ascontiguousarray(P1, dtype=PART1)
-        _check("sph_upload_state", lib().sph_upload_state(self.h, _p(P1), len(P1)))
+        p1, keep1, n = records_arg(P1, PART1)
+        _check("sph_upload_state", lib().sph_upload_state(self.h, p1, n))
 
     def download(self, want=(1, 2, 3)):
         P1 = np.zeros(self.n, PART1) if 1 in want else None
@@ -188,8 +221,19 @@ class Simulation:
         _check("sph_download", lib().sph_download(self.h, _p(P1), _p(P2), _p(P3)))
         return P1, P2, P3
 
-    def download_into(self, P1):
-        _check("sph_download", lib().sph_download(self.h, _p(P1), None, None))
+    def download_into(self, P1, P2=None, P3=None):
+        """Downloads into caller arrays: host records (numpy, contiguous) or
+        device arrays (__cuda_array_interface__) of self.n records each."""
+        ptrs = []
+        for a, dt in ((P1, PART1), (P2, PART2), (P3, PART3)):
+            if a is None:
+                ptrs.append(None)
+                continue
+            if getattr(a, "__cuda_array_interface__", None) is None and not (
+                    isinstance(a, np.ndarray) and a.flags.c_contiguous and a.dtype == dt):
+                raise ValueError("download_into needs contiguous %s records or a device array" % dt)
+            ptrs.append(records_arg(a, dt, self.n)[0])
+        _check("sph_download", lib().sph_download(self.h, *ptrs))
 
     def nnps(self):
         _check("sph_nnps", lib().sph_nnps(self.h))
